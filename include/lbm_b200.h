@@ -1,0 +1,203 @@
+/*
+ * lbm_b200.h -- C ABI of the B200 lattice-Boltzmann force kernel.
+ *
+ * This is the drop-in boundary for the per-step fluid and particle-coupling path of openmm-lbm.
+ * Each entry point replaces one method of the plugin kernel interface
+ * `LBMPlugin::CalcLBMForceKernel` (openmmapi/include/LBMKernels.h:97-189) and takes the
+ * lattice-unit parameter block `LBMPlugin::LBMLatticeParameters` (LBMKernels.h:30-92) flattened
+ * into a plain C struct.  Everything crossing the boundary is a plain pointer, a size or a POD
+ * struct: no C++ or torch types.
+ *
+ * OpenMM's ContextImpl is replaced by explicit arguments: the step count of the integrator
+ * (ContextImpl::getStepCount) and the particle arrays (positions, velocities, forces of the coupled
+ * particles, in the order in which they were coupled) that the Reference platform reads from
+ * ReferencePlatform::PlatformData and the CUDA platform from its posq/velm/force buffers.
+ *
+ * Units are those of LBMLatticeParameters: dx (nm), dt (ps), density (Da/nm^3), friction (1/ps),
+ * kT (kJ/mol); velocities and accelerations of the fluid in lattice units; particle positions in
+ * nm, velocities in nm/ps, forces in kJ/mol/nm.
+ *
+ * Every call returns an LbmStatus; on failure lbm_last_error() gives the message (thread-local).
+ * A handle is driven by one host thread at a time; distinct handles are independent.
+ */
+#ifndef LBM_B200_H_
+#define LBM_B200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_NUM_VELOCITIES 19
+
+/* Status codes.  The reference throws OpenMMException with a message in each of these cases. */
+typedef enum LbmStatus {
+    LBM_OK = 0,
+    LBM_ERR_INVALID_ARGUMENT = 1,   /* bad setup (LBMForceImpl.cpp:44-214 checks), wrong sizes, null pointers */
+    LBM_ERR_MACH_LIMIT = 2,         /* Mach number above the limit (ReferenceLBMKernels.cpp:412-420) */
+    LBM_ERR_CG_NOT_CONVERGED = 3,   /* centred stencil drag: no convergence in 1000 iterations (:864-866) */
+    LBM_ERR_DEVICE_TIMEOUT = 4,     /* a bounded device-side wait ran out */
+    LBM_ERR_CUDA = 5,               /* a CUDA runtime call failed */
+    LBM_ERR_OUT_OF_MEMORY = 6,
+    LBM_ERR_NOT_SUPPORTED = 7,      /* e.g. a storage type that the option set does not allow */
+    LBM_ERR_CHECKPOINT = 8          /* a checkpoint of another lattice, precision or particle count */
+} LbmStatus;
+
+/* Enumerations with the values of LBMForce.h:46-138. */
+enum { LBM_DRAG_EXPLICIT = 0, LBM_DRAG_CENTERED = 1 };
+enum { LBM_STENCIL_NEAREST = 0, LBM_STENCIL_TRILINEAR = 1, LBM_STENCIL_THREEPOINT = 2, LBM_STENCIL_KEYS = 3 };
+enum { LBM_WALL_BOUNCEBACK = 0, LBM_WALL_REGULARIZED = 1 };
+enum { LBM_FACE_XMIN = 0, LBM_FACE_XMAX = 1, LBM_FACE_YMIN = 2, LBM_FACE_YMAX = 3, LBM_FACE_ZMIN = 4, LBM_FACE_ZMAX = 5 };
+enum { LBM_BOUNDARY_PERIODIC = 0, LBM_BOUNDARY_VELOCITY = 1, LBM_BOUNDARY_DENSITY = 2, LBM_BOUNDARY_DENSITY_VELOCITY = 3 };
+
+/* Storage type of the population deviations f_q - w_q in device memory.  The collision computes in
+   double for LBM_STORAGE_F64 and in float for the others. */
+enum { LBM_STORAGE_F64 = 0, LBM_STORAGE_F32 = 1, LBM_STORAGE_F16 = 2, LBM_STORAGE_BF16 = 3 };
+
+/* Where the particle arrays of a call live. */
+enum { LBM_MEMORY_HOST = 0, LBM_MEMORY_DEVICE = 1 };
+
+/*
+ * The lattice parameters in lattice units and the conversion factors, as LBMLatticeParameters
+ * (LBMKernels.h:30-92) for one domain (procs = 1,1,1; the MPI fields are absent).  particles and
+ * solidNodes are passed separately to lbm_create().
+ */
+typedef struct LbmLatticeParameters {
+    int nx, ny, nz;
+    double dx, dt, density;              /* nm, ps, Da/nm^3 */
+    double tau, omega;                   /* omega = 1/tau */
+    double initial_velocity[3];          /* lattice units */
+    double body_acceleration[3];         /* lattice units */
+    double friction;                     /* 1/ps */
+    double kT;                           /* kJ/mol, 0 without random force (NVE) */
+    int drag_scheme;                     /* LBM_DRAG_* */
+    int interpolation_stencil;           /* LBM_STENCIL_* */
+    int fluid_fluctuations;              /* 0 or 1 */
+    double fluid_kT;                     /* kJ/mol, 0 without fluctuations */
+    int random_number_seed;
+    int momentum_removal_frequency;      /* 0 = never */
+    int mach_check_frequency;            /* 0 = never */
+    double mach_number_limit;
+    int wall_scheme;                     /* LBM_WALL_* */
+    int face_boundary[6];                /* LBM_BOUNDARY_* per LBM_FACE_* */
+    double face_velocity[6][3];          /* lattice units */
+    double face_density[6];              /* lattice units, 1 = fluid at rest */
+} LbmLatticeParameters;
+
+/* Options of this implementation that have no counterpart in the reference. */
+typedef struct LbmOptions {
+    int storage;            /* LBM_STORAGE_* (the reference stores FP64 on its Reference platform) */
+    int device;             /* CUDA device ordinal */
+    void* stream;           /* cudaStream_t to launch on; NULL = a stream owned by the handle */
+} LbmOptions;
+
+/*
+ * The coupled particles seen by one call, in coupling order (index i of LBMForce::addParticle()):
+ * positions (nm), velocities (nm/ps) and forces (kJ/mol/nm), 3 doubles per particle, either all in
+ * host memory or all in device memory of the handle's device.  lbm_begin_step() may reverse
+ * velocities (reflection at walls); lbm_execute() adds the coupling forces to forces, and with the
+ * centred drag reads the other forces already accumulated there (LBMForce must be the last force).
+ */
+typedef struct LbmParticleArrays {
+    double* positions;
+    double* velocities;
+    double* forces;
+    int memory;             /* LBM_MEMORY_* */
+} LbmParticleArrays;
+
+/*
+ * The parameters of an LBMForce in OpenMM units, as set with its setters (LBMForce.h:162-666) and with
+ * the defaults of its constructor (LBMForce.cpp:19-29, see lbm_default_force_description()).
+ */
+typedef struct LbmForceDescription {
+    int nx, ny, nz;                      /* setGridSize */
+    double fluid_density;                /* Da/nm^3, setFluidDensity */
+    double kinematic_viscosity;          /* nm^2/ps, setKinematicViscosity */
+    double friction;                     /* 1/ps, setFriction */
+    double temperature;                  /* K, setTemperature */
+    int coupling_scheme;                 /* 0 EulerMaruyama, 1 NVE (setCouplingScheme) */
+    int drag_scheme;                     /* LBM_DRAG_* */
+    int interpolation_stencil;           /* LBM_STENCIL_* */
+    int fluid_fluctuations;              /* setFluidFluctuations */
+    int wall_scheme;                     /* LBM_WALL_* */
+    int face_boundary[6];                /* LBM_BOUNDARY_* */
+    double face_velocity[6][3];          /* nm/ps */
+    double face_density[6];              /* Da/nm^3, 0 = the fluid density */
+    int random_number_seed;
+    double body_acceleration[3];         /* nm/ps^2 */
+    double initial_velocity[3];          /* nm/ps */
+    int momentum_removal_frequency;
+    int mach_check_frequency;
+    double mach_number_limit;
+} LbmForceDescription;
+
+typedef struct LbmKernel LbmKernel;
+
+/* Message of the last failed call on this thread (empty if none). */
+const char* lbm_last_error(void);
+
+/* The defaults of LBMForce's constructor (LBMForce.cpp:19-29). */
+void lbm_default_force_description(LbmForceDescription* force);
+
+/*
+ * LBMForceImpl::computeLatticeParameters (openmmapi/src/LBMForceImpl.cpp:44-214): checks the setup and
+ * converts it to lattice units, for a rectangular periodic box (box[3], nm), the integrator step size
+ * (ps), the masses of the System's particles (Da) and the indices of the coupled ones.  The same error
+ * messages as the reference.  Needs no GPU.
+ */
+LbmStatus lbm_compute_lattice_parameters(const LbmForceDescription* force, const double box[3], double step_size,
+                                         int num_system_particles, const double* system_masses,
+                                         int num_coupled, const int* coupled_particles,
+                                         int num_solid_nodes, const int* solid_nodes,
+                                         LbmLatticeParameters* lattice);
+
+/* CalcLBMForceKernel::initialize (LBMKernels.h:111); masses in Da, solid node indices sorted or not. */
+LbmStatus lbm_create(const LbmLatticeParameters* lattice, const LbmOptions* options,
+                     int num_particles, const double* particle_masses,
+                     int num_solid_nodes, const int* solid_nodes, LbmKernel** kernel);
+
+void lbm_destroy(LbmKernel* kernel);
+
+/* CalcLBMForceKernel::beginStep (LBMKernels.h:119). */
+LbmStatus lbm_begin_step(LbmKernel* kernel, long long step_count, const LbmParticleArrays* particles);
+
+/* CalcLBMForceKernel::execute (LBMKernels.h:128); the energy is always 0 (the coupling is dissipative). */
+LbmStatus lbm_execute(LbmKernel* kernel, long long step_count, const LbmParticleArrays* particles,
+                      int include_forces, int include_energy, double* energy);
+
+/* CalcLBMForceKernel::copyParametersToContext (LBMKernels.h:135). */
+LbmStatus lbm_copy_parameters(LbmKernel* kernel, const LbmLatticeParameters* lattice);
+
+/* CalcLBMForceKernel::getFluidFields (LBMKernels.h:144), one domain, no halo: density[N] in Da/nm^3 and
+   velocity[3N] in nm/ps (x, y, z per node), node index order; zero at solid nodes. */
+LbmStatus lbm_get_fluid_fields(LbmKernel* kernel, double* density, double* velocity);
+
+/* CalcLBMForceKernel::getFluidMachNumber (LBMKernels.h:149). */
+LbmStatus lbm_get_fluid_mach_number(LbmKernel* kernel, double* mach);
+
+/* CalcLBMForceKernel::getWallForce (LBMKernels.h:154): kJ/mol/nm. */
+LbmStatus lbm_get_wall_force(LbmKernel* kernel, double force[3]);
+
+/* CalcLBMForceKernel::getFluidState / setFluidState (LBMKernels.h:159-164): deviations f_q - w_q as
+   double, [q*N + node]. */
+LbmStatus lbm_get_fluid_state(LbmKernel* kernel, double* state);
+LbmStatus lbm_set_fluid_state(LbmKernel* kernel, const double* state);
+
+/* CalcLBMForceKernel::createCheckpoint / loadCheckpoint (LBMKernels.h:170-174): a byte image of the
+   kernel state (populations in the storage type, random key, wall momentum, step bookkeeping). */
+LbmStatus lbm_checkpoint_size(LbmKernel* kernel, size_t* bytes);
+LbmStatus lbm_create_checkpoint(LbmKernel* kernel, void* buffer, size_t bytes);
+LbmStatus lbm_load_checkpoint(LbmKernel* kernel, const void* buffer, size_t bytes);
+
+/* Number of device nodes N = nx*ny*nz and the storage type actually used. */
+LbmStatus lbm_get_info(LbmKernel* kernel, long long* num_nodes, int* storage);
+
+/* The CUDA stream that the handle launches on (cudaStream_t), for callers that order work with it. */
+void* lbm_get_stream(LbmKernel* kernel);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_B200_H_ */

@@ -1,0 +1,11 @@
+"""B200-native LBM force kernel: the per-step fluid and particle-coupling path of openmm-lbm on one B200.
+
+    abi      ctypes mirror of include/lbm_b200.h and the loader of liblbm_b200.so (the CUDA build)
+    force    LBMForce, the reference's parameter API, and its conversion into lattice units
+    kernel   B200Kernel, the platform kernel (CalcLBMForceKernel) behind the C ABI
+    harness  System / Context / VerletIntegrator: the OpenMM call order that drives the kernel
+"""
+from .abi import LbmError, LbmLatticeParameters, load_library  # noqa: F401
+from .force import LBMForce  # noqa: F401
+from .harness import Context, ExternalForce, PairForce, System, VerletIntegrator  # noqa: F401
+from .kernel import B200Kernel  # noqa: F401

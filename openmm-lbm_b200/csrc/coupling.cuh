@@ -1,0 +1,50 @@
+// Particle coupling of the B200 LBM force kernel: drag and random force through the nearest node or an
+// interpolation stencil (trilinear, three-point, Keys), explicit or centred, and the reaction of the
+// particles on the fluid (the reference's coupling, platforms/reference/src/ReferenceLBMKernels.cpp:503-1018).
+#pragma once
+
+#include "fluid.cuh"
+
+namespace lbm {
+
+class CouplingEngine {
+public:
+    CouplingEngine(const LbmLatticeParameters& lattice, FluidEngine& fluid, const Geometry& geometry, int numParticles,
+                   const double* masses, cudaStream_t stream);
+    ~CouplingEngine();
+    void setParameters(const LbmLatticeParameters& lattice);
+    // Load the particle arrays of a call into the device buffers (copies for host arrays).
+    void load(const LbmParticleArrays* particles, bool withForces);
+    // Reflection at the walls (beginStep, ReferenceLBMKernels.cpp:315-338): reverses velocities on the device and
+    // returns the momentum given to the wall, Da nm/ps (synchronizes).  The velocities are stored back.
+    void reflect(const LbmParticleArrays* particles, double wallMomentum[3]);
+    // Coupling forces of step `step` on the current fluid (isStep: also the reaction on the fluid, with the
+    // momentum removal `remove`).  Returns the momentum of the reactions on solid nodes, Da nm/ps (isStep only).
+    void couple(long long step, bool isStep, bool remove);
+    // Add the coupling forces to the force array of the call.
+    void addForces(const LbmParticleArrays* particles);
+    // Clear the reaction of the last step from the fluid's reaction buffers.
+    void clearReaction();
+    // Momentum given to solid nodes by the reactions of the last coupling step (lattice units), read on demand.
+    void reactionWallMomentum(double out[3]);
+    int numParticles() const { return np; }
+private:
+    void stageIn(const LbmParticleArrays* particles, bool withForces);
+    LbmLatticeParameters lattice;
+    FluidEngine& fluid;
+    cudaStream_t stream;
+    int np;
+    int storageType;
+    // device buffers (double precision for the particles)
+    double *posDev, *velDev, *forceInDev, *forceOutDev, *massDev;
+    int* slotNodeDev;          // S per particle
+    double* slotWeightDev;     // S per particle
+    double* scratchDev;        // particle-side vectors of the centred solves
+    void* nodeAccumDev;        // per-node accumulators of the centred drag (spread vectors, sums)
+    double* wallDev;           // 3 doubles: momentum of reactions on solid nodes
+    int* statusDev;            // device status word of the conjugate gradients
+    double* pinned;            // pinned staging for host particle arrays
+    int stencilSlots;
+};
+
+} // namespace lbm

@@ -1,0 +1,1031 @@
+// Fluid kernels of the B200 LBM force kernel (sm_100a).
+//
+//  streamCollideKernel   the dense, fused step: pull streaming, moments, momentum removal, regularized
+//                        collision with Guo forcing (+ particle reaction, + Philox fluctuations), store;
+//                        HBM-bound, 2*19 population transfers per fluid node.  Restates, fused, the
+//                        reference's computeMoments, removeFluidMomentum and collideAndStream
+//                        (platforms/reference/src/ReferenceLBMKernels.cpp:430-501, 1066-1120).
+//  bounceBackKernel      halfway bounce-back and wall momentum exchange over the wall links
+//                        (ReferenceLBMKernels.cpp:1156-1205), writing into the slots of solid nodes.
+//  boundaryKernel        regularized walls and open faces (ReferenceLBMKernels.cpp:1207-1343), writing
+//                        into the slots that the boundary node pulls.
+//  finishKernel          deterministic reduction of the per-block partial sums of a step.
+//  momentsKernel         mass, momentum and largest speed of the current state (Mach check, start-up).
+//  gather/scatter        conversion between the pull layout and the reference's state layout.
+#include "fluid.cuh"
+#include "lbm_device.cuh"
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <utility>
+
+namespace lbm {
+
+#define CUDA_CHECK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) \
+    throw Error(LBM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); } while (0)
+
+namespace {
+
+constexpr int TX = 32, TY = 8, THREADS = TX*TY;
+constexpr int NPART = 8;           // doubles per partial record: mass, momentum[3], wall[3], maxSpeed2
+
+template <typename F, int... I>
+__device__ __forceinline__ void staticForImpl(F&& f, std::integer_sequence<int, I...>) {
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void staticFor(F&& f) {
+    staticForImpl(f, std::make_integer_sequence<int, N>{});
+}
+
+// Block reduction of a partial record (sums, and max for the last entry) into partials[slot], deterministic.
+__device__ void blockReduceStore(double v[NPART], double* out) {
+    __shared__ double red[THREADS/32][NPART];
+    int lane = threadIdx.x%32, warp = threadIdx.x/32, warps = blockDim.x/32;
+#pragma unroll
+    for (int i = 0; i < NPART; i++)
+        for (int offset = 16; offset > 0; offset >>= 1) {
+            double o = __shfl_down_sync(0xffffffffu, v[i], offset);
+            v[i] = (i == NPART-1 ? fmax(v[i], o) : v[i] + o);
+        }
+    if (lane == 0)
+        for (int i = 0; i < NPART; i++)
+            red[warp][i] = v[i];
+    __syncthreads();
+    if (threadIdx.x < NPART) {
+        int i = threadIdx.x;
+        double s = red[0][i];
+        for (int w = 1; w < warps; w++)
+            s = (i == NPART-1 ? fmax(s, red[w][i]) : s + red[w][i]);
+        out[i] = s;
+    }
+}
+
+struct Coords {
+    int x, y, z;
+};
+
+__device__ __forceinline__ Coords nodeCoords(long long node, int nx, int ny) {
+    Coords c;
+    c.x = (int) (node%nx);
+    long long r = node/nx;
+    c.y = (int) (r%ny);
+    c.z = (int) (r/ny);
+    return c;
+}
+
+__device__ __forceinline__ int wrap(int i, int n) {
+    return (i < 0 ? i + n : (i >= n ? i - n : i));
+}
+
+// Index of node (x + dx, y + dy, z + dz), periodic.
+__device__ __forceinline__ long long shifted(const FluidView& v, int x, int y, int z, int dx, int dy, int dz) {
+    return wrap(x + dx, v.nx) + (long long) v.nx*(wrap(y + dy, v.ny) + (long long) v.ny*wrap(z + dz, v.nz));
+}
+
+__device__ __forceinline__ int cxr(int q) { return cxOf(q); }
+__device__ __forceinline__ int cyr(int q) { return cyOf(q); }
+__device__ __forceinline__ int czr(int q) { return czOf(q); }
+
+// Moments of 19 post-stream deviations: density deviation, momentum and non-equilibrium second moment
+// Pi_neq = sum_q H2(c_q) df_q - j j/rho (xx, yy, zz, xy, xz, yz).  For the D3Q19 second-order
+// equilibrium, sum_q H2(c_q) (feq_q - w_q) = j j/rho exactly, so this equals the reference's
+// sum_q H2(c_q) (df_q - dfeq_q) (D3Q19.h:98-110).
+template <typename R>
+struct Moments {
+    R dr, jx, jy, jz, pxx, pyy, pzz, pxy, pxz, pyz;
+};
+
+template <typename R>
+__device__ __forceinline__ Moments<R> momentsOf(const R f[19]) {
+    Moments<R> m;
+    R dr = 0, jx = 0, jy = 0, jz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+    staticFor<19>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+        R fq = f[q];
+        dr += fq;
+        if (cx == 1) jx += fq; else if (cx == -1) jx -= fq;
+        if (cy == 1) jy += fq; else if (cy == -1) jy -= fq;
+        if (cz == 1) jz += fq; else if (cz == -1) jz -= fq;
+        if (cx != 0) sxx += fq;
+        if (cy != 0) syy += fq;
+        if (cz != 0) szz += fq;
+        if (cx*cy == 1) sxy += fq; else if (cx*cy == -1) sxy -= fq;
+        if (cx*cz == 1) sxz += fq; else if (cx*cz == -1) sxz -= fq;
+        if (cy*cz == 1) syz += fq; else if (cy*cz == -1) syz -= fq;
+    });
+    R inv = R(1)/(R(1) + dr);
+    R third = dr*R(1.0/3.0);
+    m.dr = dr; m.jx = jx; m.jy = jy; m.jz = jz;
+    m.pxx = sxx - third - jx*jx*inv;
+    m.pyy = syy - third - jy*jy*inv;
+    m.pzz = szz - third - jz*jz*inv;
+    m.pxy = sxy - jx*jy*inv;
+    m.pxz = sxz - jx*jz*inv;
+    m.pyz = syz - jy*jz*inv;
+    return m;
+}
+
+// Amplitudes a_k = phi_k r_k/sqrt(b_k) of the 15 non-conserved modes (D3Q19::fluctuation).
+template <typename R>
+__device__ __forceinline__ void modeAmplitudes(const R r[15], R stress, R ghost, R a[15]) {
+#pragma unroll
+    for (int k = 4; k < 19; k++)
+        a[k-4] = r[k-4]*(k < 10 ? stress : ghost)*R(invSqrtModeNorm(k));
+}
+
+// Even and odd parts (in c_q) of xi_q = w_q sum_k e_k(c_q) a_k for one direction q.
+template <typename R, int q>
+__device__ __forceinline__ void fluctuationParts(const R a[15], R& even, R& odd) {
+    R e = 0, o = 0;
+    staticFor<15>([&](auto kc) {
+        constexpr int k = decltype(kc)::value + 4;
+        constexpr double m = modeValue(k, q);
+        if (m != 0.0) {
+            if (k >= 10 && k <= 15)
+                o += R(m)*a[k-4];
+            else
+                e += R(m)*a[k-4];
+        }
+    });
+    even = wOf<R>(q)*e;
+    odd = wOf<R>(q)*o;
+}
+
+// Runtime-q fluctuation (slow paths): xi_q = w_q sum_k e_k(c_q) a_k.
+template <typename R>
+__device__ R fluctuationAt(int q, const R a[15]) {
+    R sum = 0;
+    R x = cxr(q), y = cyr(q), z = czr(q);
+    R x2 = x*x, y2 = y*y, z2 = z*z;
+    R e[15] = {x2 - R(1.0/3.0), y2 - R(1.0/3.0), z2 - R(1.0/3.0), x*y, x*z, y*z, y*(x2 - R(1.0/3.0)),
+               z*(x2 - R(1.0/3.0)), x*(y2 - R(1.0/3.0)), R(0.5)*x*(y2 + R(2)*z2 - R(1)), R(0.5)*y*(x2 + R(2)*z2 - R(1)),
+               R(0.5)*z*(x2 + R(2)*y2 - R(1)), x2*y2 - x2/R(3) - y2/R(3) + z2/R(6) + R(1.0/18.0),
+               R(2.0/7.0)*x2*y2 + x2*z2 - R(3.0/7.0)*x2 + y2/R(14) - R(2.0/7.0)*z2 + R(1.0/14.0),
+               R(0.4)*x2*y2 + R(0.4)*x2*z2 + y2*z2 - R(0.1)*x2 - R(0.4)*y2 - R(0.4)*z2 + R(0.1)};
+#pragma unroll
+    for (int k = 0; k < 15; k++)
+        sum += e[k]*a[k];
+    R w = (q == 0 ? R(1.0/3.0) : (q <= 6 ? R(1.0/18.0) : R(1.0/36.0)));
+    return w*sum;
+}
+
+template <typename R>
+__device__ __forceinline__ R weightOf(int q) {
+    return (q == 0 ? R(1.0/3.0) : (q <= 6 ? R(1.0/18.0) : R(1.0/36.0)));
+}
+
+// ---------------------------------------------------------------------------------------------------
+// The dense step.
+// ---------------------------------------------------------------------------------------------------
+
+template <typename T, typename R, bool SOLID, bool REACT, bool FLUCT>
+__global__ void __launch_bounds__(THREADS)
+streamCollideKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int remove, long long step) {
+    const int lane = threadIdx.x%32, warp = threadIdx.x/32;
+    const long long N = v.n;
+    const int nx = v.nx, ny = v.ny, nz = v.nz;
+    const R omega = R(v.omega), om1 = R(1) - omega;
+    const R gx = R(v.g[0]), gy = R(v.g[1]), gz = R(v.g[2]);
+    R ux0 = 0, uy0 = 0, uz0 = 0;
+    if (remove) {
+        ux0 = R(v.stats->ucm[0]);
+        uy0 = R(v.stats->ucm[1]);
+        uz0 = R(v.stats->ucm[2]);
+    }
+    R stressFactor = 0, muR = 0;
+    if (FLUCT) {
+        muR = R(v.mu);
+        stressFactor = omega*(R(2) - omega);
+    }
+    double acc[NPART] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (long long t = blockIdx.x; t < v.numTiles; t += gridDim.x) {
+        int tx = (int) (t%v.tilesX);
+        long long rr = t/v.tilesX;
+        int ty = (int) (rr%v.tilesY);
+        int z = (int) (rr/v.tilesY);
+        int x = tx*TX + lane, y = ty*TY + warp;
+        if (x >= nx || y >= ny)
+            continue;
+        long long row = (long long) z*ny + y;
+        if (SOLID) {
+            uint32_t word = __ldg(&v.solidMask[row*v.wordsPerRow + tx]);
+            if ((word >> lane) & 1u)
+                continue;
+        }
+        long long node = row*nx + x;
+        // Source rows and columns of the pull, periodic: index 0 is the coordinate - 1, 2 is + 1.
+        int xs[3] = {x == 0 ? nx-1 : x-1, x, x == nx-1 ? 0 : x+1};
+        int ys[3] = {y == 0 ? ny-1 : y-1, y, y == ny-1 ? 0 : y+1};
+        int zs[3] = {z == 0 ? nz-1 : z-1, z, z == nz-1 ? 0 : z+1};
+        R f[19];
+        staticFor<19>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+            long long src = ((long long) zs[1-cz]*ny + ys[1-cy])*nx + xs[1-cx];
+            f[q] = Storage<T>::template load<q>(A + (long long) q*N + src);
+        });
+        Moments<R> m = momentsOf<R>(f);
+        R rho = R(1) + m.dr, inv = R(1)/rho;
+        R jx = m.jx, jy = m.jy, jz = m.jz;
+        if (remove) {
+            jx -= rho*ux0;
+            jy -= rho*uy0;
+            jz -= rho*uz0;
+        }
+        R Fx = rho*gx, Fy = rho*gy, Fz = rho*gz;
+        if (REACT) {
+            uint32_t word = __ldg(&v.reactMask[row*v.wordsPerRow + tx]);
+            if ((word >> lane) & 1u) {
+                const R* rp = reinterpret_cast<const R*>(v.reaction) + 4*node;
+                Fx += rp[0];
+                Fy += rp[1];
+                Fz += rp[2];
+            }
+        }
+        R ux = (jx + R(0.5)*Fx)*inv, uy = (jy + R(0.5)*Fy)*inv, uz = (jz + R(0.5)*Fz)*inv;
+        R uu = ux*ux + uy*uy + uz*uz, uf = ux*Fx + uy*Fy + uz*Fz;
+        R trace = (m.pxx + m.pyy + m.pzz)*R(1.0/3.0);
+        R a[15];
+        if (FLUCT) {
+            R r[15];
+            philoxNormals<R, 15>(v.seed, PurposeFluid, node, step, r);
+            R ghost = sqrt(muR*rho);
+            modeAmplitudes<R>(r, sqrt(muR*rho*stressFactor), ghost, a);
+        }
+        R outMass = 0, outX = 0, outY = 0, outZ = 0;
+        // q = 0
+        {
+            R value = R(1.0/3.0)*(m.dr - R(1.5)*rho*uu) - om1*R(4.5/3.0)*trace - R(0.5/3.0)*R(3)*uf;
+            if (FLUCT) {
+                R e, o;
+                fluctuationParts<R, 0>(a, e, o);
+                value += e;
+            }
+            R stored = Storage<T>::template store<0>(B + node, value);
+            outMass += stored;
+        }
+        // Pairs (q, q+1) with c_{q+1} = -c_q.
+        staticFor<9>([&](auto pc) {
+            constexpr int q = 2*decltype(pc)::value + 1;
+            constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+            constexpr R w = wOf<R>(q);
+            R cu = R(cx)*ux + R(cy)*uy + R(cz)*uz;
+            R cf = R(cx)*Fx + R(cy)*Fy + R(cz)*Fz;
+            R h2pi = R(cx*cx)*m.pxx + R(cy*cy)*m.pyy + R(cz*cz)*m.pzz - trace
+                   + R(2)*(R(cx*cy)*m.pxy + R(cx*cz)*m.pxz + R(cy*cz)*m.pyz);
+            R even = w*(m.dr + rho*(R(4.5)*cu*cu - R(1.5)*uu)) + om1*(R(4.5)*w)*h2pi
+                   + R(0.5)*w*(R(9)*cu*cf - R(3)*uf);
+            R odd = R(3)*w*(rho*cu + R(0.5)*cf);
+            if (FLUCT) {
+                R e, o;
+                fluctuationParts<R, q>(a, e, o);
+                even += e;
+                odd += o;
+            }
+            R s1 = Storage<T>::template store<q>(B + (long long) q*N + node, even + odd);
+            R s2 = Storage<T>::template store<q+1>(B + (long long) (q+1)*N + node, even - odd);
+            outMass += s1 + s2;
+            R d = s1 - s2;
+            if (cx != 0) outX += R(cx)*d;
+            if (cy != 0) outY += R(cy)*d;
+            if (cz != 0) outZ += R(cz)*d;
+        });
+        acc[0] += (double) outMass;
+        acc[1] += (double) outX;
+        acc[2] += (double) outY;
+        acc[3] += (double) outZ;
+    }
+    blockReduceStore(acc, v.partials + NPART*(long long) blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Bounce-back over the wall links (after the dense step, on the output array).
+// ---------------------------------------------------------------------------------------------------
+
+template <typename T, typename R>
+__global__ void __launch_bounds__(THREADS)
+bounceBackKernel(T* __restrict__ B, const int* __restrict__ wall, int numWall, FluidView v, double* partials) {
+    double acc[NPART] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = blockIdx.x*blockDim.x + threadIdx.x; b < numWall; b += gridDim.x*blockDim.x) {
+        long long node = wall[2*b];
+        int links = wall[2*b+1];
+        Coords c = nodeCoords(node, v.nx, v.ny);
+        for (int q = 1; q < 19; q++) {
+            if (!(links & (1<<q)))
+                continue;
+            // The population x built for q streamed into the solid node s = x + c_q; x takes it back along
+            // -c_q, so it goes into the slot of s that x pulls for opp(q).  Opposite directions have the same
+            // weight, so the stored element is copied as it is.
+            long long s = shifted(v, c.x, c.y, c.z, cxr(q), cyr(q), czr(q));
+            T raw = B[(long long) q*v.n + node];
+            B[(long long) oppOf(q)*v.n + s] = raw;
+            double value = (double) loadq<T, R>(&raw, q);
+            double w = weightOf<double>(q);
+            // The fluid momentum of the population is reversed; the wall receives 2 c_q (f + w)
+            // (ReferenceLBMKernels.cpp:1176-1205, momentum exchange of Ladd 1994).
+            acc[1] -= 2.0*cxr(q)*value;
+            acc[2] -= 2.0*cyr(q)*value;
+            acc[3] -= 2.0*czr(q)*value;
+            acc[4] += 2.0*cxr(q)*(value + w);
+            acc[5] += 2.0*cyr(q)*(value + w);
+            acc[6] += 2.0*czr(q)*(value + w);
+        }
+    }
+    blockReduceStore(acc, partials + NPART*(long long) blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Regularized walls and open faces (applyBoundaries, ReferenceLBMKernels.cpp:1207-1343), on the boundary
+// node list, after the dense step: A is the input of the step (its moments are recomputed from it) and B
+// its output.
+// ---------------------------------------------------------------------------------------------------
+
+template <typename R>
+__device__ void eqDeviation(R drho, R ux, R uy, R uz, int q, R& out) {
+    R rho = R(1) + drho;
+    R uu = ux*ux + uy*uy + uz*uz;
+    R cu = cxr(q)*ux + cyr(q)*uy + czr(q)*uz;
+    out = weightOf<R>(q)*(drho + rho*(R(3)*cu + R(4.5)*cu*cu - R(1.5)*uu));
+}
+
+template <typename R>
+__device__ R guoAt(int q, R ux, R uy, R uz, R fx, R fy, R fz) {
+    R uf = ux*fx + uy*fy + uz*fz;
+    R cu = cxr(q)*ux + cyr(q)*uy + czr(q)*uz;
+    R cf = cxr(q)*fx + cyr(q)*fy + czr(q)*fz;
+    return weightOf<R>(q)*(R(3)*(cf - uf) + R(9)*cu*cf);
+}
+
+template <typename R>
+__device__ R fneqAt(int q, const Moments<R>& m) {
+    R cx = cxr(q), cy = cyr(q), cz = czr(q);
+    R h0 = cx*cx - R(1.0/3.0), h1 = cy*cy - R(1.0/3.0), h2 = cz*cz - R(1.0/3.0);
+    return R(4.5)*weightOf<R>(q)*(h0*m.pxx + h1*m.pyy + h2*m.pzz + R(2)*(cx*cy*m.pxy + cx*cz*m.pxz + cy*cz*m.pyz));
+}
+
+template <typename T, typename R, bool FLUCT>
+__global__ void __launch_bounds__(128)
+boundaryKernel(const T* __restrict__ A, T* __restrict__ B, const int* __restrict__ bnd, int numBoundary, FluidView v,
+               int remove, long long step, double* partials, const double* faceData) {
+    // faceData: per face (6): velocity[3], density, then boundary stress weight c, and the flags.
+    double acc[NPART] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const long long N = v.n;
+    const R omega = R(v.omega);
+    const R gx = R(v.g[0]), gy = R(v.g[1]), gz = R(v.g[2]);
+    for (int b = blockIdx.x*blockDim.x + threadIdx.x; b < numBoundary; b += gridDim.x*blockDim.x) {
+        long long node = bnd[4*b];
+        int unknown = bnd[4*b+1], solid = bnd[4*b+2];
+        int kind = bnd[4*b+3] & 255, face = (bnd[4*b+3] >> 8) - 1;
+        Coords c = nodeCoords(node, v.nx, v.ny);
+        // Moments of x at this step, from the input array, as in the dense kernel.
+        R f[19];
+        for (int q = 0; q < 19; q++)
+            f[q] = loadq<T, R>(A + (long long) q*N + shifted(v, c.x, c.y, c.z, -cxr(q), -cyr(q), -czr(q)), q);
+        Moments<R> m = momentsOf<R>(f);
+        R rhoNode = R(1) + m.dr;
+        R jx = m.jx, jy = m.jy, jz = m.jz;
+        if (remove) {
+            jx -= rhoNode*R(v.stats->ucm[0]);
+            jy -= rhoNode*R(v.stats->ucm[1]);
+            jz -= rhoNode*R(v.stats->ucm[2]);
+        }
+        // The post-stream value of x for direction p: B_p(x - c_p).
+        auto arrived = [&](int p) -> R {
+            return loadq<T, R>(B + (long long) p*N + shifted(v, c.x, c.y, c.z, -cxr(p), -cyr(p), -czr(p)), p);
+        };
+        R rb = rhoNode, dr = m.dr;
+        R ub[3] = {(jx + R(0.5)*(rb*gx))/rb, (jy + R(0.5)*(rb*gy))/rb, (jz + R(0.5)*(rb*gz))/rb};
+        if (kind == KindWall || kind == KindDensityAtRest)
+            ub[0] = ub[1] = ub[2] = 0;
+        if (kind == KindVelocity || kind == KindDensityVelocity)
+            for (int a = 0; a < 3; a++)
+                ub[a] = R(faceData[4*face + a]);
+        if (kind == KindDensity || kind == KindDensityAtRest || kind == KindDensityVelocity) {
+            dr = R(faceData[4*face + 3]) - R(1);
+            rb = R(faceData[4*face + 3]);
+        }
+        if (kind == KindDensity) {
+            int axis = face/2;
+            R inward = (face%2 == 0 ? R(1) : R(-1)), sum = 0;
+            for (int q = 0; q < 19; q++)
+                sum += arrived((unknown & (1<<q)) ? oppOf(q) : q);
+            ub[axis] = R(0.5)*(inward*(dr - sum)/rb + ub[axis]);
+        }
+        R xi[19];
+        bool fluct = FLUCT;
+        if (FLUCT) {
+            R mu = R(v.mu);
+            R cw = R(faceData[24]);
+            if (hasEquilibriumNoise(kind)) {
+                // Random part of a node at equilibrium (D3Q19::equilibriumFluctuation) minus c times the
+                // stress part of the random part of the collision of x (ReferenceLBMKernels.cpp:1278-1284).
+                R r[19], a[15], rc[15], ac[15];
+                philoxNormals<R, 19>(v.seed, PurposeBoundary, node, step, r);
+                R oneMinusC = R(1) - cw;
+                modeAmplitudes<R>(r, sqrt(mu*rb*(oneMinusC > R(0) ? oneMinusC : R(0))), sqrt(mu*rb), a);
+                philoxNormals<R, 15>(v.seed, PurposeFluid, node, step, rc);
+                modeAmplitudes<R>(rc, sqrt(mu*rhoNode*omega*(R(2) - omega)), R(0), ac);
+                R conserved = sqrt(mu*rb);
+                for (int q = 0; q < 19; q++) {
+                    xi[q] = fluctuationAt<R>(q, a)
+                          + weightOf<R>(q)*conserved*(r[15] + R(1.7320508075688772)*(cxr(q)*r[16] + cyr(q)*r[17] + czr(q)*r[18]))
+                          - cw*fluctuationAt<R>(q, ac);
+                }
+            }
+            else {
+                R r[15], a[15];
+                philoxNormals<R, 15>(v.seed, PurposeBoundary, node, step, r);
+                modeAmplitudes<R>(r, sqrt(mu*rb*omega*(R(2) - omega)), sqrt(mu*rb), a);
+                for (int q = 0; q < 19; q++)
+                    xi[q] = fluctuationAt<R>(q, a);
+            }
+        }
+        R Fb[3] = {gx*rb, gy*rb, gz*rb};
+        if (kind == KindWall || kind == KindVelocity) {
+            // Mass balance (ReferenceLBMKernels.cpp:1290-1325), linear in rho_b = 1 + dr.
+            R numerator = 0, denominator = 0;
+            for (int q = 1; q < 19; q++) {
+                if (!(unknown & (1<<q)))
+                    continue;
+                R arriving, flux = 0;
+                if (solid & (1<<q))
+                    arriving = loadq<T, R>(B + (long long) oppOf(q)*N + node, oppOf(q));
+                else if (!(unknown & (1<<oppOf(q)))) {
+                    arriving = arrived(oppOf(q));
+                    flux = R(6)*weightOf<R>(q)*(cxr(q)*ub[0] + cyr(q)*ub[1] + czr(q)*ub[2]);
+                }
+                else
+                    continue;
+                R e0;
+                eqDeviation<R>(R(0), ub[0], ub[1], ub[2], q, e0);
+                R sg = guoAt<R>(q, ub[0], ub[1], ub[2], gx, gy, gz);
+                R rest = (R(1) - omega)*fneqAt<R>(q, m) + (fluct ? xi[q] : R(0));
+                numerator += arriving - rest - e0 - R(0.5)*sg + flux;
+                denominator += weightOf<R>(q) + e0 + R(0.5)*sg - flux;
+            }
+            if (denominator != R(0)) {
+                dr = numerator/denominator;
+                rb = R(1) + dr;
+                Fb[0] = gx*rb; Fb[1] = gy*rb; Fb[2] = gz*rb;
+            }
+        }
+        for (int q = 1; q < 19; q++) {
+            if (!(unknown & (1<<q)))
+                continue;
+            R dfeq;
+            eqDeviation<R>(dr, ub[0], ub[1], ub[2], q, dfeq);
+            R value = dfeq + (R(1) - omega)*fneqAt<R>(q, m) + R(0.5)*guoAt<R>(q, ub[0], ub[1], ub[2], Fb[0], Fb[1], Fb[2]);
+            if (fluct)
+                value += xi[q];
+            long long src = shifted(v, c.x, c.y, c.z, -cxr(q), -cyr(q), -czr(q));
+            T* slot = B + (long long) q*N + src;
+            // Mass and momentum bookkeeping of the step sums: the value that would have arrived leaves, the rebuilt
+            // one enters.  For a solid source the population that x sent into the wall leaves instead.
+            double old = 0;
+            if (solid & (1<<q)) {
+                R sent = loadq<T, R>(B + (long long) oppOf(q)*N + node, oppOf(q));
+                old = (double) sent;
+                acc[1] += (double) sent*cxr(q);     // sent moves along -c_q
+                acc[2] += (double) sent*cyr(q);
+                acc[3] += (double) sent*czr(q);
+                // The wall receives the momentum of the population sent along -c_q and gives that of the rebuilt
+                // one along c_q (full populations, ReferenceLBMKernels.cpp:1332-1338).
+                double w = weightOf<double>(q);
+                acc[4] -= cxr(q)*((double) sent + (double) value + 2.0*w);
+                acc[5] -= cyr(q)*((double) sent + (double) value + 2.0*w);
+                acc[6] -= czr(q)*((double) sent + (double) value + 2.0*w);
+                acc[0] -= old;
+            }
+            else if (v.solidMask != nullptr && ((v.solidMask[(src/v.nx)*v.wordsPerRow + (src%v.nx)/32] >> ((src%v.nx)%32)) & 1u)) {
+                // The node across the face is solid: the dense step wrote nothing there.
+            }
+            else {
+                old = (double) loadq<T, R>(slot, q);
+                acc[0] -= old;
+                acc[1] -= old*cxr(q);
+                acc[2] -= old*cyr(q);
+                acc[3] -= old*czr(q);
+            }
+            storeq<T, R>(slot, q, value);
+            double stored = (double) loadq<T, R>(slot, q);
+            acc[0] += stored;
+            acc[1] += stored*cxr(q);
+            acc[2] += stored*cyr(q);
+            acc[3] += stored*czr(q);
+        }
+    }
+    // Block of 128 threads: pad the reduction to the generic routine.
+    blockReduceStore(acc, partials + NPART*(long long) blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Deterministic finish of the step sums: one block adds the partial records in a fixed order.
+// ---------------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(THREADS) finishKernel(const double* partials, int count, FluidView v, int mode) {
+    // mode 0: the sums of a step (mass, momentum, ucm, wall); 1: a moments pass that sets the sums and the largest
+    // speed; 2: a moments pass for the largest speed only (the sums of the step are kept).
+    double acc[NPART] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < count; i += blockDim.x)
+        for (int k = 0; k < NPART; k++)
+            acc[k] = (k == NPART-1 ? fmax(acc[k], partials[NPART*(long long) i + k]) : acc[k] + partials[NPART*(long long) i + k]);
+    __shared__ double total[NPART];
+    blockReduceStore(acc, total);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        StepStats* s = v.stats;
+        if (mode != 2) {
+            s->mass = total[0];
+            double mass = v.numFluid + total[0];
+            for (int a = 0; a < 3; a++) {
+                s->momentum[a] = total[1+a];
+                s->ucm[a] = total[1+a]/mass;
+            }
+        }
+        if (mode == 0)
+            for (int a = 0; a < 3; a++)
+                s->wall[a] = total[4+a];
+        if (mode != 0)
+            s->maxSpeed2 = total[7];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Moments of the current state (post-stream values pulled from the input array).
+// ---------------------------------------------------------------------------------------------------
+
+template <typename T, typename R>
+__global__ void __launch_bounds__(THREADS) momentsKernel(const T* __restrict__ A, FluidView v) {
+    double acc[NPART] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int lane = threadIdx.x%32, warp = threadIdx.x/32;
+    for (long long t = blockIdx.x; t < v.numTiles; t += gridDim.x) {
+        int tx = (int) (t%v.tilesX);
+        long long rr = t/v.tilesX;
+        int ty = (int) (rr%v.tilesY);
+        int z = (int) (rr/v.tilesY);
+        int x = tx*TX + lane, y = ty*TY + warp;
+        if (x >= v.nx || y >= v.ny)
+            continue;
+        long long row = (long long) z*v.ny + y;
+        if (v.solidMask != nullptr && ((__ldg(&v.solidMask[row*v.wordsPerRow + tx]) >> lane) & 1u))
+            continue;
+        R dr = 0, jx = 0, jy = 0, jz = 0;
+        for (int q = 0; q < 19; q++) {
+            R fq = loadq<T, R>(A + (long long) q*v.n + shifted(v, x, y, z, -cxr(q), -cyr(q), -czr(q)), q);
+            dr += fq;
+            jx += cxr(q)*fq;
+            jy += cyr(q)*fq;
+            jz += czr(q)*fq;
+        }
+        double r = 1.0 + (double) dr;
+        acc[0] += (double) dr;
+        acc[1] += (double) jx;
+        acc[2] += (double) jy;
+        acc[3] += (double) jz;
+        double s2 = ((double) jx*jx + (double) jy*jy + (double) jz*jz)/(r*r);
+        acc[7] = fmax(acc[7], s2);
+    }
+    blockReduceStore(acc, v.partials + NPART*(long long) blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Initial state and state transfer.
+// ---------------------------------------------------------------------------------------------------
+
+// Equilibrium at the initial velocity on fluid nodes and -w_q on solid nodes, in the pull layout:
+// A_q(y) = f_q(y + c_q) (ReferenceLBMKernels.cpp:53-79).
+template <typename T, typename R>
+__global__ void initKernel(T* A, T* B, FluidView v, const char* fluid, double ux, double uy, double uz) {
+    long long total = 19*v.n;
+    for (long long i = blockIdx.x*(long long) blockDim.x + threadIdx.x; i < total; i += (long long) gridDim.x*blockDim.x) {
+        int q = (int) (i/v.n);
+        long long y = i%v.n;
+        Coords c = nodeCoords(y, v.nx, v.ny);
+        long long target = shifted(v, c.x, c.y, c.z, cxr(q), cyr(q), czr(q));
+        double value;
+        if (fluid != nullptr && !fluid[target])
+            value = -weightOf<double>(q);
+        else {
+            double uu = ux*ux + uy*uy + uz*uz;
+            double cu = cxr(q)*ux + cyr(q)*uy + czr(q)*uz;
+            value = weightOf<double>(q)*(0.0 + 1.0*(3.0*cu + 4.5*cu*cu - 1.5*uu));
+        }
+        storeq<T, R>(A + i, q, (R) value);
+        storeq<T, R>(B + i, q, (R) value);
+    }
+}
+
+// Plane q of the state: out[x] = f_q(x) = A_q(x - c_q).
+template <typename T, typename R>
+__global__ void gatherKernel(const T* A, int q, FluidView v, double* out) {
+    for (long long x = blockIdx.x*(long long) blockDim.x + threadIdx.x; x < v.n; x += (long long) gridDim.x*blockDim.x) {
+        Coords c = nodeCoords(x, v.nx, v.ny);
+        out[x] = (double) loadq<T, R>(A + (long long) q*v.n + shifted(v, c.x, c.y, c.z, -cxr(q), -cyr(q), -czr(q)), q);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ bool bitsEqual(const T& a, const T& b) {
+    const unsigned char* pa = reinterpret_cast<const unsigned char*>(&a);
+    const unsigned char* pb = reinterpret_cast<const unsigned char*>(&b);
+    for (int i = 0; i < (int) sizeof(T); i++)
+        if (pa[i] != pb[i])
+            return false;
+    return true;
+}
+
+// Plane q of a state into both arrays: A_q(y) = f_q(y + c_q).  *changed is set when a stored element of A
+// changes, so that setting the state a kernel already holds keeps the sums of its last step (bitwise restarts).
+template <typename T, typename R>
+__global__ void scatterKernel(T* A, T* B, int q, FluidView v, const double* in, int* changed) {
+    for (long long y = blockIdx.x*(long long) blockDim.x + threadIdx.x; y < v.n; y += (long long) gridDim.x*blockDim.x) {
+        Coords c = nodeCoords(y, v.nx, v.ny);
+        R value = (R) in[shifted(v, c.x, c.y, c.z, cxr(q), cyr(q), czr(q))];
+        T before = A[(long long) q*v.n + y];
+        storeq<T, R>(A + (long long) q*v.n + y, q, value);
+        T after = A[(long long) q*v.n + y];
+        if (!bitsEqual(before, after))
+            *changed = 1;
+        storeq<T, R>(B + (long long) q*v.n + y, q, value);
+    }
+}
+
+// Density and velocity u = j/rho + g/2 of every node, zero at solid nodes (nodeFields,
+// ReferenceLBMKernels.cpp:1349-1368).
+template <typename T, typename R>
+__global__ void fieldsKernel(const T* A, FluidView v, double* out, double densityScale, double velocityScale) {
+    for (long long x = blockIdx.x*(long long) blockDim.x + threadIdx.x; x < v.n; x += (long long) gridDim.x*blockDim.x) {
+        Coords c = nodeCoords(x, v.nx, v.ny);
+        long long row = (long long) c.z*v.ny + c.y;
+        if (v.solidMask != nullptr && ((v.solidMask[row*v.wordsPerRow + c.x/32] >> (c.x%32)) & 1u)) {
+            for (int k = 0; k < 4; k++)
+                out[4*x + k] = 0;
+            continue;
+        }
+        double r = 1.0, jx = 0, jy = 0, jz = 0;
+        for (int q = 0; q < 19; q++) {
+            double fq = (double) loadq<T, R>(A + (long long) q*v.n + shifted(v, c.x, c.y, c.z, -cxr(q), -cyr(q), -czr(q)), q);
+            r += fq;
+            jx += cxr(q)*fq;
+            jy += cyr(q)*fq;
+            jz += czr(q)*fq;
+        }
+        out[4*x] = r*densityScale;
+        out[4*x+1] = (jx*(1.0/r) + v.g[0]*0.5)*velocityScale;
+        out[4*x+2] = (jy*(1.0/r) + v.g[1]*0.5)*velocityScale;
+        out[4*x+3] = (jz*(1.0/r) + v.g[2]*0.5)*velocityScale;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Launch tables per storage type.
+// ---------------------------------------------------------------------------------------------------
+
+template <typename T> struct ComputeOf { typedef float type; };
+template <> struct ComputeOf<double> { typedef double type; };
+
+template <typename T>
+struct Launcher {
+    typedef typename ComputeOf<T>::type R;
+
+    template <bool S, bool RE, bool FL>
+    static void dense(const void* A, void* B, const FluidView& v, int remove, long long step, int grid, cudaStream_t s) {
+        streamCollideKernel<T, R, S, RE, FL><<<grid, THREADS, 0, s>>>((const T*) A, (T*) B, v, remove, step);
+    }
+    template <bool S, bool RE>
+    static void denseF(bool fl, const void* A, void* B, const FluidView& v, int remove, long long step, int grid, cudaStream_t s) {
+        if (fl) dense<S, RE, true>(A, B, v, remove, step, grid, s);
+        else dense<S, RE, false>(A, B, v, remove, step, grid, s);
+    }
+    template <bool S>
+    static void denseR(bool re, bool fl, const void* A, void* B, const FluidView& v, int remove, long long step, int grid, cudaStream_t s) {
+        if (re) denseF<S, true>(fl, A, B, v, remove, step, grid, s);
+        else denseF<S, false>(fl, A, B, v, remove, step, grid, s);
+    }
+    static void denseAny(bool so, bool re, bool fl, const void* A, void* B, const FluidView& v, int remove, long long step,
+                         int grid, cudaStream_t s) {
+        if (so) denseR<true>(re, fl, A, B, v, remove, step, grid, s);
+        else denseR<false>(re, fl, A, B, v, remove, step, grid, s);
+    }
+    static int occupancy() {
+        int blocks = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, streamCollideKernel<T, R, false, false, false>, THREADS, 0);
+        return std::max(blocks, 1);
+    }
+    static void bounceBack(void* B, const int* wall, int numWall, const FluidView& v, double* partials, int grid, cudaStream_t s) {
+        bounceBackKernel<T, R><<<grid, THREADS, 0, s>>>((T*) B, wall, numWall, v, partials);
+    }
+    static void boundary(bool fl, const void* A, void* B, const int* bnd, int count, const FluidView& v, int remove, long long step,
+                         double* partials, const double* faceData, int grid, cudaStream_t s) {
+        if (fl) boundaryKernel<T, R, true><<<grid, 128, 0, s>>>((const T*) A, (T*) B, bnd, count, v, remove, step, partials, faceData);
+        else boundaryKernel<T, R, false><<<grid, 128, 0, s>>>((const T*) A, (T*) B, bnd, count, v, remove, step, partials, faceData);
+    }
+    static void moments(const void* A, const FluidView& v, int grid, cudaStream_t s) {
+        momentsKernel<T, R><<<grid, THREADS, 0, s>>>((const T*) A, v);
+    }
+    static void init(void* A, void* B, const FluidView& v, const char* fluid, const double* u, cudaStream_t s) {
+        initKernel<T, R><<<1184, 256, 0, s>>>((T*) A, (T*) B, v, fluid, u[0], u[1], u[2]);
+    }
+    static void gather(const void* A, int q, const FluidView& v, double* out, cudaStream_t s) {
+        gatherKernel<T, R><<<1184, 256, 0, s>>>((const T*) A, q, v, out);
+    }
+    static void scatter(void* A, void* B, int q, const FluidView& v, const double* in, int* changed, cudaStream_t s) {
+        scatterKernel<T, R><<<1184, 256, 0, s>>>((T*) A, (T*) B, q, v, in, changed);
+    }
+    static void fields(const void* A, const FluidView& v, double* out, double ds, double vs, cudaStream_t s) {
+        fieldsKernel<T, R><<<1184, 256, 0, s>>>((const T*) A, v, out, ds, vs);
+    }
+};
+
+template <typename F>
+void dispatchStorage(int storage, F&& f) {
+    switch (storage) {
+    case LBM_STORAGE_F64: f(Launcher<double>()); break;
+    case LBM_STORAGE_F32: f(Launcher<float>()); break;
+    case LBM_STORAGE_F16: f(Launcher<__half>()); break;
+    case LBM_STORAGE_BF16: f(Launcher<__nv_bfloat16>()); break;
+    default: throw Error(LBM_ERR_NOT_SUPPORTED, "unknown storage type");
+    }
+}
+
+size_t elementSizeOf(int storage) {
+    switch (storage) {
+    case LBM_STORAGE_F64: return 8;
+    case LBM_STORAGE_F32: return 4;
+    case LBM_STORAGE_F16: return 2;
+    case LBM_STORAGE_BF16: return 2;
+    default: throw Error(LBM_ERR_NOT_SUPPORTED, "unknown storage type");
+    }
+}
+
+const int kGridSparse = 148;      // blocks of the sparse passes (one wave)
+
+} // namespace
+
+FluidEngine::FluidEngine(const LbmLatticeParameters& l, int storage, const Geometry& g, cudaStream_t s)
+        : lattice(l), storageType(storage), elementSize(elementSizeOf(storage)), stream(s), cur(0), gridBlocks(0),
+          solidMaskDev(nullptr), reactMaskDev(nullptr), reactionDev(nullptr), partialsDev(nullptr), statsDev(nullptr),
+          numWall(0), numBoundary(0), wallDev(nullptr), boundaryDev(nullptr), equilibriumNoise(false),
+          stagingDev(nullptr), extraBlocks(0), faceDev(nullptr) {
+    pop[0] = pop[1] = nullptr;
+    std::memset(&view, 0, sizeof(view));
+    view.nx = l.nx;
+    view.ny = l.ny;
+    view.nz = l.nz;
+    view.n = (long long) l.nx*l.ny*l.nz;
+    view.wordsPerRow = (l.nx + 31)/32;
+    view.tilesX = (l.nx + TX - 1)/TX;
+    view.tilesY = (l.ny + TY - 1)/TY;
+    view.numTiles = (long long) view.tilesX*view.tilesY*l.nz;
+    view.numFluid = (double) (view.n - (long long) g.solidNodes.size());
+    solidNodes = g.solidNodes;
+    try {
+        CUDA_CHECK(cudaMalloc(&faceDev, sizeof(double)*32));
+        setParameters(l);
+        size_t bytes = (size_t) 19*view.n*elementSize;
+        CUDA_CHECK(cudaMalloc(&pop[0], bytes));
+        CUDA_CHECK(cudaMalloc(&pop[1], bytes));
+        int device = 0, sms = 0;
+        CUDA_CHECK(cudaGetDevice(&device));
+        CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        int occupancy = 1;
+        dispatchStorage(storage, [&](auto L) { occupancy = decltype(L)::occupancy(); });
+        long long wanted = (long long) sms*occupancy;
+        gridBlocks = (int) std::max(1LL, std::min(wanted, view.numTiles));
+        extraBlocks = 2*kGridSparse;
+        CUDA_CHECK(cudaMalloc(&partialsDev, sizeof(double)*NPART*(size_t) (gridBlocks + extraBlocks + 1)));
+        CUDA_CHECK(cudaMalloc(&statsDev, sizeof(StepStats)));
+        CUDA_CHECK(cudaMemsetAsync(statsDev, 0, sizeof(StepStats), stream));
+        view.partials = partialsDev;
+        view.stats = statsDev;
+
+        // Solid mask, rows padded to 32-bit words.
+        char* fluidDev = nullptr;
+        if (!g.solidNodes.empty()) {
+            size_t words = (size_t) view.wordsPerRow*l.ny*l.nz;
+            std::vector<uint32_t> mask(words, 0u);
+            for (int sn : g.solidNodes) {
+                long long row = sn/l.nx;
+                int x = (int) (sn%l.nx);
+                mask[row*view.wordsPerRow + x/32] |= 1u << (x%32);
+            }
+            CUDA_CHECK(cudaMalloc(&solidMaskDev, sizeof(uint32_t)*words));
+            CUDA_CHECK(cudaMemcpyAsync(solidMaskDev, mask.data(), sizeof(uint32_t)*words, cudaMemcpyHostToDevice, stream));
+            CUDA_CHECK(cudaMalloc(&fluidDev, view.n));
+            CUDA_CHECK(cudaMemcpyAsync(fluidDev, g.fluid.data(), view.n, cudaMemcpyHostToDevice, stream));
+        }
+        view.solidMask = solidMaskDev;
+        numWall = (int) g.wallNodes.size();
+        if (numWall > 0) {
+            std::vector<int> w(2*numWall);
+            for (int i = 0; i < numWall; i++) {
+                w[2*i] = g.wallNodes[i];
+                w[2*i+1] = g.wallLinks[i];
+            }
+            CUDA_CHECK(cudaMalloc(&wallDev, sizeof(int)*w.size()));
+            CUDA_CHECK(cudaMemcpyAsync(wallDev, w.data(), sizeof(int)*w.size(), cudaMemcpyHostToDevice, stream));
+        }
+        numBoundary = (int) g.boundaryNodes.size();
+        if (numBoundary > 0) {
+            std::vector<int> b(4*numBoundary);
+            for (int i = 0; i < numBoundary; i++) {
+                b[4*i] = g.boundaryNodes[i];
+                b[4*i+1] = g.unknown[i];
+                b[4*i+2] = g.solidBits[i];
+                b[4*i+3] = g.kind[i] | ((g.face[i] + 1) << 8);
+                equilibriumNoise = equilibriumNoise || hasEquilibriumNoise(g.kind[i]);
+            }
+            CUDA_CHECK(cudaMalloc(&boundaryDev, sizeof(int)*b.size()));
+            CUDA_CHECK(cudaMemcpyAsync(boundaryDev, b.data(), sizeof(int)*b.size(), cudaMemcpyHostToDevice, stream));
+        }
+        double u[3] = {l.initial_velocity[0], l.initial_velocity[1], l.initial_velocity[2]};
+        dispatchStorage(storage, [&](auto L) { decltype(L)::init(pop[0], pop[1], view, fluidDev, u, stream); });
+        CUDA_CHECK(cudaGetLastError());
+        if (fluidDev) {
+            CUDA_CHECK(cudaStreamSynchronize(stream));
+            cudaFree(fluidDev);
+        }
+        momentsPass(true);
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+    }
+    catch (...) {
+        this->~FluidEngine();
+        throw;
+    }
+}
+
+FluidEngine::~FluidEngine() {
+    cudaFree(pop[0]);
+    cudaFree(pop[1]);
+    cudaFree(solidMaskDev);
+    cudaFree(reactMaskDev);
+    cudaFree(reactionDev);
+    cudaFree(partialsDev);
+    cudaFree(statsDev);
+    cudaFree(wallDev);
+    cudaFree(boundaryDev);
+    cudaFree(stagingDev);
+    cudaFree(faceDev);
+    faceDev = nullptr;
+    pop[0] = pop[1] = nullptr;
+    solidMaskDev = reactMaskDev = nullptr;
+    reactionDev = stagingDev = nullptr;
+    partialsDev = nullptr;
+    statsDev = nullptr;
+    wallDev = boundaryDev = nullptr;
+}
+
+void FluidEngine::setParameters(const LbmLatticeParameters& l) {
+    lattice = l;
+    view.omega = l.omega;
+    for (int a = 0; a < 3; a++)
+        view.g[a] = l.body_acceleration[a];
+    uint32_t seed = (uint32_t) l.random_number_seed;
+    view.seed = seed;
+    double cellMass = l.density*l.dx*l.dx*l.dx;
+    bool fluctuate = l.fluid_fluctuations && l.fluid_kT > 0;
+    view.mu = fluctuate ? 3.0*l.fluid_kT*l.dt*l.dt/(cellMass*l.dx*l.dx) : 0.0;
+    // Face velocities and densities, and the boundary stress weight c = (1 - omega)^2/(omega (2 - omega))
+    // (D3Q19.h:206-208), for the boundary kernel.
+    for (int f = 0; f < 6; f++) {
+        for (int a = 0; a < 3; a++)
+            faceHost[4*f + a] = l.face_velocity[f][a];
+        faceHost[4*f + 3] = l.face_density[f];
+    }
+    faceHost[24] = (1.0-l.omega)*(1.0-l.omega)/(l.omega*(2.0-l.omega));
+    CUDA_CHECK(cudaMemcpyAsync(faceDev, faceHost, sizeof(double)*25, cudaMemcpyHostToDevice, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+}
+
+void FluidEngine::enableReaction() {
+    if (reactionDev != nullptr)
+        return;
+    size_t words = (size_t) view.wordsPerRow*lattice.ny*lattice.nz;
+    size_t r = (storageType == LBM_STORAGE_F64 ? 8 : 4);
+    CUDA_CHECK(cudaMalloc(&reactMaskDev, sizeof(uint32_t)*words));
+    CUDA_CHECK(cudaMemsetAsync(reactMaskDev, 0, sizeof(uint32_t)*words, stream));
+    CUDA_CHECK(cudaMalloc(&reactionDev, 4*r*(size_t) view.n));
+    CUDA_CHECK(cudaMemsetAsync(reactionDev, 0, 4*r*(size_t) view.n, stream));
+    view.reactMask = reactMaskDev;
+    view.reaction = reactionDev;
+}
+
+void FluidEngine::step(long long stepIndex, bool remove, bool react) {
+    const void* A = pop[cur];
+    void* B = pop[1-cur];
+    bool fluct = view.mu > 0;
+    bool solids = solidMaskDev != nullptr;
+    dispatchStorage(storageType, [&](auto L) {
+        decltype(L)::denseAny(solids, react && reactionDev != nullptr, fluct, A, B, view, remove ? 1 : 0, stepIndex,
+                              gridBlocks, stream);
+    });
+    CUDA_CHECK(cudaGetLastError());
+    int count = gridBlocks;
+    if (numWall > 0) {
+        int grid = std::min(kGridSparse, (numWall + THREADS - 1)/THREADS);
+        double* part = partialsDev + NPART*(size_t) count;
+        dispatchStorage(storageType, [&](auto L) { decltype(L)::bounceBack(B, wallDev, numWall, view, part, grid, stream); });
+        CUDA_CHECK(cudaGetLastError());
+        count += grid;
+    }
+    if (numBoundary > 0) {
+        int grid = std::min(kGridSparse, (numBoundary + 127)/128);
+        double* part = partialsDev + NPART*(size_t) count;
+        // Face velocities and densities, and the boundary stress weight c (D3Q19.h:206-208), in a small table
+        // that lives in the partials buffer tail (read-only for the kernel).
+        dispatchStorage(storageType, [&](auto L) {
+            decltype(L)::boundary(fluct, A, B, boundaryDev, numBoundary, view, remove ? 1 : 0, stepIndex, part,
+                                  faceDev, grid, stream);
+        });
+        CUDA_CHECK(cudaGetLastError());
+        count += grid;
+    }
+    finishKernel<<<1, THREADS, 0, stream>>>(partialsDev, count, view, 0);
+    CUDA_CHECK(cudaGetLastError());
+    cur = 1-cur;
+}
+
+void FluidEngine::momentsPass(bool setSums) {
+    dispatchStorage(storageType, [&](auto L) { decltype(L)::moments(pop[cur], view, gridBlocks, stream); });
+    CUDA_CHECK(cudaGetLastError());
+    finishKernel<<<1, THREADS, 0, stream>>>(partialsDev, gridBlocks, view, setSums ? 1 : 2);
+    CUDA_CHECK(cudaGetLastError());
+}
+
+void FluidEngine::restoreStats(const StepStats& stats) {
+    statsHost = stats;
+    CUDA_CHECK(cudaMemcpyAsync(statsDev, &statsHost, sizeof(StepStats), cudaMemcpyHostToDevice, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+}
+
+StepStats FluidEngine::readStats() {
+    StepStats s;
+    CUDA_CHECK(cudaMemcpyAsync(&s, statsDev, sizeof(StepStats), cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    return s;
+}
+
+void FluidEngine::getState(double* host) {
+    if (stagingDev == nullptr)
+        CUDA_CHECK(cudaMalloc(&stagingDev, sizeof(double)*4*(size_t) view.n));
+    for (int q = 0; q < 19; q++) {
+        dispatchStorage(storageType, [&](auto L) { decltype(L)::gather(pop[cur], q, view, (double*) stagingDev, stream); });
+        CUDA_CHECK(cudaGetLastError());
+        CUDA_CHECK(cudaMemcpyAsync(host + (size_t) q*view.n, stagingDev, sizeof(double)*view.n, cudaMemcpyDeviceToHost, stream));
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+    }
+}
+
+void FluidEngine::setState(const double* host) {
+    if (stagingDev == nullptr)
+        CUDA_CHECK(cudaMalloc(&stagingDev, sizeof(double)*4*(size_t) view.n));
+    int* changedDev = reinterpret_cast<int*>(partialsDev);
+    CUDA_CHECK(cudaMemsetAsync(changedDev, 0, sizeof(int), stream));
+    for (int q = 0; q < 19; q++) {
+        CUDA_CHECK(cudaMemcpyAsync(stagingDev, host + (size_t) q*view.n, sizeof(double)*view.n, cudaMemcpyHostToDevice, stream));
+        dispatchStorage(storageType, [&](auto L) {
+            decltype(L)::scatter(pop[cur], pop[1-cur], q, view, (const double*) stagingDev, changedDev, stream);
+        });
+        CUDA_CHECK(cudaGetLastError());
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+    }
+    int changed = 0;
+    CUDA_CHECK(cudaMemcpy(&changed, changedDev, sizeof(int), cudaMemcpyDeviceToHost));
+    if (changed)
+        momentsPass(true);
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+}
+
+void FluidEngine::fields(double* density, double* velocity, double densityScale, double velocityScale) {
+    if (stagingDev == nullptr)
+        CUDA_CHECK(cudaMalloc(&stagingDev, sizeof(double)*4*(size_t) view.n));
+    dispatchStorage(storageType, [&](auto L) {
+        decltype(L)::fields(pop[cur], view, (double*) stagingDev, densityScale, velocityScale, stream);
+    });
+    CUDA_CHECK(cudaGetLastError());
+    std::vector<double> all(4*(size_t) view.n);
+    CUDA_CHECK(cudaMemcpyAsync(all.data(), stagingDev, sizeof(double)*all.size(), cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    for (long long x = 0; x < view.n; x++) {
+        density[x] = all[4*x];
+        for (int a = 0; a < 3; a++)
+            velocity[3*x+a] = all[4*x+1+a];
+    }
+}
+
+void FluidEngine::copyStateOut(void* host) {
+    CUDA_CHECK(cudaMemcpyAsync(host, pop[cur], stateBytes(), cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+}
+
+void FluidEngine::copyStateIn(const void* host) {
+    CUDA_CHECK(cudaMemcpyAsync(pop[cur], host, stateBytes(), cudaMemcpyHostToDevice, stream));
+    CUDA_CHECK(cudaMemcpyAsync(pop[1-cur], pop[cur], stateBytes(), cudaMemcpyDeviceToDevice, stream));
+    momentsPass(true);
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+}
+
+} // namespace lbm

@@ -1,0 +1,265 @@
+// Host object of the B200 LBM force kernel (see kernel.cuh).
+#include "kernel.cuh"
+#include "coupling.cuh"
+#include <cmath>
+#include <cstring>
+#include <sstream>
+
+namespace lbm {
+
+#define CUDA_CHECK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) \
+    throw Error(LBM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); } while (0)
+
+namespace {
+
+const uint64_t kCheckpointMagic = 0x314B43423230304CULL;   // "L002BCK1"
+const int kCheckpointVersion = 1;
+
+struct CheckpointHeader {
+    uint64_t magic;
+    int version, storage;
+    int nx, ny, nz, numParticles;
+    int stepForcesCurrent, stepWallValid, pad[2];
+    long long stepIndex;
+    double hostWall[3];
+    StepStats stats;
+};
+
+} // namespace
+
+B200Kernel::B200Kernel(const LbmLatticeParameters& l, const LbmOptions& options, int np, const double* masses,
+                       int numSolid, const int* solid)
+        : lattice(l), stream(nullptr), ownStream(false), device(options.device), numParticles(np), stepPending(false),
+          stepForcesCurrent(false), stepWallValid(false), stepIndex(0) {
+    hostWallMomentum[0] = hostWallMomentum[1] = hostWallMomentum[2] = 0;
+    if (l.nx <= 0 || l.ny <= 0 || l.nz <= 0)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: the grid size must be set to positive values with setGridSize()");
+    if (!(l.tau > 0.5) || std::fabs(l.omega*l.tau - 1.0) > 1e-12)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: the relaxation time must exceed 1/2 and omega must be 1/tau");
+    if (np < 0 || numSolid < 0 || (np > 0 && masses == nullptr) || (numSolid > 0 && solid == nullptr))
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_create: invalid particle or solid node arrays");
+    long long n = (long long) l.nx*l.ny*l.nz;
+    for (int i = 0; i < numSolid; i++)
+        if (solid[i] < 0 || solid[i] >= n)
+            throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: a solid node index is out of range");
+    for (int i = 0; i < np; i++)
+        if (!(masses[i] > 0))
+            throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: coupled particles must have a positive mass");
+    CUDA_CHECK(cudaSetDevice(device));
+    if (options.stream != nullptr)
+        stream = (cudaStream_t) options.stream;
+    else {
+        CUDA_CHECK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        ownStream = true;
+    }
+    buildGeometry(l, numSolid, solid, geometry);
+    for (size_t i = 1; i < geometry.solidNodes.size(); i++)
+        if (geometry.solidNodes[i] == geometry.solidNodes[i-1])
+            throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: a solid node is listed more than once");
+    if ((long long) geometry.solidNodes.size() == n)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: all lattice nodes are solid");
+    fluid.reset(new FluidEngine(l, options.storage, geometry, stream));
+    if (np > 0) {
+        fluid->enableReaction();
+        coupling.reset(new CouplingEngine(l, *fluid, geometry, np, masses, stream));
+    }
+}
+
+B200Kernel::~B200Kernel() {
+    coupling.reset();
+    fluid.reset();
+    if (ownStream && stream != nullptr)
+        cudaStreamDestroy(stream);
+}
+
+// beginStep (ReferenceLBMKernels.cpp:308-339).
+void B200Kernel::beginStep(long long stepCount, const LbmParticleArrays* particles) {
+    CUDA_CHECK(cudaSetDevice(device));
+    stepIndex = stepCount;
+    stepPending = true;
+    stepWallValid = false;
+    hostWallMomentum[0] = hostWallMomentum[1] = hostWallMomentum[2] = 0;
+    if (!geometry.solidNodes.empty() && numParticles > 0) {
+        if (particles == nullptr)
+            throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_begin_step: the particle arrays are missing");
+        coupling->reflect(particles, hostWallMomentum);
+    }
+}
+
+// execute (ReferenceLBMKernels.cpp:341-365).
+double B200Kernel::execute(long long stepCount, const LbmParticleArrays* particles, bool includeForces, bool) {
+    CUDA_CHECK(cudaSetDevice(device));
+    if (numParticles > 0 && particles == nullptr)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_execute: the particle arrays are missing");
+    bool repeatedStep = (stepForcesCurrent && stepCount == stepIndex-1);
+    if (stepPending) {
+        stepPending = false;
+        advanceFluid(particles);
+    }
+    else if (includeForces && numParticles > 0 && stepCount > 0 && !repeatedStep)
+        computeNextStepForces(stepCount, particles);
+    if (includeForces && numParticles > 0)
+        coupling->addForces(particles);
+    return 0.0;
+}
+
+// advanceFluid (ReferenceLBMKernels.cpp:367-389).
+void B200Kernel::advanceFluid(const LbmParticleArrays* particles) {
+    bool remove = lattice.momentum_removal_frequency > 0 && stepIndex%lattice.momentum_removal_frequency == 0;
+    bool react = false;
+    if (numParticles > 0) {
+        coupling->load(particles, lattice.drag_scheme == LBM_DRAG_CENTERED);
+        coupling->couple(stepIndex, true, remove);
+        react = true;
+    }
+    fluid->step(stepIndex, remove, react);
+    if (react)
+        coupling->clearReaction();
+    stepWallValid = true;
+    stepForcesCurrent = true;
+    stepIndex++;
+    if (lattice.mach_check_frequency > 0 && stepIndex%lattice.mach_check_frequency == 0)
+        checkMachNumber();
+}
+
+// computeNextStepForces (ReferenceLBMKernels.cpp:391-401).
+void B200Kernel::computeNextStepForces(long long stepCount, const LbmParticleArrays* particles) {
+    stepForcesCurrent = false;
+    bool remove = lattice.momentum_removal_frequency > 0 && stepCount%lattice.momentum_removal_frequency == 0;
+    coupling->load(particles, lattice.drag_scheme == LBM_DRAG_CENTERED);
+    coupling->couple(stepCount, false, remove);
+}
+
+// checkMachNumber (ReferenceLBMKernels.cpp:412-428).
+void B200Kernel::checkMachNumber() {
+    double mach = getFluidMachNumber();
+    if (mach > lattice.mach_number_limit) {
+        std::stringstream msg;
+        msg << "LBMForce: the Mach number of the fluid is " << mach << " after " << stepIndex << " lattice steps, "
+            << "above the limit " << lattice.mach_number_limit << " (docs/theory.md, section 6). Reduce the forces on the "
+            << "fluid, the time step or the friction.";
+        throw Error(LBM_ERR_MACH_LIMIT, msg.str());
+    }
+}
+
+void B200Kernel::copyParameters(const LbmLatticeParameters& l) {
+    CUDA_CHECK(cudaSetDevice(device));
+    if (l.nx != lattice.nx || l.ny != lattice.ny || l.nz != lattice.nz)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "updateParametersInContext: the grid size cannot be changed");
+    if (l.density != lattice.density || l.tau != lattice.tau)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "updateParametersInContext: the fluid density and viscosity cannot be changed");
+    if (l.wall_scheme != lattice.wall_scheme)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "updateParametersInContext: the wall scheme cannot be changed");
+    for (int f = 0; f < 6; f++)
+        if (l.face_boundary[f] != lattice.face_boundary[f])
+            throw Error(LBM_ERR_INVALID_ARGUMENT, "updateParametersInContext: the boundary types of the faces cannot be changed");
+    if (l.drag_scheme != lattice.drag_scheme)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "updateParametersInContext: the drag scheme cannot be changed");
+    if (l.interpolation_stencil != lattice.interpolation_stencil)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "updateParametersInContext: the interpolation stencil cannot be changed");
+    if (l.fluid_fluctuations != lattice.fluid_fluctuations)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "updateParametersInContext: the fluid fluctuations cannot be switched on or off");
+    lattice = l;
+    fluid->setParameters(l);
+    if (coupling)
+        coupling->setParameters(l);
+}
+
+void B200Kernel::getFluidFields(double* density, double* velocity) {
+    CUDA_CHECK(cudaSetDevice(device));
+    fluid->fields(density, velocity, lattice.density, lattice.dx/lattice.dt);
+}
+
+double B200Kernel::getFluidMachNumber() {
+    CUDA_CHECK(cudaSetDevice(device));
+    // The pass keeps the sums of the last step for the next removal, so that the result of a run does not
+    // depend on when the Mach number is read.
+    fluid->momentsPass(false);
+    StepStats s = fluid->readStats();
+    return std::sqrt(3.0*s.maxSpeed2);
+}
+
+// getWallForce (ReferenceLBMKernels.cpp:1438-1443): the momentum given to the solid nodes in the last step,
+// divided by the time step.
+void B200Kernel::getWallForce(double force[3]) {
+    CUDA_CHECK(cudaSetDevice(device));
+    double cellMass = lattice.density*lattice.dx*lattice.dx*lattice.dx;
+    double scale = cellMass*lattice.dx/lattice.dt;
+    double total[3] = {hostWallMomentum[0], hostWallMomentum[1], hostWallMomentum[2]};
+    if (stepWallValid) {
+        StepStats s = fluid->readStats();
+        for (int a = 0; a < 3; a++)
+            total[a] += s.wall[a]*scale;
+        if (coupling) {
+            double r[3];
+            coupling->reactionWallMomentum(r);
+            for (int a = 0; a < 3; a++)
+                total[a] += r[a]*scale;
+        }
+    }
+    for (int a = 0; a < 3; a++)
+        force[a] = total[a]/lattice.dt;
+}
+
+void B200Kernel::getFluidState(double* state) {
+    CUDA_CHECK(cudaSetDevice(device));
+    fluid->getState(state);
+}
+
+// setFluidState (ReferenceLBMKernels.cpp:1488-1505).
+void B200Kernel::setFluidState(const double* state) {
+    CUDA_CHECK(cudaSetDevice(device));
+    fluid->setState(state);
+    stepForcesCurrent = false;
+}
+
+size_t B200Kernel::checkpointSize() {
+    return sizeof(CheckpointHeader) + fluid->stateBytes();
+}
+
+// createCheckpoint / loadCheckpoint (LBMKernels.h:170-174): the populations in the storage type and pull
+// layout, the step statistics (the sums of the next momentum removal), the wall momentum and the evaluation
+// state.  The random numbers are a function of the seed and the step, so no generator state is saved.
+void B200Kernel::createCheckpoint(void* buffer, size_t bytes) {
+    CUDA_CHECK(cudaSetDevice(device));
+    if (bytes < checkpointSize())
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_create_checkpoint: the buffer is too small");
+    CheckpointHeader h;
+    std::memset(&h, 0, sizeof(h));
+    h.magic = kCheckpointMagic;
+    h.version = kCheckpointVersion;
+    h.storage = fluid->storage();
+    h.nx = lattice.nx; h.ny = lattice.ny; h.nz = lattice.nz;
+    h.numParticles = numParticles;
+    h.stepForcesCurrent = 0;
+    h.stepWallValid = stepWallValid;
+    h.stepIndex = stepIndex;
+    for (int a = 0; a < 3; a++)
+        h.hostWall[a] = hostWallMomentum[a];
+    h.stats = fluid->readStats();
+    std::memcpy(buffer, &h, sizeof(h));
+    fluid->copyStateOut((char*) buffer + sizeof(h));
+}
+
+void B200Kernel::loadCheckpoint(const void* buffer, size_t bytes) {
+    CUDA_CHECK(cudaSetDevice(device));
+    if (bytes < sizeof(CheckpointHeader))
+        throw Error(LBM_ERR_CHECKPOINT, "LBMForce: the checkpoint is truncated");
+    CheckpointHeader h;
+    std::memcpy(&h, buffer, sizeof(h));
+    if (h.magic != kCheckpointMagic || h.version != kCheckpointVersion)
+        throw Error(LBM_ERR_CHECKPOINT, "LBMForce: the checkpoint was not written by this kernel");
+    if (h.storage != fluid->storage() || h.nx != lattice.nx || h.ny != lattice.ny || h.nz != lattice.nz ||
+            h.numParticles != numParticles)
+        throw Error(LBM_ERR_CHECKPOINT, "LBMForce: the checkpoint belongs to another lattice, precision or set of particles");
+    if (bytes < checkpointSize())
+        throw Error(LBM_ERR_CHECKPOINT, "LBMForce: the checkpoint is truncated");
+    fluid->copyStateIn((const char*) buffer + sizeof(h));
+    fluid->restoreStats(h.stats);
+    stepForcesCurrent = false;
+    stepWallValid = h.stepWallValid != 0;
+    for (int a = 0; a < 3; a++)
+        hostWallMomentum[a] = h.hostWall[a];
+}
+
+} // namespace lbm

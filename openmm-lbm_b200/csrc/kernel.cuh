@@ -1,0 +1,52 @@
+// The B200 LBM force kernel: the host object behind the C ABI.  It mirrors the platform kernel
+// interface CalcLBMForceKernel (openmmapi/include/LBMKernels.h:97-189) and the evaluation rules of the
+// reference's ReferenceCalcLBMForceKernel (platforms/reference/src/ReferenceLBMKernels.cpp:308-401):
+// the fluid advances once per integration step, on the first evaluation after beginStep(); evaluations
+// between steps give the coupling force of the next step without its reaction; a repeated evaluation of a
+// step reuses its forces.
+#pragma once
+
+#include "fluid.cuh"
+#include <memory>
+
+namespace lbm {
+
+class CouplingEngine;
+
+class B200Kernel {
+public:
+    B200Kernel(const LbmLatticeParameters& lattice, const LbmOptions& options, int numParticles, const double* masses,
+               int numSolid, const int* solid);
+    ~B200Kernel();
+    void beginStep(long long stepCount, const LbmParticleArrays* particles);
+    double execute(long long stepCount, const LbmParticleArrays* particles, bool includeForces, bool includeEnergy);
+    void copyParameters(const LbmLatticeParameters& lattice);
+    void getFluidFields(double* density, double* velocity);
+    double getFluidMachNumber();
+    void getWallForce(double force[3]);
+    void getFluidState(double* state);
+    void setFluidState(const double* state);
+    size_t checkpointSize();
+    void createCheckpoint(void* buffer, size_t bytes);
+    void loadCheckpoint(const void* buffer, size_t bytes);
+    long long numNodes() const { return fluid->numNodes(); }
+    int storage() const { return fluid->storage(); }
+    cudaStream_t getStream() const { return stream; }
+private:
+    void advanceFluid(const LbmParticleArrays* particles);
+    void computeNextStepForces(long long stepCount, const LbmParticleArrays* particles);
+    void checkMachNumber();
+    LbmLatticeParameters lattice;
+    Geometry geometry;
+    cudaStream_t stream;
+    bool ownStream;
+    int device;
+    std::unique_ptr<FluidEngine> fluid;
+    std::unique_ptr<CouplingEngine> coupling;
+    int numParticles;
+    bool stepPending, stepForcesCurrent, stepWallValid;
+    long long stepIndex;
+    double hostWallMomentum[3];     // reflection at the walls and reactions on solid nodes, Da nm/ps
+};
+
+} // namespace lbm

@@ -1,0 +1,92 @@
+"""The parity cases of the tests, built like the reference's cross-platform tests
+(python/tests/TestLBMForce.py:501-635): the same Systems, in the harness of lbm_b200."""
+import numpy as np
+
+import lbm_b200
+from lbm_b200 import LBMForce
+
+FLUID_WALLS = ('periodic', 'walls', 'regularized', 'faces', 'dvfaces')
+
+
+def fluid_case(walls, kernel_factory=None, properties=None):
+    """test_fluid_agrees_with_reference (TestLBMForce.py:505-570): a 6x5x4 lattice with a perturbed fluid, a body
+    force and the removal of the momentum every third step, with solid nodes (the plane j = 0 and a block),
+    bounce-back or regularized walls, and open faces.  Returns (context, force); the fluid is perturbed."""
+    system = lbm_b200.System()
+    system.setDefaultPeriodicBoxVectors((3, 0, 0), (0, 2.5, 0), (0, 0, 2))
+    system.addParticle(1.0)
+    force = LBMForce()
+    force.setGridSize(6, 5, 4)
+    force.setKinematicViscosity((0.8 - 0.5)/3*0.25/0.01)
+    force.setBodyAcceleration((0.5, -0.2, 0.1))
+    force.setInitialFluidVelocity((0.5, 0.2, -0.3))
+    force.setFluidMomentumRemovalFrequency(0 if walls in ('faces', 'dvfaces') else 3)
+    if walls != 'periodic':
+        force.setSolidNodes([i + 6*5*k for k in range(4) for i in range(6)] +
+                            [i + 6*(j + 5*k) for k in (1, 2) for j in (2, 3) for i in (2, 3)])
+    if walls in ('regularized', 'faces', 'dvfaces'):
+        force.setWallScheme(LBMForce.Regularized)
+    if walls == 'dvfaces':
+        force.setFaceBoundary(LBMForce.XMin, LBMForce.DensityVelocity)
+        force.setFaceBoundary(LBMForce.XMax, LBMForce.Velocity)
+        force.setFaceBoundary(LBMForce.ZMin, LBMForce.Density)
+        force.setFaceBoundary(LBMForce.ZMax, LBMForce.DensityVelocity)
+        force.setFaceVelocity(LBMForce.XMin, (0.5, 0.1, 0.0))
+        force.setFaceDensity(LBMForce.XMin, 605.0)
+        force.setFaceVelocity(LBMForce.XMax, (0.4, 0.0, 0.1))
+        force.setFaceDensity(LBMForce.ZMax, 600.0)
+        force.setFaceVelocity(LBMForce.ZMax, (0.2, -0.1, 0.0))
+    if walls == 'faces':
+        force.setFaceBoundary(LBMForce.XMin, LBMForce.Velocity)
+        force.setFaceBoundary(LBMForce.XMax, LBMForce.Density)
+        force.setFaceVelocity(LBMForce.XMin, (0.5, 0.1, 0.0))
+        force.setFaceDensity(LBMForce.XMax, 605.0)
+    system.addForce(force)
+    integrator = lbm_b200.VerletIntegrator(0.01)
+    context = lbm_b200.Context(system, integrator, kernel_factory, properties)
+    context.setPositions([(0.1, 0.7, 0.3)])
+    state = force.getFluidState(context)
+    state = state + 1e-3*np.sin(1.3*np.arange(len(state)))
+    force.setFluidState(context, state)
+    return context, force
+
+
+COUPLING_CASES = ([(walls, drag, 'NearestNode') for walls in (False, True, 'faces') for drag in ('Explicit', 'Centered')] +
+                  [(walls, drag, stencil) for walls in (False, True) for drag in ('Explicit', 'Centered')
+                   for stencil in ('Trilinear', 'ThreePoint', 'Keys')])
+
+
+def coupling_case(walls, drag, stencil, kernel_factory=None, properties=None, temperature=0.0):
+    """test_coupling_agrees_with_reference (TestLBMForce.py:573-635): 4 particles of mass 100 on an 8^3 lattice,
+    friction 10/ps, a constant external field and a soft pair force, explicit or centred drag, every stencil,
+    with the wall plane j = 0 or open faces along x."""
+    system = lbm_b200.System()
+    system.setDefaultPeriodicBoxVectors((4, 0, 0), (0, 4, 0), (0, 0, 4))
+    force = LBMForce()
+    force.setGridSize(8, 8, 8)
+    for i in range(4):
+        system.addParticle(100.0)
+        force.addParticle(i)
+    # CustomExternalForce('-3*x+2*y-z'): F = -grad U = (3, -2, 1).
+    system.addForce(lbm_b200.ExternalForce(lambda p: np.tile([3.0, -2.0, 1.0], (len(p), 1))))
+    # CustomNonbondedForce('50*(1-r)^2') with a periodic cutoff 1: dU/dr = -100 (1 - r).
+    system.addForce(lbm_b200.PairForce(lambda r: -100.0*(1.0 - r), 1.0))
+    system.addForce(force)
+    force.setDragScheme(getattr(LBMForce, drag))
+    force.setInterpolationStencil(getattr(LBMForce, stencil))
+    force.setFriction(10.0)
+    force.setTemperature(temperature)
+    force.setFluidMomentumRemovalFrequency(0)
+    if walls == 'faces':
+        force.setFaceBoundary(LBMForce.XMin, LBMForce.Velocity)
+        force.setFaceBoundary(LBMForce.XMax, LBMForce.Density)
+        force.setFaceVelocity(LBMForce.XMin, (0.2, 0.0, 0.0))
+        force.setFaceDensity(LBMForce.XMax, 603.0)
+    elif walls:
+        force.setSolidNodes([i + 64*k for k in range(8) for i in range(8)])
+    integrator = lbm_b200.VerletIntegrator(0.01)
+    context = lbm_b200.Context(system, integrator, kernel_factory, properties)
+    context.setPositions([(1.02, 2.01, 0.98), (0.97, 1.99, 1.03), (3.98, 0.52, 3.96),
+                          (3.55 if walls == 'faces' else 2.3, 0.6, 0.6)])
+    context.setVelocities([(0.5, -0.2, 0.3), (-0.4, 0.1, 0.2), (2.0, -1.5, 1.0), (0.0, -2.0, -0.6)])
+    return context, force
