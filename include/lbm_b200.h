@@ -196,6 +196,15 @@ LbmStatus lbm_get_info(LbmKernel* kernel, long long* num_nodes, int* storage);
 /* The CUDA stream that the handle launches on (cudaStream_t), for callers that order work with it. */
 void* lbm_get_stream(LbmKernel* kernel);
 
+/* Timing of the dense stream-collide kernel with CUDA events recorded on the handle's stream around each of its
+   launches, while enabled (enable = 1 also clears the record).  lbm_dense_kernel_time synchronizes the stream
+   and returns the number of timed launches and their total duration in milliseconds. */
+LbmStatus lbm_profile_dense_kernel(LbmKernel* kernel, int enable);
+LbmStatus lbm_dense_kernel_time(LbmKernel* kernel, long long* launches, double* total_ms);
+
+/* Number of CUDA kernels this handle has launched since it was created. */
+LbmStatus lbm_kernel_launches(LbmKernel* kernel, long long* launches);
+
 #ifdef __cplusplus
 }
 #endif

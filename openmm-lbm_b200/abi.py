@@ -99,6 +99,9 @@ SIGNATURES = {
     'lbm_load_checkpoint': (ctypes.c_int, [_P, _P, ctypes.c_size_t]),
     'lbm_get_info': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]),
     'lbm_get_stream': (_P, [_P]),
+    'lbm_profile_dense_kernel': (ctypes.c_int, [_P, ctypes.c_int]),
+    'lbm_dense_kernel_time': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong), _D]),
+    'lbm_kernel_launches': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong)]),
 }
 
 LIBRARY_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'liblbm_b200.so')

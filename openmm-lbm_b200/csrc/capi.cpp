@@ -192,4 +192,24 @@ void* lbm_get_stream(LbmKernel* kernel) {
     return (void*) kernel->impl->getStream();
 }
 
+LbmStatus lbm_profile_dense_kernel(LbmKernel* kernel, int enable) {
+    CHECK_HANDLE(kernel);
+    return guard([&] { kernel->impl->fluidEngine().profileDense(enable != 0); });
+}
+
+LbmStatus lbm_dense_kernel_time(LbmKernel* kernel, long long* launches, double* total_ms) {
+    CHECK_HANDLE(kernel);
+    if (!launches || !total_ms)
+        return fail(LBM_ERR_INVALID_ARGUMENT, "lbm_dense_kernel_time: null argument");
+    return guard([&] { kernel->impl->fluidEngine().denseTime(launches, total_ms); });
+}
+
+LbmStatus lbm_kernel_launches(LbmKernel* kernel, long long* launches) {
+    CHECK_HANDLE(kernel);
+    if (!launches)
+        return fail(LBM_ERR_INVALID_ARGUMENT, "lbm_kernel_launches: null argument");
+    *launches = kernel->impl->fluidEngine().launches;
+    return LBM_OK;
+}
+
 } // extern "C"

@@ -769,7 +769,8 @@ FluidEngine::FluidEngine(const LbmLatticeParameters& l, int storage, const Geome
         : lattice(l), storageType(storage), elementSize(elementSizeOf(storage)), stream(s), cur(0), gridBlocks(0),
           solidMaskDev(nullptr), reactMaskDev(nullptr), reactionDev(nullptr), partialsDev(nullptr), statsDev(nullptr),
           numWall(0), numBoundary(0), wallDev(nullptr), boundaryDev(nullptr), equilibriumNoise(false),
-          stagingDev(nullptr), extraBlocks(0), faceDev(nullptr) {
+          stagingDev(nullptr), extraBlocks(0), faceDev(nullptr), profiling(false), profileUsed(0) {
+    launches = 0;
     pop[0] = pop[1] = nullptr;
     std::memset(&view, 0, sizeof(view));
     view.nx = l.nx;
@@ -870,6 +871,9 @@ FluidEngine::~FluidEngine() {
     cudaFree(stagingDev);
     cudaFree(faceDev);
     faceDev = nullptr;
+    for (cudaEvent_t e : profileEvents)
+        cudaEventDestroy(e);
+    profileEvents.clear();
     pop[0] = pop[1] = nullptr;
     solidMaskDev = reactMaskDev = nullptr;
     reactionDev = stagingDev = nullptr;
@@ -918,17 +922,32 @@ void FluidEngine::step(long long stepIndex, bool remove, bool react) {
     void* B = pop[1-cur];
     bool fluct = view.mu > 0;
     bool solids = solidMaskDev != nullptr;
+    if (profiling) {
+        if (profileUsed + 2 > profileEvents.size())
+            for (int i = 0; i < 2; i++) {
+                cudaEvent_t e;
+                CUDA_CHECK(cudaEventCreate(&e));
+                profileEvents.push_back(e);
+            }
+        CUDA_CHECK(cudaEventRecord(profileEvents[profileUsed], stream));
+    }
     dispatchStorage(storageType, [&](auto L) {
         decltype(L)::denseAny(solids, react && reactionDev != nullptr, fluct, A, B, view, remove ? 1 : 0, stepIndex,
                               gridBlocks, stream);
     });
     CUDA_CHECK(cudaGetLastError());
+    launches++;
+    if (profiling) {
+        CUDA_CHECK(cudaEventRecord(profileEvents[profileUsed + 1], stream));
+        profileUsed += 2;
+    }
     int count = gridBlocks;
     if (numWall > 0) {
         int grid = std::min(kGridSparse, (numWall + THREADS - 1)/THREADS);
         double* part = partialsDev + NPART*(size_t) count;
         dispatchStorage(storageType, [&](auto L) { decltype(L)::bounceBack(B, wallDev, numWall, view, part, grid, stream); });
         CUDA_CHECK(cudaGetLastError());
+        launches++;
         count += grid;
     }
     if (numBoundary > 0) {
@@ -941,11 +960,31 @@ void FluidEngine::step(long long stepIndex, bool remove, bool react) {
                                   faceDev, grid, stream);
         });
         CUDA_CHECK(cudaGetLastError());
+        launches++;
         count += grid;
     }
     finishKernel<<<1, THREADS, 0, stream>>>(partialsDev, count, view, 0);
     CUDA_CHECK(cudaGetLastError());
+    launches++;
     cur = 1-cur;
+}
+
+void FluidEngine::profileDense(bool enable) {
+    profiling = enable;
+    if (enable)
+        profileUsed = 0;
+}
+
+void FluidEngine::denseTime(long long* launches, double* totalMs) {
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    double total = 0;
+    for (size_t i = 0; i + 1 < profileUsed; i += 2) {
+        float ms = 0;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, profileEvents[i], profileEvents[i+1]));
+        total += ms;
+    }
+    *launches = (long long) (profileUsed/2);
+    *totalMs = total;
 }
 
 void FluidEngine::momentsPass(bool setSums) {
@@ -953,6 +992,7 @@ void FluidEngine::momentsPass(bool setSums) {
     CUDA_CHECK(cudaGetLastError());
     finishKernel<<<1, THREADS, 0, stream>>>(partialsDev, gridBlocks, view, setSums ? 1 : 2);
     CUDA_CHECK(cudaGetLastError());
+    launches += 2;
 }
 
 void FluidEngine::restoreStats(const StepStats& stats) {

@@ -78,6 +78,11 @@ public:
     cudaStream_t getStream() const { return stream; }
     int wordsPerRow() const { return view.wordsPerRow; }
     int numSolid() const { return (int) solidNodes.size(); }
+    // CUDA events around each dense launch (profiling of the step, lbm_profile_dense_kernel).
+    void profileDense(bool enable);
+    void denseTime(long long* launches, double* totalMs);
+    // Kernels launched by the engines of this lattice (fluid and coupling).
+    long long launches;
 private:
     void launchStreamCollide(long long stepIndex, bool remove, bool react);
     void launchFinish(int numBlocks, int numExtra);
@@ -104,6 +109,9 @@ private:
     double* faceDev;           // face velocities/densities and the boundary stress weight
     double faceHost[32];
     StepStats statsHost;
+    bool profiling;
+    std::vector<cudaEvent_t> profileEvents;   // start/stop pairs
+    size_t profileUsed;
 };
 
 } // namespace lbm

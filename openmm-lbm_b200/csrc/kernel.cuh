@@ -32,6 +32,7 @@ public:
     long long numNodes() const { return fluid->numNodes(); }
     int storage() const { return fluid->storage(); }
     cudaStream_t getStream() const { return stream; }
+    FluidEngine& fluidEngine() { return *fluid; }
 private:
     void advanceFluid(const LbmParticleArrays* particles);
     void computeNextStepForces(long long stepCount, const LbmParticleArrays* particles);

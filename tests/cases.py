@@ -90,3 +90,59 @@ def coupling_case(walls, drag, stencil, kernel_factory=None, properties=None, te
                           (3.55 if walls == 'faces' else 2.3, 0.6, 0.6)])
     context.setVelocities([(0.5, -0.2, 0.3), (-0.4, 0.1, 0.2), (2.0, -1.5, 1.0), (0.0, -2.0, -0.6)])
     return context, force
+
+
+# The fluid tests of the reference (tests/TestLBMFluid.h:22-50): lattice spacing (nm), time step (ps), density.
+FLUID_DX, FLUID_DT, FLUID_DENSITY = 0.5, 0.01, 602.2
+
+
+def fluid_system(nx, ny, nz, tau):
+    """createFluidSystem (TestLBMFluid.h:41-52): a fluid of nx*ny*nz nodes with relaxation time tau, no momentum
+    removal, one particle that is not coupled.  Returns (system, force)."""
+    system = lbm_b200.System()
+    system.setDefaultPeriodicBoxVectors((nx*FLUID_DX, 0, 0), (0, ny*FLUID_DX, 0), (0, 0, nz*FLUID_DX))
+    system.addParticle(1.0)
+    force = LBMForce()
+    force.setGridSize(nx, ny, nz)
+    force.setFluidDensity(FLUID_DENSITY)
+    force.setKinematicViscosity((tau - 0.5)/3.0*FLUID_DX*FLUID_DX/FLUID_DT)
+    force.setFluidMomentumRemovalFrequency(0)
+    system.addForce(force)
+    return system, force
+
+
+def make_context(system, kernel_factory=None, properties=None):
+    context = lbm_b200.Context(system, lbm_b200.VerletIntegrator(FLUID_DT), kernel_factory, properties)
+    context.setPositions([(0.1, 0.2, 0.3)]*system.getNumParticles())
+    return context
+
+
+W = np.array([1/3] + [1/18]*6 + [1/36]*12)
+C = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1], [1, 1, 0], [-1, -1, 0],
+              [1, -1, 0], [-1, 1, 0], [0, 1, 1], [0, -1, -1], [0, 1, -1], [0, -1, 1], [1, 0, 1], [-1, 0, -1],
+              [-1, 0, 1], [1, 0, -1]], dtype=float)
+
+
+def uniform_state(num_nodes, rho, u):
+    """uniformState (TestLBMFluid.h:58-73): equilibrium deviations at density rho and velocity u."""
+    u = np.asarray(u, dtype=float)
+    cu = C @ u
+    dfeq = W*((rho - 1.0) + rho*(3.0*cu + 4.5*cu*cu - 1.5*u.dot(u)))
+    return np.repeat(dfeq, num_nodes)
+
+
+def total_moments(state):
+    """totalMoments (TestLBMFluid.h:76-91): mass = numNodes + sum(f - w) and momentum, lattice units."""
+    f = state.reshape(19, -1)
+    return f.shape[1] + f.sum(), C.T @ f.sum(axis=1)
+
+
+def wall_plane(nx, ny, nz):
+    """wallPlane (TestLBMFluid.h:450-456): the nodes of the plane j = 0."""
+    return [i + nx*ny*k for k in range(nz) for i in range(nx)]
+
+
+def wall_test_nodes(nx, ny, nz):
+    """wallTestNodes (TestLBMFluid.h:632-641): the plane i = 0 and a 2x2x2 block."""
+    return [i + nx*(j + ny*k) for k in range(nz) for j in range(ny) for i in range(nx)
+            if i == 0 or (2 <= i < 4 and 1 <= j < 3 and 1 <= k < 3)]

@@ -1,0 +1,94 @@
+"""CPU tests of the host logic of the C ABI and of the library itself: the conversion into lattice units and its
+checks (the reference's LBMForceImpl::computeLatticeParameters, openmmapi/src/LBMForceImpl.cpp:44-214), and the
+exports of liblbm_b200.so against include/lbm_b200.h."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import lbm_b200
+from lbm_b200 import LBMForce
+from lbm_b200.abi import SIGNATURES, load_library
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    text = open(os.path.join(ROOT, 'include', 'lbm_b200.h')).read()
+    return sorted(set(re.findall(r'^\w[\w\s\*]*?\b(lbm_\w+)\s*\(', text, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = load_library()
+    names = declared_functions()
+    assert len(names) >= 18
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in SIGNATURES, name
+
+
+def lattice_of(force, box=(3.0, 3.0, 3.0), dt=0.01, masses=(1.0,)):
+    return force.latticeParameters(np.array(box), dt, np.array(masses))
+
+
+def test_lattice_units():
+    force = LBMForce()
+    force.setGridSize(6, 6, 6)
+    force.setKinematicViscosity(0.3/3*0.25/0.01)
+    force.setBodyAcceleration((0.5, -0.2, 0.1))
+    force.setInitialFluidVelocity((0.5, 0.2, -0.3))
+    force.setFaceDensity(LBMForce.XMin, 0.0)
+    lattice = lattice_of(force)
+    assert lattice.dx == 0.5 and lattice.dt == 0.01
+    assert abs(lattice.tau - 0.8) < 1e-14 and abs(lattice.omega - 1/0.8) < 1e-14
+    assert abs(lattice.body_acceleration[0] - 0.5*0.01**2/0.5) < 1e-18
+    assert abs(lattice.initial_velocity[2] + 0.3*0.01/0.5) < 1e-18
+    assert abs(lattice.kT - 0.0083144626181532*300) < 1e-9
+    assert lattice.fluid_kT == 0.0 and lattice.face_density[0] == 1.0
+    assert lattice.momentum_removal_frequency == 1 and lattice.mach_check_frequency == 100
+
+
+@pytest.mark.parametrize('setup,message', [
+    (lambda f: f.setGridSize(0, 4, 4), 'grid size'),
+    (lambda f: f.setKinematicViscosity(-1), 'viscosity'),
+    (lambda f: f.setFriction(-1), 'friction'),
+    (lambda f: f.setFaceBoundary(LBMForce.XMin, LBMForce.Velocity), 'both periodic or both open'),
+    (lambda f: (f.setFaceBoundary(LBMForce.XMin, LBMForce.Velocity),
+                f.setFaceBoundary(LBMForce.XMax, LBMForce.Velocity)), 'momentum cannot be removed'),
+    (lambda f: (f.setFluidFluctuations(True), f.setFaceBoundary(LBMForce.ZMin, LBMForce.Density),
+                f.setFaceBoundary(LBMForce.ZMax, LBMForce.Density), f.setFluidMomentumRemovalFrequency(0)),
+     'Density faces cannot be used with fluid fluctuations'),
+    (lambda f: f.setSolidNodes([1, 1]), 'more than once'),
+    (lambda f: f.setSolidNodes([64]), 'out of range'),
+    (lambda f: f.setSolidNodes(list(range(64))), 'all lattice nodes are solid'),
+    (lambda f: f.setMachNumberLimit(0), 'Mach number limit'),
+    (lambda f: f.addParticle(5), 'out of range'),
+])
+def test_lattice_checks(setup, message):
+    force = LBMForce()
+    force.setGridSize(4, 4, 4)
+    setup(force)
+    with pytest.raises(lbm_b200.LbmError) as error:
+        lattice_of(force, box=(2.0, 2.0, 2.0))
+    assert message in str(error.value)
+    assert error.value.status == 1
+
+
+def test_cells_must_be_cubic():
+    force = LBMForce()
+    force.setGridSize(4, 4, 4)
+    with pytest.raises(lbm_b200.LbmError, match='cubic'):
+        lattice_of(force, box=(2.0, 2.0, 2.5))
+
+
+def test_kernel_calls_fail_cleanly_without_a_device():
+    """Without a CUDA device the product path reports LBM_ERR_CUDA: there is no CPU fallback."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip('a device is present')
+    force = LBMForce()
+    force.setGridSize(4, 4, 4)
+    with pytest.raises(lbm_b200.LbmError) as error:
+        lbm_b200.B200Kernel(lattice_of(force, box=(2.0, 2.0, 2.0)), [], [])
+    assert error.value.status == 5
