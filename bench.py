@@ -48,7 +48,7 @@ def lattice_parameters(lbm, n, tau, kT, seed):
     force.setGridSize(n, n, n)
     force.setFluidDensity(1.0)
     force.setKinematicViscosity((tau - 0.5)/3.0)
-    force.setFluidFluctuations(True)
+    force.setFluidFluctuations(kT > 0)
     force.setTemperature(kT/BOLTZ)
     force.setRandomNumberSeed(seed)
     return force.latticeParameters(np.array([n, n, n], dtype=float), 1.0, np.array([1.0]))
@@ -98,11 +98,21 @@ def stop_clock_sampler(proc, path, device):
     return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': smax, 'reasons': sorted(reasons), 'samples': len(sm)}
 
 
+def workload(args):
+    w = dict(WORKLOAD)
+    if args.size != w['n'] or args.no_fluctuations:
+        w['n'] = args.size
+        w['kT'] = 0.0 if args.no_fluctuations else w['kT']
+        w['name'] = '%d^3 periodic D3Q19 fluid, tau 0.6%s (lattice units)' % (
+            args.size, '' if args.no_fluctuations else ', kT 1e-4, fluctuating')
+    return w
+
+
 def run_b200(args, rank, world, device):
     import torch
     lbm = load_package()
     torch.cuda.set_device(device)
-    w = WORKLOAD
+    w = workload(args)
     lattice = lattice_parameters(lbm, w['n'], w['tau'], w['kT'], w['seed'] + rank)
     kernel = lbm.B200Kernel(lattice, [], [], args.precision, device=device)
     lib = kernel.lib
@@ -264,6 +274,8 @@ def main():
     parser.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     parser.add_argument('--precision', default='single', choices=list(STORAGE_BYTES))
     parser.add_argument('--no-cpu-baseline', action='store_true')
+    parser.add_argument('--size', type=int, default=WORKLOAD['n'], help='lattice edge (profiling of smaller cases)')
+    parser.add_argument('--no-fluctuations', action='store_true', help='plain fluid (profiling of the kernel variant)')
     args = parser.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get('WORLD_SIZE', '1'))

@@ -104,7 +104,9 @@ SIGNATURES = {
     'lbm_kernel_launches': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong)]),
 }
 
-LIBRARY_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'liblbm_b200.so')
+# LBM_B200_LIBRARY selects another build of the library (for example one compiled with other kernel options).
+LIBRARY_PATH = os.environ.get('LBM_B200_LIBRARY',
+                              os.path.join(os.path.dirname(os.path.abspath(__file__)), 'liblbm_b200.so'))
 _library = None
 
 

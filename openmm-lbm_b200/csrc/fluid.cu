@@ -154,6 +154,25 @@ __device__ __forceinline__ void fluctuationParts(const R a[15], R& even, R& odd)
     odd = wOf<R>(q)*o;
 }
 
+// Even and odd parts of the ghost-mode part (k = 10..18) of xi_q; the stress modes are merged into the
+// non-equilibrium tensor of the dense kernel.
+template <typename R, int q>
+__device__ __forceinline__ void ghostParts(const R a[15], R& even, R& odd) {
+    R e = 0, o = 0;
+    staticFor<9>([&](auto kc) {
+        constexpr int k = decltype(kc)::value + 10;
+        constexpr double m = modeValue(k, q);
+        if (m != 0.0) {
+            if (k <= 15)
+                o += R(m)*a[k-4];
+            else
+                e += R(m)*a[k-4];
+        }
+    });
+    even = wOf<R>(q)*e;
+    odd = wOf<R>(q)*o;
+}
+
 // Runtime-q fluctuation (slow paths): xi_q = w_q sum_k e_k(c_q) a_k.
 template <typename R>
 __device__ R fluctuationAt(int q, const R a[15]) {
@@ -181,8 +200,16 @@ __device__ __forceinline__ R weightOf(int q) {
 // The dense step.
 // ---------------------------------------------------------------------------------------------------
 
+// Resident blocks of 256 threads per SM that the register allocation of the dense kernel must allow: 4 for float
+// arithmetic (64 registers, 32 warps per SM to hide the latency of the 19 loads) and 2 for double.
+#ifdef LBM_DENSE_MIN_BLOCKS
+template <typename R> constexpr int denseMinBlocks() { return LBM_DENSE_MIN_BLOCKS; }
+#else
+template <typename R> constexpr int denseMinBlocks() { return sizeof(R) == 4 ? 4 : 2; }
+#endif
+
 template <typename T, typename R, bool SOLID, bool REACT, bool FLUCT>
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(THREADS, denseMinBlocks<R>())
 streamCollideKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int remove, long long step) {
     const int lane = threadIdx.x%32, warp = threadIdx.x/32;
     const long long N = v.n;
@@ -247,21 +274,29 @@ streamCollideKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int
         }
         R ux = (jx + R(0.5)*Fx)*inv, uy = (jy + R(0.5)*Fy)*inv, uz = (jz + R(0.5)*Fz)*inv;
         R uu = ux*ux + uy*uy + uz*uz, uf = ux*Fx + uy*Fy + uz*Fz;
-        R trace = (m.pxx + m.pyy + m.pzz)*R(1.0/3.0);
+        // The regularized non-equilibrium part (1 - omega) 4.5 w_q H2(c_q):Pi_neq and the random stress modes
+        // w_q sum_{k=4..9} e_k(c_q) a_k are both quadratic forms in c_q: they are merged into one tensor Q, so that
+        // each direction evaluates w_q (c Q c - tr Q/3) once.  The ghost modes (k = 10..18) are added per direction.
+        const R s45 = om1*R(4.5), s9 = om1*R(9);
+        R qxx = s45*m.pxx, qyy = s45*m.pyy, qzz = s45*m.pzz;
+        R qxy = s9*m.pxy, qxz = s9*m.pxz, qyz = s9*m.pyz;
         R a[15];
         if (FLUCT) {
             R r[15];
             philoxNormals<R, 15>(v.seed, PurposeFluid, node, step, r);
             R ghost = sqrt(muR*rho);
             modeAmplitudes<R>(r, sqrt(muR*rho*stressFactor), ghost, a);
+            qxx += a[0]; qyy += a[1]; qzz += a[2];
+            qxy += a[3]; qxz += a[4]; qyz += a[5];
         }
+        R qtr = (qxx + qyy + qzz)*R(1.0/3.0);
         R outMass = 0, outX = 0, outY = 0, outZ = 0;
         // q = 0
         {
-            R value = R(1.0/3.0)*(m.dr - R(1.5)*rho*uu) - om1*R(4.5/3.0)*trace - R(0.5/3.0)*R(3)*uf;
+            R value = R(1.0/3.0)*(m.dr - R(1.5)*rho*uu - qtr) - R(0.5/3.0)*R(3)*uf;
             if (FLUCT) {
                 R e, o;
-                fluctuationParts<R, 0>(a, e, o);
+                ghostParts<R, 0>(a, e, o);
                 value += e;
             }
             R stored = Storage<T>::template store<0>(B + node, value);
@@ -274,14 +309,13 @@ streamCollideKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int
             constexpr R w = wOf<R>(q);
             R cu = R(cx)*ux + R(cy)*uy + R(cz)*uz;
             R cf = R(cx)*Fx + R(cy)*Fy + R(cz)*Fz;
-            R h2pi = R(cx*cx)*m.pxx + R(cy*cy)*m.pyy + R(cz*cz)*m.pzz - trace
-                   + R(2)*(R(cx*cy)*m.pxy + R(cx*cz)*m.pxz + R(cy*cz)*m.pyz);
-            R even = w*(m.dr + rho*(R(4.5)*cu*cu - R(1.5)*uu)) + om1*(R(4.5)*w)*h2pi
-                   + R(0.5)*w*(R(9)*cu*cf - R(3)*uf);
+            R cqc = R(cx*cx)*qxx + R(cy*cy)*qyy + R(cz*cz)*qzz - qtr
+                  + R(cx*cy)*qxy + R(cx*cz)*qxz + R(cy*cz)*qyz;
+            R even = w*(m.dr + rho*(R(4.5)*cu*cu - R(1.5)*uu) + cqc + R(0.5)*(R(9)*cu*cf - R(3)*uf));
             R odd = R(3)*w*(rho*cu + R(0.5)*cf);
             if (FLUCT) {
                 R e, o;
-                fluctuationParts<R, q>(a, e, o);
+                ghostParts<R, q>(a, e, o);
                 even += e;
                 odd += o;
             }
@@ -691,29 +725,52 @@ template <typename T>
 struct Launcher {
     typedef typename ComputeOf<T>::type R;
 
+    // The persistent grid of a kernel variant: one wave of resident blocks (blocks per SM of this variant times
+    // the SMs), so that every block processes the same number of tiles in one wave.
     template <bool S, bool RE, bool FL>
-    static void dense(const void* A, void* B, const FluidView& v, int remove, long long step, int grid, cudaStream_t s) {
+    static int residentGrid(const FluidView& v) {
+        static int blocks = 0;
+        if (blocks == 0) {
+            int perSM = 0, device = 0, sms = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, streamCollideKernel<T, R, S, RE, FL>, THREADS, 0);
+            cudaGetDevice(&device);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+            blocks = std::max(1, perSM)*std::max(1, sms);
+        }
+        return (int) std::max(1LL, std::min((long long) blocks, v.numTiles));
+    }
+    template <bool S, bool RE, bool FL>
+    static int dense(const void* A, void* B, const FluidView& v, int remove, long long step, int maxGrid, cudaStream_t s) {
+        int grid = std::min(maxGrid, residentGrid<S, RE, FL>(v));
         streamCollideKernel<T, R, S, RE, FL><<<grid, THREADS, 0, s>>>((const T*) A, (T*) B, v, remove, step);
+        return grid;
     }
     template <bool S, bool RE>
-    static void denseF(bool fl, const void* A, void* B, const FluidView& v, int remove, long long step, int grid, cudaStream_t s) {
-        if (fl) dense<S, RE, true>(A, B, v, remove, step, grid, s);
-        else dense<S, RE, false>(A, B, v, remove, step, grid, s);
+    static int denseF(bool fl, const void* A, void* B, const FluidView& v, int remove, long long step, int grid, cudaStream_t s) {
+        return fl ? dense<S, RE, true>(A, B, v, remove, step, grid, s) : dense<S, RE, false>(A, B, v, remove, step, grid, s);
     }
     template <bool S>
-    static void denseR(bool re, bool fl, const void* A, void* B, const FluidView& v, int remove, long long step, int grid, cudaStream_t s) {
-        if (re) denseF<S, true>(fl, A, B, v, remove, step, grid, s);
-        else denseF<S, false>(fl, A, B, v, remove, step, grid, s);
+    static int denseR(bool re, bool fl, const void* A, void* B, const FluidView& v, int remove, long long step, int grid, cudaStream_t s) {
+        return re ? denseF<S, true>(fl, A, B, v, remove, step, grid, s) : denseF<S, false>(fl, A, B, v, remove, step, grid, s);
     }
-    static void denseAny(bool so, bool re, bool fl, const void* A, void* B, const FluidView& v, int remove, long long step,
-                         int grid, cudaStream_t s) {
-        if (so) denseR<true>(re, fl, A, B, v, remove, step, grid, s);
-        else denseR<false>(re, fl, A, B, v, remove, step, grid, s);
+    // Launch the dense step; returns the grid it used (one partial record per block).
+    static int denseAny(bool so, bool re, bool fl, const void* A, void* B, const FluidView& v, int remove, long long step,
+                        int grid, cudaStream_t s) {
+        return so ? denseR<true>(re, fl, A, B, v, remove, step, grid, s) : denseR<false>(re, fl, A, B, v, remove, step, grid, s);
     }
     static int occupancy() {
-        int blocks = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, streamCollideKernel<T, R, false, false, false>, THREADS, 0);
-        return std::max(blocks, 1);
+        // The largest grid any variant uses (the partial sums are sized for it).
+        int best = 1;
+        auto probe = [&](auto kernel) {
+            int blocks = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, THREADS, 0);
+            best = std::max(best, blocks);
+        };
+        probe(streamCollideKernel<T, R, false, false, false>);
+        probe(streamCollideKernel<T, R, false, false, true>);
+        probe(streamCollideKernel<T, R, true, true, true>);
+        probe(streamCollideKernel<T, R, true, false, false>);
+        return best;
     }
     static void bounceBack(void* B, const int* wall, int numWall, const FluidView& v, double* partials, int grid, cudaStream_t s) {
         bounceBackKernel<T, R><<<grid, THREADS, 0, s>>>((T*) B, wall, numWall, v, partials);
@@ -931,9 +988,10 @@ void FluidEngine::step(long long stepIndex, bool remove, bool react) {
             }
         CUDA_CHECK(cudaEventRecord(profileEvents[profileUsed], stream));
     }
+    int denseGrid = gridBlocks;
     dispatchStorage(storageType, [&](auto L) {
-        decltype(L)::denseAny(solids, react && reactionDev != nullptr, fluct, A, B, view, remove ? 1 : 0, stepIndex,
-                              gridBlocks, stream);
+        denseGrid = decltype(L)::denseAny(solids, react && reactionDev != nullptr, fluct, A, B, view, remove ? 1 : 0,
+                                          stepIndex, gridBlocks, stream);
     });
     CUDA_CHECK(cudaGetLastError());
     launches++;
@@ -941,7 +999,7 @@ void FluidEngine::step(long long stepIndex, bool remove, bool react) {
         CUDA_CHECK(cudaEventRecord(profileEvents[profileUsed + 1], stream));
         profileUsed += 2;
     }
-    int count = gridBlocks;
+    int count = denseGrid;
     if (numWall > 0) {
         int grid = std::min(kGridSparse, (numWall + THREADS - 1)/THREADS);
         double* part = partialsDev + NPART*(size_t) count;

@@ -80,7 +80,7 @@ template <> __device__ __forceinline__ void storeq<__nv_bfloat16, float>(__nv_bf
 // with the published multipliers 0xD2511F53, 0xCD9E8D57 and Weyl increments 0x9E3779B9, 0xBB67AE85.
 // The normal number m of (purpose, index, step) comes from the counter (index, step low, step high,
 // purpose*256 + m/4) and the key (seed, 0x4C424D32): lanes (0,1) and (2,3) of the output are Box-Muller
-// pairs, u = (x + 1/2) 2^-32, r = sqrt(-2 ln u_a), normals r cos(2 pi u_b) and r sin(2 pi u_b).
+// pairs, u = (x + 1/2) 2^-32, r = sqrt(-2 ln u_a), normals r cos(2 pi (u_b - 1/2)) and r sin(2 pi (u_b - 1/2)).
 // ------------------------------------------------------------------------------------------------------
 
 enum { PurposeFluid = 0, PurposeBoundary = 1, PurposeParticle = 2 };
@@ -103,15 +103,27 @@ __device__ __forceinline__ uint4 philoxBlock(uint32_t seed, int purpose, long lo
     return philox4x32_10(c, seed, 0x4C424D32u);
 }
 
-// Four normals from one Philox block, in the compute precision R.
+// Four normals from one Philox block, in the compute precision R.  Angles are taken in (-pi, pi):
+// normals r cos(2 pi (u_b - 1/2)) and r sin(2 pi (u_b - 1/2)).
 __device__ __forceinline__ void boxMuller(uint4 x, float out[4]) {
     const float scale = 2.3283064365386963e-10f;        // 2^-32
-    float ua = fmaf((float) x.x, scale, 0.5f*scale), ub = fmaf((float) x.y, scale, 0.5f*scale);
-    float uc = fmaf((float) x.z, scale, 0.5f*scale), ud = fmaf((float) x.w, scale, 0.5f*scale);
+    const float below1 = 0.99999994f;                   // 1 - 2^-24: keeps log(u) < 0 after rounding to float
+    float ua = fminf(fmaf((float) x.x, scale, 0.5f*scale), below1), ub = fmaf((float) x.y, scale, 0.5f*scale);
+    float uc = fminf(fmaf((float) x.z, scale, 0.5f*scale), below1), ud = fmaf((float) x.w, scale, 0.5f*scale);
+#ifdef LBM_ACCURATE_FLOAT_NORMALS
     float r0 = sqrtf(-2.0f*logf(ua)), r1 = sqrtf(-2.0f*logf(uc));
     float s0, c0, s1, c1;
-    sincospif(2.0f*ub, &s0, &c0);
-    sincospif(2.0f*ud, &s1, &c1);
+    sincospif(2.0f*ub - 1.0f, &s0, &c0);
+    sincospif(2.0f*ud - 1.0f, &s1, &c1);
+#else
+    // Hardware approximations (MUFU): -2 ln u = -2 ln2 log2(u), and sin/cos of an angle in (-pi, pi), where their
+    // absolute error is about 2^-21.
+    float r0 = sqrtf(fmaxf(-1.3862943611198906f*__log2f(ua), 0.0f));
+    float r1 = sqrtf(fmaxf(-1.3862943611198906f*__log2f(uc), 0.0f));
+    float s0, c0, s1, c1;
+    __sincosf(6.283185307179586f*(ub - 0.5f), &s0, &c0);
+    __sincosf(6.283185307179586f*(ud - 0.5f), &s1, &c1);
+#endif
     out[0] = r0*c0; out[1] = r0*s0; out[2] = r1*c1; out[3] = r1*s1;
 }
 __device__ __forceinline__ void boxMuller(uint4 x, double out[4]) {
@@ -120,8 +132,8 @@ __device__ __forceinline__ void boxMuller(uint4 x, double out[4]) {
     double uc = ((double) x.z + 0.5)*scale, ud = ((double) x.w + 0.5)*scale;
     double r0 = sqrt(-2.0*log(ua)), r1 = sqrt(-2.0*log(uc));
     double s0, c0, s1, c1;
-    sincospi(2.0*ub, &s0, &c0);
-    sincospi(2.0*ud, &s1, &c1);
+    sincospi(2.0*ub - 1.0, &s0, &c0);
+    sincospi(2.0*ud - 1.0, &s1, &c1);
     out[0] = r0*c0; out[1] = r0*s0; out[2] = r1*c1; out[3] = r1*s1;
 }
 

@@ -140,7 +140,7 @@ void oracle_philox4x32_10(const uint32_t counter[4], const uint32_t key[2], uint
 
 /* The counter of normal number m of (purpose, index, step): counter = (index, step low, step high,
    purpose*256 + m/4), key = (seed, 0x4C424D32).  Lanes (0,1) and (2,3) of the output are Box-Muller
-   pairs: u = (x + 1/2) 2^-32, r = sqrt(-2 ln u_a), normals r cos(2 pi u_b) and r sin(2 pi u_b). */
+   pairs: u = (x + 1/2) 2^-32, r = sqrt(-2 ln u_a), normals r cos(2 pi (u_b - 1/2)) and r sin(2 pi (u_b - 1/2)). */
 double oracle_philox_normal(uint32_t seed, int purpose, long long index, long long step, int m) {
     uint32_t counter[4] = {(uint32_t) index, (uint32_t) step, (uint32_t) ((unsigned long long) step >> 32),
                            (uint32_t) (purpose*256 + m/4)};
@@ -152,7 +152,7 @@ double oracle_philox_normal(uint32_t seed, int purpose, long long index, long lo
     double ua = ((double) a + 0.5)*(1.0/4294967296.0);
     double ub = ((double) b + 0.5)*(1.0/4294967296.0);
     double r = sqrt(-2.0*log(ua));
-    double angle = 6.283185307179586476925287*ub;
+    double angle = 6.283185307179586476925287*(ub - 0.5);
     return (lane%2 == 0 ? r*cos(angle) : r*sin(angle));
 }
 
