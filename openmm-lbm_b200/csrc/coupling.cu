@@ -1,19 +1,1099 @@
-// Particle coupling (placeholder until the coupling kernels are in place).
+// Particle coupling kernels of the B200 LBM force kernel (sm_100a).
+//
+// The coupling of the reference (platforms/reference/src/ReferenceLBMKernels.cpp:503-1018), on the device:
+//   stencilKernel        one thread per (particle, stencil slot): the node and weight of the slot
+//                        (LBMStencils::axisWeights, LBMStencils.h:73-95) and the moments of the node pulled from the
+//                        populations (density, momentum after the momentum removal; a solid node has rho = 0)
+//   explicitKernel       explicit drag F = -gamma m (v - u) + sqrt(2 gamma m kT) xi with u interpolated over the
+//                        stencil (:503-553, :643-697), and the reaction -w F on the stencil nodes
+//   sortByNode           stable LSD radix sort of the particles by nearest node (8-bit digits)
+//   centeredNearestKernel the closed form of the centred drag per node (:555-641), particles of a node summed in
+//                        particle order
+//   centeredStencilKernel the centred drag with a stencil: Jacobi-preconditioned conjugate gradients for
+//                        (1 + a) F_k + a m_k sum_l K_kl F_l = b_k (:726-901), the whole solve in one cooperative launch
+//                        with a bounded grid barrier, no host round trip per iteration
+//   reflectKernel        reversal of the particles that move into a wall (:315-338, wallNormal :1020-1050)
+// Reactions are added with atomics into the fluid's node reaction buffer, and their nodes flagged in its bitmask, so
+// the dense kernel reads the reaction only where there is one.
 #include "coupling.cuh"
+#include "lbm_device.cuh"
+#include <cooperative_groups.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
 
 namespace lbm {
 
-CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, const Geometry&, int n, const double*,
-                               cudaStream_t s) : lattice(l), fluid(f), stream(s), np(n) {
-    throw Error(LBM_ERR_NOT_SUPPORTED, "coupled particles are not supported yet");
+#define CUDA_CHECK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) \
+    throw Error(LBM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); } while (0)
+
+namespace {
+
+const int kThreads = 256;
+
+struct CouplingView {
+    int np, width, slots, stencil;
+    int nx, ny, nz;
+    int open[3];
+    long long n;
+    int wordsPerRow;
+    double dx, velocityScale, forceScale;
+    double gamma, kT, h, a;
+    double g[3];
+    uint32_t seed;
+    int randomForce;
+    const uint32_t* solidMask;
+    const double* mass;          // m/m_c per particle
+};
+
+__device__ __forceinline__ bool isSolid(const uint32_t* mask, int wordsPerRow, int nx, long long node) {
+    if (mask == nullptr)
+        return false;
+    long long row = node/nx;
+    int x = (int) (node - row*nx);
+    return (__ldg(&mask[row*wordsPerRow + x/32]) >> (x%32)) & 1u;
 }
-CouplingEngine::~CouplingEngine() {}
-void CouplingEngine::setParameters(const LbmLatticeParameters& l) { lattice = l; }
-void CouplingEngine::load(const LbmParticleArrays*, bool) {}
-void CouplingEngine::reflect(const LbmParticleArrays*, double w[3]) { w[0] = w[1] = w[2] = 0; }
-void CouplingEngine::couple(long long, bool, bool) {}
-void CouplingEngine::addForces(const LbmParticleArrays*) {}
-void CouplingEngine::clearReaction() {}
-void CouplingEngine::reactionWallMomentum(double out[3]) { out[0] = out[1] = out[2] = 0; }
+
+// Lattice coordinate of a position along an axis, wrapped into [0, n) (ReferenceLBMKernels.cpp:978-979).
+__device__ __forceinline__ double latticeCoordinate(double x, double dx, int n) {
+    double s = x/dx;
+    s -= floor(s/n)*n;
+    return s;
+}
+
+// LBMStencils::kernel (LBMStencils.h:42-62).
+__device__ double stencilKernel1(int stencil, double r) {
+    double s = fabs(r);
+    switch (stencil) {
+    case LBM_STENCIL_TRILINEAR:
+        return (s < 1.0 ? 1.0-s : 0.0);
+    case LBM_STENCIL_THREEPOINT:
+        if (s <= 0.5)
+            return (1.0 + sqrt(1.0-3.0*s*s))/3.0;
+        if (s < 1.5)
+            return (5.0 - 3.0*s - sqrt(fmax(0.0, 1.0-3.0*(1.0-s)*(1.0-s))))/6.0;
+        return 0.0;
+    case LBM_STENCIL_KEYS:
+        if (s <= 1.0)
+            return 1.0 - 2.5*s*s + 1.5*s*s*s;
+        if (s < 2.0)
+            return 2.0 - 4.0*s + 2.5*s*s - 0.5*s*s*s;
+        return 0.0;
+    default:
+        return (r >= -0.5 && r < 0.5 ? 1.0 : 0.0);
+    }
+}
+
+// LBMStencils::axisWeights (LBMStencils.h:73-95): the nodes of the stencil along one axis and their weights,
+// clamped at open faces, with repeated nodes merged into their first slot.
+__device__ void axisWeights(int stencil, int width, double s, int n, bool open, int* index, double* weight) {
+    int first;
+    if (stencil == LBM_STENCIL_THREEPOINT)
+        first = (int) floor(s + 0.5) - 1;
+    else if (stencil == LBM_STENCIL_KEYS)
+        first = (int) floor(s) - 1;
+    else if (stencil == LBM_STENCIL_TRILINEAR)
+        first = (int) floor(s);
+    else
+        first = (int) floor(s + 0.5);
+    for (int i = 0; i < width; i++) {
+        weight[i] = stencilKernel1(stencil, s - (first + i));
+        int idx = first + i;
+        index[i] = open ? min(max(idx, 0), n - 1) : ((idx%n) + n)%n;
+    }
+    for (int i = 1; i < width; i++)
+        for (int j = 0; j < i; j++)
+            if (index[j] == index[i]) {
+                weight[j] += weight[i];
+                weight[i] = 0.0;
+                break;
+            }
+}
+
+// Density deviation and momentum of the post-stream populations of a node (pulled from the input array).
+template <typename T>
+__device__ void pullMoments(const T* A, const FluidView& f, long long node, double& dr, double& jx, double& jy, double& jz) {
+    int x = (int) (node%f.nx);
+    long long r = node/f.nx;
+    int y = (int) (r%f.ny), z = (int) (r/f.ny);
+    dr = jx = jy = jz = 0;
+    for (int q = 0; q < 19; q++) {
+        int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+        int sx = x - cx, sy = y - cy, sz = z - cz;
+        sx = sx < 0 ? sx + f.nx : (sx >= f.nx ? sx - f.nx : sx);
+        sy = sy < 0 ? sy + f.ny : (sy >= f.ny ? sy - f.ny : sy);
+        sz = sz < 0 ? sz + f.nz : (sz >= f.nz ? sz - f.nz : sz);
+        long long src = sx + (long long) f.nx*(sy + (long long) f.ny*sz);
+        typedef typename std::conditional<std::is_same<T, double>::value, double, float>::type R;
+        double v = (double) loadq<T, R>(A + (long long) q*f.n + src, q);
+        dr += v;
+        jx += cx*v;
+        jy += cy*v;
+        jz += cz*v;
+    }
+}
+
+// One thread per (particle, slot): node, weight and the node's velocity and density.  centred: the velocity is
+// u~ = (j + h rho g)/rho (ReferenceLBMKernels.cpp:622, 773), explicit: u = j/rho (:539, :672).
+template <typename T>
+__global__ void stencilKernel(const T* __restrict__ A, FluidView f, CouplingView c, const double* __restrict__ pos,
+                              int remove, int centred, int* slotNode, double* slotWeight, double4* slotU) {
+    long long total = (long long) c.np*c.slots;
+    for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x) {
+        int i = (int) (t/c.slots), s = (int) (t%c.slots);
+        int size[3] = {c.nx, c.ny, c.nz};
+        int idx[3];
+        double w = 1.0;
+        if (c.stencil == LBM_STENCIL_NEAREST) {
+            // nearestNode (ReferenceLBMKernels.cpp:973-983): periodic wrap on every axis.
+            for (int a = 0; a < 3; a++) {
+                double sc = latticeCoordinate(pos[3*i+a], c.dx, size[a]);
+                idx[a] = ((int) floor(sc + 0.5))%size[a];
+            }
+        }
+        else {
+            int sub[3] = {s%c.width, (s/c.width)%c.width, s/(c.width*c.width)};
+            for (int a = 0; a < 3; a++) {
+                int index[4];
+                double weight[4];
+                axisWeights(c.stencil, c.width, latticeCoordinate(pos[3*i+a], c.dx, size[a]), size[a], c.open[a] != 0,
+                            index, weight);
+                idx[a] = index[sub[a]];
+                w *= weight[sub[a]];
+            }
+        }
+        long long node = idx[0] + (long long) c.nx*(idx[1] + (long long) c.ny*idx[2]);
+        slotNode[t] = (int) node;
+        slotWeight[t] = w;
+        double4 u = make_double4(0, 0, 0, 0);
+        if (w != 0.0 && !isSolid(c.solidMask, c.wordsPerRow, c.nx, node)) {
+            double dr, jx, jy, jz;
+            pullMoments<T>(A, f, node, dr, jx, jy, jz);
+            double rho = 1.0 + dr;
+            if (remove) {
+                jx -= rho*f.stats->ucm[0];
+                jy -= rho*f.stats->ucm[1];
+                jz -= rho*f.stats->ucm[2];
+            }
+            if (centred) {
+                jx += c.h*rho*c.g[0];
+                jy += c.h*rho*c.g[1];
+                jz += c.h*rho*c.g[2];
+            }
+            u = make_double4(jx*(1.0/rho), jy*(1.0/rho), jz*(1.0/rho), rho);
+        }
+        slotU[t] = u;
+    }
+}
+
+// Reaction -w F on a node: added into the fluid's reaction buffer, the node flagged, and for a solid node counted
+// as momentum given to the wall (applyReaction, ReferenceLBMKernels.cpp:959-971).
+template <typename R>
+__device__ void addReaction(const FluidView& f, const CouplingView& c, R* reaction, uint32_t* mask, double* wall,
+                            long long node, double fx, double fy, double fz) {
+    if (isSolid(c.solidMask, c.wordsPerRow, c.nx, node)) {
+        atomicAdd(&wall[0], fx);
+        atomicAdd(&wall[1], fy);
+        atomicAdd(&wall[2], fz);
+        return;
+    }
+    R* r = reaction + 4*node;
+    atomicAdd(&r[0], (R) fx);
+    atomicAdd(&r[1], (R) fy);
+    atomicAdd(&r[2], (R) fz);
+    long long row = node/f.nx;
+    int x = (int) (node - row*f.nx);
+    uint32_t bit = 1u << (x%32);
+    uint32_t* word = &mask[row*f.wordsPerRow + x/32];
+    if (!(*((volatile uint32_t*) word) & bit))
+        atomicOr(word, bit);
+}
+
+// Three normals of particle i for step `step` (Philox, purpose 2), in double.
+__device__ void particleNoise(uint32_t seed, int i, long long step, double xi[3]) {
+    double v[4];
+    boxMuller(philoxBlock(seed, PurposeParticle, i, step, 0), v);
+    xi[0] = v[0]; xi[1] = v[1]; xi[2] = v[2];
+}
+
+// Explicit drag, nearest node or stencil (ReferenceLBMKernels.cpp:503-553, 643-697).
+template <typename R>
+__global__ void explicitKernel(FluidView f, CouplingView c, const double* __restrict__ vel, const int* __restrict__ slotNode,
+                               const double* __restrict__ slotWeight, const double4* __restrict__ slotU, long long step,
+                               int isStep, double* fout, R* reaction, uint32_t* mask, double* wall) {
+    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x) {
+        double u[3] = {0, 0, 0};
+        for (int s = 0; s < c.slots; s++) {
+            long long t = (long long) i*c.slots + s;
+            double4 su = slotU[t];
+            if (su.w > 0) {
+                double w = slotWeight[t];
+                u[0] += su.x*w;
+                u[1] += su.y*w;
+                u[2] += su.z*w;
+            }
+        }
+        double m = c.mass[i];
+        double xi[3];
+        if (c.randomForce)
+            particleNoise(c.seed, i, step, xi);
+        double F[3];
+        for (int a = 0; a < 3; a++) {
+            double v = vel[3*i+a]*(1.0/c.velocityScale);
+            F[a] = (v - u[a])*(-c.gamma*m);
+            if (c.randomForce)
+                F[a] += xi[a]*sqrt(2.0*c.gamma*m*c.kT);
+            fout[3*i+a] = F[a]*c.forceScale;
+        }
+        if (isStep)
+            for (int s = 0; s < c.slots; s++) {
+                long long t = (long long) i*c.slots + s;
+                double w = slotWeight[t];
+                if (w != 0.0)
+                    addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*F[0], -w*F[1], -w*F[2]);
+            }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------
+// Stable LSD radix sort of 32-bit keys with 32-bit values, 8 bits per pass.
+// ------------------------------------------------------------------------------------------------------
+
+const int kSortItems = 1024;     // items per block (one per thread)
+
+__global__ void __launch_bounds__(kSortItems) radixHistogram(const unsigned* keys, int n, int shift, unsigned* hist, int numBlocks) {
+    __shared__ unsigned counts[256];
+    for (int b = threadIdx.x; b < 256; b += blockDim.x)
+        counts[b] = 0;
+    __syncthreads();
+    int i = blockIdx.x*kSortItems + threadIdx.x;
+    if (i < n)
+        atomicAdd(&counts[(keys[i] >> shift) & 255u], 1u);
+    __syncthreads();
+    for (int b = threadIdx.x; b < 256; b += blockDim.x)
+        hist[b*numBlocks + blockIdx.x] = counts[b];
+}
+
+// Exclusive scan of hist (256 x numBlocks, digit-major) in one block.
+__global__ void __launch_bounds__(1024) radixScan(unsigned* hist, int count) {
+    __shared__ unsigned partial[1024];
+    int per = (count + blockDim.x - 1)/blockDim.x;
+    int begin = threadIdx.x*per, end = min(count, begin + per);
+    unsigned sum = 0;
+    for (int i = begin; i < end; i++)
+        sum += hist[i];
+    partial[threadIdx.x] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned run = 0;
+        for (int t = 0; t < (int) blockDim.x; t++) {
+            unsigned v = partial[t];
+            partial[t] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    unsigned run = partial[threadIdx.x];
+    for (int i = begin; i < end; i++) {
+        unsigned v = hist[i];
+        hist[i] = run;
+        run += v;
+    }
+}
+
+__global__ void __launch_bounds__(kSortItems) radixScatter(const unsigned* keys, const int* values, int n, int shift,
+                                                           const unsigned* hist, int numBlocks, unsigned* keysOut, int* valuesOut) {
+    __shared__ unsigned warpCount[256][kSortItems/32];
+    int lane = threadIdx.x%32, warp = threadIdx.x/32;
+    for (int k = threadIdx.x; k < 256*(kSortItems/32); k += blockDim.x)
+        warpCount[k/(kSortItems/32)][k%(kSortItems/32)] = 0;
+    __syncthreads();
+    int i = blockIdx.x*kSortItems + threadIdx.x;
+    bool valid = i < n;
+    unsigned key = valid ? keys[i] : 0u;
+    unsigned digit = valid ? ((key >> shift) & 255u) : 256u;
+    unsigned peers = __match_any_sync(0xffffffffu, digit);
+    int rank = __popc(peers & ((1u << lane) - 1u));
+    if (valid && rank == 0)
+        warpCount[digit][warp] = __popc(peers);
+    __syncthreads();
+    // Exclusive prefix over the warps of each digit (warps are in item order, so the sort is stable).
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) {
+        unsigned run = 0;
+        for (int w = 0; w < kSortItems/32; w++) {
+            unsigned v = warpCount[d][w];
+            warpCount[d][w] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    if (valid) {
+        unsigned dest = hist[digit*numBlocks + blockIdx.x] + warpCount[digit][warp] + rank;
+        keysOut[dest] = key;
+        valuesOut[dest] = values[i];
+    }
+}
+
+// Keys: nearest node of each particle (ReferenceLBMKernels.cpp:596, the key node*N + k sorted).
+__global__ void nodeKeysKernel(const int* slotNode, int np, unsigned* keys, int* values) {
+    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < np; i += gridDim.x*blockDim.x) {
+        keys[i] = (unsigned) slotNode[i];
+        values[i] = i;
+    }
+}
+
+// Centred drag at the nearest node (ReferenceLBMKernels.cpp:555-641): one thread per run of particles with the same
+// node in the sorted order; sums in particle order.
+template <typename R>
+__global__ void centeredNearestKernel(FluidView f, CouplingView c, const unsigned* keys, const int* order,
+                                      const double* __restrict__ vel, const double* __restrict__ fin,
+                                      const double4* __restrict__ slotU, long long step, int isStep, double* fout,
+                                      R* reaction, uint32_t* mask, double* wall) {
+    for (int k = blockIdx.x*blockDim.x + threadIdx.x; k < c.np; k += gridDim.x*blockDim.x) {
+        if (k > 0 && keys[k-1] == keys[k])
+            continue;
+        int end = k;
+        while (end < c.np && keys[end] == keys[k])
+            end++;
+        long long node = keys[k];
+        double mass = 0, pm[3] = {0, 0, 0}, rs[3] = {0, 0, 0};
+        for (int e = k; e < end; e++) {
+            int i = order[e];
+            double m = c.mass[i];
+            double xi[3] = {0, 0, 0};
+            if (c.randomForce)
+                particleNoise(c.seed, i, step, xi);
+            mass += m;
+            for (int a = 0; a < 3; a++) {
+                double known = vel[3*i+a]*(1.0/c.velocityScale) + fin[3*i+a]*(c.h/(m*c.forceScale));
+                pm[a] += known*m;
+                rs[a] += c.randomForce ? xi[a]*sqrt(2.0*c.gamma*m*c.kT) : 0.0;
+            }
+        }
+        double4 su = slotU[order[k]];
+        double u[3] = {0, 0, 0}, sum[3];
+        if (su.w > 0) {
+            double rho = su.w, kn[3] = {su.x, su.y, su.z};
+            for (int a = 0; a < 3; a++)
+                sum[a] = ((pm[a] - kn[a]*mass)*(-c.gamma) + rs[a])*(1.0/(1.0 + c.a + c.a*mass/rho));
+            for (int a = 0; a < 3; a++)
+                u[a] = kn[a] - sum[a]*(c.h/rho);
+        }
+        else
+            for (int a = 0; a < 3; a++)
+                sum[a] = ((pm[a] - u[a]*mass)*(-c.gamma) + rs[a])*(1.0/(1.0 + c.a));
+        for (int e = k; e < end; e++) {
+            int i = order[e];
+            double m = c.mass[i];
+            double xi[3] = {0, 0, 0};
+            if (c.randomForce)
+                particleNoise(c.seed, i, step, xi);
+            for (int a = 0; a < 3; a++) {
+                double known = vel[3*i+a]*(1.0/c.velocityScale) + fin[3*i+a]*(c.h/(m*c.forceScale));
+                double random = c.randomForce ? xi[a]*sqrt(2.0*c.gamma*m*c.kT) : 0.0;
+                fout[3*i+a] = ((known - u[a])*(-c.gamma*m) + random)*(1.0/(1.0 + c.a))*c.forceScale;
+            }
+        }
+        if (isStep)
+            addReaction<R>(f, c, reaction, mask, wall, node, -sum[0], -sum[1], -sum[2]);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------
+// Centred drag with a stencil: conjugate gradients in one cooperative launch.
+// ------------------------------------------------------------------------------------------------------
+
+struct CgBuffers {
+    double* rhs;      // 3 per particle
+    double* diag;     // 1 per particle
+    double* F;        // solution
+    double* r;
+    double* z;
+    double* p;
+    double* Ap;
+    double* partials; // 8 per block
+    unsigned* barrier;// [0] arrival count, [1] generation
+    int* status;      // 0 ok, LBM_ERR_CG_NOT_CONVERGED, LBM_ERR_DEVICE_TIMEOUT
+    int* iterations;
+};
+
+// Grid barrier for a cooperative launch (all blocks resident), with a bounded spin: after about 2^26 polls the
+// waiting block gives up, records a timeout in the status word and returns false; every block then leaves the
+// solve at its next barrier.
+__device__ bool gridBarrier(unsigned* bar, int* status, unsigned& generation) {
+    __syncthreads();
+    bool ok = true;
+    if (threadIdx.x == 0) {
+        unsigned target = generation + 1;
+        __threadfence();
+        unsigned arrived = atomicAdd(&bar[0], 1u);
+        if (arrived == gridDim.x - 1) {
+            bar[0] = 0;
+            __threadfence();
+            atomicExch(&bar[1], target);
+        }
+        else {
+            long long polls = 0;
+            while (atomicAdd(&bar[1], 0u) != target) {
+                if (++polls > (1LL << 26) || atomicAdd(status, 0) == LBM_ERR_DEVICE_TIMEOUT) {
+                    atomicExch(status, LBM_ERR_DEVICE_TIMEOUT);
+                    ok = false;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        generation = target;
+    }
+    __shared__ int okShared;
+    if (threadIdx.x == 0)
+        okShared = ok;
+    __syncthreads();
+    return okShared != 0 && *((volatile int*) status) != LBM_ERR_DEVICE_TIMEOUT;
+}
+
+// Sum of per-block partial records (8 doubles) in block order, by every block (the same result in all blocks).
+__device__ void reducePartials(const double* partials, int count, double out[8]) {
+    __shared__ double total[8];
+    if (threadIdx.x < 8) {
+        double s = 0;
+        for (int b = 0; b < count; b++)
+            s += ((volatile const double*) partials)[8*b + threadIdx.x];
+        total[threadIdx.x] = s;
+    }
+    __syncthreads();
+    for (int k = 0; k < 8; k++)
+        out[k] = total[k];
+    __syncthreads();
+}
+
+__device__ void blockSum8(double v[8], double* out) {
+    __shared__ double red[32][8];
+    int lane = threadIdx.x%32, warp = threadIdx.x/32, warps = blockDim.x/32;
+    for (int k = 0; k < 8; k++)
+        for (int o = 16; o > 0; o >>= 1)
+            v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    if (lane == 0)
+        for (int k = 0; k < 8; k++)
+            red[warp][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        double s = 0;
+        for (int w = 0; w < warps; w++)
+            s += red[w][threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// (A p)_i = p_i (1 + a)/m_i + a sum_s w_s spread(node_s)/rho_s, spread(n) = sum of w p over the slots on n.
+template <typename R>
+__device__ void spreadVector(const CouplingView& c, const int* slotNode, const double* slotWeight, const double* p,
+                             R* spread, int i) {
+    for (int s = 0; s < c.slots; s++) {
+        long long t = (long long) i*c.slots + s;
+        double w = slotWeight[t];
+        if (w == 0.0)
+            continue;
+        R* sp = spread + 4*(long long) slotNode[t];
+        atomicAdd(&sp[0], (R) (w*p[3*i]));
+        atomicAdd(&sp[1], (R) (w*p[3*i+1]));
+        atomicAdd(&sp[2], (R) (w*p[3*i+2]));
+    }
+}
+
+template <typename R>
+__global__ void centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ vel,
+                                      const double* __restrict__ fin, const int* __restrict__ slotNode,
+                                      const double* __restrict__ slotWeight, const double4* __restrict__ slotU,
+                                      long long step, int isStep, double tolerance, int maxIterations, CgBuffers b,
+                                      R* spread, double* fout, R* reaction, uint32_t* mask, double* wall) {
+    const int stride = gridDim.x*blockDim.x;
+    const int first = blockIdx.x*blockDim.x + threadIdx.x;
+    unsigned generation = 0;
+    if (threadIdx.x == 0)
+        generation = *((volatile unsigned*) &b.barrier[1]);
+    const double a = c.a;
+    // Right-hand side and diagonal (ReferenceLBMKernels.cpp:758-782).
+    for (int i = first; i < c.np; i += stride) {
+        double m = c.mass[i];
+        double u[3] = {0, 0, 0}, self = 0;
+        for (int s = 0; s < c.slots; s++) {
+            long long t = (long long) i*c.slots + s;
+            double4 su = slotU[t];
+            if (su.w > 0) {
+                double w = slotWeight[t];
+                u[0] += su.x*w;
+                u[1] += su.y*w;
+                u[2] += su.z*w;
+                self += w*w/su.w;
+            }
+        }
+        double xi[3] = {0, 0, 0};
+        if (c.randomForce)
+            particleNoise(c.seed, i, step, xi);
+        for (int d = 0; d < 3; d++) {
+            double known = vel[3*i+d]*(1.0/c.velocityScale) + fin[3*i+d]*(c.h/(m*c.forceScale));
+            double rhs = (known - u[d])*(-c.gamma*m);
+            if (c.randomForce)
+                rhs += xi[d]*sqrt(2.0*c.gamma*m*c.kT);
+            b.rhs[3*i+d] = rhs*(1.0/m);
+        }
+        b.diag[i] = (1.0 + a)/m + a*self;
+        for (int d = 0; d < 3; d++)
+            b.F[3*i+d] = b.rhs[3*i+d]*(1.0/b.diag[i]);
+        spreadVector<R>(c, slotNode, slotWeight, b.F, spread, i);
+    }
+    auto gather = [&](const double* p, int i, double out[3]) {
+        double sm[3] = {0, 0, 0};
+        for (int s = 0; s < c.slots; s++) {
+            long long t = (long long) i*c.slots + s;
+            double4 su = slotU[t];
+            if (su.w > 0) {
+                double w = slotWeight[t];
+                const R* sp = spread + 4*(long long) slotNode[t];
+                sm[0] += (double) sp[0]*(w/su.w);
+                sm[1] += (double) sp[1]*(w/su.w);
+                sm[2] += (double) sp[2]*(w/su.w);
+            }
+        }
+        for (int d = 0; d < 3; d++)
+            out[d] = p[3*i+d]*((1.0 + a)/c.mass[i]) + sm[d]*a;
+    };
+    auto clearSpread = [&](int i) {
+        for (int s = 0; s < c.slots; s++) {
+            long long t = (long long) i*c.slots + s;
+            R* sp = spread + 4*(long long) slotNode[t];
+            sp[0] = 0; sp[1] = 0; sp[2] = 0;
+        }
+    };
+    if (!gridBarrier(b.barrier, b.status, generation))
+        return;
+    // r = rhs - A F, z = r/diag, p = z; rz and the norm of the right-hand side per component.
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = first; i < c.np; i += stride) {
+        double Ap[3];
+        gather(b.F, i, Ap);
+        for (int d = 0; d < 3; d++) {
+            double r = b.rhs[3*i+d] - Ap[d];
+            double z = r*(1.0/b.diag[i]);
+            b.r[3*i+d] = r;
+            b.z[3*i+d] = z;
+            b.p[3*i+d] = z;
+            acc[d] += r*z;
+            acc[3+d] += b.rhs[3*i+d]*b.rhs[3*i+d];
+        }
+    }
+    __shared__ double blockTotal[8];
+    blockSum8(acc, blockTotal);
+    if (threadIdx.x < 8)
+        b.partials[8*blockIdx.x + threadIdx.x] = blockTotal[threadIdx.x];
+    if (!gridBarrier(b.barrier, b.status, generation))
+        return;
+    double tot[8];
+    reducePartials(b.partials, gridDim.x, tot);
+    double rz[3] = {tot[0], tot[1], tot[2]}, norm[3] = {tot[3], tot[4], tot[5]};
+    // Residual of the start.
+    for (int i = first; i < c.np; i += stride)
+        clearSpread(i);
+    double acc2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = first; i < c.np; i += stride)
+        for (int d = 0; d < 3; d++)
+            acc2[d] += b.r[3*i+d]*b.r[3*i+d];
+    blockSum8(acc2, blockTotal);
+    if (!gridBarrier(b.barrier, b.status, generation))
+        return;
+    if (threadIdx.x < 8)
+        b.partials[8*blockIdx.x + threadIdx.x] = blockTotal[threadIdx.x];
+    if (!gridBarrier(b.barrier, b.status, generation))
+        return;
+    reducePartials(b.partials, gridDim.x, tot);
+    double residual[3] = {tot[0], tot[1], tot[2]};
+    int iteration = 0;
+    bool failed = false;       // the same in every block: every decision comes from the same reduced sums
+    for (;; iteration++) {
+        bool converged = true;
+        for (int d = 0; d < 3; d++)
+            if (residual[d] > tolerance*tolerance*norm[d])
+                converged = false;
+        if (converged)
+            break;
+        if (iteration == maxIterations) {
+            if (first == 0)
+                atomicExch(b.status, LBM_ERR_CG_NOT_CONVERGED);
+            failed = true;
+            break;
+        }
+        // Ap = A p.
+        for (int i = first; i < c.np; i += stride)
+            spreadVector<R>(c, slotNode, slotWeight, b.p, spread, i);
+        if (!gridBarrier(b.barrier, b.status, generation))
+            return;
+        double acc3[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = first; i < c.np; i += stride) {
+            double Ap[3];
+            gather(b.p, i, Ap);
+            for (int d = 0; d < 3; d++) {
+                b.Ap[3*i+d] = Ap[d];
+                acc3[d] += b.p[3*i+d]*Ap[d];
+            }
+        }
+        blockSum8(acc3, blockTotal);
+        if (threadIdx.x < 8)
+            b.partials[8*blockIdx.x + threadIdx.x] = blockTotal[threadIdx.x];
+        if (!gridBarrier(b.barrier, b.status, generation))
+            return;
+        reducePartials(b.partials, gridDim.x, tot);
+        double alpha[3];
+        for (int d = 0; d < 3; d++)
+            alpha[d] = (tot[d] > 0 ? rz[d]/tot[d] : 0.0);
+        double acc4[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = first; i < c.np; i += stride) {
+            clearSpread(i);
+            for (int d = 0; d < 3; d++) {
+                b.F[3*i+d] += alpha[d]*b.p[3*i+d];
+                double r = b.r[3*i+d] - alpha[d]*b.Ap[3*i+d];
+                b.r[3*i+d] = r;
+                double z = r*(1.0/b.diag[i]);
+                b.z[3*i+d] = z;
+                acc4[d] += r*z;
+                acc4[3+d] += r*r;
+            }
+        }
+        blockSum8(acc4, blockTotal);
+        // All blocks have read the partials of pAp above (reducePartials ends with a block barrier, and the
+        // grid barrier below separates the next writes); write the new partials after the barrier.
+        if (!gridBarrier(b.barrier, b.status, generation))
+            return;
+        if (threadIdx.x < 8)
+            b.partials[8*blockIdx.x + threadIdx.x] = blockTotal[threadIdx.x];
+        if (!gridBarrier(b.barrier, b.status, generation))
+            return;
+        reducePartials(b.partials, gridDim.x, tot);
+        double beta[3];
+        for (int d = 0; d < 3; d++) {
+            beta[d] = (rz[d] > 0 ? tot[d]/rz[d] : 0.0);
+            rz[d] = tot[d];
+            residual[d] = tot[3+d];
+        }
+        for (int i = first; i < c.np; i += stride)
+            for (int d = 0; d < 3; d++)
+                b.p[3*i+d] = b.z[3*i+d] + beta[d]*b.p[3*i+d];
+        // The next spread reads only this thread's p; the spread buffer was cleared before the last barrier.
+        if (!gridBarrier(b.barrier, b.status, generation))
+            return;
+    }
+    if (first == 0)
+        *b.iterations = iteration;
+    if (failed)
+        return;
+    // Forces and reactions (ReferenceLBMKernels.cpp:889-900).
+    for (int i = first; i < c.np; i += stride) {
+        for (int d = 0; d < 3; d++)
+            fout[3*i+d] = b.F[3*i+d]*c.forceScale;
+        if (isStep)
+            for (int s = 0; s < c.slots; s++) {
+                long long t = (long long) i*c.slots + s;
+                double w = slotWeight[t];
+                if (w != 0.0)
+                    addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*b.F[3*i], -w*b.F[3*i+1], -w*b.F[3*i+2]);
+            }
+    }
+}
+
+// Clear the reaction of the slots of the last step (and their mask bits).
+template <typename R>
+__global__ void clearReactionKernel(FluidView f, const int* slotNode, long long total, R* reaction, uint32_t* mask) {
+    for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x) {
+        long long node = slotNode[t];
+        R* r = reaction + 4*node;
+        r[0] = 0; r[1] = 0; r[2] = 0;
+        long long row = node/f.nx;
+        int x = (int) (node - row*f.nx);
+        mask[row*f.wordsPerRow + x/32] = 0u;
+    }
+}
+
+// Reflection at the walls (beginStep, ReferenceLBMKernels.cpp:315-338).
+__global__ void reflectKernel(CouplingView c, const double* pos, double* vel, double cellMass, double* wall) {
+    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x) {
+        int size[3] = {c.nx, c.ny, c.nz};
+        int near[3], index[3][2];
+        double weight[3][2];
+        for (int a = 0; a < 3; a++) {
+            double s = latticeCoordinate(pos[3*i+a], c.dx, size[a]);
+            near[a] = ((int) floor(s + 0.5))%size[a];
+            double lower = floor(s);
+            index[a][0] = ((int) lower)%size[a];
+            index[a][1] = (index[a][0] + 1)%size[a];
+            weight[a][1] = s - lower;
+            weight[a][0] = 1.0 - weight[a][1];
+        }
+        long long node = near[0] + (long long) c.nx*(near[1] + (long long) c.ny*near[2]);
+        if (!isSolid(c.solidMask, c.wordsPerRow, c.nx, node))
+            continue;
+        double solid[2][2][2];
+        for (int x = 0; x < 2; x++)
+            for (int y = 0; y < 2; y++)
+                for (int z = 0; z < 2; z++)
+                    solid[x][y][z] = isSolid(c.solidMask, c.wordsPerRow, c.nx,
+                                             index[0][x] + (long long) c.nx*(index[1][y] + (long long) c.ny*index[2][z])) ? 1.0 : 0.0;
+        double n[3] = {0, 0, 0};
+        for (int p = 0; p < 2; p++)
+            for (int q = 0; q < 2; q++) {
+                n[0] += weight[1][p]*weight[2][q]*(solid[1][p][q] - solid[0][p][q]);
+                n[1] += weight[0][p]*weight[2][q]*(solid[p][1][q] - solid[p][0][q]);
+                n[2] += weight[0][p]*weight[1][q]*(solid[p][q][1] - solid[p][q][0]);
+            }
+        double* v = &vel[3*i];
+        if (v[0]*n[0] + v[1]*n[1] + v[2]*n[2] > 0) {
+            for (int a = 0; a < 3; a++) {
+                atomicAdd(&wall[a], v[a]*(2.0*c.mass[i]*cellMass));
+                v[a] = -v[a];
+            }
+        }
+    }
+}
+
+__global__ void addForcesKernel(const double* fout, double* forces, int count) {
+    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < count; i += gridDim.x*blockDim.x)
+        forces[i] += fout[i];
+}
+
+int widthOf(int stencil) {
+    return stencil == LBM_STENCIL_TRILINEAR ? 2 : stencil == LBM_STENCIL_THREEPOINT ? 3 : stencil == LBM_STENCIL_KEYS ? 4 : 1;
+}
+
+} // namespace
+
+// ------------------------------------------------------------------------------------------------------
+// Host side.
+// ------------------------------------------------------------------------------------------------------
+
+struct CouplingEngine::Device {
+    int* slotNode = nullptr;
+    double* slotWeight = nullptr;
+    double4* slotU = nullptr;
+    unsigned* keys[2] = {nullptr, nullptr};
+    int* values[2] = {nullptr, nullptr};
+    unsigned* hist = nullptr;
+    CgBuffers cg;
+    void* spread = nullptr;
+    double* reflectWall = nullptr;
+    int cgGrid = 0;
+    size_t histCount = 0;
+};
+
+CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, const Geometry& g, int n,
+                               const double* masses, cudaStream_t s)
+        : lattice(l), fluid(f), stream(s), np(n), storageType(f.storage()), posDev(nullptr), velDev(nullptr),
+          forceInDev(nullptr), forceOutDev(nullptr), massDev(nullptr), wallDev(nullptr), statusDev(nullptr),
+          pinned(nullptr), dev(new Device()) {
+    (void) g;
+    stencilSlots = widthOf(l.interpolation_stencil);
+    stencilSlots = stencilSlots*stencilSlots*stencilSlots;
+    try {
+        size_t v3 = sizeof(double)*3*(size_t) np;
+        CUDA_CHECK(cudaMalloc(&posDev, v3));
+        CUDA_CHECK(cudaMalloc(&velDev, v3));
+        CUDA_CHECK(cudaMalloc(&forceInDev, v3));
+        CUDA_CHECK(cudaMalloc(&forceOutDev, v3));
+        CUDA_CHECK(cudaMemsetAsync(forceOutDev, 0, v3, stream));
+        CUDA_CHECK(cudaMemsetAsync(forceInDev, 0, v3, stream));
+        CUDA_CHECK(cudaMalloc(&massDev, sizeof(double)*np));
+        double cellMass = l.density*l.dx*l.dx*l.dx;
+        std::vector<double> m(np);
+        for (int i = 0; i < np; i++)
+            m[i] = masses[i]/cellMass;
+        CUDA_CHECK(cudaMemcpy(massDev, m.data(), sizeof(double)*np, cudaMemcpyHostToDevice));
+        CUDA_CHECK(cudaMalloc(&wallDev, sizeof(double)*8));
+        CUDA_CHECK(cudaMemsetAsync(wallDev, 0, sizeof(double)*8, stream));
+        dev->reflectWall = wallDev + 4;
+        CUDA_CHECK(cudaMalloc(&statusDev, sizeof(int)*4));
+        CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, stream));
+        size_t slots = (size_t) np*stencilSlots;
+        CUDA_CHECK(cudaMalloc(&dev->slotNode, sizeof(int)*slots));
+        CUDA_CHECK(cudaMalloc(&dev->slotWeight, sizeof(double)*slots));
+        CUDA_CHECK(cudaMalloc(&dev->slotU, sizeof(double4)*slots));
+        CUDA_CHECK(cudaMemsetAsync(dev->slotNode, 0, sizeof(int)*slots, stream));
+        CUDA_CHECK(cudaMemsetAsync(dev->slotWeight, 0, sizeof(double)*slots, stream));
+        if (l.drag_scheme == LBM_DRAG_CENTERED && l.interpolation_stencil == LBM_STENCIL_NEAREST) {
+            int blocks = (np + kSortItems - 1)/kSortItems;
+            dev->histCount = (size_t) 256*blocks;
+            CUDA_CHECK(cudaMalloc(&dev->hist, sizeof(unsigned)*dev->histCount));
+            for (int k = 0; k < 2; k++) {
+                CUDA_CHECK(cudaMalloc(&dev->keys[k], sizeof(unsigned)*np));
+                CUDA_CHECK(cudaMalloc(&dev->values[k], sizeof(int)*np));
+            }
+        }
+        if (l.drag_scheme == LBM_DRAG_CENTERED && l.interpolation_stencil != LBM_STENCIL_NEAREST) {
+            CgBuffers& b = dev->cg;
+            CUDA_CHECK(cudaMalloc(&b.rhs, v3));
+            CUDA_CHECK(cudaMalloc(&b.diag, sizeof(double)*np));
+            CUDA_CHECK(cudaMalloc(&b.F, v3));
+            CUDA_CHECK(cudaMalloc(&b.r, v3));
+            CUDA_CHECK(cudaMalloc(&b.z, v3));
+            CUDA_CHECK(cudaMalloc(&b.p, v3));
+            CUDA_CHECK(cudaMalloc(&b.Ap, v3));
+            b.status = statusDev;
+            b.iterations = statusDev + 1;
+            CUDA_CHECK(cudaMalloc(&b.barrier, sizeof(unsigned)*2));
+            CUDA_CHECK(cudaMemsetAsync(b.barrier, 0, sizeof(unsigned)*2, stream));
+            int device = 0, sms = 0, perSM = 0;
+            CUDA_CHECK(cudaGetDevice(&device));
+            CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+            if (storageType == LBM_STORAGE_F64)
+                CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, centeredStencilKernel<double>, kThreads, 0));
+            else
+                CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, centeredStencilKernel<float>, kThreads, 0));
+            int wanted = (np + kThreads - 1)/kThreads;
+            dev->cgGrid = std::max(1, std::min(wanted, std::max(1, perSM)*sms));
+            CUDA_CHECK(cudaMalloc(&b.partials, sizeof(double)*8*(size_t) dev->cgGrid));
+            size_t r = (storageType == LBM_STORAGE_F64 ? 8 : 4);
+            CUDA_CHECK(cudaMalloc(&dev->spread, 4*r*(size_t) f.numNodes()));
+            CUDA_CHECK(cudaMemsetAsync(dev->spread, 0, 4*r*(size_t) f.numNodes(), stream));
+        }
+        CUDA_CHECK(cudaMallocHost(&pinned, v3));
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+    }
+    catch (...) {
+        release();
+        throw;
+    }
+    setParameters(l);
+}
+
+void CouplingEngine::release() {
+    cudaFree(posDev); cudaFree(velDev); cudaFree(forceInDev); cudaFree(forceOutDev); cudaFree(massDev);
+    cudaFree(wallDev); cudaFree(statusDev);
+    posDev = velDev = forceInDev = forceOutDev = massDev = wallDev = nullptr;
+    statusDev = nullptr;
+    if (pinned)
+        cudaFreeHost(pinned);
+    pinned = nullptr;
+    if (dev) {
+        cudaFree(dev->slotNode); cudaFree(dev->slotWeight); cudaFree(dev->slotU);
+        for (int k = 0; k < 2; k++) {
+            cudaFree(dev->keys[k]);
+            cudaFree(dev->values[k]);
+        }
+        cudaFree(dev->hist);
+        CgBuffers& b = dev->cg;
+        cudaFree(b.rhs); cudaFree(b.diag); cudaFree(b.F); cudaFree(b.r); cudaFree(b.z); cudaFree(b.p); cudaFree(b.Ap);
+        cudaFree(b.partials); cudaFree(b.barrier);
+        cudaFree(dev->spread);
+        delete dev;
+        dev = nullptr;
+    }
+}
+
+CouplingEngine::~CouplingEngine() {
+    release();
+}
+
+void CouplingEngine::setParameters(const LbmLatticeParameters& l) {
+    lattice = l;
+}
+
+// The coupling parameters in lattice units (ReferenceLBMKernels.cpp:520-525).
+static CouplingView makeView(const LbmLatticeParameters& l, const FluidView& f, int np, int width, const double* mass) {
+    CouplingView c;
+    std::memset(&c, 0, sizeof(c));
+    c.np = np;
+    c.width = width;
+    c.slots = width*width*width;
+    c.stencil = l.interpolation_stencil;
+    c.nx = l.nx; c.ny = l.ny; c.nz = l.nz;
+    for (int a = 0; a < 3; a++)
+        c.open[a] = l.face_boundary[2*a] != LBM_BOUNDARY_PERIODIC;
+    c.n = f.n;
+    c.wordsPerRow = f.wordsPerRow;
+    double cellMass = l.density*l.dx*l.dx*l.dx;
+    c.dx = l.dx;
+    c.velocityScale = l.dx/l.dt;
+    c.forceScale = cellMass*l.dx/(l.dt*l.dt);
+    c.gamma = l.friction*l.dt;
+    c.kT = l.kT*l.dt*l.dt/(cellMass*l.dx*l.dx);
+    c.h = 0.5;
+    c.a = c.gamma*c.h;
+    for (int a = 0; a < 3; a++)
+        c.g[a] = l.body_acceleration[a];
+    c.seed = (uint32_t) l.random_number_seed;
+    c.randomForce = (c.kT > 0 && c.gamma > 0) ? 1 : 0;
+    c.solidMask = f.solidMask;
+    c.mass = mass;
+    return c;
+}
+
+void CouplingEngine::load(const LbmParticleArrays* p, bool withForces) {
+    size_t v3 = sizeof(double)*3*(size_t) np;
+    if (p->memory == LBM_MEMORY_DEVICE) {
+        CUDA_CHECK(cudaMemcpyAsync(posDev, p->positions, v3, cudaMemcpyDeviceToDevice, stream));
+        CUDA_CHECK(cudaMemcpyAsync(velDev, p->velocities, v3, cudaMemcpyDeviceToDevice, stream));
+        if (withForces)
+            CUDA_CHECK(cudaMemcpyAsync(forceInDev, p->forces, v3, cudaMemcpyDeviceToDevice, stream));
+    }
+    else {
+        CUDA_CHECK(cudaMemcpyAsync(posDev, p->positions, v3, cudaMemcpyHostToDevice, stream));
+        CUDA_CHECK(cudaMemcpyAsync(velDev, p->velocities, v3, cudaMemcpyHostToDevice, stream));
+        if (withForces)
+            CUDA_CHECK(cudaMemcpyAsync(forceInDev, p->forces, v3, cudaMemcpyHostToDevice, stream));
+    }
+}
+
+void CouplingEngine::reflect(const LbmParticleArrays* p, double wallMomentum[3]) {
+    load(p, false);
+    const FluidView& f = fluid.deviceView();
+    CouplingView c = makeView(lattice, f, np, 1, massDev);
+    CUDA_CHECK(cudaMemsetAsync(dev->reflectWall, 0, sizeof(double)*3, stream));
+    double cellMass = lattice.density*lattice.dx*lattice.dx*lattice.dx;
+    reflectKernel<<<std::max(1, std::min(1184, (np + kThreads - 1)/kThreads)), kThreads, 0, stream>>>(c, posDev, velDev, cellMass, dev->reflectWall);
+    CUDA_CHECK(cudaGetLastError());
+    fluid.launches++;
+    size_t v3 = sizeof(double)*3*(size_t) np;
+    if (p->memory == LBM_MEMORY_DEVICE)
+        CUDA_CHECK(cudaMemcpyAsync(p->velocities, velDev, v3, cudaMemcpyDeviceToDevice, stream));
+    else
+        CUDA_CHECK(cudaMemcpyAsync(p->velocities, velDev, v3, cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaMemcpyAsync(wallMomentum, dev->reflectWall, sizeof(double)*3, cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+}
+
+template <typename T>
+static void launchStencil(const void* A, const FluidView& f, const CouplingView& c, const double* pos, int remove, int centred,
+                          int* slotNode, double* slotWeight, double4* slotU, cudaStream_t s) {
+    long long total = (long long) c.np*c.slots;
+    int grid = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
+    stencilKernel<T><<<grid, kThreads, 0, s>>>((const T*) A, f, c, pos, remove, centred, slotNode, slotWeight, slotU);
+}
+
+void CouplingEngine::couple(long long step, bool isStep, bool remove) {
+    const FluidView& f = fluid.deviceView();
+    CouplingView c = makeView(lattice, f, np, widthOf(lattice.interpolation_stencil), massDev);
+    bool centred = lattice.drag_scheme == LBM_DRAG_CENTERED;
+    const void* A = fluid.inputArray();
+    switch (storageType) {
+    case LBM_STORAGE_F64: launchStencil<double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
+    case LBM_STORAGE_F32: launchStencil<float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
+    case LBM_STORAGE_F16: launchStencil<__half>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
+    default: launchStencil<__nv_bfloat16>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
+    }
+    CUDA_CHECK(cudaGetLastError());
+    fluid.launches++;
+    if (isStep)
+        CUDA_CHECK(cudaMemsetAsync(wallDev, 0, sizeof(double)*3, stream));
+    int gridP = std::max(1, std::min(1184, (np + kThreads - 1)/kThreads));
+    bool f64 = storageType == LBM_STORAGE_F64;
+    void* reaction = fluid.reactionBuffer();
+    uint32_t* mask = fluid.reactMask();
+    if (!centred) {
+        if (f64)
+            explicitKernel<double><<<gridP, kThreads, 0, stream>>>(f, c, velDev, dev->slotNode, dev->slotWeight, dev->slotU, step,
+                                                                    isStep, forceOutDev, (double*) reaction, mask, wallDev);
+        else
+            explicitKernel<float><<<gridP, kThreads, 0, stream>>>(f, c, velDev, dev->slotNode, dev->slotWeight, dev->slotU, step,
+                                                                   isStep, forceOutDev, (float*) reaction, mask, wallDev);
+        CUDA_CHECK(cudaGetLastError());
+        fluid.launches++;
+        return;
+    }
+    if (lattice.interpolation_stencil == LBM_STENCIL_NEAREST) {
+        // Sort the particles by node, stably (particle order within a node).
+        nodeKeysKernel<<<gridP, kThreads, 0, stream>>>(dev->slotNode, np, dev->keys[0], dev->values[0]);
+        CUDA_CHECK(cudaGetLastError());
+        fluid.launches++;
+        int blocks = (np + kSortItems - 1)/kSortItems;
+        int bits = 1;
+        while (bits < 32 && (1LL << bits) < f.n)
+            bits++;
+        int cur = 0;
+        for (int shift = 0; shift < bits; shift += 8) {
+            radixHistogram<<<blocks, kSortItems, 0, stream>>>(dev->keys[cur], np, shift, dev->hist, blocks);
+            radixScan<<<1, 1024, 0, stream>>>(dev->hist, 256*blocks);
+            radixScatter<<<blocks, kSortItems, 0, stream>>>(dev->keys[cur], dev->values[cur], np, shift, dev->hist, blocks,
+                                                            dev->keys[1-cur], dev->values[1-cur]);
+            CUDA_CHECK(cudaGetLastError());
+            fluid.launches += 3;
+            cur = 1 - cur;
+        }
+        if (f64)
+            centeredNearestKernel<double><<<gridP, kThreads, 0, stream>>>(f, c, dev->keys[cur], dev->values[cur], velDev, forceInDev,
+                                                                           dev->slotU, step, isStep, forceOutDev, (double*) reaction, mask, wallDev);
+        else
+            centeredNearestKernel<float><<<gridP, kThreads, 0, stream>>>(f, c, dev->keys[cur], dev->values[cur], velDev, forceInDev,
+                                                                          dev->slotU, step, isStep, forceOutDev, (float*) reaction, mask, wallDev);
+        CUDA_CHECK(cudaGetLastError());
+        fluid.launches++;
+        return;
+    }
+    // Centred drag with a stencil: the conjugate gradients on the device (ReferenceLBMKernels.cpp:834-888, tolerance
+    // 1e-13 in double; 1e-5 with single-precision storage, as the reference's GPU platforms in single precision).
+    CgBuffers b = dev->cg;
+    CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*2, stream));
+    double tolerance = f64 ? 1e-13 : 1e-5;
+    int maxIterations = 1000;
+    long long stepArg = step;
+    int isStepArg = isStep ? 1 : 0;
+    void* spread = dev->spread;
+    double* fout = forceOutDev;
+    double* wall = wallDev;
+    double* fin = forceInDev;
+    double* vel = velDev;
+    int* sn = dev->slotNode;
+    double* sw = dev->slotWeight;
+    double4* su = dev->slotU;
+    FluidView fv = f;
+    void* args[] = {&fv, &c, &vel, &fin, &sn, &sw, &su, &stepArg, &isStepArg, &tolerance, &maxIterations, &b, &spread,
+                    &fout, &reaction, &mask, &wall};
+    if (f64)
+        CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredStencilKernel<double>, dev->cgGrid, kThreads, args, 0, stream));
+    else
+        CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredStencilKernel<float>, dev->cgGrid, kThreads, args, 0, stream));
+    fluid.launches++;
+    int status[2] = {0, 0};
+    CUDA_CHECK(cudaMemcpyAsync(status, statusDev, sizeof(int)*2, cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    lastIterations = status[1];
+    if (status[0] == LBM_ERR_CG_NOT_CONVERGED)
+        throw Error(LBM_ERR_CG_NOT_CONVERGED, "LBMForce: the centred drag with the interpolation stencil did not converge "
+                    "in 1000 iterations of the conjugate gradients");
+    if (status[0] == LBM_ERR_DEVICE_TIMEOUT)
+        throw Error(LBM_ERR_DEVICE_TIMEOUT, "LBMForce: a grid barrier of the conjugate gradients timed out");
+}
+
+void CouplingEngine::addForces(const LbmParticleArrays* p) {
+    size_t count = 3*(size_t) np;
+    if (p->memory == LBM_MEMORY_DEVICE) {
+        addForcesKernel<<<std::max(1, std::min(1184, (int) ((count + kThreads - 1)/kThreads))), kThreads, 0, stream>>>(
+            forceOutDev, p->forces, (int) count);
+        CUDA_CHECK(cudaGetLastError());
+        fluid.launches++;
+        return;
+    }
+    CUDA_CHECK(cudaMemcpyAsync(pinned, forceOutDev, sizeof(double)*count, cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    for (size_t i = 0; i < count; i++)
+        p->forces[i] += pinned[i];
+}
+
+void CouplingEngine::clearReaction() {
+    const FluidView& f = fluid.deviceView();
+    long long total = (long long) np*stencilSlots;
+    int grid = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
+    if (storageType == LBM_STORAGE_F64)
+        clearReactionKernel<double><<<grid, kThreads, 0, stream>>>(f, dev->slotNode, total, (double*) fluid.reactionBuffer(), fluid.reactMask());
+    else
+        clearReactionKernel<float><<<grid, kThreads, 0, stream>>>(f, dev->slotNode, total, (float*) fluid.reactionBuffer(), fluid.reactMask());
+    CUDA_CHECK(cudaGetLastError());
+    fluid.launches++;
+}
+
+void CouplingEngine::reactionWallMomentum(double out[3]) {
+    CUDA_CHECK(cudaMemcpyAsync(out, wallDev, sizeof(double)*3, cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+}
 
 } // namespace lbm

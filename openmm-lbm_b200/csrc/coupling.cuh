@@ -28,8 +28,11 @@ public:
     // Momentum given to solid nodes by the reactions of the last coupling step (lattice units), read on demand.
     void reactionWallMomentum(double out[3]);
     int numParticles() const { return np; }
+    // Conjugate-gradient iterations of the last centred stencil solve.
+    int lastIterations = 0;
 private:
-    void stageIn(const LbmParticleArrays* particles, bool withForces);
+    struct Device;
+    void release();
     LbmLatticeParameters lattice;
     FluidEngine& fluid;
     cudaStream_t stream;
@@ -37,13 +40,10 @@ private:
     int storageType;
     // device buffers (double precision for the particles)
     double *posDev, *velDev, *forceInDev, *forceOutDev, *massDev;
-    int* slotNodeDev;          // S per particle
-    double* slotWeightDev;     // S per particle
-    double* scratchDev;        // particle-side vectors of the centred solves
-    void* nodeAccumDev;        // per-node accumulators of the centred drag (spread vectors, sums)
     double* wallDev;           // 3 doubles: momentum of reactions on solid nodes
     int* statusDev;            // device status word of the conjugate gradients
     double* pinned;            // pinned staging for host particle arrays
+    Device* dev;               // slot, sort and solver buffers
     int stencilSlots;
 };
 

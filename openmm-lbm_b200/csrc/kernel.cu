@@ -109,7 +109,15 @@ void B200Kernel::advanceFluid(const LbmParticleArrays* particles) {
     bool react = false;
     if (numParticles > 0) {
         coupling->load(particles, lattice.drag_scheme == LBM_DRAG_CENTERED);
-        coupling->couple(stepIndex, true, remove);
+        try {
+            coupling->couple(stepIndex, true, remove);
+        }
+        catch (const Error&) {
+            // A failed solve may have written part of the reactions: clear them, so that no later step sees them.
+            coupling->clearReaction();
+            cudaStreamSynchronize(stream);
+            throw;
+        }
         react = true;
     }
     fluid->step(stepIndex, remove, react);

@@ -146,3 +146,36 @@ def wall_test_nodes(nx, ny, nz):
     """wallTestNodes (TestLBMFluid.h:632-641): the plane i = 0 and a 2x2x2 block."""
     return [i + nx*(j + ny*k) for k in range(nz) for j in range(ny) for i in range(nx)
             if i == 0 or (2 <= i < 4 and 1 <= j < 3 and 1 <= k < 3)]
+
+
+COUPLING_MASS = 100.0
+
+
+def coupled_system(num_particles, friction, temperature, coupled=None, seed=1):
+    """createCoupledSystem (TestLBMCoupling.h:39-61): particles of mass 100 on an 8^3 fluid (tau = 0.8), no momentum
+    removal, a fixed seed.  Returns (system, force)."""
+    n = 8
+    system = lbm_b200.System()
+    system.setDefaultPeriodicBoxVectors((n*FLUID_DX, 0, 0), (0, n*FLUID_DX, 0), (0, 0, n*FLUID_DX))
+    force = LBMForce()
+    force.setGridSize(n, n, n)
+    force.setFluidDensity(FLUID_DENSITY)
+    force.setKinematicViscosity((0.8 - 0.5)/3.0*FLUID_DX*FLUID_DX/FLUID_DT)
+    force.setFluidMomentumRemovalFrequency(0)
+    force.setFriction(friction)
+    force.setTemperature(temperature)
+    force.setRandomNumberSeed(seed)
+    for _ in range(num_particles):
+        system.addParticle(COUPLING_MASS)
+    for particle in (coupled if coupled is not None else range(num_particles)):
+        force.addParticle(particle)
+    system.addForce(force)
+    return system, force
+
+
+def total_momentum(context, force):
+    """totalMomentum (TestLBMCoupling.h:64-79): particles (half step) plus fluid, Da nm/ps."""
+    p = (context.velocities*np.array(context.system.masses)[:, None]).sum(axis=0)
+    mass, j = total_moments(force.getFluidState(context))
+    cell_mass = force.getFluidDensity()*FLUID_DX**3
+    return p + j*(cell_mass*FLUID_DX/FLUID_DT)

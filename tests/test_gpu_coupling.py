@@ -1,0 +1,109 @@
+"""GPU tests of the particle coupling through the C ABI: parity with the oracle on the reference's coupling cases
+(TestLBMForce.py:573-635: both drags, every stencil, walls and open faces, a soft pair force and a field), pathwise
+agreement with noise (the same Philox numbers), and the reference's known answers (tests/TestLBMCoupling.h)."""
+import numpy as np
+import pytest
+
+from cases import (COUPLING_CASES, COUPLING_MASS, FLUID_DT, coupled_system, coupling_case, make_context,
+                   total_momentum, uniform_state)
+from oracle import OracleKernel
+from lbm_b200 import LBMForce
+
+pytestmark = pytest.mark.gpu
+
+
+def run_case(walls, drag, stencil, factory, props, temperature=0.0, steps=60):
+    context, force = coupling_case(walls, drag, stencil, factory, props, temperature=temperature)
+    if temperature > 0:
+        force.setRandomNumberSeed(77)
+    context.integrator.step(steps)
+    out = (context.positions.copy(), context.velocities.copy(), force.getFluidState(context),
+           force.getWallForce(context))
+    context.close()
+    return out
+
+
+@pytest.mark.parametrize('walls,drag,stencil', COUPLING_CASES)
+def test_coupling_agrees_with_oracle_double(walls, drag, stencil):
+    ref = run_case(walls, drag, stencil, OracleKernel, None)
+    got = run_case(walls, drag, stencil, None, {'Precision': 'double'})
+    for a, b, name in zip(ref, got, ('positions', 'velocities', 'state', 'wall')):
+        # TestLBMForce.py:633-635.
+        assert abs(b - a).max() <= 1e-10*max(1.0, abs(a).max()), name
+
+
+@pytest.mark.parametrize('walls,drag,stencil', [c for c in COUPLING_CASES if c[0] is not 'faces'])
+def test_coupling_agrees_with_oracle_single(walls, drag, stencil):
+    ref = run_case(walls, drag, stencil, OracleKernel, None)
+    got = run_case(walls, drag, stencil, None, {'Precision': 'single'})
+    for a, b, name in zip(ref, got, ('positions', 'velocities', 'state', 'wall')):
+        assert abs(b - a).max() <= 1e-5*max(1.0, abs(a).max()), name
+
+
+@pytest.mark.parametrize('drag,stencil', [('Explicit', 'NearestNode'), ('Centered', 'NearestNode'),
+                                          ('Explicit', 'Keys'), ('Centered', 'ThreePoint')])
+def test_noisy_coupling_follows_oracle_pathwise(drag, stencil):
+    """At 300 K the random forces of the particles come from the same Philox counters on the GPU and in the oracle."""
+    ref = run_case(True, drag, stencil, OracleKernel, None, temperature=300.0, steps=20)
+    got = run_case(True, drag, stencil, None, {'Precision': 'double'}, temperature=300.0, steps=20)
+    for a, b, name in zip(ref, got, ('positions', 'velocities', 'state', 'wall')):
+        assert abs(b - a).max() <= 1e-10*max(1.0, abs(a).max()), name
+
+
+@pytest.mark.parametrize('precision', ['double', 'single'])
+def test_first_step_drag(precision):
+    """testFirstStepDrag (TestLBMCoupling.h:84-103): v1 = v0 (1 - gamma dt); the force between steps is that of the
+    next step."""
+    friction = 5.0
+    system, force = coupled_system(1, friction, 0.0)
+    context = make_context(system, properties={'Precision': precision})
+    context.setPositions([(1.1, 1.3, 1.7)])
+    v0 = np.array([0.3, -0.2, 0.1])
+    context.setVelocities([v0])
+    assert not context.getForces().any()
+    context.integrator.step(1)
+    v1 = context.velocities[0].copy()
+    forces = context.getForces()
+    tol = 1e-14 if precision == 'double' else 2e-6
+    assert abs(v1 - v0*(1.0 - friction*FLUID_DT)).max() <= tol
+    context.integrator.step(1)
+    v2 = context.velocities[0].copy()
+    assert abs((v2 - v1)*(COUPLING_MASS/FLUID_DT) - forces[0]).max() <= (1e-12 if precision == 'double' else 2e-6)*100
+
+
+@pytest.mark.parametrize('drag', ['Explicit', 'Centered'])
+@pytest.mark.parametrize('rho0', [1.0, 1.2])
+def test_momentum_conservation(drag, rho0):
+    """testMomentumConservation (TestLBMCoupling.h:146-172): particles and fluid together conserve momentum with drag
+    and random forces; two particles share a node and one crosses the periodic boundary."""
+    system, force = coupled_system(4, 10.0, 300.0)
+    force.setDragScheme(getattr(LBMForce, drag))
+    context = make_context(system, properties={'Precision': 'double'})
+    positions = [(1.02, 2.01, 0.98), (0.97, 1.99, 1.03), (3.98, 0.02, 3.96), (2.3, 1.1, 0.6)]
+    velocities = np.array([(0.5, -0.2, 0.3), (-0.4, 0.1, 0.2), (2.0, -1.5, 1.0), (0.0, 0.3, -0.6)])
+    context.setPositions(positions)
+    context.setVelocities(velocities)
+    force.setFluidState(context, uniform_state(512, rho0, [0, 0, 0]))
+    scale = (COUPLING_MASS*np.sqrt((velocities**2).sum(axis=1))).sum()
+    p0 = total_momentum(context, force)
+    context.integrator.step(50)
+    p1 = total_momentum(context, force)
+    assert np.sqrt(((p1 - p0)**2).sum())/scale <= 1e-11
+    assert context.positions[2][0] > 4.0
+
+
+@pytest.mark.parametrize('drag', ['Explicit', 'Centered'])
+@pytest.mark.parametrize('stencil', ['NearestNode', 'Trilinear', 'Keys'])
+def test_comoving_particle_feels_no_force(drag, stencil):
+    """testComoving (TestLBMCoupling.h:178-193)."""
+    for u in ([1.0, 0, 0], [0, 1.0, 0], [0, 0, 1.0], [0.6, -0.5, 0.6]):
+        system, force = coupled_system(1, 10.0, 0.0)
+        force.setDragScheme(getattr(LBMForce, drag))
+        force.setInterpolationStencil(getattr(LBMForce, stencil))
+        force.setInitialFluidVelocity(u)
+        context = make_context(system, properties={'Precision': 'double'})
+        context.setPositions([(1.1, 1.3, 1.7)])
+        context.setVelocities([u])
+        context.integrator.step(100)
+        assert abs(context.velocities[0] - np.array(u)).max() <= 1e-13
+        context.close()
