@@ -9,3 +9,4 @@ from .abi import LbmError, LbmLatticeParameters, load_library  # noqa: F401
 from .force import LBMForce  # noqa: F401
 from .harness import Context, ExternalForce, PairForce, System, VerletIntegrator  # noqa: F401
 from .kernel import B200Kernel  # noqa: F401
+from .md import BeadDynamics, random_walk_chains  # noqa: F401

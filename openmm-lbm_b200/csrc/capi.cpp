@@ -38,6 +38,12 @@ LbmStatus guard(F&& f) {
 
 } // namespace
 
+namespace lbm {
+void setLastError(const std::string& message) {
+    lastError = message;
+}
+}
+
 extern "C" {
 
 const char* lbm_last_error(void) {

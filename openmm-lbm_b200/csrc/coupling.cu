@@ -17,6 +17,7 @@
 // the dense kernel reads the reaction only where there is one.
 #include "coupling.cuh"
 #include "lbm_device.cuh"
+#include "radix_sort.cuh"
 #include <cooperative_groups.h>
 #include <algorithm>
 #include <cmath>
@@ -254,85 +255,6 @@ __global__ void explicitKernel(FluidView f, CouplingView c, const double* __rest
                 if (w != 0.0)
                     addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*F[0], -w*F[1], -w*F[2]);
             }
-    }
-}
-
-// ------------------------------------------------------------------------------------------------------
-// Stable LSD radix sort of 32-bit keys with 32-bit values, 8 bits per pass.
-// ------------------------------------------------------------------------------------------------------
-
-const int kSortItems = 1024;     // items per block (one per thread)
-
-__global__ void __launch_bounds__(kSortItems) radixHistogram(const unsigned* keys, int n, int shift, unsigned* hist, int numBlocks) {
-    __shared__ unsigned counts[256];
-    for (int b = threadIdx.x; b < 256; b += blockDim.x)
-        counts[b] = 0;
-    __syncthreads();
-    int i = blockIdx.x*kSortItems + threadIdx.x;
-    if (i < n)
-        atomicAdd(&counts[(keys[i] >> shift) & 255u], 1u);
-    __syncthreads();
-    for (int b = threadIdx.x; b < 256; b += blockDim.x)
-        hist[b*numBlocks + blockIdx.x] = counts[b];
-}
-
-// Exclusive scan of hist (256 x numBlocks, digit-major) in one block.
-__global__ void __launch_bounds__(1024) radixScan(unsigned* hist, int count) {
-    __shared__ unsigned partial[1024];
-    int per = (count + blockDim.x - 1)/blockDim.x;
-    int begin = threadIdx.x*per, end = min(count, begin + per);
-    unsigned sum = 0;
-    for (int i = begin; i < end; i++)
-        sum += hist[i];
-    partial[threadIdx.x] = sum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned run = 0;
-        for (int t = 0; t < (int) blockDim.x; t++) {
-            unsigned v = partial[t];
-            partial[t] = run;
-            run += v;
-        }
-    }
-    __syncthreads();
-    unsigned run = partial[threadIdx.x];
-    for (int i = begin; i < end; i++) {
-        unsigned v = hist[i];
-        hist[i] = run;
-        run += v;
-    }
-}
-
-__global__ void __launch_bounds__(kSortItems) radixScatter(const unsigned* keys, const int* values, int n, int shift,
-                                                           const unsigned* hist, int numBlocks, unsigned* keysOut, int* valuesOut) {
-    __shared__ unsigned warpCount[256][kSortItems/32];
-    int lane = threadIdx.x%32, warp = threadIdx.x/32;
-    for (int k = threadIdx.x; k < 256*(kSortItems/32); k += blockDim.x)
-        warpCount[k/(kSortItems/32)][k%(kSortItems/32)] = 0;
-    __syncthreads();
-    int i = blockIdx.x*kSortItems + threadIdx.x;
-    bool valid = i < n;
-    unsigned key = valid ? keys[i] : 0u;
-    unsigned digit = valid ? ((key >> shift) & 255u) : 256u;
-    unsigned peers = __match_any_sync(0xffffffffu, digit);
-    int rank = __popc(peers & ((1u << lane) - 1u));
-    if (valid && rank == 0)
-        warpCount[digit][warp] = __popc(peers);
-    __syncthreads();
-    // Exclusive prefix over the warps of each digit (warps are in item order, so the sort is stable).
-    for (int d = threadIdx.x; d < 256; d += blockDim.x) {
-        unsigned run = 0;
-        for (int w = 0; w < kSortItems/32; w++) {
-            unsigned v = warpCount[d][w];
-            warpCount[d][w] = run;
-            run += v;
-        }
-    }
-    __syncthreads();
-    if (valid) {
-        unsigned dest = hist[digit*numBlocks + blockIdx.x] + warpCount[digit][warp] + rank;
-        keysOut[dest] = key;
-        valuesOut[dest] = values[i];
     }
 }
 
@@ -1005,20 +927,11 @@ void CouplingEngine::couple(long long step, bool isStep, bool remove) {
         nodeKeysKernel<<<gridP, kThreads, 0, stream>>>(dev->slotNode, np, dev->keys[0], dev->values[0]);
         CUDA_CHECK(cudaGetLastError());
         fluid.launches++;
-        int blocks = (np + kSortItems - 1)/kSortItems;
         int bits = 1;
         while (bits < 32 && (1LL << bits) < f.n)
             bits++;
-        int cur = 0;
-        for (int shift = 0; shift < bits; shift += 8) {
-            radixHistogram<<<blocks, kSortItems, 0, stream>>>(dev->keys[cur], np, shift, dev->hist, blocks);
-            radixScan<<<1, 1024, 0, stream>>>(dev->hist, 256*blocks);
-            radixScatter<<<blocks, kSortItems, 0, stream>>>(dev->keys[cur], dev->values[cur], np, shift, dev->hist, blocks,
-                                                            dev->keys[1-cur], dev->values[1-cur]);
-            CUDA_CHECK(cudaGetLastError());
-            fluid.launches += 3;
-            cur = 1 - cur;
-        }
+        int cur = radixSortByKey(dev->keys, dev->values, dev->hist, np, bits, stream);
+        fluid.launches += 3*((bits + 7)/8);
         if (f64)
             centeredNearestKernel<double><<<gridP, kThreads, 0, stream>>>(f, c, dev->keys[cur], dev->values[cur], velDev, forceInDev,
                                                                            dev->slotU, step, isStep, forceOutDev, (double*) reaction, mask, wallDev);

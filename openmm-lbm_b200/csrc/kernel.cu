@@ -3,6 +3,7 @@
 #include "coupling.cuh"
 #include <cmath>
 #include <cstring>
+#include <random>
 #include <sstream>
 
 namespace lbm {
@@ -52,16 +53,24 @@ B200Kernel::B200Kernel(const LbmLatticeParameters& l, const LbmOptions& options,
         CUDA_CHECK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         ownStream = true;
     }
+    // A seed of 0 asks for a unique one, chosen when the kernel is created (ReferenceLBMKernels.cpp:293-295).  The
+    // random numbers are a function of (seed, step, node or particle), so the seed is the whole generator state.
+    if (lattice.random_number_seed == 0) {
+        std::random_device device;
+        do
+            lattice.random_number_seed = (int) (device() & 0x7fffffffu);
+        while (lattice.random_number_seed == 0);
+    }
     buildGeometry(l, numSolid, solid, geometry);
     for (size_t i = 1; i < geometry.solidNodes.size(); i++)
         if (geometry.solidNodes[i] == geometry.solidNodes[i-1])
             throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: a solid node is listed more than once");
     if ((long long) geometry.solidNodes.size() == n)
         throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: all lattice nodes are solid");
-    fluid.reset(new FluidEngine(l, options.storage, geometry, stream));
+    fluid.reset(new FluidEngine(lattice, options.storage, geometry, stream));
     if (np > 0) {
         fluid->enableReaction();
-        coupling.reset(new CouplingEngine(l, *fluid, geometry, np, masses, stream));
+        coupling.reset(new CouplingEngine(lattice, *fluid, geometry, np, masses, stream));
     }
 }
 
@@ -167,10 +176,14 @@ void B200Kernel::copyParameters(const LbmLatticeParameters& l) {
         throw Error(LBM_ERR_INVALID_ARGUMENT, "updateParametersInContext: the interpolation stencil cannot be changed");
     if (l.fluid_fluctuations != lattice.fluid_fluctuations)
         throw Error(LBM_ERR_INVALID_ARGUMENT, "updateParametersInContext: the fluid fluctuations cannot be switched on or off");
+    // The generator is not reseeded by a parameter update: it keeps the seed of the kernel's creation, as the
+    // reference's kernel keeps its generator state.
+    int seed = lattice.random_number_seed;
     lattice = l;
-    fluid->setParameters(l);
+    lattice.random_number_seed = seed;
+    fluid->setParameters(lattice);
     if (coupling)
-        coupling->setParameters(l);
+        coupling->setParameters(lattice);
 }
 
 void B200Kernel::getFluidFields(double* density, double* velocity) {

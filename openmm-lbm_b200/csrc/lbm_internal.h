@@ -22,6 +22,9 @@ public:
     LbmStatus status;
 };
 
+// The message that lbm_last_error() returns on this thread.
+void setLastError(const std::string& message);
+
 void defaultForceDescription(LbmForceDescription* force);
 void computeLatticeParameters(const LbmForceDescription& force, const double box[3], double stepSize,
                               int numSystemParticles, const double* systemMasses, int numCoupled,

@@ -1420,3 +1420,74 @@ LbmStatus oracle_set_fluid_state(OracleKernel* k, const double* state) {
     k->step_forces_current = 0;
     return LBM_OK;
 }
+
+/* ------------------------------------------------------------------------------------------------ */
+/* Bead forces on the CPU (the stand-in for OpenMM's forces in the benchmark configurations)          */
+/* ------------------------------------------------------------------------------------------------ */
+
+/* Harmonic bonds k/2 (r - r0)^2 and WCA (pair_type 1) or truncated Lennard-Jones (2) pairs within the cutoff, bonded
+   pairs excluded, minimum image; brute force over pairs.  forces is overwritten. */
+void oracle_md_forces(int n, const double* pos, const double box[3], int num_bonds, const int* bonds, double k, double r0,
+                      int pair_type, double sigma, double eps, double cutoff, double* forces) {
+    memset(forces, 0, sizeof(double)*3*(size_t) n);
+    for (int b = 0; b < num_bonds; b++) {
+        int i = bonds[2*b], j = bonds[2*b+1];
+        double d[3];
+        for (int a = 0; a < 3; a++) {
+            d[a] = pos[3*i+a] - pos[3*j+a];
+            d[a] -= box[a]*nearbyint(d[a]/box[a]);
+        }
+        double r = sqrt(d[0]*d[0] + d[1]*d[1] + d[2]*d[2]);
+        if (r == 0.0)
+            continue;
+        double s = -k*(r - r0)/r;
+        for (int a = 0; a < 3; a++) {
+            forces[3*i+a] += s*d[a];
+            forces[3*j+a] -= s*d[a];
+        }
+    }
+    if (pair_type == 0)
+        return;
+    double rc = (pair_type == 1 ? pow(2.0, 1.0/6.0)*sigma : cutoff), rc2 = rc*rc, s2 = sigma*sigma;
+    /* bonded partners for the exclusions */
+    int* count = (int*) calloc(n + 1, sizeof(int));
+    for (int b = 0; b < num_bonds; b++) {
+        count[bonds[2*b]+1]++;
+        count[bonds[2*b+1]+1]++;
+    }
+    for (int i = 0; i < n; i++)
+        count[i+1] += count[i];
+    int* partner = (int*) malloc(sizeof(int)*(2*(size_t) num_bonds + 1));
+    int* fill = (int*) malloc(sizeof(int)*(n + 1));
+    memcpy(fill, count, sizeof(int)*(n + 1));
+    for (int b = 0; b < num_bonds; b++) {
+        partner[fill[bonds[2*b]]++] = bonds[2*b+1];
+        partner[fill[bonds[2*b+1]]++] = bonds[2*b];
+    }
+    for (int i = 0; i < n; i++)
+        for (int j = i+1; j < n; j++) {
+            double d[3];
+            for (int a = 0; a < 3; a++) {
+                d[a] = pos[3*i+a] - pos[3*j+a];
+                d[a] -= box[a]*nearbyint(d[a]/box[a]);
+            }
+            double r2 = d[0]*d[0] + d[1]*d[1] + d[2]*d[2];
+            if (r2 >= rc2 || r2 == 0.0)
+                continue;
+            int excluded = 0;
+            for (int p = count[i]; p < count[i+1]; p++)
+                if (partner[p] == j)
+                    excluded = 1;
+            if (excluded)
+                continue;
+            double q = s2/r2, q6 = q*q*q;
+            double s = 24.0*eps*q6*(2.0*q6 - 1.0)/r2;
+            for (int a = 0; a < 3; a++) {
+                forces[3*i+a] += s*d[a];
+                forces[3*j+a] -= s*d[a];
+            }
+        }
+    free(count);
+    free(partner);
+    free(fill);
+}

@@ -56,6 +56,10 @@ void oracle_fluctuation(const double r[15], double stress_amplitude, double ghos
 int oracle_find_boundaries(const LbmLatticeParameters* lattice, int num_solid, const int* solid,
                            int* nodes, int* unknown, int* solid_bits, int* kind, int* face);
 
+/* Bead forces (bonds, WCA or Lennard-Jones pairs) by brute force, the CPU counterpart of lbm_md_compute_forces. */
+void oracle_md_forces(int n, const double* pos, const double box[3], int num_bonds, const int* bonds, double k, double r0,
+                      int pair_type, double sigma, double eps, double cutoff, double* forces);
+
 #ifdef __cplusplus
 }
 #endif

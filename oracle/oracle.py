@@ -236,6 +236,23 @@ def fluctuation(normals, stress, ghost):
     return xi
 
 
+def md_forces(positions, box, bonds, k, r0, pair, sigma, eps, cutoff):
+    """Bead forces on the CPU (oracle_md_forces): bonds and WCA ('wca') or Lennard-Jones ('lj') pairs."""
+    lib = library('oracle')
+    fn = lib.cdll.oracle_md_forces
+    D = ctypes.POINTER(ctypes.c_double)
+    fn.restype = None
+    fn.argtypes = [ctypes.c_int, D, D, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_double, ctypes.c_double,
+                   ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, D]
+    pos = np.ascontiguousarray(positions, dtype=np.float64)
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    bonds = np.ascontiguousarray(np.asarray(bonds, dtype=np.int32).reshape(-1))
+    forces = np.zeros_like(pos)
+    fn(len(pos), dptr(pos), dptr(box), len(bonds)//2, bonds.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), k, r0,
+       {'none': 0, 'wca': 1, 'lj': 2}[pair], sigma, eps, cutoff, dptr(forces))
+    return forces
+
+
 def find_boundaries(lattice, solid_nodes):
     lib = library('oracle')
     solid = np.ascontiguousarray(solid_nodes, dtype=np.int32)

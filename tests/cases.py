@@ -56,7 +56,7 @@ COUPLING_CASES = ([(walls, drag, 'NearestNode') for walls in (False, True, 'face
                    for stencil in ('Trilinear', 'ThreePoint', 'Keys')])
 
 
-def coupling_case(walls, drag, stencil, kernel_factory=None, properties=None, temperature=0.0):
+def coupling_case(walls, drag, stencil, kernel_factory=None, properties=None, temperature=0.0, seed=0):
     """test_coupling_agrees_with_reference (TestLBMForce.py:573-635): 4 particles of mass 100 on an 8^3 lattice,
     friction 10/ps, a constant external field and a soft pair force, explicit or centred drag, every stencil,
     with the wall plane j = 0 or open faces along x."""
@@ -76,6 +76,7 @@ def coupling_case(walls, drag, stencil, kernel_factory=None, properties=None, te
     force.setInterpolationStencil(getattr(LBMForce, stencil))
     force.setFriction(10.0)
     force.setTemperature(temperature)
+    force.setRandomNumberSeed(seed)
     force.setFluidMomentumRemovalFrequency(0)
     if walls == 'faces':
         force.setFaceBoundary(LBMForce.XMin, LBMForce.Velocity)

@@ -45,3 +45,12 @@ def pytest_collection_modifyitems(config, items):
     for item in items:
         if 'gpu' in item.keywords:
             item.add_marker(skip)
+
+
+@pytest.fixture(autouse=True)
+def _release_kernels():
+    """Destroy the kernels and device objects a test leaves behind while the test session is still running, so that
+    none is finalized during interpreter shutdown."""
+    yield
+    import gc
+    gc.collect()

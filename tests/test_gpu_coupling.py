@@ -13,9 +13,7 @@ pytestmark = pytest.mark.gpu
 
 
 def run_case(walls, drag, stencil, factory, props, temperature=0.0, steps=60):
-    context, force = coupling_case(walls, drag, stencil, factory, props, temperature=temperature)
-    if temperature > 0:
-        force.setRandomNumberSeed(77)
+    context, force = coupling_case(walls, drag, stencil, factory, props, temperature=temperature, seed=77)
     context.integrator.step(steps)
     out = (context.positions.copy(), context.velocities.copy(), force.getFluidState(context),
            force.getWallForce(context))
@@ -32,12 +30,15 @@ def test_coupling_agrees_with_oracle_double(walls, drag, stencil):
         assert abs(b - a).max() <= 1e-10*max(1.0, abs(a).max()), name
 
 
-@pytest.mark.parametrize('walls,drag,stencil', [c for c in COUPLING_CASES if c[0] is not 'faces'])
+@pytest.mark.parametrize('walls,drag,stencil', [c for c in COUPLING_CASES if c[0] != 'faces'])
 def test_coupling_agrees_with_oracle_single(walls, drag, stencil):
     ref = run_case(walls, drag, stencil, OracleKernel, None)
     got = run_case(walls, drag, stencil, None, {'Precision': 'single'})
     for a, b, name in zip(ref, got, ('positions', 'velocities', 'state', 'wall')):
-        assert abs(b - a).max() <= 1e-5*max(1.0, abs(a).max()), name
+        # The wall force is a sum of populations with cancellations: in single precision the reference allows it
+        # 5e-5 (TestLBMFluid.h:530-534, 623-626).
+        tol = 5e-5 if name == 'wall' else 1e-5
+        assert abs(b - a).max() <= tol*max(1.0, abs(a).max()), name
 
 
 @pytest.mark.parametrize('drag,stencil', [('Explicit', 'NearestNode'), ('Centered', 'NearestNode'),
