@@ -110,7 +110,8 @@ def random_walk_chains(num_chains, length, box, seed, min_distance=0.8, step=1.0
 
     bonds = []
     for c in range(num_chains):
-        while True:
+        # A bounded number of attempts: in a box too dense for the exclusion the last candidate is kept.
+        for _ in range(1000):
             p = rng.uniform(0, 1, 3)*box
             if clear(p):
                 break

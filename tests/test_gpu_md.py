@@ -34,10 +34,12 @@ def numpy_forces(pos, box, bonds, k, r0, pair, sigma, eps, cutoff):
     return f
 
 
-@pytest.mark.parametrize('pair,box', [('wca', 6.0), ('wca', 3.0), ('lj', 11.0), ('lj', 4.0)])
-def test_forces_match_numpy(pair, box):
+@pytest.mark.parametrize('pair,box,chains,length', [('wca', 6.0, 4, 25), ('wca', 3.0, 2, 6), ('lj', 11.0, 4, 25),
+                                                    ('lj', 4.0, 2, 10)])
+def test_forces_match_numpy(pair, box, chains, length):
+    """Boxes of 5 and more cells per axis use the cell list, the others the brute-force pass."""
     import torch
-    pos, bonds = lbm_b200.random_walk_chains(4, 25, (box, box, box), seed=3)
+    pos, bonds = lbm_b200.random_walk_chains(chains, length, (box, box, box), seed=3)
     pos = pos + np.random.default_rng(1).normal(scale=0.05, size=pos.shape)
     masses = np.ones(len(pos))
     md = lbm_b200.BeadDynamics(masses, (box, box, box), bonds, 5.0, 1.0, pair, 1.0, 0.7, 2.5)
