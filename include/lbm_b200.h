@@ -205,6 +205,27 @@ LbmStatus lbm_dense_kernel_time(LbmKernel* kernel, long long* launches, double* 
 /* Number of CUDA kernels this handle has launched since it was created. */
 LbmStatus lbm_kernel_launches(LbmKernel* kernel, long long* launches);
 
+/*
+ * Fluid moments of a state that the caller owns, without allocating any memory.  It has no counterpart in the
+ * reference: it is for callers that cannot call cudaMalloc -- a plugin whose host program owns the device memory
+ * through its own allocator (an MD engine's context, a framework's caching allocator that holds the pool), or a
+ * time-critical loop that cannot take the device synchronization cudaMalloc and cudaFree may imply.
+ *
+ * state: device array of 19*num_nodes doubles in the layout of lbm_get_fluid_state ([q*N + node], f_q - w_q);
+ * is_fluid: device array of num_nodes bytes, nonzero for fluid nodes, or NULL when every node is fluid;
+ * moments: device array of 5 doubles that receives the sum of the deviations over the fluid nodes (the fluid's mass
+ * minus the number of fluid nodes), the fluid's momentum (x, y, z) and the Mach number sqrt(3 max |j/rho|^2) that
+ * lbm_get_fluid_mach_number gives.  Launched on `stream` (a cudaStream_t, NULL for the default stream).
+ *
+ * The partial sums live in a fixed device array of the library (128 KB on every GPU that loads it, kept until the
+ * process exits): at most 67,108,864 nodes (2048 chunks of 32,768); larger lattices are rejected with
+ * LBM_ERR_INVALID_ARGUMENT.  The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  All calls share the array: calls that overlap on the
+ * GPU race, and must be ordered (one stream, or events).
+ */
+LbmStatus lbm_fluid_moments_noalloc(const double* state, long long num_nodes, const unsigned char* is_fluid,
+                                    double* moments, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

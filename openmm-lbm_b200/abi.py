@@ -102,6 +102,7 @@ SIGNATURES = {
     'lbm_profile_dense_kernel': (ctypes.c_int, [_P, ctypes.c_int]),
     'lbm_dense_kernel_time': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong), _D]),
     'lbm_kernel_launches': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong)]),
+    'lbm_fluid_moments_noalloc': (ctypes.c_int, [_P, ctypes.c_longlong, _P, _P, _P]),
 }
 
 # LBM_B200_LIBRARY selects another build of the library (for example one compiled with other kernel options).
