@@ -242,6 +242,9 @@ def run_b200(args, w, rank, world, device):
         if md is not None:
             observables['bead_kT'] = md.twice_kinetic(vel, stream_ptr)/(3*np_)
             observables['steps_run'] = s
+            iterations = ctypes.c_int()
+            lib.lbm_solver_iterations(kernel.handle, ctypes.byref(iterations))
+            observables['cg_iterations_last_step'] = iterations.value
     kernel.close()
 
     value = world*nodes*args.steps/(ms*1e-3)/1e6

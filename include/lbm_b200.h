@@ -205,6 +205,9 @@ LbmStatus lbm_dense_kernel_time(LbmKernel* kernel, long long* launches, double* 
 /* Number of CUDA kernels this handle has launched since it was created. */
 LbmStatus lbm_kernel_launches(LbmKernel* kernel, long long* launches);
 
+/* Conjugate-gradient iterations of the last centred stencil drag solve (0 for the other coupling schemes). */
+LbmStatus lbm_solver_iterations(LbmKernel* kernel, int* iterations);
+
 /*
  * Fluid moments of a state that the caller owns, without allocating any memory.  It has no counterpart in the
  * reference: it is for callers that cannot call cudaMalloc -- a plugin whose host program owns the device memory

@@ -102,6 +102,7 @@ SIGNATURES = {
     'lbm_profile_dense_kernel': (ctypes.c_int, [_P, ctypes.c_int]),
     'lbm_dense_kernel_time': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong), _D]),
     'lbm_kernel_launches': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong)]),
+    'lbm_solver_iterations': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     'lbm_fluid_moments_noalloc': (ctypes.c_int, [_P, ctypes.c_longlong, _P, _P, _P]),
 }
 

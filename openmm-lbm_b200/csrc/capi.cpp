@@ -210,6 +210,14 @@ LbmStatus lbm_dense_kernel_time(LbmKernel* kernel, long long* launches, double* 
     return guard([&] { kernel->impl->fluidEngine().denseTime(launches, total_ms); });
 }
 
+LbmStatus lbm_solver_iterations(LbmKernel* kernel, int* iterations) {
+    CHECK_HANDLE(kernel);
+    if (!iterations)
+        return fail(LBM_ERR_INVALID_ARGUMENT, "lbm_solver_iterations: null argument");
+    *iterations = kernel->impl->solverIterations();
+    return LBM_OK;
+}
+
 LbmStatus lbm_kernel_launches(LbmKernel* kernel, long long* launches) {
     CHECK_HANDLE(kernel);
     if (!launches)

@@ -1,28 +1,29 @@
 // Particle coupling kernels of the B200 LBM force kernel (sm_100a).
 //
 // The coupling of the reference (platforms/reference/src/ReferenceLBMKernels.cpp:503-1018), on the device:
-//   stencilKernel        one thread per (particle, stencil slot): the node and weight of the slot
-//                        (LBMStencils::axisWeights, LBMStencils.h:73-95) and the moments of the node pulled from the
-//                        populations (density, momentum after the momentum removal; a solid node has rho = 0)
-//   explicitKernel       explicit drag F = -gamma m (v - u) + sqrt(2 gamma m kT) xi with u interpolated over the
-//                        stencil (:503-553, :643-697), and the reaction -w F on the stencil nodes
-//   sortByNode           stable LSD radix sort of the particles by nearest node (8-bit digits)
-//   centeredNearestKernel the closed form of the centred drag per node (:555-641), particles of a node summed in
-//                        particle order
+//   stencilKernel         one thread per (particle, stencil slot): the node and weight of the slot
+//                         (LBMStencils::axisWeights, LBMStencils.h:73-95) and the moments of the node pulled from the
+//                         populations (density, momentum after the momentum removal; a solid node has rho = 0)
+//   explicitKernel        one warp per particle: explicit drag F = -gamma m (v - u) + sqrt(2 gamma m kT) xi with u
+//                         interpolated over the stencil (:503-553, :643-697), reaction -w F on the stencil nodes
+//   centeredNearestKernel the closed form of the centred drag per node (:555-641), after a stable radix sort of the
+//                         particles by node; the particles of a node summed in particle order
 //   centeredStencilKernel the centred drag with a stencil: Jacobi-preconditioned conjugate gradients for
-//                        (1 + a) F_k + a m_k sum_l K_kl F_l = b_k (:726-901), the whole solve in one cooperative launch
-//                        with a bounded grid barrier, no host round trip per iteration
-//   reflectKernel        reversal of the particles that move into a wall (:315-338, wallNormal :1020-1050)
-// Reactions are added with atomics into the fluid's node reaction buffer, and their nodes flagged in its bitmask, so
-// the dense kernel reads the reaction only where there is one.
+//                         (1 + a) F_k + a m_k sum_l K_kl F_l = b_k (:726-901), the whole solve in one cooperative
+//                         launch, one warp per particle, with a bounded grid barrier and no host round trip
+//   reflectKernel         reversal of the particles that move into a wall (:315-338, wallNormal :1020-1050)
+// Slot data, reactions and the spread vectors are kept in the precision of the fluid's arithmetic (double with FP64
+// storage, float otherwise); particle quantities and all reductions are double.  Reactions are added with (vector)
+// atomics into the fluid's node reaction buffer and their nodes flagged in its bitmask, so the dense kernel reads a
+// reaction only where there is one.
 #include "coupling.cuh"
 #include "lbm_device.cuh"
 #include "radix_sort.cuh"
-#include <cooperative_groups.h>
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace lbm {
@@ -30,10 +31,7 @@ namespace lbm {
 #define CUDA_CHECK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) \
     throw Error(LBM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); } while (0)
 
-namespace {
-
-const int kThreads = 256;
-
+// The coupling parameters in lattice units, by value to the kernels.
 struct CouplingView {
     int np, width, slots, stencil;
     int nx, ny, nz;
@@ -48,6 +46,30 @@ struct CouplingView {
     const uint32_t* solidMask;
     const double* mass;          // m/m_c per particle
 };
+
+namespace {
+
+const int kThreads = 256;
+
+template <typename R> struct Vec4;
+template <> struct Vec4<float> {
+    typedef float4 type;
+    static __device__ __forceinline__ float4 make(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
+};
+template <> struct Vec4<double> {
+    typedef double4 type;
+    static __device__ __forceinline__ double4 make(double a, double b, double c, double d) { return make_double4(a, b, c, d); }
+};
+
+// r[0..2] += (x, y, z): one vector atomic for float (sm_90 and later), three for double.
+__device__ __forceinline__ void atomicAdd3(float* r, double x, double y, double z) {
+    atomicAdd(reinterpret_cast<float4*>(r), make_float4((float) x, (float) y, (float) z, 0.0f));
+}
+__device__ __forceinline__ void atomicAdd3(double* r, double x, double y, double z) {
+    atomicAdd(&r[0], x);
+    atomicAdd(&r[1], y);
+    atomicAdd(&r[2], z);
+}
 
 __device__ __forceinline__ bool isSolid(const uint32_t* mask, int wordsPerRow, int nx, long long node) {
     if (mask == nullptr)
@@ -116,31 +138,32 @@ __device__ void axisWeights(int stencil, int width, double s, int n, bool open, 
 // Density deviation and momentum of the post-stream populations of a node (pulled from the input array).
 template <typename T>
 __device__ void pullMoments(const T* A, const FluidView& f, long long node, double& dr, double& jx, double& jy, double& jz) {
+    typedef typename std::conditional<std::is_same<T, double>::value, double, float>::type R;
     int x = (int) (node%f.nx);
     long long r = node/f.nx;
     int y = (int) (r%f.ny), z = (int) (r/f.ny);
-    dr = jx = jy = jz = 0;
+    int xs[3] = {x == 0 ? f.nx-1 : x-1, x, x == f.nx-1 ? 0 : x+1};
+    int ys[3] = {y == 0 ? f.ny-1 : y-1, y, y == f.ny-1 ? 0 : y+1};
+    int zs[3] = {z == 0 ? f.nz-1 : z-1, z, z == f.nz-1 ? 0 : z+1};
+    R d = 0, a = 0, b = 0, c = 0;
+#pragma unroll
     for (int q = 0; q < 19; q++) {
-        int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
-        int sx = x - cx, sy = y - cy, sz = z - cz;
-        sx = sx < 0 ? sx + f.nx : (sx >= f.nx ? sx - f.nx : sx);
-        sy = sy < 0 ? sy + f.ny : (sy >= f.ny ? sy - f.ny : sy);
-        sz = sz < 0 ? sz + f.nz : (sz >= f.nz ? sz - f.nz : sz);
-        long long src = sx + (long long) f.nx*(sy + (long long) f.ny*sz);
-        typedef typename std::conditional<std::is_same<T, double>::value, double, float>::type R;
-        double v = (double) loadq<T, R>(A + (long long) q*f.n + src, q);
-        dr += v;
-        jx += cx*v;
-        jy += cy*v;
-        jz += cz*v;
+        const int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+        long long src = xs[1-cx] + (long long) f.nx*(ys[1-cy] + (long long) f.ny*zs[1-cz]);
+        R v = loadq<T, R>(A + (long long) q*f.n + src, q);
+        d += v;
+        a += cx*v;
+        b += cy*v;
+        c += cz*v;
     }
+    dr = d; jx = a; jy = b; jz = c;
 }
 
 // One thread per (particle, slot): node, weight and the node's velocity and density.  centred: the velocity is
-// u~ = (j + h rho g)/rho (ReferenceLBMKernels.cpp:622, 773), explicit: u = j/rho (:539, :672).
-template <typename T>
+// u~ = (j + h rho g)/rho (ReferenceLBMKernels.cpp:622, 773); explicit: u = j/rho (:539, :672).
+template <typename T, typename R>
 __global__ void stencilKernel(const T* __restrict__ A, FluidView f, CouplingView c, const double* __restrict__ pos,
-                              int remove, int centred, int* slotNode, double* slotWeight, double4* slotU) {
+                              int remove, int centred, int* slotNode, R* slotWeight, typename Vec4<R>::type* slotU) {
     long long total = (long long) c.np*c.slots;
     for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x) {
         int i = (int) (t/c.slots), s = (int) (t%c.slots);
@@ -167,12 +190,12 @@ __global__ void stencilKernel(const T* __restrict__ A, FluidView f, CouplingView
         }
         long long node = idx[0] + (long long) c.nx*(idx[1] + (long long) c.ny*idx[2]);
         slotNode[t] = (int) node;
-        slotWeight[t] = w;
-        double4 u = make_double4(0, 0, 0, 0);
+        slotWeight[t] = (R) w;
+        double ux = 0, uy = 0, uz = 0, rho = 0;
         if (w != 0.0 && !isSolid(c.solidMask, c.wordsPerRow, c.nx, node)) {
             double dr, jx, jy, jz;
             pullMoments<T>(A, f, node, dr, jx, jy, jz);
-            double rho = 1.0 + dr;
+            rho = 1.0 + dr;
             if (remove) {
                 jx -= rho*f.stats->ucm[0];
                 jy -= rho*f.stats->ucm[1];
@@ -183,14 +206,16 @@ __global__ void stencilKernel(const T* __restrict__ A, FluidView f, CouplingView
                 jy += c.h*rho*c.g[1];
                 jz += c.h*rho*c.g[2];
             }
-            u = make_double4(jx*(1.0/rho), jy*(1.0/rho), jz*(1.0/rho), rho);
+            ux = jx*(1.0/rho);
+            uy = jy*(1.0/rho);
+            uz = jz*(1.0/rho);
         }
-        slotU[t] = u;
+        slotU[t] = Vec4<R>::make((R) ux, (R) uy, (R) uz, (R) rho);
     }
 }
 
-// Reaction -w F on a node: added into the fluid's reaction buffer, the node flagged, and for a solid node counted
-// as momentum given to the wall (applyReaction, ReferenceLBMKernels.cpp:959-971).
+// Reaction (fx, fy, fz) on a node: added into the fluid's reaction buffer and the node flagged, or for a solid node
+// counted as momentum given to the wall (applyReaction, ReferenceLBMKernels.cpp:959-971).
 template <typename R>
 __device__ void addReaction(const FluidView& f, const CouplingView& c, R* reaction, uint32_t* mask, double* wall,
                             long long node, double fx, double fy, double fz) {
@@ -200,10 +225,7 @@ __device__ void addReaction(const FluidView& f, const CouplingView& c, R* reacti
         atomicAdd(&wall[2], fz);
         return;
     }
-    R* r = reaction + 4*node;
-    atomicAdd(&r[0], (R) fx);
-    atomicAdd(&r[1], (R) fy);
-    atomicAdd(&r[2], (R) fz);
+    atomicAdd3(reaction + 4*node, fx, fy, fz);
     long long row = node/f.nx;
     int x = (int) (node - row*f.nx);
     uint32_t bit = 1u << (x%32);
@@ -213,31 +235,43 @@ __device__ void addReaction(const FluidView& f, const CouplingView& c, R* reacti
 }
 
 // Three normals of particle i for step `step` (Philox, purpose 2), in double.
-__device__ void particleNoise(uint32_t seed, int i, long long step, double xi[3]) {
+__device__ __forceinline__ void particleNoise(uint32_t seed, int i, long long step, double xi[3]) {
     double v[4];
     boxMuller(philoxBlock(seed, PurposeParticle, i, step, 0), v);
     xi[0] = v[0]; xi[1] = v[1]; xi[2] = v[2];
 }
 
-// Explicit drag, nearest node or stencil (ReferenceLBMKernels.cpp:503-553, 643-697).
+__device__ __forceinline__ double warpSum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Explicit drag, nearest node or stencil (ReferenceLBMKernels.cpp:503-553, 643-697): one warp per particle, the
+// lanes over the stencil slots.
 template <typename R>
 __global__ void explicitKernel(FluidView f, CouplingView c, const double* __restrict__ vel, const int* __restrict__ slotNode,
-                               const double* __restrict__ slotWeight, const double4* __restrict__ slotU, long long step,
-                               int isStep, double* fout, R* reaction, uint32_t* mask, double* wall) {
-    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x) {
+                               const R* __restrict__ slotWeight, const typename Vec4<R>::type* __restrict__ slotU,
+                               long long step, int isStep, double* fout, R* reaction, uint32_t* mask, double* wall) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x*blockDim.x) >> 5;
+    for (int i = (blockIdx.x*blockDim.x + threadIdx.x) >> 5; i < c.np; i += warps) {
         double u[3] = {0, 0, 0};
-        for (int s = 0; s < c.slots; s++) {
+        for (int s = lane; s < c.slots; s += 32) {
             long long t = (long long) i*c.slots + s;
-            double4 su = slotU[t];
+            typename Vec4<R>::type su = slotU[t];
             if (su.w > 0) {
-                double w = slotWeight[t];
-                u[0] += su.x*w;
-                u[1] += su.y*w;
-                u[2] += su.z*w;
+                double w = (double) slotWeight[t];
+                u[0] += (double) su.x*w;
+                u[1] += (double) su.y*w;
+                u[2] += (double) su.z*w;
             }
         }
+        for (int a = 0; a < 3; a++)
+            u[a] = warpSum(u[a]);
         double m = c.mass[i];
-        double xi[3];
+        double xi[3] = {0, 0, 0};
         if (c.randomForce)
             particleNoise(c.seed, i, step, xi);
         double F[3];
@@ -246,12 +280,14 @@ __global__ void explicitKernel(FluidView f, CouplingView c, const double* __rest
             F[a] = (v - u[a])*(-c.gamma*m);
             if (c.randomForce)
                 F[a] += xi[a]*sqrt(2.0*c.gamma*m*c.kT);
-            fout[3*i+a] = F[a]*c.forceScale;
         }
+        if (lane == 0)
+            for (int a = 0; a < 3; a++)
+                fout[3*i+a] = F[a]*c.forceScale;
         if (isStep)
-            for (int s = 0; s < c.slots; s++) {
+            for (int s = lane; s < c.slots; s += 32) {
                 long long t = (long long) i*c.slots + s;
-                double w = slotWeight[t];
+                double w = (double) slotWeight[t];
                 if (w != 0.0)
                     addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*F[0], -w*F[1], -w*F[2]);
             }
@@ -271,8 +307,8 @@ __global__ void nodeKeysKernel(const int* slotNode, int np, unsigned* keys, int*
 template <typename R>
 __global__ void centeredNearestKernel(FluidView f, CouplingView c, const unsigned* keys, const int* order,
                                       const double* __restrict__ vel, const double* __restrict__ fin,
-                                      const double4* __restrict__ slotU, long long step, int isStep, double* fout,
-                                      R* reaction, uint32_t* mask, double* wall) {
+                                      const typename Vec4<R>::type* __restrict__ slotU, long long step, int isStep,
+                                      double* fout, R* reaction, uint32_t* mask, double* wall) {
     for (int k = blockIdx.x*blockDim.x + threadIdx.x; k < c.np; k += gridDim.x*blockDim.x) {
         if (k > 0 && keys[k-1] == keys[k])
             continue;
@@ -294,10 +330,10 @@ __global__ void centeredNearestKernel(FluidView f, CouplingView c, const unsigne
                 rs[a] += c.randomForce ? xi[a]*sqrt(2.0*c.gamma*m*c.kT) : 0.0;
             }
         }
-        double4 su = slotU[order[k]];
+        typename Vec4<R>::type su = slotU[order[k]];
         double u[3] = {0, 0, 0}, sum[3];
         if (su.w > 0) {
-            double rho = su.w, kn[3] = {su.x, su.y, su.z};
+            double rho = su.w, kn[3] = {(double) su.x, (double) su.y, (double) su.z};
             for (int a = 0; a < 3; a++)
                 sum[a] = ((pm[a] - kn[a]*mass)*(-c.gamma) + rs[a])*(1.0/(1.0 + c.a + c.a*mass/rho));
             for (int a = 0; a < 3; a++)
@@ -327,17 +363,18 @@ __global__ void centeredNearestKernel(FluidView f, CouplingView c, const unsigne
 // Centred drag with a stencil: conjugate gradients in one cooperative launch.
 // ------------------------------------------------------------------------------------------------------
 
+constexpr int kPartial = 12;   // doubles per block record
+
 struct CgBuffers {
-    double* rhs;      // 3 per particle
-    double* diag;     // 1 per particle
-    double* F;        // solution
+    double* rhs;           // 3 per particle (b/m)
+    double* diag;          // 1 per particle
+    double* F;             // solution
     double* r;
-    double* z;
+    double* z;             // holds A p between the product and the update
     double* p;
-    double* Ap;
-    double* partials; // 8 per block
-    unsigned* barrier;// [0] arrival count, [1] generation
-    int* status;      // 0 ok, LBM_ERR_CG_NOT_CONVERGED, LBM_ERR_DEVICE_TIMEOUT
+    double* partials[2];   // kPartial doubles per block, two buffers used alternately
+    unsigned* barrier;     // [0] arrival count, [1] generation
+    int* status;           // 0 ok, LBM_ERR_CG_NOT_CONVERGED, LBM_ERR_DEVICE_TIMEOUT
     int* iterations;
 };
 
@@ -377,165 +414,173 @@ __device__ bool gridBarrier(unsigned* bar, int* status, unsigned& generation) {
     return okShared != 0 && *((volatile int*) status) != LBM_ERR_DEVICE_TIMEOUT;
 }
 
-// Sum of per-block partial records (8 doubles) in block order, by every block (the same result in all blocks).
-__device__ void reducePartials(const double* partials, int count, double out[8]) {
-    __shared__ double total[8];
-    if (threadIdx.x < 8) {
+// Block sum of a record (thread values v) into partials[block]; after a grid barrier (by the caller) every block adds
+// the records of all blocks in block order, so every block gets the same result, bit for bit.
+__device__ void blockSumStore(double v[kPartial], double* partials) {
+    __shared__ double red[kThreads/32][kPartial];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < kPartial; k++)
+        v[k] = warpSum(v[k]);
+    if (lane == 0)
+        for (int k = 0; k < kPartial; k++)
+            red[warp][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < kPartial) {
+        double s = 0;
+        for (int w = 0; w < (int) blockDim.x/32; w++)
+            s += red[w][threadIdx.x];
+        partials[kPartial*blockIdx.x + threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+__device__ void reducePartials(const double* partials, int count, double out[kPartial]) {
+    __shared__ double total[kPartial];
+    if (threadIdx.x < kPartial) {
         double s = 0;
         for (int b = 0; b < count; b++)
-            s += ((volatile const double*) partials)[8*b + threadIdx.x];
+            s += ((volatile const double*) partials)[kPartial*b + threadIdx.x];
         total[threadIdx.x] = s;
     }
     __syncthreads();
-    for (int k = 0; k < 8; k++)
+    for (int k = 0; k < kPartial; k++)
         out[k] = total[k];
     __syncthreads();
 }
 
-__device__ void blockSum8(double v[8], double* out) {
-    __shared__ double red[32][8];
-    int lane = threadIdx.x%32, warp = threadIdx.x/32, warps = blockDim.x/32;
-    for (int k = 0; k < 8; k++)
-        for (int o = 16; o > 0; o >>= 1)
-            v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-    if (lane == 0)
-        for (int k = 0; k < 8; k++)
-            red[warp][k] = v[k];
-    __syncthreads();
-    if (threadIdx.x < 8) {
-        double s = 0;
-        for (int w = 0; w < warps; w++)
-            s += red[w][threadIdx.x];
-        out[threadIdx.x] = s;
-    }
-    __syncthreads();
-}
-
-// (A p)_i = p_i (1 + a)/m_i + a sum_s w_s spread(node_s)/rho_s, spread(n) = sum of w p over the slots on n.
+// The barriers of one iteration: after the spread of A p (products complete), after the partial sums of p.Ap
+// (alpha), and after the partial sums of r.z and r.r (beta, convergence).  The two partial buffers alternate, so a
+// buffer is never written while another block may still read it.
 template <typename R>
-__device__ void spreadVector(const CouplingView& c, const int* slotNode, const double* slotWeight, const double* p,
-                             R* spread, int i) {
-    for (int s = 0; s < c.slots; s++) {
-        long long t = (long long) i*c.slots + s;
-        double w = slotWeight[t];
-        if (w == 0.0)
-            continue;
-        R* sp = spread + 4*(long long) slotNode[t];
-        atomicAdd(&sp[0], (R) (w*p[3*i]));
-        atomicAdd(&sp[1], (R) (w*p[3*i+1]));
-        atomicAdd(&sp[2], (R) (w*p[3*i+2]));
-    }
-}
-
-template <typename R>
-__global__ void centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ vel,
-                                      const double* __restrict__ fin, const int* __restrict__ slotNode,
-                                      const double* __restrict__ slotWeight, const double4* __restrict__ slotU,
-                                      long long step, int isStep, double tolerance, int maxIterations, CgBuffers b,
-                                      R* spread, double* fout, R* reaction, uint32_t* mask, double* wall) {
-    const int stride = gridDim.x*blockDim.x;
-    const int first = blockIdx.x*blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kThreads)
+centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ vel, const double* __restrict__ fin,
+                      const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
+                      const typename Vec4<R>::type* __restrict__ slotU, R* coef, long long step, int isStep,
+                      double tolerance, int maxIterations, CgBuffers b, R* spread, double* fout, R* reaction,
+                      uint32_t* mask, double* wall) {
+    typedef typename Vec4<R>::type V;
+    const int lane = threadIdx.x & 31;
+    const int firstWarp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
+    const int warps = (gridDim.x*blockDim.x) >> 5;
+    const int S = c.slots;
+    const double a = c.a;
     unsigned generation = 0;
     if (threadIdx.x == 0)
         generation = *((volatile unsigned*) &b.barrier[1]);
-    const double a = c.a;
-    // Right-hand side and diagonal (ReferenceLBMKernels.cpp:758-782).
-    for (int i = first; i < c.np; i += stride) {
-        double m = c.mass[i];
-        double u[3] = {0, 0, 0}, self = 0;
-        for (int s = 0; s < c.slots; s++) {
-            long long t = (long long) i*c.slots + s;
-            double4 su = slotU[t];
-            if (su.w > 0) {
-                double w = slotWeight[t];
-                u[0] += su.x*w;
-                u[1] += su.y*w;
-                u[2] += su.z*w;
-                self += w*w/su.w;
+    // spread(n) += w p_i on the stencil nodes of particle i.
+    auto spreadP = [&](int i, const double* p) {
+        double p0 = p[3*i], p1 = p[3*i+1], p2 = p[3*i+2];
+        for (int s = lane; s < S; s += 32) {
+            long long t = (long long) i*S + s;
+            double w = (double) slotWeight[t];
+            if (w != 0.0)
+                atomicAdd3(spread + 4*(long long) slotNode[t], w*p0, w*p1, w*p2);
+        }
+    };
+    // sum_s (w_s/rho_s) spread(n_s), in every lane.
+    auto gather = [&](int i, double g[3]) {
+        g[0] = g[1] = g[2] = 0;
+        for (int s = lane; s < S; s += 32) {
+            long long t = (long long) i*S + s;
+            double k = (double) coef[t];
+            if (k != 0.0) {
+                V v = *reinterpret_cast<const V*>(spread + 4*(long long) slotNode[t]);
+                g[0] += k*(double) v.x;
+                g[1] += k*(double) v.y;
+                g[2] += k*(double) v.z;
             }
         }
+        for (int d = 0; d < 3; d++)
+            g[d] = warpSum(g[d]);
+    };
+    auto clearSpread = [&](int i) {
+        for (int s = lane; s < S; s += 32) {
+            long long t = (long long) i*S + s;
+            if (slotWeight[t] != (R) 0)
+                *reinterpret_cast<V*>(spread + 4*(long long) slotNode[t]) = Vec4<R>::make(0, 0, 0, 0);
+        }
+    };
+    // Right-hand side, diagonal and the start F = rhs/diag (ReferenceLBMKernels.cpp:758-782, 839-840); coef = w/rho.
+    for (int i = firstWarp; i < c.np; i += warps) {
+        double m = c.mass[i];
+        double u[3] = {0, 0, 0}, self = 0;
+        for (int s = lane; s < S; s += 32) {
+            long long t = (long long) i*S + s;
+            V su = slotU[t];
+            double w = (double) slotWeight[t];
+            double k = 0;
+            if (su.w > 0) {
+                u[0] += (double) su.x*w;
+                u[1] += (double) su.y*w;
+                u[2] += (double) su.z*w;
+                self += w*w/(double) su.w;
+                k = w/(double) su.w;
+            }
+            coef[t] = (R) k;
+        }
+        for (int d = 0; d < 3; d++)
+            u[d] = warpSum(u[d]);
+        self = warpSum(self);
         double xi[3] = {0, 0, 0};
         if (c.randomForce)
             particleNoise(c.seed, i, step, xi);
+        double diag = (1.0 + a)/m + a*self;
+        double F[3];
         for (int d = 0; d < 3; d++) {
             double known = vel[3*i+d]*(1.0/c.velocityScale) + fin[3*i+d]*(c.h/(m*c.forceScale));
-            double rhs = (known - u[d])*(-c.gamma*m);
+            double v = (known - u[d])*(-c.gamma*m);
             if (c.randomForce)
-                rhs += xi[d]*sqrt(2.0*c.gamma*m*c.kT);
-            b.rhs[3*i+d] = rhs*(1.0/m);
-        }
-        b.diag[i] = (1.0 + a)/m + a*self;
-        for (int d = 0; d < 3; d++)
-            b.F[3*i+d] = b.rhs[3*i+d]*(1.0/b.diag[i]);
-        spreadVector<R>(c, slotNode, slotWeight, b.F, spread, i);
-    }
-    auto gather = [&](const double* p, int i, double out[3]) {
-        double sm[3] = {0, 0, 0};
-        for (int s = 0; s < c.slots; s++) {
-            long long t = (long long) i*c.slots + s;
-            double4 su = slotU[t];
-            if (su.w > 0) {
-                double w = slotWeight[t];
-                const R* sp = spread + 4*(long long) slotNode[t];
-                sm[0] += (double) sp[0]*(w/su.w);
-                sm[1] += (double) sp[1]*(w/su.w);
-                sm[2] += (double) sp[2]*(w/su.w);
+                v += xi[d]*sqrt(2.0*c.gamma*m*c.kT);
+            double rhs = v*(1.0/m);
+            F[d] = rhs*(1.0/diag);
+            if (lane == 0) {
+                b.rhs[3*i+d] = rhs;
+                b.F[3*i+d] = F[d];
             }
         }
-        for (int d = 0; d < 3; d++)
-            out[d] = p[3*i+d]*((1.0 + a)/c.mass[i]) + sm[d]*a;
-    };
-    auto clearSpread = [&](int i) {
-        for (int s = 0; s < c.slots; s++) {
-            long long t = (long long) i*c.slots + s;
-            R* sp = spread + 4*(long long) slotNode[t];
-            sp[0] = 0; sp[1] = 0; sp[2] = 0;
-        }
-    };
-    if (!gridBarrier(b.barrier, b.status, generation))
-        return;
-    // r = rhs - A F, z = r/diag, p = z; rz and the norm of the right-hand side per component.
-    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int i = first; i < c.np; i += stride) {
-        double Ap[3];
-        gather(b.F, i, Ap);
-        for (int d = 0; d < 3; d++) {
-            double r = b.rhs[3*i+d] - Ap[d];
-            double z = r*(1.0/b.diag[i]);
-            b.r[3*i+d] = r;
-            b.z[3*i+d] = z;
-            b.p[3*i+d] = z;
-            acc[d] += r*z;
-            acc[3+d] += b.rhs[3*i+d]*b.rhs[3*i+d];
+        if (lane == 0)
+            b.diag[i] = diag;
+        for (int s = lane; s < S; s += 32) {
+            long long t = (long long) i*S + s;
+            double w = (double) slotWeight[t];
+            if (w != 0.0)
+                atomicAdd3(spread + 4*(long long) slotNode[t], w*F[0], w*F[1], w*F[2]);
         }
     }
-    __shared__ double blockTotal[8];
-    blockSum8(acc, blockTotal);
-    if (threadIdx.x < 8)
-        b.partials[8*blockIdx.x + threadIdx.x] = blockTotal[threadIdx.x];
     if (!gridBarrier(b.barrier, b.status, generation))
         return;
-    double tot[8];
-    reducePartials(b.partials, gridDim.x, tot);
-    double rz[3] = {tot[0], tot[1], tot[2]}, norm[3] = {tot[3], tot[4], tot[5]};
-    // Residual of the start.
-    for (int i = first; i < c.np; i += stride)
+    // r = rhs - A F, z = r/diag, p = z; r.z, the norm of the right-hand side and r.r per component.
+    double acc[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = firstWarp; i < c.np; i += warps) {
+        double g[3];
+        gather(i, g);
+        double m = c.mass[i], diag = b.diag[i];
+        for (int d = 0; d < 3; d++) {
+            double Ap = b.F[3*i+d]*((1.0 + a)/m) + g[d]*a;
+            double rhs = b.rhs[3*i+d];
+            double r = rhs - Ap;
+            double z = r*(1.0/diag);
+            if (lane == 0) {
+                b.r[3*i+d] = r;
+                b.z[3*i+d] = z;
+                b.p[3*i+d] = z;
+                acc[d] += r*z;
+                acc[3+d] += rhs*rhs;
+                acc[6+d] += r*r;
+            }
+        }
+    }
+    blockSumStore(acc, b.partials[1]);
+    if (!gridBarrier(b.barrier, b.status, generation))
+        return;
+    for (int i = firstWarp; i < c.np; i += warps)
         clearSpread(i);
-    double acc2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int i = first; i < c.np; i += stride)
-        for (int d = 0; d < 3; d++)
-            acc2[d] += b.r[3*i+d]*b.r[3*i+d];
-    blockSum8(acc2, blockTotal);
-    if (!gridBarrier(b.barrier, b.status, generation))
-        return;
-    if (threadIdx.x < 8)
-        b.partials[8*blockIdx.x + threadIdx.x] = blockTotal[threadIdx.x];
-    if (!gridBarrier(b.barrier, b.status, generation))
-        return;
-    reducePartials(b.partials, gridDim.x, tot);
-    double residual[3] = {tot[0], tot[1], tot[2]};
+    double tot[kPartial];
+    reducePartials(b.partials[1], gridDim.x, tot);
+    double rz[3] = {tot[0], tot[1], tot[2]}, norm[3] = {tot[3], tot[4], tot[5]}, residual[3] = {tot[6], tot[7], tot[8]};
     int iteration = 0;
     bool failed = false;       // the same in every block: every decision comes from the same reduced sums
+    bool clearBeforeSpread = true;
     for (;; iteration++) {
         bool converged = true;
         for (int d = 0; d < 3; d++)
@@ -544,95 +589,103 @@ __global__ void centeredStencilKernel(FluidView f, CouplingView c, const double*
         if (converged)
             break;
         if (iteration == maxIterations) {
-            if (first == 0)
+            if (firstWarp == 0 && lane == 0)
                 atomicExch(b.status, LBM_ERR_CG_NOT_CONVERGED);
             failed = true;
             break;
         }
-        // Ap = A p.
-        for (int i = first; i < c.np; i += stride)
-            spreadVector<R>(c, slotNode, slotWeight, b.p, spread, i);
+        // The spread buffer was cleared by every block before the last barrier (the clearing of the start comes
+        // before the barrier at the top of the first iteration's spread below).
+        if (clearBeforeSpread) {
+            if (!gridBarrier(b.barrier, b.status, generation))
+                return;
+            clearBeforeSpread = false;
+        }
+        for (int i = firstWarp; i < c.np; i += warps)
+            spreadP(i, b.p);
         if (!gridBarrier(b.barrier, b.status, generation))
             return;
-        double acc3[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int i = first; i < c.np; i += stride) {
-            double Ap[3];
-            gather(b.p, i, Ap);
+        double acc3[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = firstWarp; i < c.np; i += warps) {
+            double g[3];
+            gather(i, g);
+            double m = c.mass[i];
             for (int d = 0; d < 3; d++) {
-                b.Ap[3*i+d] = Ap[d];
-                acc3[d] += b.p[3*i+d]*Ap[d];
+                double p = b.p[3*i+d];
+                double Ap = p*((1.0 + a)/m) + g[d]*a;
+                if (lane == 0) {
+                    acc3[d] += p*Ap;
+                    b.z[3*i+d] = Ap;
+                }
             }
         }
-        blockSum8(acc3, blockTotal);
-        if (threadIdx.x < 8)
-            b.partials[8*blockIdx.x + threadIdx.x] = blockTotal[threadIdx.x];
+        blockSumStore(acc3, b.partials[0]);
         if (!gridBarrier(b.barrier, b.status, generation))
             return;
-        reducePartials(b.partials, gridDim.x, tot);
+        reducePartials(b.partials[0], gridDim.x, tot);
         double alpha[3];
         for (int d = 0; d < 3; d++)
             alpha[d] = (tot[d] > 0 ? rz[d]/tot[d] : 0.0);
-        double acc4[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int i = first; i < c.np; i += stride) {
+        double acc4[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = firstWarp; i < c.np; i += warps) {
             clearSpread(i);
-            for (int d = 0; d < 3; d++) {
-                b.F[3*i+d] += alpha[d]*b.p[3*i+d];
-                double r = b.r[3*i+d] - alpha[d]*b.Ap[3*i+d];
-                b.r[3*i+d] = r;
-                double z = r*(1.0/b.diag[i]);
-                b.z[3*i+d] = z;
-                acc4[d] += r*z;
-                acc4[3+d] += r*r;
+            if (lane == 0) {
+                double diag = b.diag[i];
+                for (int d = 0; d < 3; d++) {
+                    b.F[3*i+d] += alpha[d]*b.p[3*i+d];
+                    double r = b.r[3*i+d] - alpha[d]*b.z[3*i+d];
+                    b.r[3*i+d] = r;
+                    double z = r*(1.0/diag);
+                    b.z[3*i+d] = z;
+                    acc4[d] += r*z;
+                    acc4[3+d] += r*r;
+                }
             }
         }
-        blockSum8(acc4, blockTotal);
-        // All blocks have read the partials of pAp above (reducePartials ends with a block barrier, and the
-        // grid barrier below separates the next writes); write the new partials after the barrier.
+        blockSumStore(acc4, b.partials[1]);
         if (!gridBarrier(b.barrier, b.status, generation))
             return;
-        if (threadIdx.x < 8)
-            b.partials[8*blockIdx.x + threadIdx.x] = blockTotal[threadIdx.x];
-        if (!gridBarrier(b.barrier, b.status, generation))
-            return;
-        reducePartials(b.partials, gridDim.x, tot);
+        reducePartials(b.partials[1], gridDim.x, tot);
         double beta[3];
         for (int d = 0; d < 3; d++) {
             beta[d] = (rz[d] > 0 ? tot[d]/rz[d] : 0.0);
             rz[d] = tot[d];
             residual[d] = tot[3+d];
         }
-        for (int i = first; i < c.np; i += stride)
-            for (int d = 0; d < 3; d++)
-                b.p[3*i+d] = b.z[3*i+d] + beta[d]*b.p[3*i+d];
-        // The next spread reads only this thread's p; the spread buffer was cleared before the last barrier.
-        if (!gridBarrier(b.barrier, b.status, generation))
-            return;
+        if (lane == 0)
+            for (int i = firstWarp; i < c.np; i += warps)
+                for (int d = 0; d < 3; d++)
+                    b.p[3*i+d] = b.z[3*i+d] + beta[d]*b.p[3*i+d];
+        __syncwarp();
     }
-    if (first == 0)
+    if (firstWarp == 0 && lane == 0)
         *b.iterations = iteration;
     if (failed)
         return;
     // Forces and reactions (ReferenceLBMKernels.cpp:889-900).
-    for (int i = first; i < c.np; i += stride) {
-        for (int d = 0; d < 3; d++)
-            fout[3*i+d] = b.F[3*i+d]*c.forceScale;
+    for (int i = firstWarp; i < c.np; i += warps) {
+        double F0 = b.F[3*i], F1 = b.F[3*i+1], F2 = b.F[3*i+2];
+        if (lane == 0) {
+            fout[3*i] = F0*c.forceScale;
+            fout[3*i+1] = F1*c.forceScale;
+            fout[3*i+2] = F2*c.forceScale;
+        }
         if (isStep)
-            for (int s = 0; s < c.slots; s++) {
-                long long t = (long long) i*c.slots + s;
-                double w = slotWeight[t];
+            for (int s = lane; s < S; s += 32) {
+                long long t = (long long) i*S + s;
+                double w = (double) slotWeight[t];
                 if (w != 0.0)
-                    addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*b.F[3*i], -w*b.F[3*i+1], -w*b.F[3*i+2]);
+                    addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*F0, -w*F1, -w*F2);
             }
     }
 }
 
-// Clear the reaction of the slots of the last step (and their mask bits).
+// Clear the reaction of the slots of the last step (and their mask words).
 template <typename R>
 __global__ void clearReactionKernel(FluidView f, const int* slotNode, long long total, R* reaction, uint32_t* mask) {
     for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x) {
         long long node = slotNode[t];
-        R* r = reaction + 4*node;
-        r[0] = 0; r[1] = 0; r[2] = 0;
+        *reinterpret_cast<typename Vec4<R>::type*>(reaction + 4*node) = Vec4<R>::make(0, 0, 0, 0);
         long long row = node/f.nx;
         int x = (int) (node - row*f.nx);
         mask[row*f.wordsPerRow + x/32] = 0u;
@@ -689,6 +742,11 @@ int widthOf(int stencil) {
     return stencil == LBM_STENCIL_TRILINEAR ? 2 : stencil == LBM_STENCIL_THREEPOINT ? 3 : stencil == LBM_STENCIL_KEYS ? 4 : 1;
 }
 
+// Blocks for one warp per particle.
+int warpGrid(long long particles) {
+    return (int) std::max(1LL, std::min(4736LL, (particles*32 + kThreads - 1)/kThreads));
+}
+
 } // namespace
 
 // ------------------------------------------------------------------------------------------------------
@@ -697,8 +755,9 @@ int widthOf(int stencil) {
 
 struct CouplingEngine::Device {
     int* slotNode = nullptr;
-    double* slotWeight = nullptr;
-    double4* slotU = nullptr;
+    void* slotWeight = nullptr;   // R per slot
+    void* slotU = nullptr;        // 4 R per slot
+    void* coef = nullptr;         // R per slot (centred stencil)
     unsigned* keys[2] = {nullptr, nullptr};
     int* values[2] = {nullptr, nullptr};
     unsigned* hist = nullptr;
@@ -715,8 +774,11 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
           forceInDev(nullptr), forceOutDev(nullptr), massDev(nullptr), wallDev(nullptr), statusDev(nullptr),
           pinned(nullptr), dev(new Device()) {
     (void) g;
+    std::memset(&dev->cg, 0, sizeof(CgBuffers));
     stencilSlots = widthOf(l.interpolation_stencil);
     stencilSlots = stencilSlots*stencilSlots*stencilSlots;
+    bool f64 = storageType == LBM_STORAGE_F64;
+    size_t r = f64 ? 8 : 4;
     try {
         size_t v3 = sizeof(double)*3*(size_t) np;
         CUDA_CHECK(cudaMalloc(&posDev, v3));
@@ -738,10 +800,10 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
         CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, stream));
         size_t slots = (size_t) np*stencilSlots;
         CUDA_CHECK(cudaMalloc(&dev->slotNode, sizeof(int)*slots));
-        CUDA_CHECK(cudaMalloc(&dev->slotWeight, sizeof(double)*slots));
-        CUDA_CHECK(cudaMalloc(&dev->slotU, sizeof(double4)*slots));
+        CUDA_CHECK(cudaMalloc(&dev->slotWeight, r*slots));
+        CUDA_CHECK(cudaMalloc(&dev->slotU, 4*r*slots));
         CUDA_CHECK(cudaMemsetAsync(dev->slotNode, 0, sizeof(int)*slots, stream));
-        CUDA_CHECK(cudaMemsetAsync(dev->slotWeight, 0, sizeof(double)*slots, stream));
+        CUDA_CHECK(cudaMemsetAsync(dev->slotWeight, 0, r*slots, stream));
         if (l.drag_scheme == LBM_DRAG_CENTERED && l.interpolation_stencil == LBM_STENCIL_NEAREST) {
             int blocks = (np + kSortItems - 1)/kSortItems;
             dev->histCount = (size_t) 256*blocks;
@@ -759,7 +821,7 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
             CUDA_CHECK(cudaMalloc(&b.r, v3));
             CUDA_CHECK(cudaMalloc(&b.z, v3));
             CUDA_CHECK(cudaMalloc(&b.p, v3));
-            CUDA_CHECK(cudaMalloc(&b.Ap, v3));
+            CUDA_CHECK(cudaMalloc(&dev->coef, r*slots));
             b.status = statusDev;
             b.iterations = statusDev + 1;
             CUDA_CHECK(cudaMalloc(&b.barrier, sizeof(unsigned)*2));
@@ -767,14 +829,14 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
             int device = 0, sms = 0, perSM = 0;
             CUDA_CHECK(cudaGetDevice(&device));
             CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-            if (storageType == LBM_STORAGE_F64)
+            if (f64)
                 CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, centeredStencilKernel<double>, kThreads, 0));
             else
                 CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, centeredStencilKernel<float>, kThreads, 0));
-            int wanted = (np + kThreads - 1)/kThreads;
-            dev->cgGrid = std::max(1, std::min(wanted, std::max(1, perSM)*sms));
-            CUDA_CHECK(cudaMalloc(&b.partials, sizeof(double)*8*(size_t) dev->cgGrid));
-            size_t r = (storageType == LBM_STORAGE_F64 ? 8 : 4);
+            long long wanted = ((long long) np*32 + kThreads - 1)/kThreads;     // one warp per particle
+            dev->cgGrid = (int) std::max(1LL, std::min(wanted, (long long) std::max(1, perSM)*sms));
+            for (int k = 0; k < 2; k++)
+                CUDA_CHECK(cudaMalloc(&b.partials[k], sizeof(double)*kPartial*(size_t) dev->cgGrid));
             CUDA_CHECK(cudaMalloc(&dev->spread, 4*r*(size_t) f.numNodes()));
             CUDA_CHECK(cudaMemsetAsync(dev->spread, 0, 4*r*(size_t) f.numNodes(), stream));
         }
@@ -797,15 +859,15 @@ void CouplingEngine::release() {
         cudaFreeHost(pinned);
     pinned = nullptr;
     if (dev) {
-        cudaFree(dev->slotNode); cudaFree(dev->slotWeight); cudaFree(dev->slotU);
+        cudaFree(dev->slotNode); cudaFree(dev->slotWeight); cudaFree(dev->slotU); cudaFree(dev->coef);
         for (int k = 0; k < 2; k++) {
             cudaFree(dev->keys[k]);
             cudaFree(dev->values[k]);
         }
         cudaFree(dev->hist);
         CgBuffers& b = dev->cg;
-        cudaFree(b.rhs); cudaFree(b.diag); cudaFree(b.F); cudaFree(b.r); cudaFree(b.z); cudaFree(b.p); cudaFree(b.Ap);
-        cudaFree(b.partials); cudaFree(b.barrier);
+        cudaFree(b.rhs); cudaFree(b.diag); cudaFree(b.F); cudaFree(b.r); cudaFree(b.z); cudaFree(b.p);
+        cudaFree(b.partials[0]); cudaFree(b.partials[1]); cudaFree(b.barrier);
         cudaFree(dev->spread);
         delete dev;
         dev = nullptr;
@@ -852,18 +914,11 @@ static CouplingView makeView(const LbmLatticeParameters& l, const FluidView& f, 
 
 void CouplingEngine::load(const LbmParticleArrays* p, bool withForces) {
     size_t v3 = sizeof(double)*3*(size_t) np;
-    if (p->memory == LBM_MEMORY_DEVICE) {
-        CUDA_CHECK(cudaMemcpyAsync(posDev, p->positions, v3, cudaMemcpyDeviceToDevice, stream));
-        CUDA_CHECK(cudaMemcpyAsync(velDev, p->velocities, v3, cudaMemcpyDeviceToDevice, stream));
-        if (withForces)
-            CUDA_CHECK(cudaMemcpyAsync(forceInDev, p->forces, v3, cudaMemcpyDeviceToDevice, stream));
-    }
-    else {
-        CUDA_CHECK(cudaMemcpyAsync(posDev, p->positions, v3, cudaMemcpyHostToDevice, stream));
-        CUDA_CHECK(cudaMemcpyAsync(velDev, p->velocities, v3, cudaMemcpyHostToDevice, stream));
-        if (withForces)
-            CUDA_CHECK(cudaMemcpyAsync(forceInDev, p->forces, v3, cudaMemcpyHostToDevice, stream));
-    }
+    cudaMemcpyKind kind = p->memory == LBM_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CUDA_CHECK(cudaMemcpyAsync(posDev, p->positions, v3, kind, stream));
+    CUDA_CHECK(cudaMemcpyAsync(velDev, p->velocities, v3, kind, stream));
+    if (withForces)
+        CUDA_CHECK(cudaMemcpyAsync(forceInDev, p->forces, v3, kind, stream));
 }
 
 void CouplingEngine::reflect(const LbmParticleArrays* p, double wallMomentum[3]) {
@@ -876,52 +931,38 @@ void CouplingEngine::reflect(const LbmParticleArrays* p, double wallMomentum[3])
     CUDA_CHECK(cudaGetLastError());
     fluid.launches++;
     size_t v3 = sizeof(double)*3*(size_t) np;
-    if (p->memory == LBM_MEMORY_DEVICE)
-        CUDA_CHECK(cudaMemcpyAsync(p->velocities, velDev, v3, cudaMemcpyDeviceToDevice, stream));
-    else
-        CUDA_CHECK(cudaMemcpyAsync(p->velocities, velDev, v3, cudaMemcpyDeviceToHost, stream));
+    cudaMemcpyKind kind = p->memory == LBM_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    CUDA_CHECK(cudaMemcpyAsync(p->velocities, velDev, v3, kind, stream));
     CUDA_CHECK(cudaMemcpyAsync(wallMomentum, dev->reflectWall, sizeof(double)*3, cudaMemcpyDeviceToHost, stream));
     CUDA_CHECK(cudaStreamSynchronize(stream));
 }
 
-template <typename T>
+template <typename T, typename R>
 static void launchStencil(const void* A, const FluidView& f, const CouplingView& c, const double* pos, int remove, int centred,
-                          int* slotNode, double* slotWeight, double4* slotU, cudaStream_t s) {
+                          int* slotNode, void* slotWeight, void* slotU, cudaStream_t s) {
     long long total = (long long) c.np*c.slots;
     int grid = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
-    stencilKernel<T><<<grid, kThreads, 0, s>>>((const T*) A, f, c, pos, remove, centred, slotNode, slotWeight, slotU);
+    stencilKernel<T, R><<<grid, kThreads, 0, s>>>((const T*) A, f, c, pos, remove, centred, slotNode, (R*) slotWeight,
+                                                   (typename Vec4<R>::type*) slotU);
 }
 
-void CouplingEngine::couple(long long step, bool isStep, bool remove) {
+template <typename R>
+void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView* cv) {
+    const CouplingView& c = *cv;
     const FluidView& f = fluid.deviceView();
-    CouplingView c = makeView(lattice, f, np, widthOf(lattice.interpolation_stencil), massDev);
     bool centred = lattice.drag_scheme == LBM_DRAG_CENTERED;
-    const void* A = fluid.inputArray();
-    switch (storageType) {
-    case LBM_STORAGE_F64: launchStencil<double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
-    case LBM_STORAGE_F32: launchStencil<float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
-    case LBM_STORAGE_F16: launchStencil<__half>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
-    default: launchStencil<__nv_bfloat16>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
-    }
-    CUDA_CHECK(cudaGetLastError());
-    fluid.launches++;
-    if (isStep)
-        CUDA_CHECK(cudaMemsetAsync(wallDev, 0, sizeof(double)*3, stream));
-    int gridP = std::max(1, std::min(1184, (np + kThreads - 1)/kThreads));
-    bool f64 = storageType == LBM_STORAGE_F64;
-    void* reaction = fluid.reactionBuffer();
+    R* reaction = (R*) fluid.reactionBuffer();
     uint32_t* mask = fluid.reactMask();
+    const R* sw = (const R*) dev->slotWeight;
+    const typename Vec4<R>::type* su = (const typename Vec4<R>::type*) dev->slotU;
     if (!centred) {
-        if (f64)
-            explicitKernel<double><<<gridP, kThreads, 0, stream>>>(f, c, velDev, dev->slotNode, dev->slotWeight, dev->slotU, step,
-                                                                    isStep, forceOutDev, (double*) reaction, mask, wallDev);
-        else
-            explicitKernel<float><<<gridP, kThreads, 0, stream>>>(f, c, velDev, dev->slotNode, dev->slotWeight, dev->slotU, step,
-                                                                   isStep, forceOutDev, (float*) reaction, mask, wallDev);
+        explicitKernel<R><<<warpGrid(np), kThreads, 0, stream>>>(f, c, velDev, dev->slotNode, sw, su, step, isStep,
+                                                                 forceOutDev, reaction, mask, wallDev);
         CUDA_CHECK(cudaGetLastError());
         fluid.launches++;
         return;
     }
+    int gridP = std::max(1, std::min(1184, (np + kThreads - 1)/kThreads));
     if (lattice.interpolation_stencil == LBM_STENCIL_NEAREST) {
         // Sort the particles by node, stably (particle order within a node).
         nodeKeysKernel<<<gridP, kThreads, 0, stream>>>(dev->slotNode, np, dev->keys[0], dev->values[0]);
@@ -932,39 +973,32 @@ void CouplingEngine::couple(long long step, bool isStep, bool remove) {
             bits++;
         int cur = radixSortByKey(dev->keys, dev->values, dev->hist, np, bits, stream);
         fluid.launches += 3*((bits + 7)/8);
-        if (f64)
-            centeredNearestKernel<double><<<gridP, kThreads, 0, stream>>>(f, c, dev->keys[cur], dev->values[cur], velDev, forceInDev,
-                                                                           dev->slotU, step, isStep, forceOutDev, (double*) reaction, mask, wallDev);
-        else
-            centeredNearestKernel<float><<<gridP, kThreads, 0, stream>>>(f, c, dev->keys[cur], dev->values[cur], velDev, forceInDev,
-                                                                          dev->slotU, step, isStep, forceOutDev, (float*) reaction, mask, wallDev);
+        centeredNearestKernel<R><<<gridP, kThreads, 0, stream>>>(f, c, dev->keys[cur], dev->values[cur], velDev, forceInDev,
+                                                                  su, step, isStep, forceOutDev, reaction, mask, wallDev);
         CUDA_CHECK(cudaGetLastError());
         fluid.launches++;
         return;
     }
     // Centred drag with a stencil: the conjugate gradients on the device (ReferenceLBMKernels.cpp:834-888, tolerance
-    // 1e-13 in double; 1e-5 with single-precision storage, as the reference's GPU platforms in single precision).
+    // 1e-13 in double; 1e-5 with single-precision arithmetic, as the reference's GPU platforms in single precision).
     CgBuffers b = dev->cg;
     CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*2, stream));
-    double tolerance = f64 ? 1e-13 : 1e-5;
+    double tolerance = std::is_same<R, double>::value ? 1e-13 : 1e-5;
     int maxIterations = 1000;
     long long stepArg = step;
     int isStepArg = isStep ? 1 : 0;
-    void* spread = dev->spread;
+    R* spread = (R*) dev->spread;
+    R* coef = (R*) dev->coef;
     double* fout = forceOutDev;
     double* wall = wallDev;
     double* fin = forceInDev;
     double* vel = velDev;
     int* sn = dev->slotNode;
-    double* sw = dev->slotWeight;
-    double4* su = dev->slotU;
     FluidView fv = f;
-    void* args[] = {&fv, &c, &vel, &fin, &sn, &sw, &su, &stepArg, &isStepArg, &tolerance, &maxIterations, &b, &spread,
-                    &fout, &reaction, &mask, &wall};
-    if (f64)
-        CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredStencilKernel<double>, dev->cgGrid, kThreads, args, 0, stream));
-    else
-        CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredStencilKernel<float>, dev->cgGrid, kThreads, args, 0, stream));
+    CouplingView cc = c;
+    void* args[] = {&fv, &cc, &vel, &fin, &sn, &sw, &su, &coef, &stepArg, &isStepArg, &tolerance, &maxIterations, &b,
+                    &spread, &fout, &reaction, &mask, &wall};
+    CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredStencilKernel<R>, dev->cgGrid, kThreads, args, 0, stream));
     fluid.launches++;
     int status[2] = {0, 0};
     CUDA_CHECK(cudaMemcpyAsync(status, statusDev, sizeof(int)*2, cudaMemcpyDeviceToHost, stream));
@@ -975,6 +1009,27 @@ void CouplingEngine::couple(long long step, bool isStep, bool remove) {
                     "in 1000 iterations of the conjugate gradients");
     if (status[0] == LBM_ERR_DEVICE_TIMEOUT)
         throw Error(LBM_ERR_DEVICE_TIMEOUT, "LBMForce: a grid barrier of the conjugate gradients timed out");
+}
+
+void CouplingEngine::couple(long long step, bool isStep, bool remove) {
+    const FluidView& f = fluid.deviceView();
+    CouplingView c = makeView(lattice, f, np, widthOf(lattice.interpolation_stencil), massDev);
+    bool centred = lattice.drag_scheme == LBM_DRAG_CENTERED;
+    const void* A = fluid.inputArray();
+    switch (storageType) {
+    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
+    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
+    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
+    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
+    }
+    CUDA_CHECK(cudaGetLastError());
+    fluid.launches++;
+    if (isStep)
+        CUDA_CHECK(cudaMemsetAsync(wallDev, 0, sizeof(double)*3, stream));
+    if (storageType == LBM_STORAGE_F64)
+        coupleWith<double>(step, isStep, &c);
+    else
+        coupleWith<float>(step, isStep, &c);
 }
 
 void CouplingEngine::addForces(const LbmParticleArrays* p) {

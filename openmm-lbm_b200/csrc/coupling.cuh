@@ -7,6 +7,8 @@
 
 namespace lbm {
 
+struct CouplingView;
+
 class CouplingEngine {
 public:
     CouplingEngine(const LbmLatticeParameters& lattice, FluidEngine& fluid, const Geometry& geometry, int numParticles,
@@ -33,6 +35,8 @@ public:
 private:
     struct Device;
     void release();
+    template <typename R>
+    void coupleWith(long long step, bool isStep, const CouplingView* view);
     LbmLatticeParameters lattice;
     FluidEngine& fluid;
     cudaStream_t stream;

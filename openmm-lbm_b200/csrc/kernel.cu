@@ -222,6 +222,10 @@ void B200Kernel::getWallForce(double force[3]) {
         force[a] = total[a]/lattice.dt;
 }
 
+int B200Kernel::solverIterations() const {
+    return coupling ? coupling->lastIterations : 0;
+}
+
 void B200Kernel::getFluidState(double* state) {
     CUDA_CHECK(cudaSetDevice(device));
     fluid->getState(state);

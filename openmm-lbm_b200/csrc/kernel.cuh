@@ -33,6 +33,7 @@ public:
     int storage() const { return fluid->storage(); }
     cudaStream_t getStream() const { return stream; }
     FluidEngine& fluidEngine() { return *fluid; }
+    int solverIterations() const;
 private:
     void advanceFluid(const LbmParticleArrays* particles);
     void computeNextStepForces(long long stepCount, const LbmParticleArrays* particles);

@@ -31,18 +31,28 @@ __global__ void __launch_bounds__(1024) radixScan(unsigned* hist, int count) {
     unsigned sum = 0;
     for (int i = begin; i < end; i++)
         sum += hist[i];
-    partial[threadIdx.x] = sum;
+    // Exclusive scan of the per-thread sums: inclusive scans within the warps (shuffles), then over the warp totals.
+    int lane = threadIdx.x%32, warp = threadIdx.x/32;
+    unsigned inclusive = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned v = __shfl_up_sync(0xffffffffu, inclusive, o);
+        if (lane >= o)
+            inclusive += v;
+    }
+    if (lane == 31)
+        partial[warp] = inclusive;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned run = 0;
-        for (int t = 0; t < (int) blockDim.x; t++) {
-            unsigned v = partial[t];
-            partial[t] = run;
-            run += v;
+    if (warp == 0) {
+        unsigned total = lane < (int) blockDim.x/32 ? partial[lane] : 0u, scan = total;
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned v = __shfl_up_sync(0xffffffffu, scan, o);
+            if (lane >= o)
+                scan += v;
         }
+        partial[32 + lane] = scan - total;       // exclusive prefix of the warp totals
     }
     __syncthreads();
-    unsigned run = partial[threadIdx.x];
+    unsigned run = partial[32 + warp] + inclusive - sum;
     for (int i = begin; i < end; i++) {
         unsigned v = hist[i];
         hist[i] = run;
