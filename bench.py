@@ -1,14 +1,17 @@
 """Benchmark of the per-step fluid and particle-coupling path on B200: MLUPS, and the HBM roofline of the dense
 stream-collide kernel.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload coupled|fluid]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload coupled|fluid|channel]
+                    [--precision double|single|half|bfloat16] [--size EDGE]
 
 Workload "coupled" (default, the scale configuration): a 256^3 periodic fluctuating D3Q19 fluid (tau 0.6, kT 1e-4 in
 lattice units, Philox seed), FP32 storage, momentum removal every step, Mach check every 100 steps; 512 bead-spring
 chains of 100 beads (51,200 beads, mass 1) placed as seeded random walks, harmonic bonds (k = 100 kT/sigma^2, r0 = 1)
 and WCA repulsion (sigma 1, epsilon = kT), coupled through the Keys stencil with the centred drag (friction 1 per
 lattice step, solved by conjugate gradients on the device).  One step: beginStep, bead forces, execute (coupling +
-fluid) and the leapfrog of the beads, all on the device.  "fluid": the fluid alone (kernel profiling).
+fluid) and the leapfrog of the beads, all on the device.  "fluid": the fluid alone (kernel profiling).  "channel": the
+precision configuration, a 384x384x192 Poiseuille channel between bounce-back planes (g_x 5e-7, tau 0.55), for the
+MLUPS of each storage format.
 
 value = fluid nodes x steps / device time (MLUPS).  e2e = the same metric through the C ABI with the beads' positions
 and velocities in pinned host memory: copied to the device before and back after every step.  With N > 1 (torchrun,
@@ -87,6 +90,66 @@ class Workload:
         kT = self.kT if self.kT > 0 else 1e-4
         return dict(k=100.0*kT, r0=1.0, pair='wca', sigma=1.0, epsilon=kT, cutoff=2.0**(1/6))
 
+    @property
+    def shape(self):
+        return (self.n,)*3
+
+    def solids(self):
+        return []
+
+    def fluid_nodes(self):
+        return self.n**3
+
+    def profile_tag(self):
+        return '%s_%d' % ('fluct' if self.kT > 0 else 'plain', self.n)
+
+    def sample(self, n):
+        """A sample on an n^3 lattice with the same bead density."""
+        chains = int(round(self.chains*(n/self.n)**3)) if self.coupled else 0
+        return Workload(n=n, chains=chains, length=self.length, coupled=self.coupled, fluctuations=self.kT > 0,
+                        seed=self.seed)
+
+
+class ChannelWorkload:
+    """The precision configuration: a Poiseuille channel between bounce-back planes z = 0 and z = nz - 1, Guo body
+    force g_x = 5e-7, tau 0.55, no fluctuations, no momentum removal, started from rest (lattice units)."""
+
+    def __init__(self, shape=(384, 384, 192)):
+        self.shape = tuple(shape)
+        self.n = max(shape)
+        self.chains, self.length, self.coupled = 0, 0, False
+        self.tau, self.kT, self.g, self.seed = 0.55, 0.0, 5e-7, 2026
+
+    def name(self):
+        return ('%dx%dx%d Poiseuille channel, bounce-back planes z = 0 and z = %d, g_x 5e-7, tau 0.55, no fluctuations '
+                '(lattice units)' % (self.shape + (self.shape[2] - 1,)))
+
+    def lattice(self, lbm):
+        nx, ny, nz = self.shape
+        force = lbm.LBMForce()
+        force.setGridSize(nx, ny, nz)
+        force.setFluidDensity(1.0)
+        force.setKinematicViscosity((self.tau - 0.5)/3.0)
+        force.setBodyAcceleration((self.g, 0.0, 0.0))
+        force.setFluidMomentumRemovalFrequency(0)
+        return force.latticeParameters(np.array(self.shape, dtype=float), 1.0, np.ones(1))
+
+    def solids(self):
+        nx, ny, nz = self.shape
+        plane = np.arange(nx*ny, dtype=np.int64)
+        return np.concatenate([plane, plane + nx*ny*(nz - 1)])
+
+    def fluid_nodes(self):
+        nx, ny, nz = self.shape
+        return nx*ny*(nz - 2)
+
+    def profile_tag(self):
+        return 'channel_%dx%dx%d' % self.shape
+
+    def sample(self, n):
+        """A sample with the same aspect ratio and edge n in x."""
+        return ChannelWorkload((n, n, max(4, n//2)))
+
 
 def peaks():
     path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
@@ -143,13 +206,13 @@ def run_b200(args, w, rank, world, device):
     # orders with events on that stream) outlive nothing they depend on.
     stream = torch.cuda.Stream()
     stream_ptr = stream.cuda_stream
-    kernel = lbm.B200Kernel(lattice, masses, [], args.precision, device=device, stream=stream_ptr)
+    kernel = lbm.B200Kernel(lattice, masses, w.solids(), args.precision, device=device, stream=stream_ptr)
     lib = kernel.lib
-    nodes = w.n**3
+    nodes = w.fluid_nodes()
     md = None
     if np_ > 0:
         pos0, bonds = w.beads(lbm)
-        md = lbm.BeadDynamics(masses, (w.n,)*3, bonds, device=device, **w.md_parameters())
+        md = lbm.BeadDynamics(masses, w.shape, bonds, device=device, **w.md_parameters())
         pos = torch.tensor(pos0, device='cuda', dtype=torch.float64)
         vel = torch.zeros_like(pos)
         frc = torch.zeros_like(pos)
@@ -254,15 +317,15 @@ def run_b200(args, w, rank, world, device):
     achieved = bytes_per_node*nodes/avg_dense_s/1e9
     peak, peak_kind = peaks()
     config = {'workload': w.name(), 'nodes_per_gpu': nodes, 'beads_per_gpu': np_, 'storage': args.precision,
-              'momentum_removal_frequency': 1, 'mach_check_frequency': 100,
+              'momentum_removal_frequency': 0 if isinstance(w, ChannelWorkload) else 1, 'mach_check_frequency': 100,
               'l2': 'inputs larger than L2 (2 x %.2f GB of populations)' % (19*nodes*STORAGE_BYTES[args.precision]/1e9),
               'parallelism': 'independent replicas, one per GPU' if world > 1 else 'single GPU'}
     return {
-        'metric': 'MLUPS (fluid nodes x lattice steps / s) of the coupled lattice step',
+        'metric': metric_name(w),
         'value': value, 'unit': 'MLUPS', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': ms/args.steps, 'coupled_steps_per_s': 1e3*args.steps/ms, 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None, 'dtype': DTYPE[args.precision],
-        'data': 'synthetic: seeded random-walk chains in a fluid at rest, thermal noise from Philox', 'config': config,
+        'data': data_name(w), 'config': config,
         'roofline': {'bound': 'hbm', 'kernel': 'streamCollideKernel', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                      'frac': achieved/peak, 'peak_kind': peak_kind, 'algorithmic_bytes_per_launch': bytes_per_node*nodes,
                      'algorithmic_bytes_per_node': bytes_per_node, 'avg_launch_ms': avg_dense_s*1e3,
@@ -275,10 +338,22 @@ def run_b200(args, w, rank, world, device):
     }
 
 
+def metric_name(w):
+    return 'MLUPS (fluid nodes x lattice steps / s) of the %s lattice step' % ('coupled' if w.coupled else 'fluid')
+
+
+def data_name(w):
+    if w.coupled:
+        return 'synthetic: seeded random-walk chains in a fluid at rest, thermal noise from Philox'
+    if w.kT > 0:
+        return 'synthetic: a fluid at rest, thermal noise from Philox'
+    return 'synthetic: a fluid started from rest'
+
+
 def traffic_per_launch(args, w):
     """DRAM bytes per launch of the dense kernel from the committed ncu summary of this variant, if there is one."""
-    name = 'stream_collide_%s_%s_%d.md' % ({'double': 'f64', 'single': 'f32', 'half': 'f16', 'bfloat16': 'bf16'}[args.precision],
-                                          'fluct' if w.kT > 0 else 'plain', w.n)
+    name = 'stream_collide_%s_%s.md' % ({'double': 'f64', 'single': 'f32', 'half': 'f16', 'bfloat16': 'bf16'}[args.precision],
+                                       w.profile_tag())
     path = os.path.join(ROOT, 'profiles', name)
     if not os.path.exists(path):
         return None
@@ -289,8 +364,8 @@ def traffic_per_launch(args, w):
 
 
 def cpu_step_fn(lbm, oracle, w, kernel, pos, vel, bonds, masses):
-    params = w.md_parameters()
-    box = np.array([w.n]*3, dtype=float)
+    params = w.md_parameters() if len(pos) else None
+    box = np.array(w.shape, dtype=float)
     frc = np.zeros_like(pos)
 
     def step(s):
@@ -316,7 +391,7 @@ def run_cpu(args, w, steps, warmup):
     lattice = w.lattice(lbm)
     np_ = w.chains*w.length
     masses = np.ones(np_)
-    kernel = factory(lattice, masses, [])
+    kernel = factory(lattice, masses, w.solids())
     if np_:
         pos, bonds = w.beads(lbm)
     else:
@@ -334,13 +409,7 @@ def run_cpu(args, w, steps, warmup):
         s += 1
     dt = (time.perf_counter() - t0)/steps
     kernel.close()
-    return w.n**3/dt/1e6, kind, dt
-
-
-def sample_of(w, n):
-    """A sample of workload w on an n^3 lattice with the same bead density."""
-    chains = int(round(w.chains*(n/w.n)**3)) if w.coupled else 0
-    return Workload(n=n, chains=chains, length=w.length, coupled=w.coupled, fluctuations=w.kT > 0, seed=w.seed)
+    return w.fluid_nodes()/dt/1e6, kind, dt
 
 
 def main():
@@ -349,9 +418,9 @@ def main():
     parser.add_argument('--steps', type=int, default=30)
     parser.add_argument('--warmup', type=int, default=5)
     parser.add_argument('--impl', default='b200', choices=['b200', 'reference'])
-    parser.add_argument('--workload', default='coupled', choices=['coupled', 'fluid'])
+    parser.add_argument('--workload', default='coupled', choices=['coupled', 'fluid', 'channel'])
     parser.add_argument('--precision', default='single', choices=list(STORAGE_BYTES))
-    parser.add_argument('--size', type=int, default=256, help='lattice edge (smaller cases for profiling)')
+    parser.add_argument('--size', type=int, default=0, help='lattice edge in x (smaller cases for profiling)')
     parser.add_argument('--no-fluctuations', action='store_true')
     parser.add_argument('--no-cpu-baseline', action='store_true')
     parser.add_argument('--observables', action='store_true', help='fluid and bead temperatures after the run')
@@ -360,17 +429,20 @@ def main():
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     local = int(os.environ.get('LOCAL_RANK', '0'))
-    base = Workload(coupled=args.workload == 'coupled', fluctuations=not args.no_fluctuations)
-    w = sample_of(base, args.size) if args.size != base.n else base
+    if args.workload == 'channel':
+        base = ChannelWorkload()
+    else:
+        base = Workload(coupled=args.workload == 'coupled', fluctuations=not args.no_fluctuations)
+    w = base.sample(args.size) if args.size and args.size != base.shape[0] else base
     if args.impl == 'reference':
         if rank != 0:
             return
         # Each step is a bounded sample: a 128^3 lattice with 1/8 of the beads (the same densities and per-node
         # work); the reference takes ~30 s per step of the full 256^3 fluid on one core.
-        sample = sample_of(w, min(w.n, 128))
+        sample = w.sample(min(w.shape[0], 128))
         value, kind, dt = run_cpu(args, sample, args.steps, args.warmup)
         print(json.dumps({
-            'metric': 'MLUPS (fluid nodes x lattice steps / s) of the coupled lattice step', 'impl': 'reference',
+            'metric': metric_name(w), 'impl': 'reference',
             'value': value, 'unit': 'MLUPS', 'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': dt*1e3, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
             'data': 'synthetic', 'config': {'workload': w.name(), 'sample': sample.name()},
@@ -385,7 +457,7 @@ def main():
         torch.distributed.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
     result = run_b200(args, w, rank, world, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sample = sample_of(w, min(w.n, 128))
+        sample = w.sample(min(w.shape[0], 128))
         value, kind, dt = run_cpu(args, sample, 2, 1)
         result['cpu_baseline'] = {'value': value, 'unit': 'MLUPS', 'cores': 1, 'kind': kind,
                                   'sample': 'two timed steps after one warm-up of %s' % sample.name()}

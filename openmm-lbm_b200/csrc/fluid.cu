@@ -92,6 +92,9 @@ __device__ __forceinline__ int czr(int q) { return czOf(q); }
 // Pi_neq = sum_q H2(c_q) df_q - j j/rho (xx, yy, zz, xy, xz, yz).  For the D3Q19 second-order
 // equilibrium, sum_q H2(c_q) (feq_q - w_q) = j j/rho exactly, so this equals the reference's
 // sum_q H2(c_q) (df_q - dfeq_q) (D3Q19.h:98-110).
+__device__ __forceinline__ double reciprocal(double x) { return 1.0/x; }
+__device__ __forceinline__ float reciprocal(float x) { return __fdividef(1.0f, x); }
+
 template <typename R>
 struct Moments {
     R dr, jx, jy, jz, pxx, pyy, pzz, pxy, pxz, pyz;
@@ -208,12 +211,49 @@ template <typename R> constexpr int denseMinBlocks() { return LBM_DENSE_MIN_BLOC
 template <typename R> constexpr int denseMinBlocks() { return sizeof(R) == 4 ? 4 : 2; }
 #endif
 
+// Moments of the 19 pulled values r_q in storage units (deviation = scale_q r_q), summed over the opposite
+// pairs (q, q+1): S = r_q + r_{q+1} feeds the even moments and D = r_q - r_{q+1} the momentum, with the
+// scales folded into the FMAs.
+template <typename T, typename R>
+__device__ __forceinline__ Moments<R> momentsOfRaw(const R r[19]) {
+    R dr = R(Storage<T>::template scale<0>())*r[0];
+    R jx = 0, jy = 0, jz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+    staticFor<9>([&](auto pc) {
+        constexpr int q = 2*decltype(pc)::value + 1;
+        constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+        constexpr R s = R(Storage<T>::template scale<q>());
+        R S = r[q] + r[q+1], D = r[q] - r[q+1];
+        dr += s*S;
+        if (cx != 0) { jx += R(cx)*s*D; sxx += s*S; }
+        if (cy != 0) { jy += R(cy)*s*D; syy += s*S; }
+        if (cz != 0) { jz += R(cz)*s*D; szz += s*S; }
+        if (cx*cy != 0) sxy += R(cx*cy)*s*S;
+        if (cx*cz != 0) sxz += R(cx*cz)*s*S;
+        if (cy*cz != 0) syz += R(cy*cz)*s*S;
+    });
+    Moments<R> m;
+    R inv = reciprocal(R(1) + dr);
+    R third = dr*R(1.0/3.0);
+    m.dr = dr; m.jx = jx; m.jy = jy; m.jz = jz;
+    m.pxx = sxx - third - jx*jx*inv;
+    m.pyy = syy - third - jy*jy*inv;
+    m.pzz = szz - third - jz*jz*inv;
+    m.pxy = sxy - jx*jy*inv;
+    m.pxz = sxz - jx*jz*inv;
+    m.pyz = syz - jy*jz*inv;
+    return m;
+}
+
+// The dense step over 32 x 8 node tiles (lane = x, warp = y), persistent blocks striding over the tiles.  Node
+// indices are 32-bit (the host limits the lattice to 2^32 nodes); the tile coordinates advance by the grid
+// stride without divisions, and the periodic pull sources are node + per-node offsets in x, y and z.
 template <typename T, typename R, bool SOLID, bool REACT, bool FLUCT>
 __global__ void __launch_bounds__(THREADS, denseMinBlocks<R>())
 streamCollideKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int remove, long long step) {
     const int lane = threadIdx.x%32, warp = threadIdx.x/32;
-    const long long N = v.n;
+    const unsigned N = (unsigned) v.n;
     const int nx = v.nx, ny = v.ny, nz = v.nz;
+    const unsigned sxy = (unsigned) nx*(unsigned) ny;
     const R omega = R(v.omega), om1 = R(1) - omega;
     const R gx = R(v.g[0]), gy = R(v.g[1]), gz = R(v.g[2]);
     R ux0 = 0, uy0 = 0, uz0 = 0;
@@ -227,35 +267,44 @@ streamCollideKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int
         muR = R(v.mu);
         stressFactor = omega*(R(2) - omega);
     }
-    double acc[NPART] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (long long t = blockIdx.x; t < v.numTiles; t += gridDim.x) {
-        int tx = (int) (t%v.tilesX);
-        long long rr = t/v.tilesX;
-        int ty = (int) (rr%v.tilesY);
-        int z = (int) (rr/v.tilesY);
-        int x = tx*TX + lane, y = ty*TY + warp;
+    R sumMass = 0, sumX = 0, sumY = 0, sumZ = 0;
+    const unsigned numTiles = (unsigned) v.numTiles, stride = gridDim.x;
+    const int tilesX = v.tilesX, tilesY = v.tilesY;
+    int tx = (int) (blockIdx.x%tilesX), ty = (int) ((blockIdx.x/tilesX)%tilesY), tz = (int) (blockIdx.x/tilesX/tilesY);
+    const int dtx = (int) (stride%tilesX), dty = (int) ((stride/tilesX)%tilesY), dtz = (int) (stride/tilesX/tilesY);
+    constexpr bool dithered = sizeof(T) == 2;
+    for (unsigned t = blockIdx.x; t < numTiles; t += stride) {
+        const int x = tx*TX + lane, y = ty*TY + warp, z = tz, tileX = tx;
+        tx += dtx;
+        int carry = tx >= tilesX;
+        tx -= carry ? tilesX : 0;
+        ty += dty + carry;
+        carry = ty >= tilesY;
+        ty -= carry ? tilesY : 0;
+        tz += dtz + carry;
         if (x >= nx || y >= ny)
             continue;
-        long long row = (long long) z*ny + y;
+        const unsigned row = (unsigned) z*ny + y;
         if (SOLID) {
-            uint32_t word = __ldg(&v.solidMask[row*v.wordsPerRow + tx]);
+            uint32_t word = __ldg(&v.solidMask[(size_t) row*v.wordsPerRow + tileX]);
             if ((word >> lane) & 1u)
                 continue;
         }
-        long long node = row*nx + x;
-        // Source rows and columns of the pull, periodic: index 0 is the coordinate - 1, 2 is + 1.
-        int xs[3] = {x == 0 ? nx-1 : x-1, x, x == nx-1 ? 0 : x+1};
-        int ys[3] = {y == 0 ? ny-1 : y-1, y, y == ny-1 ? 0 : y+1};
-        int zs[3] = {z == 0 ? nz-1 : z-1, z, z == nz-1 ? 0 : z+1};
-        R f[19];
+        const unsigned node = row*nx + x;
+        // Offsets (mod 2^32) from the node to the pull sources x - c: index 0 for c = +1, 2 for c = -1.
+        const unsigned ox[3] = {x == 0 ? (unsigned) (nx - 1) : ~0u, 0u, x == nx - 1 ? (unsigned) (1 - nx) : 1u};
+        const unsigned oy[3] = {y == 0 ? (unsigned) (ny - 1)*nx : (unsigned) -nx, 0u,
+                                y == ny - 1 ? (unsigned) (1 - ny)*nx : (unsigned) nx};
+        const unsigned oz[3] = {z == 0 ? (unsigned) (nz - 1)*sxy : 0u - sxy, 0u, z == nz - 1 ? 0u - (unsigned) (nz - 1)*sxy : sxy};
+        R r[19];
         staticFor<19>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
             constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
-            long long src = ((long long) zs[1-cz]*ny + ys[1-cy])*nx + xs[1-cx];
-            f[q] = Storage<T>::template load<q>(A + (long long) q*N + src);
+            const unsigned src = node + ox[1-cx] + oy[1-cy] + oz[1-cz];
+            r[q] = Storage<T>::template raw<q>(A + ((size_t) q*N + src));
         });
-        Moments<R> m = momentsOf<R>(f);
-        R rho = R(1) + m.dr, inv = R(1)/rho;
+        Moments<R> m = momentsOfRaw<T, R>(r);
+        R rho = R(1) + m.dr, inv = reciprocal(rho);
         R jx = m.jx, jy = m.jy, jz = m.jz;
         if (remove) {
             jx -= rho*ux0;
@@ -264,9 +313,9 @@ streamCollideKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int
         }
         R Fx = rho*gx, Fy = rho*gy, Fz = rho*gz;
         if (REACT) {
-            uint32_t word = __ldg(&v.reactMask[row*v.wordsPerRow + tx]);
+            uint32_t word = __ldg(&v.reactMask[(size_t) row*v.wordsPerRow + tileX]);
             if ((word >> lane) & 1u) {
-                const R* rp = reinterpret_cast<const R*>(v.reaction) + 4*node;
+                const R* rp = reinterpret_cast<const R*>(v.reaction) + 4*(size_t) node;
                 Fx += rp[0];
                 Fy += rp[1];
                 Fz += rp[2];
@@ -274,6 +323,9 @@ streamCollideKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int
         }
         R ux = (jx + R(0.5)*Fx)*inv, uy = (jy + R(0.5)*Fy)*inv, uz = (jz + R(0.5)*Fz)*inv;
         R uu = ux*ux + uy*uy + uz*uz, uf = ux*Fx + uy*Fy + uz*Fz;
+        // The odd part 3 w_q (rho c.u + c.F/2) = 3 w_q c.(j + F) is built from the momentum after the force, not
+        // through u = (j + F/2)/rho: a rounded rho*(1/rho) would scale the momentum by a fixed factor every step.
+        const R px = jx + Fx, py = jy + Fy, pz = jz + Fz;
         // The regularized non-equilibrium part (1 - omega) 4.5 w_q H2(c_q):Pi_neq and the random stress modes
         // w_q sum_{k=4..9} e_k(c_q) a_k are both quadratic forms in c_q: they are merged into one tensor Q, so that
         // each direction evaluates w_q (c Q c - tr Q/3) once.  The ghost modes (k = 10..18) are added per direction.
@@ -282,56 +334,63 @@ streamCollideKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int
         R qxy = s9*m.pxy, qxz = s9*m.pxz, qyz = s9*m.pyz;
         R a[15];
         if (FLUCT) {
-            R r[15];
-            philoxNormals<R, 15>(v.seed, PurposeFluid, node, step, r);
+            R rn[15];
+            philoxNormals<R, 15>(v.seed, PurposeFluid, node, step, rn);
             R ghost = sqrt(muR*rho);
-            modeAmplitudes<R>(r, sqrt(muR*rho*stressFactor), ghost, a);
+            modeAmplitudes<R>(rn, sqrt(muR*rho*stressFactor), ghost, a);
             qxx += a[0]; qyy += a[1]; qzz += a[2];
             qxy += a[3]; qxz += a[4]; qyz += a[5];
         }
         R qtr = (qxx + qyy + qzz)*R(1.0/3.0);
+        // Terms common to all directions: dr - 1.5 rho u.u - 1.5 u.F.
+        const R base = m.dr - R(1.5)*(rho*uu + uf);
         R outMass = 0, outX = 0, outY = 0, outZ = 0;
+        // Stochastic rounding of the 16-bit stores: one dither word per pair of directions.
+        Dither dither(dithered ? node : 0, dithered ? step : 0);
         // q = 0
         {
-            R value = R(1.0/3.0)*(m.dr - R(1.5)*rho*uu - qtr) - R(0.5/3.0)*R(3)*uf;
+            R value = R(1.0/3.0)*(base - qtr);
             if (FLUCT) {
                 R e, o;
                 ghostParts<R, 0>(a, e, o);
                 value += e;
             }
-            R stored = Storage<T>::template store<0>(B + node, value);
-            outMass += stored;
+            R stored = Storage<T>::template storeOne<0>(B + node, value, dithered ? dither.next() : 0u);
+            outMass += R(Storage<T>::template scale<0>())*stored;
         }
         // Pairs (q, q+1) with c_{q+1} = -c_q.
         staticFor<9>([&](auto pc) {
             constexpr int q = 2*decltype(pc)::value + 1;
             constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
             constexpr R w = wOf<R>(q);
+            constexpr R s = R(Storage<T>::template scale<q>());
             R cu = R(cx)*ux + R(cy)*uy + R(cz)*uz;
             R cf = R(cx)*Fx + R(cy)*Fy + R(cz)*Fz;
             R cqc = R(cx*cx)*qxx + R(cy*cy)*qyy + R(cz*cz)*qzz - qtr
                   + R(cx*cy)*qxy + R(cx*cz)*qxz + R(cy*cz)*qyz;
-            R even = w*(m.dr + rho*(R(4.5)*cu*cu - R(1.5)*uu) + cqc + R(0.5)*(R(9)*cu*cf - R(3)*uf));
-            R odd = R(3)*w*(rho*cu + R(0.5)*cf);
+            R even = w*(base + cqc + R(4.5)*cu*(rho*cu + cf));
+            R odd = oddOf<R>(q)*(R(cx)*px + R(cy)*py + R(cz)*pz);
             if (FLUCT) {
                 R e, o;
                 ghostParts<R, q>(a, e, o);
                 even += e;
                 odd += o;
             }
-            R s1 = Storage<T>::template store<q>(B + (long long) q*N + node, even + odd);
-            R s2 = Storage<T>::template store<q+1>(B + (long long) (q+1)*N + node, even - odd);
-            outMass += s1 + s2;
-            R d = s1 - s2;
+            R s1, s2;
+            Storage<T>::template storePair<q>(B + ((size_t) q*N + node), B + ((size_t) (q+1)*N + node), even + odd,
+                                              even - odd, dithered ? dither.next() : 0u, s1, s2);
+            outMass += s*(s1 + s2);
+            R d = s*(s1 - s2);
             if (cx != 0) outX += R(cx)*d;
             if (cy != 0) outY += R(cy)*d;
             if (cz != 0) outZ += R(cz)*d;
         });
-        acc[0] += (double) outMass;
-        acc[1] += (double) outX;
-        acc[2] += (double) outY;
-        acc[3] += (double) outZ;
+        sumMass += outMass;
+        sumX += outX;
+        sumY += outY;
+        sumZ += outZ;
     }
+    double acc[NPART] = {(double) sumMass, (double) sumX, (double) sumY, (double) sumZ, 0, 0, 0, 0};
     blockReduceStore(acc, v.partials + NPART*(long long) blockIdx.x);
 }
 
@@ -834,6 +893,10 @@ FluidEngine::FluidEngine(const LbmLatticeParameters& l, int storage, const Geome
     view.ny = l.ny;
     view.nz = l.nz;
     view.n = (long long) l.nx*l.ny*l.nz;
+    // The dense kernel indexes nodes with 32-bit unsigned integers (4.29e9 nodes: 163 GB of FP16 populations).
+    if (view.n >= (1LL << 32) || (long long) l.nx*l.ny >= (1LL << 31))
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "The lattice has too many nodes for one device (at most 2^32 nodes, "
+                    "and nx*ny below 2^31)");
     view.wordsPerRow = (l.nx + 31)/32;
     view.tilesX = (l.nx + TX - 1)/TX;
     view.tilesY = (l.ny + TY - 1)/TY;

@@ -20,59 +20,139 @@ LBM_HD constexpr int cyOf(int q) { return (q == 3 || q == 7 || q == 10 || q == 1
 LBM_HD constexpr int czOf(int q) { return (q == 5 || q == 11 || q == 14 || q == 15 || q == 17) ? 1 : (q == 6 || q == 12 || q == 13 || q == 16 || q == 18) ? -1 : 0; }
 LBM_HD constexpr int oppOf(int q) { return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1); }
 template <typename R> LBM_HD constexpr R wOf(int q) { return q == 0 ? R(1.0/3.0) : (q <= 6 ? R(1.0/18.0) : R(1.0/36.0)); }
+// Power-of-two stand-ins for 1/w_q (4, 16, 32): the 16-bit formats store the deviation times this factor, so
+// that decoding is the exact inverse of encoding.
+LBM_HD constexpr float storeFactorOf(int q) { return q == 0 ? 4.0f : (q <= 6 ? 16.0f : 32.0f); }
+LBM_HD constexpr float loadFactorOf(int q) { return q == 0 ? 0.25f : (q <= 6 ? 0.0625f : 0.03125f); }
+// Coefficients 3 w_q of the odd (momentum) part of the equilibrium, rounded so that the momentum they
+// rebuild is exact: sum_q c_qx c_qx 3 w_q = 2 (axis + 4 diagonal) = 1 holds in floating point, with the
+// diagonal value the nearest to 1/12 and the axis value 1/2 - 4 diag (exact).  With the rounded 3 w_q of
+// float, each step would scale the momentum by 1 + 3e-8, which a flow accelerated from rest accumulates.
+template <typename R> LBM_HD constexpr R oddDiagonal() { return R(1.0/12.0); }
+template <typename R> LBM_HD constexpr R oddAxis() { return R(0.5) - R(4)*oddDiagonal<R>(); }
+template <typename R> LBM_HD constexpr R oddOf(int q) { return q <= 6 ? oddAxis<R>() : oddDiagonal<R>(); }
 
 // ------------------------------------------------------------------------------------------------------
-// Storage of the deviations f_q - w_q.  FP64 and FP32 store the deviation itself.  FP16 stores the
-// deviation divided by w_q, which lifts the small deviations of the diagonal directions away from the
-// subnormal range of binary16; BF16 stores the same scaled value.
+// Storage of the deviations f_q - w_q.  FP64 and FP32 store the deviation itself, rounded to nearest.
+// The 16-bit formats store v = (f_q - w_q) k_q with k_q = 4, 16, 32 (rest, axis, diagonal), powers of two
+// near 1/w_q, which give all 19 directions values of one magnitude and make decoding exact.  FP16 stores
+// v * 2^10, so that the binary16 normal range starts at |v| = 2^-24 and ends at |v| = 64, and BF16 (the
+// exponent range of FP32) stores v itself.
+//
+// The dense kernel rounds its 16-bit stores stochastically: 13 (FP16) or 16 (BF16) dither bits are added to
+// the magnitude of the FP32 value, which is then truncated.  The stored value is the upper or the lower
+// neighbour of v with probabilities proportional to the distances, so the expected rounding error is zero.
+// Round-to-nearest would lose every change of a population smaller than half an ulp (1/2048 of the value in
+// FP16, 1/256 in BF16): a flow accelerated from rest by a small body force stalls once the per-step change
+// of its populations falls below that.  The dither bits of a store are a hash of (node, step), so runs are
+// reproducible and restarts from a checkpoint are bitwise.  The sparse kernels (boundaries, state transfer)
+// round to nearest.
 // ------------------------------------------------------------------------------------------------------
 
+constexpr float kHalfScale = 1024.0f;
+
+// Storage<T>: raw<q>(p) loads the stored value in storage units, scale<q>() converts storage units to a
+// deviation (a compile-time constant that the moment sums fold into their FMAs), storePair<q> stores the
+// deviations of directions q and q+1 (equal weights) and returns what was stored, in storage units.
 template <typename T> struct Storage;
 template <> struct Storage<double> {
-    template <int q> static __device__ __forceinline__ double load(const double* p) { return __ldg(p); }
-    template <int q> static __device__ __forceinline__ double store(double* p, double v) { *p = v; return v; }
-    template <int q> static __device__ __forceinline__ double decode(double v) { return v; }
-    template <int q> static __device__ __forceinline__ double encode(double v) { return v; }
+    template <int q> static LBM_HD constexpr double scale() { return 1.0; }
+    template <int q> static __device__ __forceinline__ double raw(const double* p) { return __ldg(p); }
+    template <int q> static __device__ __forceinline__ double storeOne(double* p, double v, uint32_t) { *p = v; return v; }
+    template <int q> static __device__ __forceinline__ void storePair(double* pa, double* pb, double a, double b, uint32_t,
+                                                                      double& ra, double& rb) {
+        *pa = a; *pb = b; ra = a; rb = b;
+    }
 };
 template <> struct Storage<float> {
-    template <int q> static __device__ __forceinline__ float load(const float* p) { return __ldg(p); }
-    template <int q> static __device__ __forceinline__ float store(float* p, float v) { *p = v; return v; }
-    template <int q> static __device__ __forceinline__ float decode(float v) { return v; }
-    template <int q> static __device__ __forceinline__ float encode(float v) { return v; }
+    template <int q> static LBM_HD constexpr float scale() { return 1.0f; }
+    template <int q> static __device__ __forceinline__ float raw(const float* p) { return __ldg(p); }
+    template <int q> static __device__ __forceinline__ float storeOne(float* p, float v, uint32_t) { *p = v; return v; }
+    template <int q> static __device__ __forceinline__ void storePair(float* pa, float* pb, float a, float b, uint32_t,
+                                                                      float& ra, float& rb) {
+        *pa = a; *pb = b; ra = a; rb = b;
+    }
 };
 template <> struct Storage<__half> {
-    template <int q> static __device__ __forceinline__ float decode(__half h) { return __half2float(h)*wOf<float>(q); }
-    template <int q> static __device__ __forceinline__ __half encode(float v) { return __float2half_rn(v*(1.0f/wOf<float>(q))); }
-    template <int q> static __device__ __forceinline__ float load(const __half* p) { return decode<q>(__ldg(p)); }
-    // Returns the value actually stored, so that sums see what the next step reads.
-    template <int q> static __device__ __forceinline__ float store(__half* p, float v) { __half h = encode<q>(v); *p = h; return decode<q>(h); }
+    template <int q> static LBM_HD constexpr float scale() { return loadFactorOf(q)*(1.0f/kHalfScale); }
+    template <int q> static __device__ __forceinline__ float raw(const __half* p) { return __half2float(__ldg(p)); }
+    template <int q> static __device__ __forceinline__ float storeOne(__half* p, float v, uint32_t dither) {
+        uint32_t bits = __float_as_uint(v*(kHalfScale*storeFactorOf(q))) + (dither & 0x1FFFu);
+        __half h = __float2half_rz(__uint_as_float(bits));
+        *p = h;
+        return __half2float(h);
+    }
+    template <int q> static __device__ __forceinline__ void storePair(__half* pa, __half* pb, float a, float b,
+                                                                      uint32_t dither, float& ra, float& rb) {
+        uint32_t ba = __float_as_uint(a*(kHalfScale*storeFactorOf(q))) + (dither & 0x1FFFu);
+        uint32_t bb = __float_as_uint(b*(kHalfScale*storeFactorOf(q))) + ((dither >> 16) & 0x1FFFu);
+        uint32_t packed;
+        asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(packed) : "f"(__uint_as_float(bb)), "f"(__uint_as_float(ba)));
+        *reinterpret_cast<unsigned short*>(pa) = (unsigned short) (packed & 0xFFFFu);
+        *reinterpret_cast<unsigned short*>(pb) = (unsigned short) (packed >> 16);
+        __half2 h2 = *reinterpret_cast<__half2*>(&packed);
+        float2 back = __half22float2(h2);
+        ra = back.x;
+        rb = back.y;
+    }
 };
 template <> struct Storage<__nv_bfloat16> {
-    template <int q> static __device__ __forceinline__ float decode(__nv_bfloat16 h) { return __bfloat162float(h)*wOf<float>(q); }
-    template <int q> static __device__ __forceinline__ __nv_bfloat16 encode(float v) { return __float2bfloat16_rn(v*(1.0f/wOf<float>(q))); }
-    template <int q> static __device__ __forceinline__ float load(const __nv_bfloat16* p) { return decode<q>(__ldg(p)); }
-    template <int q> static __device__ __forceinline__ float store(__nv_bfloat16* p, float v) { __nv_bfloat16 h = encode<q>(v); *p = h; return decode<q>(h); }
+    template <int q> static LBM_HD constexpr float scale() { return loadFactorOf(q); }
+    template <int q> static __device__ __forceinline__ float raw(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
+    template <int q> static __device__ __forceinline__ float storeOne(__nv_bfloat16* p, float v, uint32_t dither) {
+        uint32_t bits = __float_as_uint(v*storeFactorOf(q)) + (dither & 0xFFFFu);
+        *reinterpret_cast<unsigned short*>(p) = (unsigned short) (bits >> 16);
+        return __uint_as_float(bits & 0xFFFF0000u);
+    }
+    template <int q> static __device__ __forceinline__ void storePair(__nv_bfloat16* pa, __nv_bfloat16* pb, float a, float b,
+                                                                      uint32_t dither, float& ra, float& rb) {
+        uint32_t ba = __float_as_uint(a*storeFactorOf(q)) + (dither & 0xFFFFu);
+        uint32_t bb = __float_as_uint(b*storeFactorOf(q)) + (dither >> 16);
+        *reinterpret_cast<unsigned short*>(pa) = (unsigned short) (ba >> 16);
+        *reinterpret_cast<unsigned short*>(pb) = (unsigned short) (bb >> 16);
+        ra = __uint_as_float(ba & 0xFFFF0000u);
+        rb = __uint_as_float(bb & 0xFFFF0000u);
+    }
 };
 
-// Runtime-q versions (slow paths: boundaries, state transfer).
+// Dither words of the stores of one node and step: the MurmurHash3 32-bit finaliser (Appleby) of the node
+// and step mixed together seeds a xorshift32 stream (Marsaglia 2003, shifts 13, 17, 5); each word serves two
+// stores (low and high halves).
+struct Dither {
+    uint32_t state;
+    static __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+        h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
+        return h;
+    }
+    __device__ __forceinline__ Dither(long long node, long long step) {
+        uint32_t h = fmix32((uint32_t) node ^ fmix32((uint32_t) step + 0x9E3779B9u*(uint32_t) ((unsigned long long) node >> 32)));
+        state = h ? h : 0x6A09E667u;
+    }
+    __device__ __forceinline__ uint32_t next() {
+        state ^= state << 13; state ^= state >> 17; state ^= state << 5;
+        return state;
+    }
+};
+
+// Runtime-q versions (slow paths: boundaries, state transfer), rounded to nearest.
 template <typename T, typename R> __device__ __forceinline__ R loadq(const T* p, int q);
 template <typename T, typename R> __device__ __forceinline__ void storeq(T* p, int q, R v);
 
 template <> __device__ __forceinline__ double loadq<double, double>(const double* p, int) { return *p; }
 template <> __device__ __forceinline__ float loadq<float, float>(const float* p, int) { return *p; }
 template <> __device__ __forceinline__ float loadq<__half, float>(const __half* p, int q) {
-    return __half2float(*p)*(q == 0 ? 1.0f/3.0f : (q <= 6 ? 1.0f/18.0f : 1.0f/36.0f));
+    return __half2float(*p)*(loadFactorOf(q)*(1.0f/kHalfScale));
 }
 template <> __device__ __forceinline__ float loadq<__nv_bfloat16, float>(const __nv_bfloat16* p, int q) {
-    return __bfloat162float(*p)*(q == 0 ? 1.0f/3.0f : (q <= 6 ? 1.0f/18.0f : 1.0f/36.0f));
+    return __bfloat162float(*p)*loadFactorOf(q);
 }
 template <> __device__ __forceinline__ void storeq<double, double>(double* p, int, double v) { *p = v; }
 template <> __device__ __forceinline__ void storeq<float, float>(float* p, int, float v) { *p = v; }
 template <> __device__ __forceinline__ void storeq<__half, float>(__half* p, int q, float v) {
-    *p = __float2half_rn(v*(q == 0 ? 3.0f : (q <= 6 ? 18.0f : 36.0f)));
+    *p = __float2half_rn(v*(kHalfScale*storeFactorOf(q)));
 }
 template <> __device__ __forceinline__ void storeq<__nv_bfloat16, float>(__nv_bfloat16* p, int q, float v) {
-    *p = __float2bfloat16_rn(v*(q == 0 ? 3.0f : (q <= 6 ? 18.0f : 36.0f)));
+    *p = __float2bfloat16_rn(v*storeFactorOf(q));
 }
 
 // ------------------------------------------------------------------------------------------------------

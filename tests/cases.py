@@ -180,3 +180,35 @@ def total_momentum(context, force):
     mass, j = total_moments(force.getFluidState(context))
     cell_mass = force.getFluidDensity()*FLUID_DX**3
     return p + j*(cell_mass*FLUID_DX/FLUID_DT)
+
+
+# The precision channel: a Poiseuille channel between bounce-back planes z = 0 and z = nz - 1 driven by the Guo body
+# force g_x, in lattice units (dx = dt = rho0 = 1), no momentum removal, no fluctuations, started from rest.
+CHANNEL_SHAPE, CHANNEL_TAU, CHANNEL_G, CHANNEL_STEPS = (384, 384, 192), 0.55, 5e-7, 20000
+
+
+def channel_kernel(shape, precision, tau=CHANNEL_TAU, g=CHANNEL_G):
+    nx, ny, nz = shape
+    force = LBMForce()
+    force.setGridSize(nx, ny, nz)
+    force.setFluidDensity(1.0)
+    force.setKinematicViscosity((tau - 0.5)/3.0)
+    force.setBodyAcceleration((g, 0.0, 0.0))
+    force.setFluidMomentumRemovalFrequency(0)
+    lattice = force.latticeParameters(np.array(shape, dtype=float), 1.0, np.ones(1))
+    plane = np.arange(nx*ny, dtype=np.int64)
+    solids = np.concatenate([plane, plane + nx*ny*(nz - 1)])
+    return lbm_b200.B200Kernel(lattice, [], solids, precision)
+
+
+def channel_startup_profile(nz, tau, g, t, terms=4001):
+    """u_x(z) at time t of the channel flow started from rest, walls halfway between the solid and the first fluid
+    planes (h = nz - 2): the steady parabola minus its decaying odd sine modes,
+    u = g/(2 nu) s (h - s) - sum_{n odd} 4 g h^2/(nu pi^3 n^3) sin(n pi s/h) exp(-nu n^2 pi^2 t/h^2), s = z - 1/2."""
+    nu, h = (tau - 0.5)/3.0, nz - 2
+    s = np.arange(nz) - 0.5
+    u = g/(2*nu)*s*(h - s)
+    n = np.arange(1, terms + 1, 2, dtype=float)[:, None]
+    u -= (4*g*h*h/(nu*np.pi**3*n**3)*np.sin(n*np.pi*s/h)*np.exp(-nu*n*n*np.pi**2*t/(h*h))).sum(axis=0)
+    u[0] = u[-1] = 0.0
+    return u
