@@ -1,8 +1,9 @@
 """Benchmark of the per-step fluid and particle-coupling path on B200: MLUPS, and the HBM roofline of the dense
 stream-collide kernel.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload coupled|fluid|channel]
-                    [--precision double|single|half|bfloat16] [--size EDGE]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload coupled|fluid|channel|batch] [--precision double|single|half|bfloat16] [--size EDGE]
+                    [--graph-steps G] [--replicas R] [--separate]
 
 Workload "coupled" (default, the scale configuration): a 256^3 periodic fluctuating D3Q19 fluid (tau 0.6, kT 1e-4 in
 lattice units, Philox seed), FP32 storage, momentum removal every step, Mach check every 100 steps; 512 bead-spring
@@ -11,7 +12,9 @@ and WCA repulsion (sigma 1, epsilon = kT), coupled through the Keys stencil with
 lattice step, solved by conjugate gradients on the device).  One step: beginStep, bead forces, execute (coupling +
 fluid) and the leapfrog of the beads, all on the device.  "fluid": the fluid alone (kernel profiling).  "channel": the
 precision configuration, a 384x384x192 Poiseuille channel between bounce-back planes (g_x 5e-7, tau 0.55), for the
-MLUPS of each storage format.
+MLUPS of each storage format.  "batch": the batching configuration, 256 periodic fluctuating replicas of uneven sizes
+with Lennard-Jones beads, every phase one launch over all replicas, G steps per CUDA graph (--separate also times the
+replicas as separate kernels).
 
 value = fluid nodes x steps / device time (MLUPS).  e2e = the same metric through the C ABI with the beads' positions
 and velocities in pinned host memory: copied to the device before and back after every step.  With N > 1 (torchrun,
@@ -149,6 +152,185 @@ class ChannelWorkload:
     def sample(self, n):
         """A sample with the same aspect ratio and edge n in x."""
         return ChannelWorkload((n, n, max(4, n//2)))
+
+
+class BatchWorkload:
+    """The batching configuration: replicas with seeded-uniform cubic edges 16..64 and bead counts 20..200 (numpy PCG64,
+    seed 2026), each a periodic fluctuating fluid (tau 0.7, kT 1e-4, its own Philox seed) with Lennard-Jones beads
+    (sigma 1, epsilon kT, cutoff 2.5, mass 1) at random non-overlapping positions, three-point stencil, explicit drag
+    0.8 (lattice units)."""
+
+    def __init__(self, replicas=256, seed=2026):
+        rng = np.random.Generator(np.random.PCG64(seed))
+        self.replicas, self.seed = replicas, seed
+        self.sizes = rng.integers(16, 65, replicas)
+        self.beads = rng.integers(20, 201, replicas)
+        self.tau, self.kT, self.friction = 0.7, 1e-4, 0.8
+        self.coupled, self.chains, self.length = True, 0, 0
+        self.n = int(self.sizes.max())
+
+    def name(self):
+        return ('%d replicas, cubic edges U{16..64} and U{20..200} Lennard-Jones beads (seed %d): periodic fluctuating '
+                'D3Q19, tau 0.7, kT 1e-4, three-point stencil, explicit drag 0.8 (lattice units)' % (self.replicas, self.seed))
+
+    def fluid_nodes(self):
+        return int((self.sizes.astype(np.int64)**3).sum())
+
+    def lattices(self, lbm):
+        out = []
+        for r, (n, b) in enumerate(zip(self.sizes, self.beads)):
+            force = lbm.LBMForce()
+            force.setGridSize(int(n), int(n), int(n))
+            force.setFluidDensity(1.0)
+            force.setKinematicViscosity((self.tau - 0.5)/3.0)
+            force.setFluidFluctuations(True)
+            force.setTemperature(self.kT/BOLTZ)
+            force.setRandomNumberSeed(self.seed + 1 + r)
+            force.setInterpolationStencil(force.ThreePoint)
+            force.setDragScheme(force.Explicit)
+            force.setFriction(self.friction)
+            for i in range(int(b)):
+                force.addParticle(i)
+            out.append(force.latticeParameters(np.array([n, n, n], dtype=float), 1.0, np.ones(int(b))))
+        return out
+
+    def positions(self, min_distance=1.0):
+        rng = np.random.Generator(np.random.PCG64(self.seed + 1))
+        out = []
+        for n, b in zip(self.sizes, self.beads):
+            pts = np.zeros((0, 3))
+            while len(pts) < b:
+                x = rng.uniform(0, n, 3)
+                d = pts - x
+                d -= n*np.round(d/n)
+                if len(pts) == 0 or (d*d).sum(axis=1).min() >= min_distance**2:
+                    pts = np.vstack([pts, x])
+            out.append(pts)
+        return out
+
+    def sample(self, n):
+        return BatchWorkload(replicas=n, seed=self.seed)
+
+
+def run_batch(args, w, rank, world, device):
+    """The replica batch: every phase one launch over all replicas, runs of graph_steps steps replayed from a CUDA
+    graph; the dense kernel's block size chosen by the autotuner."""
+    import torch
+    lbm = load_package()
+    torch.cuda.set_device(device)
+    stream = torch.cuda.Stream()
+    lattices = w.lattices(lbm)
+    positions = w.positions()
+    beads = int(w.beads.sum())
+    batch = lbm.ReplicaBatch(lattices, w.beads, np.ones(beads), np.concatenate(positions),
+                             pair=('lj', 1.0, w.kT, 2.5), precision=args.precision, device=device,
+                             stream=stream.cuda_stream)
+    graph_steps = args.graph_steps
+    threads, dense_ms = batch.autotune(graph_steps)
+    batch.step(max(args.warmup, 3)*graph_steps)
+    torch.cuda.synchronize()
+    launches0 = batch.info()['launches']
+    clock_path = os.path.join(tempfile.gettempdir(), 'lbm_clocks_%d.csv' % rank)
+    sampler = start_clock_sampler(clock_path) if rank == 0 else None
+    time.sleep(0.5 if sampler else 0.0)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    batch.step(args.steps)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = stop_clock_sampler(sampler, clock_path, device) if sampler else None
+    ms = start.elapsed_time(stop)
+    launches = batch.info()['launches'] - launches0
+    if world > 1:
+        t = torch.tensor([ms], device='cuda')
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    # End to end through the C ABI: every run of graph_steps steps takes the beads' velocities from host memory and
+    # returns their positions and velocities to host memory.
+    pos_h, vel_h = batch.particles_state()
+    chunks = max(1, args.steps//graph_steps)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(chunks):
+        batch.set_velocities(vel_h)
+        batch.step(graph_steps)
+        pos_h, vel_h = batch.particles_state()
+    e2e_s = time.perf_counter() - t0
+    fluid_kT, bead_kT = batch.temperatures()
+    nodes = w.fluid_nodes()
+    observables = {'fluid_kT_over_kT_mean': float(np.mean(fluid_kT)/w.kT),
+                   'fluid_kT_over_kT_range': [float(fluid_kT.min()/w.kT), float(fluid_kT.max()/w.kT)],
+                   'bead_kT_over_kT_mean': float(np.mean(bead_kT)/w.kT),
+                   'steps_run': int(batch.info()['steps'])}
+    batch.close()
+    if args.separate:
+        observables['separate_launches_mlups'] = separate_launch_mlups(lbm, w, lattices, positions, args.precision, 3)
+    bytes_per_node = 2*19*STORAGE_BYTES[args.precision]
+    achieved = bytes_per_node*nodes/(dense_ms*1e-3)/1e9
+    peak, peak_kind = peaks()
+    v3 = 3*8*beads
+    return {
+        'metric': 'MLUPS (fluid nodes x lattice steps / s) of the batched replica step',
+        'value': world*nodes*args.steps/(ms*1e-3)/1e6, 'unit': 'MLUPS', 'n_gpus': world, 'steps': args.steps,
+        'warmup': max(args.warmup, 3)*graph_steps, 'ms_per_step': ms/args.steps, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': DTYPE[args.precision],
+        'data': 'synthetic: seeded replica sizes, bead counts and positions, thermal noise from Philox',
+        'config': {'workload': w.name(), 'replicas': w.replicas, 'nodes_per_gpu': nodes, 'beads_per_gpu': beads,
+                   'storage': args.precision, 'graph_steps': graph_steps, 'dense_threads_per_block': threads,
+                   'l2': 'inputs larger than L2 (2 x %.2f GB of populations)' % (19*nodes*STORAGE_BYTES[args.precision]/1e9),
+                   'parallelism': 'independent replica batches, one per GPU' if world > 1 else 'single GPU'},
+        'roofline': {'bound': 'hbm', 'kernel': 'batchStreamCollideKernel', 'achieved': achieved, 'peak': peak,
+                     'unit': 'GB/s', 'frac': achieved/peak, 'peak_kind': peak_kind,
+                     'algorithmic_bytes_per_launch': bytes_per_node*nodes, 'algorithmic_bytes_per_node': bytes_per_node,
+                     'avg_launch_ms': dense_ms, 'launches': 5, 'traffic': None},
+        'e2e': {'value': world*nodes*chunks*graph_steps/e2e_s/1e6, 'unit': 'MLUPS',
+                'h2d_bytes_per_step': v3/graph_steps, 'd2h_bytes_per_step': 2*v3/graph_steps,
+                'steps': chunks*graph_steps},
+        'gpu_launches': launches,
+        'clocks': clocks,
+        'observables': observables,
+    }
+
+
+def separate_launch_mlups(lbm, w, lattices, positions, precision, steps):
+    """The same replicas as separate kernels (one B200Kernel and one BeadDynamics each, launched replica after
+    replica on one stream): MLUPS over `steps` steps after one warm-up step."""
+    import torch
+    stream = torch.cuda.Stream()
+    runs = []
+    for lattice, pos, n in zip(lattices, positions, w.sizes):
+        m = np.ones(len(pos))
+        kernel = lbm.B200Kernel(lattice, m, [], precision, stream=stream.cuda_stream)
+        md = lbm.BeadDynamics(m, (n, n, n), np.zeros((0, 2), dtype=np.int32), k=0.0, r0=1.0, pair='lj', sigma=1.0,
+                              epsilon=w.kT, cutoff=2.5)
+        p = torch.tensor(pos, device='cuda', dtype=torch.float64)
+        runs.append((kernel, md, p, torch.zeros_like(p), torch.zeros_like(p)))
+
+    def advance(s):
+        for kernel, md, p, v, f in runs:
+            kernel.begin_step(s, p, v, f)
+            md.compute_forces(p, f, stream.cuda_stream)
+            kernel.execute(s, p, v, f)
+            md.integrate(1.0, p, v, f, stream.cuda_stream)
+
+    advance(0)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for s in range(1, steps + 1):
+        advance(s)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    for kernel, md, *_ in runs:
+        kernel.close()
+        md.close()
+    return w.fluid_nodes()*steps/(ms*1e-3)/1e6
 
 
 def peaks():
@@ -412,18 +594,61 @@ def run_cpu(args, w, steps, warmup):
     return w.fluid_nodes()/dt/1e6, kind, dt
 
 
+def run_cpu_batch(w, steps, warmup, count=4):
+    """The reference's kernel (oracle/_ref; else the C restatement) on the first `count` replicas of the batch, one
+    after another on one core, with the oracle's CPU bead forces and leapfrog.  Returns (MLUPS, kind, seconds per
+    step of the sample, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    lbm = load_package()
+    import oracle
+    kind = 'reference' if oracle.reference_available() else 'port'
+    factory = oracle.ReferenceKernel if kind == 'reference' else oracle.OracleKernel
+    lattices = w.lattices(lbm)[:count]
+    positions = w.positions()[:count]
+    runs = []
+    for lattice, pos, n in zip(lattices, positions, w.sizes[:count]):
+        m = np.ones(len(pos))
+        runs.append((factory(lattice, m, []), np.ascontiguousarray(pos), np.zeros_like(pos), m, float(n)))
+    no_bonds = np.zeros((0, 2), dtype=np.int32)
+
+    def advance(s):
+        for kernel, pos, vel, m, n in runs:
+            frc = np.zeros_like(pos)
+            kernel.begin_step(s, pos, vel, frc)
+            frc[:] = oracle.md_forces(pos, np.array([n, n, n]), no_bonds, 0.0, 1.0, 'lj', 1.0, w.kT, 2.5)
+            kernel.execute(s, pos, vel, frc)
+            vel[:] += frc/m[:, None]
+            pos[:] += vel
+
+    for s in range(warmup):
+        advance(s)
+    t0 = time.perf_counter()
+    for s in range(warmup, warmup + steps):
+        advance(s)
+    dt = (time.perf_counter() - t0)/steps
+    for kernel, *_ in runs:
+        kernel.close()
+    nodes = int((w.sizes[:count].astype(np.int64)**3).sum())
+    sample = ('per step, the first %d replicas (%d nodes, %d beads) one after another' %
+              (count, nodes, int(w.beads[:count].sum())))
+    return nodes/dt/1e6, kind, dt, sample
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument('--gpus', type=int, default=1)
     parser.add_argument('--steps', type=int, default=30)
     parser.add_argument('--warmup', type=int, default=5)
     parser.add_argument('--impl', default='b200', choices=['b200', 'reference'])
-    parser.add_argument('--workload', default='coupled', choices=['coupled', 'fluid', 'channel'])
+    parser.add_argument('--workload', default='coupled', choices=['coupled', 'fluid', 'channel', 'batch'])
     parser.add_argument('--precision', default='single', choices=list(STORAGE_BYTES))
     parser.add_argument('--size', type=int, default=0, help='lattice edge in x (smaller cases for profiling)')
     parser.add_argument('--no-fluctuations', action='store_true')
     parser.add_argument('--no-cpu-baseline', action='store_true')
     parser.add_argument('--observables', action='store_true', help='fluid and bead temperatures after the run')
+    parser.add_argument('--graph-steps', type=int, default=10, help='batch: lattice steps per CUDA graph')
+    parser.add_argument('--replicas', type=int, default=256, help='batch: number of replicas')
+    parser.add_argument('--separate', action='store_true', help='batch: also time the replicas as separate kernels')
     args = parser.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get('WORLD_SIZE', '1'))
@@ -431,9 +656,26 @@ def main():
     local = int(os.environ.get('LOCAL_RANK', '0'))
     if args.workload == 'channel':
         base = ChannelWorkload()
+    elif args.workload == 'batch':
+        base = BatchWorkload(replicas=args.replicas)
     else:
         base = Workload(coupled=args.workload == 'coupled', fluctuations=not args.no_fluctuations)
-    w = base.sample(args.size) if args.size and args.size != base.shape[0] else base
+    if args.workload == 'batch':
+        w = base
+    else:
+        w = base.sample(args.size) if args.size and args.size != base.shape[0] else base
+    if args.impl == 'reference' and args.workload == 'batch':
+        if rank != 0:
+            return
+        value, kind, dt, sample = run_cpu_batch(w, args.steps, args.warmup)
+        print(json.dumps({
+            'metric': 'MLUPS (fluid nodes x lattice steps / s) of the batched replica step', 'impl': 'reference',
+            'value': value, 'unit': 'MLUPS', 'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': dt*1e3, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+            'data': 'synthetic', 'config': {'workload': w.name(), 'sample': sample},
+            'cpu_baseline': {'value': value, 'unit': 'MLUPS', 'cores': 1, 'kind': kind, 'sample': sample},
+            'e2e': {'value': value, 'unit': 'MLUPS', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}))
+        return
     if args.impl == 'reference':
         if rank != 0:
             return
@@ -455,8 +697,14 @@ def main():
         import torch
         torch.cuda.set_device(local)
         torch.distributed.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
-    result = run_b200(args, w, rank, world, local)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if args.workload == 'batch':
+        result = run_batch(args, w, rank, world, local)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            value, kind, dt, sample = run_cpu_batch(w, 1, 1)
+            result['cpu_baseline'] = {'value': value, 'unit': 'MLUPS', 'cores': 1, 'kind': kind, 'sample': sample}
+    else:
+        result = run_b200(args, w, rank, world, local)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != 'batch':
         sample = w.sample(min(w.shape[0], 128))
         value, kind, dt = run_cpu(args, sample, 2, 1)
         result['cpu_baseline'] = {'value': value, 'unit': 'MLUPS', 'cores': 1, 'kind': kind,

@@ -4,7 +4,10 @@
     force    LBMForce, the reference's parameter API, and its conversion into lattice units
     kernel   B200Kernel, the platform kernel (CalcLBMForceKernel) behind the C ABI
     harness  System / Context / VerletIntegrator: the OpenMM call order that drives the kernel
+    md       BeadDynamics: bead forces and the leapfrog on the device (the benchmark's stand-in for OpenMM)
+    batch    ReplicaBatch: many independent periodic replicas with their beads, advanced together
 """
+from .batch import ReplicaBatch  # noqa: F401
 from .abi import LbmError, LbmLatticeParameters, load_library  # noqa: F401
 from .force import LBMForce  # noqa: F401
 from .harness import Context, ExternalForce, PairForce, System, VerletIntegrator  # noqa: F401

@@ -17,6 +17,7 @@
 // atomics into the fluid's node reaction buffer and their nodes flagged in its bitmask, so the dense kernel reads a
 // reaction only where there is one.
 #include "coupling.cuh"
+#include "coupling_device.cuh"
 #include "lbm_device.cuh"
 #include "radix_sort.cuh"
 #include <algorithm>
@@ -31,267 +32,28 @@ namespace lbm {
 #define CUDA_CHECK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) \
     throw Error(LBM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); } while (0)
 
-// The coupling parameters in lattice units, by value to the kernels.
-struct CouplingView {
-    int np, width, slots, stencil;
-    int nx, ny, nz;
-    int open[3];
-    long long n;
-    int wordsPerRow;
-    double dx, velocityScale, forceScale;
-    double gamma, kT, h, a;
-    double g[3];
-    uint32_t seed;
-    int randomForce;
-    const uint32_t* solidMask;
-    const double* mass;          // m/m_c per particle
-};
-
 namespace {
 
 const int kThreads = 256;
 
-template <typename R> struct Vec4;
-template <> struct Vec4<float> {
-    typedef float4 type;
-    static __device__ __forceinline__ float4 make(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
-};
-template <> struct Vec4<double> {
-    typedef double4 type;
-    static __device__ __forceinline__ double4 make(double a, double b, double c, double d) { return make_double4(a, b, c, d); }
-};
-
-// r[0..2] += (x, y, z): one vector atomic for float (sm_90 and later), three for double.
-__device__ __forceinline__ void atomicAdd3(float* r, double x, double y, double z) {
-    atomicAdd(reinterpret_cast<float4*>(r), make_float4((float) x, (float) y, (float) z, 0.0f));
-}
-__device__ __forceinline__ void atomicAdd3(double* r, double x, double y, double z) {
-    atomicAdd(&r[0], x);
-    atomicAdd(&r[1], y);
-    atomicAdd(&r[2], z);
-}
-
-__device__ __forceinline__ bool isSolid(const uint32_t* mask, int wordsPerRow, int nx, long long node) {
-    if (mask == nullptr)
-        return false;
-    long long row = node/nx;
-    int x = (int) (node - row*nx);
-    return (__ldg(&mask[row*wordsPerRow + x/32]) >> (x%32)) & 1u;
-}
-
-// Lattice coordinate of a position along an axis, wrapped into [0, n) (ReferenceLBMKernels.cpp:978-979).
-__device__ __forceinline__ double latticeCoordinate(double x, double dx, int n) {
-    double s = x/dx;
-    s -= floor(s/n)*n;
-    return s;
-}
-
-// LBMStencils::kernel (LBMStencils.h:42-62).
-__device__ double stencilKernel1(int stencil, double r) {
-    double s = fabs(r);
-    switch (stencil) {
-    case LBM_STENCIL_TRILINEAR:
-        return (s < 1.0 ? 1.0-s : 0.0);
-    case LBM_STENCIL_THREEPOINT:
-        if (s <= 0.5)
-            return (1.0 + sqrt(1.0-3.0*s*s))/3.0;
-        if (s < 1.5)
-            return (5.0 - 3.0*s - sqrt(fmax(0.0, 1.0-3.0*(1.0-s)*(1.0-s))))/6.0;
-        return 0.0;
-    case LBM_STENCIL_KEYS:
-        if (s <= 1.0)
-            return 1.0 - 2.5*s*s + 1.5*s*s*s;
-        if (s < 2.0)
-            return 2.0 - 4.0*s + 2.5*s*s - 0.5*s*s*s;
-        return 0.0;
-    default:
-        return (r >= -0.5 && r < 0.5 ? 1.0 : 0.0);
-    }
-}
-
-// LBMStencils::axisWeights (LBMStencils.h:73-95): the nodes of the stencil along one axis and their weights,
-// clamped at open faces, with repeated nodes merged into their first slot.
-__device__ void axisWeights(int stencil, int width, double s, int n, bool open, int* index, double* weight) {
-    int first;
-    if (stencil == LBM_STENCIL_THREEPOINT)
-        first = (int) floor(s + 0.5) - 1;
-    else if (stencil == LBM_STENCIL_KEYS)
-        first = (int) floor(s) - 1;
-    else if (stencil == LBM_STENCIL_TRILINEAR)
-        first = (int) floor(s);
-    else
-        first = (int) floor(s + 0.5);
-    for (int i = 0; i < width; i++) {
-        weight[i] = stencilKernel1(stencil, s - (first + i));
-        int idx = first + i;
-        index[i] = open ? min(max(idx, 0), n - 1) : ((idx%n) + n)%n;
-    }
-    for (int i = 1; i < width; i++)
-        for (int j = 0; j < i; j++)
-            if (index[j] == index[i]) {
-                weight[j] += weight[i];
-                weight[i] = 0.0;
-                break;
-            }
-}
-
-// Density deviation and momentum of the post-stream populations of a node (pulled from the input array).
-template <typename T>
-__device__ void pullMoments(const T* A, const FluidView& f, long long node, double& dr, double& jx, double& jy, double& jz) {
-    typedef typename std::conditional<std::is_same<T, double>::value, double, float>::type R;
-    int x = (int) (node%f.nx);
-    long long r = node/f.nx;
-    int y = (int) (r%f.ny), z = (int) (r/f.ny);
-    int xs[3] = {x == 0 ? f.nx-1 : x-1, x, x == f.nx-1 ? 0 : x+1};
-    int ys[3] = {y == 0 ? f.ny-1 : y-1, y, y == f.ny-1 ? 0 : y+1};
-    int zs[3] = {z == 0 ? f.nz-1 : z-1, z, z == f.nz-1 ? 0 : z+1};
-    R d = 0, a = 0, b = 0, c = 0;
-#pragma unroll
-    for (int q = 0; q < 19; q++) {
-        const int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
-        long long src = xs[1-cx] + (long long) f.nx*(ys[1-cy] + (long long) f.ny*zs[1-cz]);
-        R v = loadq<T, R>(A + (long long) q*f.n + src, q);
-        d += v;
-        a += cx*v;
-        b += cy*v;
-        c += cz*v;
-    }
-    dr = d; jx = a; jy = b; jz = c;
-}
-
-// One thread per (particle, slot): node, weight and the node's velocity and density.  centred: the velocity is
-// u~ = (j + h rho g)/rho (ReferenceLBMKernels.cpp:622, 773); explicit: u = j/rho (:539, :672).
+// One thread per (particle, slot).
 template <typename T, typename R>
 __global__ void stencilKernel(const T* __restrict__ A, FluidView f, CouplingView c, const double* __restrict__ pos,
                               int remove, int centred, int* slotNode, R* slotWeight, typename Vec4<R>::type* slotU) {
     long long total = (long long) c.np*c.slots;
-    for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x) {
-        int i = (int) (t/c.slots), s = (int) (t%c.slots);
-        int size[3] = {c.nx, c.ny, c.nz};
-        int idx[3];
-        double w = 1.0;
-        if (c.stencil == LBM_STENCIL_NEAREST) {
-            // nearestNode (ReferenceLBMKernels.cpp:973-983): periodic wrap on every axis.
-            for (int a = 0; a < 3; a++) {
-                double sc = latticeCoordinate(pos[3*i+a], c.dx, size[a]);
-                idx[a] = ((int) floor(sc + 0.5))%size[a];
-            }
-        }
-        else {
-            int sub[3] = {s%c.width, (s/c.width)%c.width, s/(c.width*c.width)};
-            for (int a = 0; a < 3; a++) {
-                int index[4];
-                double weight[4];
-                axisWeights(c.stencil, c.width, latticeCoordinate(pos[3*i+a], c.dx, size[a]), size[a], c.open[a] != 0,
-                            index, weight);
-                idx[a] = index[sub[a]];
-                w *= weight[sub[a]];
-            }
-        }
-        long long node = idx[0] + (long long) c.nx*(idx[1] + (long long) c.ny*idx[2]);
-        slotNode[t] = (int) node;
-        slotWeight[t] = (R) w;
-        double ux = 0, uy = 0, uz = 0, rho = 0;
-        if (w != 0.0 && !isSolid(c.solidMask, c.wordsPerRow, c.nx, node)) {
-            double dr, jx, jy, jz;
-            pullMoments<T>(A, f, node, dr, jx, jy, jz);
-            rho = 1.0 + dr;
-            if (remove) {
-                jx -= rho*f.stats->ucm[0];
-                jy -= rho*f.stats->ucm[1];
-                jz -= rho*f.stats->ucm[2];
-            }
-            if (centred) {
-                jx += c.h*rho*c.g[0];
-                jy += c.h*rho*c.g[1];
-                jz += c.h*rho*c.g[2];
-            }
-            ux = jx*(1.0/rho);
-            uy = jy*(1.0/rho);
-            uz = jz*(1.0/rho);
-        }
-        slotU[t] = Vec4<R>::make((R) ux, (R) uy, (R) uz, (R) rho);
-    }
+    for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x)
+        stencilSlot<T, R>(A, f, c, pos, t, remove, centred, slotNode, slotWeight, slotU);
 }
 
-// Reaction (fx, fy, fz) on a node: added into the fluid's reaction buffer and the node flagged, or for a solid node
-// counted as momentum given to the wall (applyReaction, ReferenceLBMKernels.cpp:959-971).
-template <typename R>
-__device__ void addReaction(const FluidView& f, const CouplingView& c, R* reaction, uint32_t* mask, double* wall,
-                            long long node, double fx, double fy, double fz) {
-    if (isSolid(c.solidMask, c.wordsPerRow, c.nx, node)) {
-        atomicAdd(&wall[0], fx);
-        atomicAdd(&wall[1], fy);
-        atomicAdd(&wall[2], fz);
-        return;
-    }
-    atomicAdd3(reaction + 4*node, fx, fy, fz);
-    long long row = node/f.nx;
-    int x = (int) (node - row*f.nx);
-    uint32_t bit = 1u << (x%32);
-    uint32_t* word = &mask[row*f.wordsPerRow + x/32];
-    if (!(*((volatile uint32_t*) word) & bit))
-        atomicOr(word, bit);
-}
-
-// Three normals of particle i for step `step` (Philox, purpose 2), in double.
-__device__ __forceinline__ void particleNoise(uint32_t seed, int i, long long step, double xi[3]) {
-    double v[4];
-    boxMuller(philoxBlock(seed, PurposeParticle, i, step, 0), v);
-    xi[0] = v[0]; xi[1] = v[1]; xi[2] = v[2];
-}
-
-__device__ __forceinline__ double warpSum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// Explicit drag, nearest node or stencil (ReferenceLBMKernels.cpp:503-553, 643-697): one warp per particle, the
-// lanes over the stencil slots.
+// One warp per particle.
 template <typename R>
 __global__ void explicitKernel(FluidView f, CouplingView c, const double* __restrict__ vel, const int* __restrict__ slotNode,
                                const R* __restrict__ slotWeight, const typename Vec4<R>::type* __restrict__ slotU,
                                long long step, int isStep, double* fout, R* reaction, uint32_t* mask, double* wall) {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x*blockDim.x) >> 5;
-    for (int i = (blockIdx.x*blockDim.x + threadIdx.x) >> 5; i < c.np; i += warps) {
-        double u[3] = {0, 0, 0};
-        for (int s = lane; s < c.slots; s += 32) {
-            long long t = (long long) i*c.slots + s;
-            typename Vec4<R>::type su = slotU[t];
-            if (su.w > 0) {
-                double w = (double) slotWeight[t];
-                u[0] += (double) su.x*w;
-                u[1] += (double) su.y*w;
-                u[2] += (double) su.z*w;
-            }
-        }
-        for (int a = 0; a < 3; a++)
-            u[a] = warpSum(u[a]);
-        double m = c.mass[i];
-        double xi[3] = {0, 0, 0};
-        if (c.randomForce)
-            particleNoise(c.seed, i, step, xi);
-        double F[3];
-        for (int a = 0; a < 3; a++) {
-            double v = vel[3*i+a]*(1.0/c.velocityScale);
-            F[a] = (v - u[a])*(-c.gamma*m);
-            if (c.randomForce)
-                F[a] += xi[a]*sqrt(2.0*c.gamma*m*c.kT);
-        }
-        if (lane == 0)
-            for (int a = 0; a < 3; a++)
-                fout[3*i+a] = F[a]*c.forceScale;
-        if (isStep)
-            for (int s = lane; s < c.slots; s += 32) {
-                long long t = (long long) i*c.slots + s;
-                double w = (double) slotWeight[t];
-                if (w != 0.0)
-                    addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*F[0], -w*F[1], -w*F[2]);
-            }
-    }
+    for (int i = (blockIdx.x*blockDim.x + threadIdx.x) >> 5; i < c.np; i += warps)
+        explicitParticle<R>(f, c, vel, slotNode, slotWeight, slotU, i, lane, step, isStep, fout, reaction, mask, wall);
 }
 
 // Keys: nearest node of each particle (ReferenceLBMKernels.cpp:596, the key node*N + k sorted).
@@ -882,36 +644,6 @@ void CouplingEngine::setParameters(const LbmLatticeParameters& l) {
     lattice = l;
 }
 
-// The coupling parameters in lattice units (ReferenceLBMKernels.cpp:520-525).
-static CouplingView makeView(const LbmLatticeParameters& l, const FluidView& f, int np, int width, const double* mass) {
-    CouplingView c;
-    std::memset(&c, 0, sizeof(c));
-    c.np = np;
-    c.width = width;
-    c.slots = width*width*width;
-    c.stencil = l.interpolation_stencil;
-    c.nx = l.nx; c.ny = l.ny; c.nz = l.nz;
-    for (int a = 0; a < 3; a++)
-        c.open[a] = l.face_boundary[2*a] != LBM_BOUNDARY_PERIODIC;
-    c.n = f.n;
-    c.wordsPerRow = f.wordsPerRow;
-    double cellMass = l.density*l.dx*l.dx*l.dx;
-    c.dx = l.dx;
-    c.velocityScale = l.dx/l.dt;
-    c.forceScale = cellMass*l.dx/(l.dt*l.dt);
-    c.gamma = l.friction*l.dt;
-    c.kT = l.kT*l.dt*l.dt/(cellMass*l.dx*l.dx);
-    c.h = 0.5;
-    c.a = c.gamma*c.h;
-    for (int a = 0; a < 3; a++)
-        c.g[a] = l.body_acceleration[a];
-    c.seed = (uint32_t) l.random_number_seed;
-    c.randomForce = (c.kT > 0 && c.gamma > 0) ? 1 : 0;
-    c.solidMask = f.solidMask;
-    c.mass = mass;
-    return c;
-}
-
 void CouplingEngine::load(const LbmParticleArrays* p, bool withForces) {
     size_t v3 = sizeof(double)*3*(size_t) np;
     cudaMemcpyKind kind = p->memory == LBM_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
@@ -924,7 +656,7 @@ void CouplingEngine::load(const LbmParticleArrays* p, bool withForces) {
 void CouplingEngine::reflect(const LbmParticleArrays* p, double wallMomentum[3]) {
     load(p, false);
     const FluidView& f = fluid.deviceView();
-    CouplingView c = makeView(lattice, f, np, 1, massDev);
+    CouplingView c = makeCouplingView(lattice, f, np, 1, massDev);
     CUDA_CHECK(cudaMemsetAsync(dev->reflectWall, 0, sizeof(double)*3, stream));
     double cellMass = lattice.density*lattice.dx*lattice.dx*lattice.dx;
     reflectKernel<<<std::max(1, std::min(1184, (np + kThreads - 1)/kThreads)), kThreads, 0, stream>>>(c, posDev, velDev, cellMass, dev->reflectWall);
@@ -1013,7 +745,7 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
 
 void CouplingEngine::couple(long long step, bool isStep, bool remove) {
     const FluidView& f = fluid.deviceView();
-    CouplingView c = makeView(lattice, f, np, widthOf(lattice.interpolation_stencil), massDev);
+    CouplingView c = makeCouplingView(lattice, f, np, widthOf(lattice.interpolation_stencil), massDev);
     bool centred = lattice.drag_scheme == LBM_DRAG_CENTERED;
     const void* A = fluid.inputArray();
     switch (storageType) {

@@ -13,6 +13,7 @@
 //  momentsKernel         mass, momentum and largest speed of the current state (Mach check, start-up).
 //  gather/scatter        conversion between the pull layout and the reference's state layout.
 #include "fluid.cuh"
+#include "collide.cuh"
 #include "lbm_device.cuh"
 #include <algorithm>
 #include <cmath>
@@ -29,15 +30,6 @@ namespace {
 
 constexpr int TX = 32, TY = 8, THREADS = TX*TY;
 constexpr int NPART = 8;           // doubles per partial record: mass, momentum[3], wall[3], maxSpeed2
-
-template <typename F, int... I>
-__device__ __forceinline__ void staticForImpl(F&& f, std::integer_sequence<int, I...>) {
-    (f(std::integral_constant<int, I>{}), ...);
-}
-template <int N, typename F>
-__device__ __forceinline__ void staticFor(F&& f) {
-    staticForImpl(f, std::make_integer_sequence<int, N>{});
-}
 
 // Block reduction of a partial record (sums, and max for the last entry) into partials[slot], deterministic.
 __device__ void blockReduceStore(double v[NPART], double* out) {
@@ -88,94 +80,6 @@ __device__ __forceinline__ int cxr(int q) { return cxOf(q); }
 __device__ __forceinline__ int cyr(int q) { return cyOf(q); }
 __device__ __forceinline__ int czr(int q) { return czOf(q); }
 
-// Moments of 19 post-stream deviations: density deviation, momentum and non-equilibrium second moment
-// Pi_neq = sum_q H2(c_q) df_q - j j/rho (xx, yy, zz, xy, xz, yz).  For the D3Q19 second-order
-// equilibrium, sum_q H2(c_q) (feq_q - w_q) = j j/rho exactly, so this equals the reference's
-// sum_q H2(c_q) (df_q - dfeq_q) (D3Q19.h:98-110).
-__device__ __forceinline__ double reciprocal(double x) { return 1.0/x; }
-__device__ __forceinline__ float reciprocal(float x) { return __fdividef(1.0f, x); }
-
-template <typename R>
-struct Moments {
-    R dr, jx, jy, jz, pxx, pyy, pzz, pxy, pxz, pyz;
-};
-
-template <typename R>
-__device__ __forceinline__ Moments<R> momentsOf(const R f[19]) {
-    Moments<R> m;
-    R dr = 0, jx = 0, jy = 0, jz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
-    staticFor<19>([&](auto qc) {
-        constexpr int q = decltype(qc)::value;
-        constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
-        R fq = f[q];
-        dr += fq;
-        if (cx == 1) jx += fq; else if (cx == -1) jx -= fq;
-        if (cy == 1) jy += fq; else if (cy == -1) jy -= fq;
-        if (cz == 1) jz += fq; else if (cz == -1) jz -= fq;
-        if (cx != 0) sxx += fq;
-        if (cy != 0) syy += fq;
-        if (cz != 0) szz += fq;
-        if (cx*cy == 1) sxy += fq; else if (cx*cy == -1) sxy -= fq;
-        if (cx*cz == 1) sxz += fq; else if (cx*cz == -1) sxz -= fq;
-        if (cy*cz == 1) syz += fq; else if (cy*cz == -1) syz -= fq;
-    });
-    R inv = R(1)/(R(1) + dr);
-    R third = dr*R(1.0/3.0);
-    m.dr = dr; m.jx = jx; m.jy = jy; m.jz = jz;
-    m.pxx = sxx - third - jx*jx*inv;
-    m.pyy = syy - third - jy*jy*inv;
-    m.pzz = szz - third - jz*jz*inv;
-    m.pxy = sxy - jx*jy*inv;
-    m.pxz = sxz - jx*jz*inv;
-    m.pyz = syz - jy*jz*inv;
-    return m;
-}
-
-// Amplitudes a_k = phi_k r_k/sqrt(b_k) of the 15 non-conserved modes (D3Q19::fluctuation).
-template <typename R>
-__device__ __forceinline__ void modeAmplitudes(const R r[15], R stress, R ghost, R a[15]) {
-#pragma unroll
-    for (int k = 4; k < 19; k++)
-        a[k-4] = r[k-4]*(k < 10 ? stress : ghost)*R(invSqrtModeNorm(k));
-}
-
-// Even and odd parts (in c_q) of xi_q = w_q sum_k e_k(c_q) a_k for one direction q.
-template <typename R, int q>
-__device__ __forceinline__ void fluctuationParts(const R a[15], R& even, R& odd) {
-    R e = 0, o = 0;
-    staticFor<15>([&](auto kc) {
-        constexpr int k = decltype(kc)::value + 4;
-        constexpr double m = modeValue(k, q);
-        if (m != 0.0) {
-            if (k >= 10 && k <= 15)
-                o += R(m)*a[k-4];
-            else
-                e += R(m)*a[k-4];
-        }
-    });
-    even = wOf<R>(q)*e;
-    odd = wOf<R>(q)*o;
-}
-
-// Even and odd parts of the ghost-mode part (k = 10..18) of xi_q; the stress modes are merged into the
-// non-equilibrium tensor of the dense kernel.
-template <typename R, int q>
-__device__ __forceinline__ void ghostParts(const R a[15], R& even, R& odd) {
-    R e = 0, o = 0;
-    staticFor<9>([&](auto kc) {
-        constexpr int k = decltype(kc)::value + 10;
-        constexpr double m = modeValue(k, q);
-        if (m != 0.0) {
-            if (k <= 15)
-                o += R(m)*a[k-4];
-            else
-                e += R(m)*a[k-4];
-        }
-    });
-    even = wOf<R>(q)*e;
-    odd = wOf<R>(q)*o;
-}
-
 // Runtime-q fluctuation (slow paths): xi_q = w_q sum_k e_k(c_q) a_k.
 template <typename R>
 __device__ R fluctuationAt(int q, const R a[15]) {
@@ -203,76 +107,31 @@ __device__ __forceinline__ R weightOf(int q) {
 // The dense step.
 // ---------------------------------------------------------------------------------------------------
 
-// Resident blocks of 256 threads per SM that the register allocation of the dense kernel must allow: 4 for float
-// arithmetic (64 registers, 32 warps per SM to hide the latency of the 19 loads) and 2 for double.
+// Resident blocks of 256 threads per SM that the register allocation of the dense kernel must allow: 3 for float
+// arithmetic (85 registers, 24 warps per SM) and 2 for double.  Measured on B200 at 256^3 (FP32, plain): 0.479 ms
+// per launch with 3 blocks, 0.549 ms with 4 (64 registers: the loads of a node are no longer all in flight).
 #ifdef LBM_DENSE_MIN_BLOCKS
 template <typename R> constexpr int denseMinBlocks() { return LBM_DENSE_MIN_BLOCKS; }
 #else
-template <typename R> constexpr int denseMinBlocks() { return sizeof(R) == 4 ? 4 : 2; }
+template <typename R> constexpr int denseMinBlocks() { return sizeof(R) == 4 ? 3 : 2; }
 #endif
-
-// Moments of the 19 pulled values r_q in storage units (deviation = scale_q r_q), summed over the opposite
-// pairs (q, q+1): S = r_q + r_{q+1} feeds the even moments and D = r_q - r_{q+1} the momentum, with the
-// scales folded into the FMAs.
-template <typename T, typename R>
-__device__ __forceinline__ Moments<R> momentsOfRaw(const R r[19]) {
-    R dr = R(Storage<T>::template scale<0>())*r[0];
-    R jx = 0, jy = 0, jz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
-    staticFor<9>([&](auto pc) {
-        constexpr int q = 2*decltype(pc)::value + 1;
-        constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
-        constexpr R s = R(Storage<T>::template scale<q>());
-        R S = r[q] + r[q+1], D = r[q] - r[q+1];
-        dr += s*S;
-        if (cx != 0) { jx += R(cx)*s*D; sxx += s*S; }
-        if (cy != 0) { jy += R(cy)*s*D; syy += s*S; }
-        if (cz != 0) { jz += R(cz)*s*D; szz += s*S; }
-        if (cx*cy != 0) sxy += R(cx*cy)*s*S;
-        if (cx*cz != 0) sxz += R(cx*cz)*s*S;
-        if (cy*cz != 0) syz += R(cy*cz)*s*S;
-    });
-    Moments<R> m;
-    R inv = reciprocal(R(1) + dr);
-    R third = dr*R(1.0/3.0);
-    m.dr = dr; m.jx = jx; m.jy = jy; m.jz = jz;
-    m.pxx = sxx - third - jx*jx*inv;
-    m.pyy = syy - third - jy*jy*inv;
-    m.pzz = szz - third - jz*jz*inv;
-    m.pxy = sxy - jx*jy*inv;
-    m.pxz = sxz - jx*jz*inv;
-    m.pyz = syz - jy*jz*inv;
-    return m;
-}
 
 // The dense step over 32 x 8 node tiles (lane = x, warp = y), persistent blocks striding over the tiles.  Node
 // indices are 32-bit (the host limits the lattice to 2^32 nodes); the tile coordinates advance by the grid
-// stride without divisions, and the periodic pull sources are node + per-node offsets in x, y and z.
+// stride without divisions.  Solid nodes are skipped by their bit in the solid mask; nodes with a particle
+// reaction add it to the body force.
 template <typename T, typename R, bool SOLID, bool REACT, bool FLUCT>
 __global__ void __launch_bounds__(THREADS, denseMinBlocks<R>())
 streamCollideKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int remove, long long step) {
     const int lane = threadIdx.x%32, warp = threadIdx.x/32;
     const unsigned N = (unsigned) v.n;
     const int nx = v.nx, ny = v.ny, nz = v.nz;
-    const unsigned sxy = (unsigned) nx*(unsigned) ny;
-    const R omega = R(v.omega), om1 = R(1) - omega;
-    const R gx = R(v.g[0]), gy = R(v.g[1]), gz = R(v.g[2]);
-    R ux0 = 0, uy0 = 0, uz0 = 0;
-    if (remove) {
-        ux0 = R(v.stats->ucm[0]);
-        uy0 = R(v.stats->ucm[1]);
-        uz0 = R(v.stats->ucm[2]);
-    }
-    R stressFactor = 0, muR = 0;
-    if (FLUCT) {
-        muR = R(v.mu);
-        stressFactor = omega*(R(2) - omega);
-    }
+    const CollideConstants<R> k = collideConstants<R>(v.omega, v.g, v.stats->ucm, remove, v.mu, v.seed);
     R sumMass = 0, sumX = 0, sumY = 0, sumZ = 0;
     const unsigned numTiles = (unsigned) v.numTiles, stride = gridDim.x;
     const int tilesX = v.tilesX, tilesY = v.tilesY;
     int tx = (int) (blockIdx.x%tilesX), ty = (int) ((blockIdx.x/tilesX)%tilesY), tz = (int) (blockIdx.x/tilesX/tilesY);
     const int dtx = (int) (stride%tilesX), dty = (int) ((stride/tilesX)%tilesY), dtz = (int) (stride/tilesX/tilesY);
-    constexpr bool dithered = sizeof(T) == 2;
     for (unsigned t = blockIdx.x; t < numTiles; t += stride) {
         const int x = tx*TX + lane, y = ty*TY + warp, z = tz, tileX = tx;
         tx += dtx;
@@ -291,104 +150,17 @@ streamCollideKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int
                 continue;
         }
         const unsigned node = row*nx + x;
-        // Offsets (mod 2^32) from the node to the pull sources x - c: index 0 for c = +1, 2 for c = -1.
-        const unsigned ox[3] = {x == 0 ? (unsigned) (nx - 1) : ~0u, 0u, x == nx - 1 ? (unsigned) (1 - nx) : 1u};
-        const unsigned oy[3] = {y == 0 ? (unsigned) (ny - 1)*nx : (unsigned) -nx, 0u,
-                                y == ny - 1 ? (unsigned) (1 - ny)*nx : (unsigned) nx};
-        const unsigned oz[3] = {z == 0 ? (unsigned) (nz - 1)*sxy : 0u - sxy, 0u, z == nz - 1 ? 0u - (unsigned) (nz - 1)*sxy : sxy};
-        R r[19];
-        staticFor<19>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
-            const unsigned src = node + ox[1-cx] + oy[1-cy] + oz[1-cz];
-            r[q] = Storage<T>::template raw<q>(A + ((size_t) q*N + src));
-        });
-        Moments<R> m = momentsOfRaw<T, R>(r);
-        R rho = R(1) + m.dr, inv = reciprocal(rho);
-        R jx = m.jx, jy = m.jy, jz = m.jz;
-        if (remove) {
-            jx -= rho*ux0;
-            jy -= rho*uy0;
-            jz -= rho*uz0;
-        }
-        R Fx = rho*gx, Fy = rho*gy, Fz = rho*gz;
+        R ex = 0, ey = 0, ez = 0;
         if (REACT) {
             uint32_t word = __ldg(&v.reactMask[(size_t) row*v.wordsPerRow + tileX]);
             if ((word >> lane) & 1u) {
                 const R* rp = reinterpret_cast<const R*>(v.reaction) + 4*(size_t) node;
-                Fx += rp[0];
-                Fy += rp[1];
-                Fz += rp[2];
+                ex = rp[0];
+                ey = rp[1];
+                ez = rp[2];
             }
         }
-        R ux = (jx + R(0.5)*Fx)*inv, uy = (jy + R(0.5)*Fy)*inv, uz = (jz + R(0.5)*Fz)*inv;
-        R uu = ux*ux + uy*uy + uz*uz, uf = ux*Fx + uy*Fy + uz*Fz;
-        // The odd part 3 w_q (rho c.u + c.F/2) = 3 w_q c.(j + F) is built from the momentum after the force, not
-        // through u = (j + F/2)/rho: a rounded rho*(1/rho) would scale the momentum by a fixed factor every step.
-        const R px = jx + Fx, py = jy + Fy, pz = jz + Fz;
-        // The regularized non-equilibrium part (1 - omega) 4.5 w_q H2(c_q):Pi_neq and the random stress modes
-        // w_q sum_{k=4..9} e_k(c_q) a_k are both quadratic forms in c_q: they are merged into one tensor Q, so that
-        // each direction evaluates w_q (c Q c - tr Q/3) once.  The ghost modes (k = 10..18) are added per direction.
-        const R s45 = om1*R(4.5), s9 = om1*R(9);
-        R qxx = s45*m.pxx, qyy = s45*m.pyy, qzz = s45*m.pzz;
-        R qxy = s9*m.pxy, qxz = s9*m.pxz, qyz = s9*m.pyz;
-        R a[15];
-        if (FLUCT) {
-            R rn[15];
-            philoxNormals<R, 15>(v.seed, PurposeFluid, node, step, rn);
-            R ghost = sqrt(muR*rho);
-            modeAmplitudes<R>(rn, sqrt(muR*rho*stressFactor), ghost, a);
-            qxx += a[0]; qyy += a[1]; qzz += a[2];
-            qxy += a[3]; qxz += a[4]; qyz += a[5];
-        }
-        R qtr = (qxx + qyy + qzz)*R(1.0/3.0);
-        // Terms common to all directions: dr - 1.5 rho u.u - 1.5 u.F.
-        const R base = m.dr - R(1.5)*(rho*uu + uf);
-        R outMass = 0, outX = 0, outY = 0, outZ = 0;
-        // Stochastic rounding of the 16-bit stores: one dither word per pair of directions.
-        Dither dither(dithered ? node : 0, dithered ? step : 0);
-        // q = 0
-        {
-            R value = R(1.0/3.0)*(base - qtr);
-            if (FLUCT) {
-                R e, o;
-                ghostParts<R, 0>(a, e, o);
-                value += e;
-            }
-            R stored = Storage<T>::template storeOne<0>(B + node, value, dithered ? dither.next() : 0u);
-            outMass += R(Storage<T>::template scale<0>())*stored;
-        }
-        // Pairs (q, q+1) with c_{q+1} = -c_q.
-        staticFor<9>([&](auto pc) {
-            constexpr int q = 2*decltype(pc)::value + 1;
-            constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
-            constexpr R w = wOf<R>(q);
-            constexpr R s = R(Storage<T>::template scale<q>());
-            R cu = R(cx)*ux + R(cy)*uy + R(cz)*uz;
-            R cf = R(cx)*Fx + R(cy)*Fy + R(cz)*Fz;
-            R cqc = R(cx*cx)*qxx + R(cy*cy)*qyy + R(cz*cz)*qzz - qtr
-                  + R(cx*cy)*qxy + R(cx*cz)*qxz + R(cy*cz)*qyz;
-            R even = w*(base + cqc + R(4.5)*cu*(rho*cu + cf));
-            R odd = oddOf<R>(q)*(R(cx)*px + R(cy)*py + R(cz)*pz);
-            if (FLUCT) {
-                R e, o;
-                ghostParts<R, q>(a, e, o);
-                even += e;
-                odd += o;
-            }
-            R s1, s2;
-            Storage<T>::template storePair<q>(B + ((size_t) q*N + node), B + ((size_t) (q+1)*N + node), even + odd,
-                                              even - odd, dithered ? dither.next() : 0u, s1, s2);
-            outMass += s*(s1 + s2);
-            R d = s*(s1 - s2);
-            if (cx != 0) outX += R(cx)*d;
-            if (cy != 0) outY += R(cy)*d;
-            if (cz != 0) outZ += R(cz)*d;
-        });
-        sumMass += outMass;
-        sumX += outX;
-        sumY += outY;
-        sumZ += outZ;
+        collideNode<T, R, FLUCT>(A, B, N, node, x, y, z, nx, ny, nz, k, ex, ey, ez, step, sumMass, sumX, sumY, sumZ);
     }
     double acc[NPART] = {(double) sumMass, (double) sumX, (double) sumY, (double) sumZ, 0, 0, 0, 0};
     blockReduceStore(acc, v.partials + NPART*(long long) blockIdx.x);

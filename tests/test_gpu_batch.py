@@ -1,0 +1,135 @@
+"""GPU tests of the replica batch (include/lbm_b200_batch.h).  Replicas of the batching configuration (periodic
+fluctuating fluids, tau 0.7, kT = 1e-4, distinct Philox seeds; Lennard-Jones beads sigma 1, epsilon kT, cutoff 2.5,
+mass 1; three-point stencil, explicit drag 0.8; lattice units dx = 1 nm, dt = 1 ps, rho0 = 1 Da/nm^3) on small lattices
+of uneven sizes:
+
+- pathwise: each replica of a batch follows a B200Kernel with the same lattice parameters and the bead dynamics of
+  the benchmark (BeadDynamics), step for step, within 1e-9 relative in FP64 over 30 steps (the bead pair forces are
+  summed in another order, and the chaotic bead dynamics amplify the last bits);
+- a run replayed from the CUDA graph equals the same run launched step by step;
+- the fluid temperature of every replica is kT (equipartition of the fluctuating fluid)."""
+import numpy as np
+import pytest
+
+import lbm_b200
+from lbm_b200 import LBMForce, ReplicaBatch
+
+pytestmark = pytest.mark.gpu
+
+BOLTZ = 6.02214076e23*1.380649e-23/1000.0
+KT, TAU, FRICTION, SIGMA, CUTOFF = 1e-4, 0.7, 0.8, 1.0, 2.5
+
+
+def replica_lattice(n, num_beads, seed, kT=KT):
+    force = LBMForce()
+    force.setGridSize(n, n, n)
+    force.setFluidDensity(1.0)
+    force.setKinematicViscosity((TAU - 0.5)/3.0)
+    force.setFluidFluctuations(kT > 0)
+    force.setTemperature(kT/BOLTZ)
+    force.setRandomNumberSeed(seed)
+    force.setInterpolationStencil(LBMForce.ThreePoint)
+    force.setDragScheme(LBMForce.Explicit)
+    force.setFriction(FRICTION)
+    for i in range(num_beads):
+        force.addParticle(i)
+    return force.latticeParameters(np.array([n, n, n], dtype=float), 1.0, np.ones(max(1, num_beads)))
+
+
+def bead_positions(n, count, rng, min_distance=1.1):
+    """Uniform positions in an n^3 periodic box at least min_distance apart (minimum image)."""
+    out = []
+    while len(out) < count:
+        x = rng.uniform(0, n, 3)
+        if all(np.linalg.norm((x - y) - n*np.round((x - y)/n)) >= min_distance for y in out):
+            out.append(x)
+    return np.array(out)
+
+
+def make_replicas(sizes, beads, seed=2026):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    lattices = [replica_lattice(n, b, 1000 + r) for r, (n, b) in enumerate(zip(sizes, beads))]
+    positions = [bead_positions(n, b, rng) for n, b in zip(sizes, beads)]
+    return lattices, positions
+
+
+def run_separately(lattice, positions, steps):
+    import torch
+    n = lattice.nx
+    count = len(positions)
+    masses = np.ones(count)
+    kernel = lbm_b200.B200Kernel(lattice, masses, [], 'double')
+    md = lbm_b200.BeadDynamics(masses, (n, n, n), np.zeros((0, 2), dtype=np.int32), k=0.0, r0=1.0, pair='lj',
+                               sigma=SIGMA, epsilon=KT, cutoff=CUTOFF)
+    stream = kernel.stream()
+    pos = torch.tensor(positions, device='cuda', dtype=torch.float64)
+    vel = torch.zeros_like(pos)
+    frc = torch.zeros_like(pos)
+    for s in range(steps):
+        kernel.begin_step(s, pos, vel, frc)
+        md.compute_forces(pos, frc, stream)
+        kernel.execute(s, pos, vel, frc)
+        md.integrate(1.0, pos, vel, frc, stream)
+    torch.cuda.synchronize()
+    out = kernel.get_fluid_state(), pos.cpu().numpy(), vel.cpu().numpy()
+    kernel.close()
+    md.close()
+    return out
+
+
+def test_batch_follows_separate_kernels():
+    sizes, beads, steps = [12, 16, 10, 14], [20, 35, 8, 26], 30
+    lattices, positions = make_replicas(sizes, beads)
+    batch = ReplicaBatch(lattices, beads, np.ones(sum(beads)), np.concatenate(positions), pair=('lj', SIGMA, KT, CUTOFF),
+                         precision='double')
+    batch.step(steps)
+    pos, vel = batch.particles_state()
+    offsets = np.concatenate([[0], np.cumsum(beads)])
+    for r in range(len(sizes)):
+        state, ref_pos, ref_vel = run_separately(lattices[r], positions[r], steps)
+        got = batch.fluid_state(r)
+        assert abs(got - state).max() <= 1e-9*abs(state).max(), r
+        b = slice(offsets[r], offsets[r+1])
+        assert abs(pos[b] - ref_pos).max() <= 1e-9*abs(ref_pos).max(), r
+        assert abs(vel[b] - ref_vel).max() <= 1e-9*abs(ref_vel).max(), r
+    batch.close()
+
+
+def test_graph_replay_equals_direct_launches():
+    sizes, beads = [16, 20, 12], [30, 50, 10]
+    lattices, positions = make_replicas(sizes, beads, seed=7)
+    runs = []
+    for graph_steps in (10, 1000):
+        batch = ReplicaBatch(lattices, beads, np.ones(sum(beads)), np.concatenate(positions),
+                             pair=('lj', SIGMA, KT, CUTOFF), precision='double')
+        batch.autotune(graph_steps)
+        launches = batch.info()['launches']
+        batch.step(25)
+        batch.step(15)
+        info = batch.info()
+        assert info['steps'] == 40 and info['launches'] - launches == 7*40
+        runs.append((batch.fluid_state(1), batch.particles_state()[1]))
+        batch.close()
+    (state_a, vel_a), (state_b, vel_b) = runs
+    # The reactions of beads that share a node are added with atomics, in any order.
+    assert abs(state_a - state_b).max() <= 1e-12*abs(state_a).max()
+    assert abs(vel_a - vel_b).max() <= 1e-12*abs(vel_a).max()
+
+
+@pytest.mark.parametrize('precision', ['single', 'double'])
+def test_fluid_temperature_of_every_replica(precision):
+    sizes = [16, 20, 24, 18, 22, 16]
+    beads = [20, 40, 60, 30, 50, 25]
+    lattices, positions = make_replicas(sizes, beads, seed=11)
+    batch = ReplicaBatch(lattices, beads, np.ones(sum(beads)), np.concatenate(positions), pair=('lj', SIGMA, KT, CUTOFF),
+                         precision=precision)
+    batch.autotune(20)
+    batch.step(300)
+    samples = []
+    for _ in range(10):
+        batch.step(20)
+        samples.append(batch.temperatures()[0])
+    batch.close()
+    fluid = np.mean(samples, axis=0)
+    # One snapshot of N nodes has a relative spread sqrt(2/(3N)) (1.3 % at 16^3); ten snapshots 20 steps apart.
+    assert np.all(abs(fluid/KT - 1) < 0.05), fluid/KT
