@@ -208,6 +208,27 @@ LbmStatus lbm_kernel_launches(LbmKernel* kernel, long long* launches);
 /* Conjugate-gradient iterations of the last centred stencil drag solve (0 for the other coupling schemes). */
 LbmStatus lbm_solver_iterations(LbmKernel* kernel, int* iterations);
 
+/* The steady-state residual r = max_nodes |u - u_prev| / (interval max_nodes |u|) over the fluid nodes, in FP64 on the
+   device, with u = j/rho of the current (post-stream) state and u_prev the velocities recorded by the previous call,
+   which this call replaces; the first call records them and returns infinity.  Called every `interval` steps it is the
+   convergence test of a steady solve (r <= 1e-6).  No counterpart in the reference, which defines no residual. */
+LbmStatus lbm_steady_residual(LbmKernel* kernel, int interval, double* residual);
+
+/* Advances a fluid without coupled particles from step first_step until the steady residual (lbm_steady_residual,
+   checked every `interval` steps, first against the state at the start) is at most `tolerance`, or for max_steps
+   steps; returns the steps taken and the last residual.  The plain solve of a steady flow, cold or warm started.
+   No counterpart in the reference. */
+LbmStatus lbm_steady_solve(LbmKernel* kernel, long long first_step, int interval, double tolerance, long long max_steps,
+                           long long* steps_taken, double* residual);
+
+/* Sets the fluid to the populations of the given fields, density [N] and velocity [N][3] in the units of
+   lbm_get_fluid_fields, in host (memory = LBM_MEMORY_HOST) or device memory (LBM_MEMORY_DEVICE): the equilibrium, plus
+   with strain != 0 the Chapman-Enskog non-equilibrium part of the strain rate (central differences of the velocity),
+   which a steady flow has; the warm start of a steady solve from predicted fields.  Solid nodes are left at rest.
+   No counterpart in the reference. */
+LbmStatus lbm_set_fluid_equilibrium(LbmKernel* kernel, const double* density, const double* velocity, int memory,
+                                    int strain);
+
 /*
  * Fluid moments of a state that the caller owns, without allocating any memory.  It has no counterpart in the
  * reference: it is for callers that cannot call cudaMalloc -- a plugin whose host program owns the device memory

@@ -218,6 +218,31 @@ LbmStatus lbm_solver_iterations(LbmKernel* kernel, int* iterations) {
     return LBM_OK;
 }
 
+LbmStatus lbm_steady_residual(LbmKernel* kernel, int interval, double* residual) {
+    CHECK_HANDLE(kernel);
+    if (!residual || interval <= 0)
+        return fail(LBM_ERR_INVALID_ARGUMENT, "lbm_steady_residual: null residual or interval not positive");
+    return guard([&] { *residual = kernel->impl->fluidEngine().steadyResidual(interval); });
+}
+
+LbmStatus lbm_steady_solve(LbmKernel* kernel, long long first_step, int interval, double tolerance, long long max_steps,
+                           long long* steps_taken, double* residual) {
+    CHECK_HANDLE(kernel);
+    return guard([&] {
+        long long s = kernel->impl->steadySolve(first_step, interval, tolerance, max_steps, residual);
+        if (steps_taken)
+            *steps_taken = s;
+    });
+}
+
+LbmStatus lbm_set_fluid_equilibrium(LbmKernel* kernel, const double* density, const double* velocity, int memory,
+                                    int strain) {
+    CHECK_HANDLE(kernel);
+    if (!density || !velocity)
+        return fail(LBM_ERR_INVALID_ARGUMENT, "lbm_set_fluid_equilibrium: null argument");
+    return guard([&] { kernel->impl->setFluidEquilibrium(density, velocity, memory == LBM_MEMORY_DEVICE, strain != 0); });
+}
+
 LbmStatus lbm_kernel_launches(LbmKernel* kernel, long long* launches) {
     CHECK_HANDLE(kernel);
     if (!launches)

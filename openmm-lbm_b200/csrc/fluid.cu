@@ -456,6 +456,66 @@ __global__ void __launch_bounds__(THREADS) momentsKernel(const T* __restrict__ A
     blockReduceStore(acc, v.partials + NPART*(long long) blockIdx.x);
 }
 
+// The steady-state residual of the build (the reference defines none): r = max over fluid nodes of |u - u_prev|,
+// and max |u|, with u = j/rho of the post-stream state in FP64; u_prev (3N doubles, [a*N + node]) is replaced by u.
+// Per block: partials[NPART*b] = max |u - u_prev|^2, partials[NPART*b + 7] = max |u|^2.
+template <typename T, typename R>
+__global__ void __launch_bounds__(THREADS) residualKernel(const T* __restrict__ A, FluidView v, double* prev, int first) {
+    double maxDiff2 = 0, maxU2 = 0;
+    const int lane = threadIdx.x%32, warp = threadIdx.x/32;
+    for (long long t = blockIdx.x; t < v.numTiles; t += gridDim.x) {
+        int tx = (int) (t%v.tilesX);
+        long long rr = t/v.tilesX;
+        int ty = (int) (rr%v.tilesY);
+        int z = (int) (rr/v.tilesY);
+        int x = tx*TX + lane, y = ty*TY + warp;
+        if (x >= v.nx || y >= v.ny)
+            continue;
+        long long row = (long long) z*v.ny + y;
+        if (v.solidMask != nullptr && ((__ldg(&v.solidMask[row*v.wordsPerRow + tx]) >> lane) & 1u))
+            continue;
+        double dr = 0, jx = 0, jy = 0, jz = 0;
+        for (int q = 0; q < 19; q++) {
+            double fq = (double) loadq<T, R>(A + (long long) q*v.n + shifted(v, x, y, z, -cxr(q), -cyr(q), -czr(q)), q);
+            dr += fq;
+            jx += cxr(q)*fq;
+            jy += cyr(q)*fq;
+            jz += czr(q)*fq;
+        }
+        double inv = 1.0/(1.0 + dr);
+        double u[3] = {jx*inv, jy*inv, jz*inv};
+        long long node = row*v.nx + x;
+        double d2 = 0;
+        for (int a = 0; a < 3; a++) {
+            double* p = prev + a*v.n + node;
+            double d = u[a] - *p;
+            d2 += d*d;
+            *p = u[a];
+        }
+        if (!first)
+            maxDiff2 = fmax(maxDiff2, d2);
+        maxU2 = fmax(maxU2, u[0]*u[0] + u[1]*u[1] + u[2]*u[2]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        maxDiff2 = fmax(maxDiff2, __shfl_down_sync(0xffffffffu, maxDiff2, o));
+        maxU2 = fmax(maxU2, __shfl_down_sync(0xffffffffu, maxU2, o));
+    }
+    __shared__ double red[THREADS/32][2];
+    if (lane == 0) {
+        red[warp][0] = maxDiff2;
+        red[warp][1] = maxU2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < THREADS/32; w++) {
+            maxDiff2 = fmax(maxDiff2, red[w][0]);
+            maxU2 = fmax(maxU2, red[w][1]);
+        }
+        v.partials[NPART*(long long) blockIdx.x] = maxDiff2;
+        v.partials[NPART*(long long) blockIdx.x + 7] = maxU2;
+    }
+}
+
 // ---------------------------------------------------------------------------------------------------
 // Initial state and state transfer.
 // ---------------------------------------------------------------------------------------------------
@@ -515,6 +575,74 @@ __global__ void scatterKernel(T* A, T* B, int q, FluidView v, const double* in, 
         if (!bitsEqual(before, after))
             *changed = 1;
         storeq<T, R>(B + (long long) q*v.n + y, q, value);
+    }
+}
+
+// Velocity component a of node (x, y, z) in lattice units, 0 at solid nodes; out-of-lattice neighbours (open faces)
+// take the value of the node itself.
+__device__ __forceinline__ double velocityAt(const FluidView& v, const double* velocity, double scale, int x, int y,
+                                            int z, int a, long long self) {
+    long long node;
+    if (x < 0 || x >= v.nx || y < 0 || y >= v.ny || z < 0 || z >= v.nz) {
+        if (v.faceOpen)
+            node = self;
+        else
+            node = wrap(x, v.nx) + (long long) v.nx*(wrap(y, v.ny) + (long long) v.ny*wrap(z, v.nz));
+    }
+    else
+        node = x + (long long) v.nx*(y + (long long) v.ny*z);
+    long long row = node/v.nx;
+    int xx = (int) (node - row*v.nx);
+    if (v.solidMask != nullptr && ((v.solidMask[row*v.wordsPerRow + xx/32] >> (xx%32)) & 1u))
+        return 0.0;
+    return velocity[3*node + a]/scale;
+}
+
+// Populations of given fields (density [N], velocity [N][3] in the units of the fields, divided by the scales into
+// lattice units), written in the pull layout of both arrays: slot (q, y) holds the population that node x = y + c_q
+// pulls, the equilibrium w_q (rho - 1 + rho (3 c.u + 4.5 (c.u)^2 - 1.5 u^2)) of x plus, with `strain`, the
+// Chapman-Enskog non-equilibrium part -3 tau w_q rho (c.S.c - tr S/3) of the strain rate S (central differences of
+// the velocity, zero velocity at solid nodes), so that a steady flow starts without the transient of a stress-free
+// state; solid nodes hold 0.
+template <typename T, typename R>
+__global__ void equilibriumKernel(T* A, T* B, FluidView v, const double* density, const double* velocity,
+                                  double densityScale, double velocityScale, int strain) {
+    for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < 19*v.n; t += (long long) gridDim.x*blockDim.x) {
+        int q = (int) (t/v.n);
+        long long y = t - q*v.n;
+        Coords c = nodeCoords(y, v.nx, v.ny);
+        long long x = shifted(v, c.x, c.y, c.z, cxr(q), cyr(q), czr(q));
+        Coords cx = nodeCoords(x, v.nx, v.ny);
+        long long row = (long long) cx.z*v.ny + cx.y;
+        double value = 0;
+        if (v.solidMask == nullptr || !((v.solidMask[row*v.wordsPerRow + cx.x/32] >> (cx.x%32)) & 1u)) {
+            double rho = density[x]/densityScale;
+            double u[3] = {velocity[3*x]/velocityScale, velocity[3*x+1]/velocityScale, velocity[3*x+2]/velocityScale};
+            double cu = cxr(q)*u[0] + cyr(q)*u[1] + czr(q)*u[2];
+            double uu = u[0]*u[0] + u[1]*u[1] + u[2]*u[2];
+            value = weightOf<double>(q)*(rho - 1.0 + rho*(3.0*cu + 4.5*cu*cu - 1.5*uu));
+            if (strain) {
+                // grad[a][b] = d u_b / d x_a
+                double grad[3][3];
+                int cxyz[3] = {cx.x, cx.y, cx.z};
+                for (int a = 0; a < 3; a++) {
+                    int p[3] = {cxyz[0], cxyz[1], cxyz[2]}, m[3] = {cxyz[0], cxyz[1], cxyz[2]};
+                    p[a]++;
+                    m[a]--;
+                    for (int b = 0; b < 3; b++)
+                        grad[a][b] = 0.5*(velocityAt(v, velocity, velocityScale, p[0], p[1], p[2], b, x)
+                                          - velocityAt(v, velocity, velocityScale, m[0], m[1], m[2], b, x));
+                }
+                double c[3] = {(double) cxr(q), (double) cyr(q), (double) czr(q)};
+                double cSc = 0, tr = grad[0][0] + grad[1][1] + grad[2][2];
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++)
+                        cSc += c[a]*c[b]*0.5*(grad[a][b] + grad[b][a]);
+                value += -3.0*(1.0/v.omega)*weightOf<double>(q)*rho*(cSc - tr/3.0);
+            }
+        }
+        storeq<T, R>(A + t, q, (R) value);
+        storeq<T, R>(B + t, q, (R) value);
     }
 }
 
@@ -613,6 +741,13 @@ struct Launcher {
     }
     static void moments(const void* A, const FluidView& v, int grid, cudaStream_t s) {
         momentsKernel<T, R><<<grid, THREADS, 0, s>>>((const T*) A, v);
+    }
+    static void equilibrium(void* A, void* B, const FluidView& v, const double* rho, const double* u, double ds,
+                            double vs, int strain, cudaStream_t s) {
+        equilibriumKernel<T, R><<<1184, 256, 0, s>>>((T*) A, (T*) B, v, rho, u, ds, vs, strain);
+    }
+    static void residual(const void* A, const FluidView& v, double* prev, int first, int grid, cudaStream_t s) {
+        residualKernel<T, R><<<grid, THREADS, 0, s>>>((const T*) A, v, prev, first);
     }
     static void init(void* A, void* B, const FluidView& v, const char* fluid, const double* u, cudaStream_t s) {
         initKernel<T, R><<<1184, 256, 0, s>>>((T*) A, (T*) B, v, fluid, u[0], u[1], u[2]);
@@ -762,6 +897,8 @@ FluidEngine::~FluidEngine() {
     cudaFree(boundaryDev);
     cudaFree(stagingDev);
     cudaFree(faceDev);
+    cudaFree(residualPrevDev);
+    residualPrevDev = nullptr;
     faceDev = nullptr;
     for (cudaEvent_t e : profileEvents)
         cudaEventDestroy(e);
@@ -781,6 +918,10 @@ void FluidEngine::setParameters(const LbmLatticeParameters& l) {
         view.g[a] = l.body_acceleration[a];
     uint32_t seed = (uint32_t) l.random_number_seed;
     view.seed = seed;
+    view.faceOpen = 0;
+    for (int f = 0; f < 6; f++)
+        if (l.face_boundary[f] != LBM_BOUNDARY_PERIODIC)
+            view.faceOpen = 1;
     double cellMass = l.density*l.dx*l.dx*l.dx;
     bool fluctuate = l.fluid_fluctuations && l.fluid_kT > 0;
     view.mu = fluctuate ? 3.0*l.fluid_kT*l.dt*l.dt/(cellMass*l.dx*l.dx) : 0.0;
@@ -888,6 +1029,28 @@ void FluidEngine::momentsPass(bool setSums) {
     launches += 2;
 }
 
+double FluidEngine::steadyResidual(int interval) {
+    bool first = residualPrevDev == nullptr;
+    if (first)
+        CUDA_CHECK(cudaMalloc(&residualPrevDev, sizeof(double)*3*(size_t) view.n));
+    dispatchStorage(storageType, [&](auto L) {
+        decltype(L)::residual(pop[cur], view, residualPrevDev, first ? 1 : 0, gridBlocks, stream);
+    });
+    CUDA_CHECK(cudaGetLastError());
+    launches++;
+    std::vector<double> partials((size_t) NPART*gridBlocks);
+    CUDA_CHECK(cudaMemcpyAsync(partials.data(), partialsDev, sizeof(double)*partials.size(), cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    double maxDiff2 = 0, maxU2 = 0;
+    for (int b = 0; b < gridBlocks; b++) {
+        maxDiff2 = std::max(maxDiff2, partials[(size_t) NPART*b]);
+        maxU2 = std::max(maxU2, partials[(size_t) NPART*b + 7]);
+    }
+    if (first || maxU2 == 0)
+        return HUGE_VAL;
+    return std::sqrt(maxDiff2)/(interval*std::sqrt(maxU2));
+}
+
 void FluidEngine::restoreStats(const StepStats& stats) {
     statsHost = stats;
     CUDA_CHECK(cudaMemcpyAsync(statsDev, &statsHost, sizeof(StepStats), cudaMemcpyHostToDevice, stream));
@@ -929,6 +1092,28 @@ void FluidEngine::setState(const double* host) {
     CUDA_CHECK(cudaMemcpy(&changed, changedDev, sizeof(int), cudaMemcpyDeviceToHost));
     if (changed)
         momentsPass(true);
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+}
+
+void FluidEngine::setEquilibrium(const double* density, const double* velocity, bool onDevice, double densityScale,
+                                 double velocityScale, bool strain) {
+    const double* rho = density;
+    const double* u = velocity;
+    if (!onDevice) {
+        if (stagingDev == nullptr)
+            CUDA_CHECK(cudaMalloc(&stagingDev, sizeof(double)*4*(size_t) view.n));
+        double* staging = (double*) stagingDev;
+        CUDA_CHECK(cudaMemcpyAsync(staging, density, sizeof(double)*view.n, cudaMemcpyHostToDevice, stream));
+        CUDA_CHECK(cudaMemcpyAsync(staging + view.n, velocity, sizeof(double)*3*view.n, cudaMemcpyHostToDevice, stream));
+        rho = staging;
+        u = staging + view.n;
+    }
+    dispatchStorage(storageType, [&](auto L) {
+        decltype(L)::equilibrium(pop[cur], pop[1-cur], view, rho, u, densityScale, velocityScale, strain ? 1 : 0, stream);
+    });
+    CUDA_CHECK(cudaGetLastError());
+    launches++;
+    momentsPass(true);
     CUDA_CHECK(cudaStreamSynchronize(stream));
 }
 

@@ -39,6 +39,7 @@ struct FluidView {
     double numFluid;
     uint32_t seed;
     double mu;                 // 3 kT of the fluid fluctuations in lattice units (0: no fluctuations)
+    int faceOpen;              // some face is not periodic
     const uint32_t* solidMask; // bit per node, rows padded to 32 bits; NULL without solid nodes
     const uint32_t* reactMask; // bit per node with a coupling reaction; NULL without particles
     const void* reaction;      // 4 values (R) per node, lattice units
@@ -60,10 +61,17 @@ public:
     void step(long long stepIndex, bool remove, bool react);
     // Full moments pass over the current state: the largest speed, and with setSums the mass, momentum and ucm.
     void momentsPass(bool setSums);
+    // The steady-state residual max|u - u_prev|/(interval max|u|) in FP64 against the velocities of the previous call
+    // (u = j/rho of the post-stream state, fluid nodes); the first call records the velocities and returns infinity.
+    double steadyResidual(int interval);
     void restoreStats(const StepStats& stats);
     // Download the stats (synchronizes the stream).
     StepStats readStats();
     void fields(double* density, double* velocity, double densityScale, double velocityScale);
+    // Sets the state to the equilibrium of the fields (density [N], velocity [N][3], divided by the scales into lattice
+    // units), from host or device memory.
+    void setEquilibrium(const double* density, const double* velocity, bool onDevice, double densityScale,
+                        double velocityScale, bool strain);
     void setParameters(const LbmLatticeParameters& lattice);
     size_t stateBytes() const { return (size_t) 19*view.n*elementSize; }
     void* currentState() const { return pop[cur]; }
@@ -107,6 +115,7 @@ private:
     void* stagingDev;          // N doubles for state transfer
     int extraBlocks;           // blocks of the sparse passes that write partials
     double* faceDev;           // face velocities/densities and the boundary stress weight
+    double* residualPrevDev = nullptr;   // 3N velocities of the last residual call
     double faceHost[32];
     StepStats statsHost;
     bool profiling;

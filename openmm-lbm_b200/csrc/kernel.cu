@@ -191,6 +191,34 @@ void B200Kernel::getFluidFields(double* density, double* velocity) {
     fluid->fields(density, velocity, lattice.density, lattice.dx/lattice.dt);
 }
 
+void B200Kernel::setFluidEquilibrium(const double* density, const double* velocity, bool onDevice, bool strain) {
+    CUDA_CHECK(cudaSetDevice(device));
+    fluid->setEquilibrium(density, velocity, onDevice, lattice.density, lattice.dx/lattice.dt, strain);
+}
+
+// Steps the fluid from step firstStep until the steady residual, taken every `interval` steps against the velocities
+// of the previous check (the first check is the state at the start), is at most `tolerance`, or maxSteps steps.
+long long B200Kernel::steadySolve(long long firstStep, int interval, double tolerance, long long maxSteps,
+                                  double* residual) {
+    CUDA_CHECK(cudaSetDevice(device));
+    if (numParticles > 0)
+        throw Error(LBM_ERR_NOT_SUPPORTED, "lbm_steady_solve: the steady solve advances a fluid without coupled particles");
+    if (interval <= 0 || maxSteps < 0)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_steady_solve: the interval must be positive");
+    double r = fluid->steadyResidual(interval);
+    long long s = 0;
+    while (s < maxSteps && !(r <= tolerance)) {
+        for (int i = 0; i < interval && s < maxSteps; i++, s++) {
+            beginStep(firstStep + s, nullptr);
+            execute(firstStep + s, nullptr, false, false);
+        }
+        r = fluid->steadyResidual(interval);
+    }
+    if (residual)
+        *residual = r;
+    return s;
+}
+
 double B200Kernel::getFluidMachNumber() {
     CUDA_CHECK(cudaSetDevice(device));
     // The pass keeps the sums of the last step for the next removal, so that the result of a run does not

@@ -34,6 +34,8 @@ public:
     cudaStream_t getStream() const { return stream; }
     FluidEngine& fluidEngine() { return *fluid; }
     int solverIterations() const;
+    void setFluidEquilibrium(const double* density, const double* velocity, bool onDevice, bool strain);
+    long long steadySolve(long long firstStep, int interval, double tolerance, long long maxSteps, double* residual);
 private:
     void advanceFluid(const LbmParticleArrays* particles);
     void computeNextStepForces(long long stepCount, const LbmParticleArrays* particles);

@@ -90,6 +90,35 @@ class B200Kernel:
         check(self.lib.lbm_get_fluid_fields(self.handle, dptr(density), dptr(velocity)), self.lib)
         return density, velocity
 
+    def steady_residual(self, interval=100):
+        """max|u - u_prev|/(interval max|u|) against the previous call (infinity on the first), FP64 on the device."""
+        r = ctypes.c_double()
+        check(self.lib.lbm_steady_residual(self.handle, int(interval), ctypes.byref(r)), self.lib)
+        return r.value
+
+    def solve_steady(self, first_step=0, interval=100, tolerance=1e-6, max_steps=10**6):
+        """Steps until the steady residual is at most `tolerance`; returns (steps taken, last residual)."""
+        steps, r = ctypes.c_longlong(), ctypes.c_double()
+        check(self.lib.lbm_steady_solve(self.handle, int(first_step), int(interval), float(tolerance), int(max_steps),
+                                        ctypes.byref(steps), ctypes.byref(r)), self.lib)
+        return steps.value, r.value
+
+    def set_fluid_equilibrium(self, density, velocity, strain=True):
+        """The populations of the fields (units of get_fluid_fields): numpy arrays, or float64 torch CUDA tensors;
+        the equilibrium plus, with strain, the non-equilibrium part of the velocity's strain rate."""
+        if hasattr(density, 'data_ptr'):
+            assert density.is_cuda and density.dtype.itemsize == 8 and density.is_contiguous()
+            assert velocity.is_cuda and velocity.dtype.itemsize == 8 and velocity.is_contiguous()
+            check(self.lib.lbm_set_fluid_equilibrium(self.handle, density.data_ptr(), velocity.data_ptr(), MEMORY_DEVICE,
+                                                     int(strain)), self.lib)
+            return
+        density = np.ascontiguousarray(density, dtype=np.float64)
+        velocity = np.ascontiguousarray(velocity, dtype=np.float64)
+        if density.size != self.num_nodes or velocity.size != 3*self.num_nodes:
+            raise ValueError('set_fluid_equilibrium: one density and three velocity components per node')
+        check(self.lib.lbm_set_fluid_equilibrium(self.handle, density.ctypes.data, velocity.ctypes.data, MEMORY_HOST,
+                                                 int(strain)), self.lib)
+
     def get_fluid_mach_number(self):
         mach = ctypes.c_double()
         check(self.lib.lbm_get_fluid_mach_number(self.handle, ctypes.byref(mach)), self.lib)

@@ -26,12 +26,14 @@ def declared_functions():
 def test_library_exports_every_declared_symbol():
     from lbm_b200.md import _SIGNATURES as MD_SIGNATURES
     from lbm_b200.batch import _SIGNATURES as BATCH_SIGNATURES
+    from lbm_b200.warmstart import _SIGNATURES as WARMSTART_SIGNATURES
     lib = load_library()
     names = declared_functions()
-    assert len(names) >= 34
+    assert len(names) >= 39
     for name in names:
         assert hasattr(lib, name), name
-        assert name in SIGNATURES or name in MD_SIGNATURES or name in BATCH_SIGNATURES, name
+        assert (name in SIGNATURES or name in MD_SIGNATURES or name in BATCH_SIGNATURES
+                or name in WARMSTART_SIGNATURES), name
 
 
 def lattice_of(force, box=(3.0, 3.0, 3.0), dt=0.01, masses=(1.0,)):
