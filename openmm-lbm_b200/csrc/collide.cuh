@@ -170,7 +170,9 @@ __device__ __forceinline__ CollideConstants<R> collideConstants(double omega, co
 // One fluid node of the dense step: pull streaming from the periodic neighbours in A, moments, momentum removal,
 // regularized collision with Guo forcing (body force plus the extra force e, the particle reaction), Philox
 // fluctuations when FLUCT, and the store into B.  Node indices are 32-bit; (x, y, z) are the node's coordinates in
-// an nx x ny x nz lattice of N nodes.  The stored mass and momentum deviations are added to the sums.
+// an nx x ny x nz lattice of N nodes.  The node's mass and momentum deviations after the collision are added to the
+// sums: the collision conserves mass and gives the momentum j + F (the fluctuation modes carry neither), so they are
+// dr and j + F, equal to the sums of the stored values up to the rounding of the stores.
 template <typename T, typename R, bool FLUCT>
 __device__ __forceinline__ void collideNode(const T* __restrict__ A, T* __restrict__ B, unsigned N, unsigned node,
                                             int x, int y, int z, int nx, int ny, int nz, const CollideConstants<R>& k,
@@ -221,7 +223,6 @@ __device__ __forceinline__ void collideNode(const T* __restrict__ A, T* __restri
     R qtr = (qxx + qyy + qzz)*R(1.0/3.0);
     // Terms common to all directions: dr - 1.5 rho u.u - 1.5 u.F.
     const R base = m.dr - R(1.5)*(rho*uu + uf);
-    R outMass = 0, outX = 0, outY = 0, outZ = 0;
     // Stochastic rounding of the 16-bit stores: one dither word per pair of directions.
     Dither dither(dithered ? node : 0, dithered ? step : 0);
     // q = 0
@@ -232,15 +233,13 @@ __device__ __forceinline__ void collideNode(const T* __restrict__ A, T* __restri
             ghostParts<R, 0>(a, e, o);
             value += e;
         }
-        R stored = Storage<T>::template storeOne<0>(B + node, value, dithered ? dither.next() : 0u);
-        outMass += R(Storage<T>::template scale<0>())*stored;
+        Storage<T>::template storeOne<0>(B + node, value, dithered ? dither.template word<0>() : 0u);
     }
     // Pairs (q, q+1) with c_{q+1} = -c_q.
     staticFor<9>([&](auto pc) {
         constexpr int q = 2*decltype(pc)::value + 1;
         constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
         constexpr R w = wOf<R>(q);
-        constexpr R s = R(Storage<T>::template scale<q>());
         R cu = R(cx)*ux + R(cy)*uy + R(cz)*uz;
         R cf = R(cx)*Fx + R(cy)*Fy + R(cz)*Fz;
         R cqc = R(cx*cx)*qxx + R(cy*cy)*qyy + R(cz*cz)*qzz - qtr
@@ -255,17 +254,12 @@ __device__ __forceinline__ void collideNode(const T* __restrict__ A, T* __restri
         }
         R s1, s2;
         Storage<T>::template storePair<q>(B + ((size_t) q*N + node), B + ((size_t) (q+1)*N + node), even + odd,
-                                          even - odd, dithered ? dither.next() : 0u, s1, s2);
-        outMass += s*(s1 + s2);
-        R d = s*(s1 - s2);
-        if (cx != 0) outX += R(cx)*d;
-        if (cy != 0) outY += R(cy)*d;
-        if (cz != 0) outZ += R(cz)*d;
+                                          even - odd, dithered ? dither.template word<(q + 1)/2>() : 0u, s1, s2);
     });
-    sumMass += outMass;
-    sumX += outX;
-    sumY += outY;
-    sumZ += outZ;
+    sumMass += m.dr;
+    sumX += px;
+    sumY += py;
+    sumZ += pz;
 }
 
 } // namespace

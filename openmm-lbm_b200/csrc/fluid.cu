@@ -17,6 +17,7 @@
 #include "lbm_device.cuh"
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <utility>
@@ -161,6 +162,223 @@ streamCollideKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int
             }
         }
         collideNode<T, R, FLUCT>(A, B, N, node, x, y, z, nx, ny, nz, k, ex, ey, ez, step, sumMass, sumX, sumY, sumZ);
+    }
+    double acc[NPART] = {(double) sumMass, (double) sumX, (double) sumY, (double) sumZ, 0, 0, 0, 0};
+    blockReduceStore(acc, v.partials + NPART*(long long) blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// The dense step for 16-bit storage without fluctuations: two x-adjacent nodes per thread, their arithmetic in
+// packed FP32 pairs (FFMA2 / FADD2 / FMUL2 of sm_100), their populations loaded and stored as 32-bit pairs.  For a
+// direction with c_x = 0 the pair of sources is one aligned word of the source row; with c_x = +1 it is the high half
+// of the word to the left and the low half of this word, with c_x = -1 the high half of this word and the low half
+// of the word to the right (the lattice has an even nx, so the periodic wrap keeps the pairs aligned).  The
+// algebra is that of collideNode (collide.cuh), written for the pairs.
+// ---------------------------------------------------------------------------------------------------
+
+struct F2 {
+    float2 v;
+};
+__device__ __forceinline__ F2 f2(float a) { return F2{make_float2(a, a)}; }
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2{__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2{__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return F2{__ffma2_rn(a.v, b.v, c.v)}; }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2{__ffma2_rn(b.v, make_float2(-1.0f, -1.0f), a.v)}; }
+
+template <typename T> struct Pair16;
+template <> struct Pair16<__half> {
+    static __device__ __forceinline__ F2 decode(uint32_t w) {
+        __half2 h = *reinterpret_cast<__half2*>(&w);
+        return F2{__half22float2(h)};
+    }
+    static constexpr uint32_t ditherMask = 0x1FFFu;
+    static __device__ __forceinline__ uint32_t pack(float lo, float hi) {   // round toward zero (after the dither)
+        uint32_t r;
+        asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+        return r;
+    }
+    static constexpr float scale = kHalfScale;
+};
+template <> struct Pair16<__nv_bfloat16> {
+    static __device__ __forceinline__ F2 decode(uint32_t w) {
+        return F2{make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xFFFF0000u))};
+    }
+    static constexpr uint32_t ditherMask = 0xFFFFu;
+    static __device__ __forceinline__ uint32_t pack(float lo, float hi) {
+        uint32_t r;
+        asm("cvt.rz.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+        return r;
+    }
+    static constexpr float scale = 1.0f;
+};
+
+// Stochastic rounding of a pair of FP32 values (two nodes, one direction) to 16 bits, packed in one word.
+template <typename T>
+__device__ __forceinline__ uint32_t ditherPack(F2 value, uint32_t da, uint32_t db) {
+    float a = __uint_as_float(__float_as_uint(value.v.x) + (da & Pair16<T>::ditherMask));
+    float b = __uint_as_float(__float_as_uint(value.v.y) + (db & Pair16<T>::ditherMask));
+    return Pair16<T>::pack(a, b);
+}
+
+constexpr int PAIR_TX = 64;         // nodes per tile row: 2 per lane
+
+// Stores the 16-bit pair of a direction, leaving the half of a solid node untouched (as the one-node kernel does).
+template <bool SOLID>
+__device__ __forceinline__ void storePairWord(uint32_t* p, uint32_t w, bool solidA, bool solidB) {
+    if (SOLID && (solidA || solidB)) {
+        unsigned short* h = reinterpret_cast<unsigned short*>(p);
+        if (!solidA)
+            h[0] = (unsigned short) (w & 0xFFFFu);
+        if (!solidB)
+            h[1] = (unsigned short) (w >> 16);
+        return;
+    }
+    *p = w;
+}
+
+template <typename T, bool SOLID, bool REACT>
+__global__ void __launch_bounds__(THREADS, 2)
+streamCollidePairKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int remove, long long step) {
+    const int lane = threadIdx.x%32, warp = threadIdx.x/32;
+    const unsigned N = (unsigned) v.n;
+    const int nx = v.nx, ny = v.ny, nz = v.nz;
+    const uint32_t* __restrict__ a32 = reinterpret_cast<const uint32_t*>(A);
+    uint32_t* __restrict__ b32 = reinterpret_cast<uint32_t*>(B);
+    const unsigned halfN = N/2;                       // words per direction plane (N is even)
+    const float om1 = 1.0f - (float) v.omega;
+    const F2 gx = f2((float) v.g[0]), gy = f2((float) v.g[1]), gz = f2((float) v.g[2]);
+    F2 nux0 = f2(0.0f), nuy0 = f2(0.0f), nuz0 = f2(0.0f);
+    if (remove) {
+        nux0 = f2(-(float) v.stats->ucm[0]);
+        nuy0 = f2(-(float) v.stats->ucm[1]);
+        nuz0 = f2(-(float) v.stats->ucm[2]);
+    }
+    float sumMass = 0, sumX = 0, sumY = 0, sumZ = 0;
+    const int tilesX = (nx + PAIR_TX - 1)/PAIR_TX, tilesY = v.tilesY;
+    const unsigned numTiles = (unsigned) tilesX*tilesY*nz, stride = gridDim.x;
+    const uint32_t stepHash = Dither::fmix32((uint32_t) step + 0x9E3779B9u*(uint32_t) ((unsigned long long) step >> 32));
+    for (unsigned t = blockIdx.x; t < numTiles; t += stride) {
+        const int tx = (int) (t%tilesX);
+        const unsigned rr = t/tilesX;
+        const int y = (int) (rr%tilesY)*TY + warp, z = (int) (rr/tilesY);
+        const int x0 = tx*PAIR_TX + 2*lane;
+        if (x0 >= nx || y >= ny)
+            continue;
+        const unsigned row = (unsigned) z*ny + y;
+        bool solidA = false, solidB = false;
+        if (SOLID) {
+            uint32_t word = __ldg(&v.solidMask[(size_t) row*v.wordsPerRow + (x0 >> 5)]);
+            solidA = (word >> (x0 & 31)) & 1u;
+            solidB = (word >> ((x0 + 1) & 31)) & 1u;
+            if (solidA && solidB)
+                continue;
+        }
+        const unsigned node = row*nx + x0;
+        // Rows of the pull sources: index [1 - cy][1 - cz] (periodic in y and z).
+        const int ys[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};
+        const int zs[3] = {z == 0 ? nz - 1 : z - 1, z, z == nz - 1 ? 0 : z + 1};
+        const int xl = x0 == 0 ? nx - 2 : x0 - 2, xr = x0 + 2 == nx ? 0 : x0 + 2;
+        F2 r[19];
+        staticFor<19>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+            const unsigned base = ((unsigned) zs[1-cz]*ny + ys[1-cy])*nx;
+            const uint32_t* plane = a32 + (size_t) q*halfN;
+            uint32_t w;
+            if (cx == 0)
+                w = __ldg(plane + (base + x0)/2);
+            else if (cx == 1)
+                w = __byte_perm(__ldg(plane + (base + xl)/2), __ldg(plane + (base + x0)/2), 0x5432);
+            else
+                w = __byte_perm(__ldg(plane + (base + x0)/2), __ldg(plane + (base + xr)/2), 0x5432);
+            r[q] = Pair16<T>::decode(w);
+        });
+        // Moments (deviations), the storage factors folded into the FMAs.
+        F2 dr = f2(Storage<T>::template scale<0>())*r[0];
+        F2 jx = f2(0), jy = f2(0), jz = f2(0), sxx = f2(0), syy = f2(0), szz = f2(0), sxy = f2(0), sxz = f2(0), syz = f2(0);
+        staticFor<9>([&](auto pc) {
+            constexpr int q = 2*decltype(pc)::value + 1;
+            constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+            constexpr float s = Storage<T>::template scale<q>();
+            const F2 S = r[q] + r[q+1], D = r[q] - r[q+1];
+            dr = fma2(f2(s), S, dr);
+            if (cx != 0) { jx = fma2(f2(cx*s), D, jx); sxx = fma2(f2(s), S, sxx); }
+            if (cy != 0) { jy = fma2(f2(cy*s), D, jy); syy = fma2(f2(s), S, syy); }
+            if (cz != 0) { jz = fma2(f2(cz*s), D, jz); szz = fma2(f2(s), S, szz); }
+            if (cx*cy != 0) sxy = fma2(f2(cx*cy*s), S, sxy);
+            if (cx*cz != 0) sxz = fma2(f2(cx*cz*s), S, sxz);
+            if (cy*cz != 0) syz = fma2(f2(cy*cz*s), S, syz);
+        });
+        const F2 rho = dr + f2(1.0f);
+        const F2 inv = F2{make_float2(__fdividef(1.0f, rho.v.x), __fdividef(1.0f, rho.v.y))};
+        const F2 ninv = F2{make_float2(-inv.v.x, -inv.v.y)};
+        const F2 dr3 = fma2(dr, f2(-1.0f/3.0f), f2(0.0f));
+        // Pi_neq = S2 - dr/3 - j j/rho.
+        const F2 jxi = jx*ninv, jyi = jy*ninv;
+        const F2 pxx = fma2(jx, jxi, sxx + dr3), pyy = fma2(jy, jyi, syy + dr3), pzz = fma2(jz, jz*ninv, szz + dr3);
+        const F2 pxy = fma2(jy, jxi, sxy), pxz = fma2(jz, jxi, sxz), pyz = fma2(jz, jyi, syz);
+        if (remove) {
+            jx = fma2(rho, nux0, jx);
+            jy = fma2(rho, nuy0, jy);
+            jz = fma2(rho, nuz0, jz);
+        }
+        F2 Fx = rho*gx, Fy = rho*gy, Fz = rho*gz;
+        if (REACT) {
+            uint32_t word = __ldg(&v.reactMask[(size_t) row*v.wordsPerRow + (x0 >> 5)]);
+            const float* rp = reinterpret_cast<const float*>(v.reaction) + 4*(size_t) node;
+            if ((word >> (x0 & 31)) & 1u) {
+                Fx.v.x += rp[0]; Fy.v.x += rp[1]; Fz.v.x += rp[2];
+            }
+            if ((word >> ((x0 + 1) & 31)) & 1u) {
+                Fx.v.y += rp[4]; Fy.v.y += rp[5]; Fz.v.y += rp[6];
+            }
+        }
+        const F2 ux = fma2(Fx, f2(0.5f), jx)*inv, uy = fma2(Fy, f2(0.5f), jy)*inv, uz = fma2(Fz, f2(0.5f), jz)*inv;
+        const F2 uu = fma2(uz, uz, fma2(uy, uy, ux*ux)), uf = fma2(uz, Fz, fma2(uy, Fy, ux*Fx));
+        const F2 px = jx + Fx, py = jy + Fy, pz = jz + Fz;
+        const F2 s45 = f2(om1*4.5f), s9 = f2(om1*9.0f);
+        const F2 qxx = s45*pxx, qyy = s45*pyy, qzz = s45*pzz, qxy = s9*pxy, qxz = s9*pxz, qyz = s9*pyz;
+        const F2 qtr = (qxx + qyy + qzz)*f2(1.0f/3.0f);
+        const F2 base = fma2(fma2(rho, uu, uf), f2(-1.5f), dr);
+        // Dither words of the two nodes (the hash of collideNode's Dither, per node).
+        const uint32_t hashA = Dither::fmix32(node ^ stepHash), hashB = Dither::fmix32((node + 1) ^ stepHash);
+        uint32_t* outPlane = b32 + node/2;
+        {
+            constexpr float k0 = Pair16<T>::scale*storeFactorOf(0);
+            const F2 value = (base - qtr)*f2(k0/3.0f);
+            storePairWord<SOLID>(outPlane, ditherPack<T>(value, hashA*0x9E3779B1u, hashB*0x9E3779B1u), solidA, solidB);
+        }
+        staticFor<9>([&](auto pc) {
+            constexpr int p = decltype(pc)::value;
+            constexpr int q = 2*p + 1;
+            constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+            constexpr float k = Pair16<T>::scale*storeFactorOf(q);
+            F2 cu = f2(0), cf = f2(0), cp = f2(0);
+            if (cx != 0) { cu = fma2(f2((float) cx), ux, cu); cf = fma2(f2((float) cx), Fx, cf); cp = fma2(f2((float) cx), px, cp); }
+            if (cy != 0) { cu = fma2(f2((float) cy), uy, cu); cf = fma2(f2((float) cy), Fy, cf); cp = fma2(f2((float) cy), py, cp); }
+            if (cz != 0) { cu = fma2(f2((float) cz), uz, cu); cf = fma2(f2((float) cz), Fz, cf); cp = fma2(f2((float) cz), pz, cp); }
+            F2 cqc = f2(0) - qtr;
+            if (cx != 0) cqc = cqc + qxx;
+            if (cy != 0) cqc = cqc + qyy;
+            if (cz != 0) cqc = cqc + qzz;
+            if (cx*cy != 0) cqc = fma2(f2((float) (cx*cy)), qxy, cqc);
+            if (cx*cz != 0) cqc = fma2(f2((float) (cx*cz)), qxz, cqc);
+            if (cy*cz != 0) cqc = fma2(f2((float) (cy*cz)), qyz, cqc);
+            // even and odd in storage units: k w_q (...) and k 3 w_q c.(j + F).
+            const F2 even = fma2(cu*fma2(rho, cu, cf), f2(4.5f), base + cqc)*f2(k*wOf<float>(q));
+            const F2 odd = cp*f2(k*oddOf<float>(q));
+            const uint32_t wa = hashA*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
+            const uint32_t wb = hashB*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
+            storePairWord<SOLID>(outPlane + (size_t) q*halfN, ditherPack<T>(even + odd, wa, wb), solidA, solidB);
+            storePairWord<SOLID>(outPlane + (size_t) (q + 1)*halfN, ditherPack<T>(even - odd, wa >> 16, wb >> 16),
+                                 solidA, solidB);
+        });
+        if (!solidA) {
+            sumMass += dr.v.x; sumX += px.v.x; sumY += py.v.x; sumZ += pz.v.x;
+        }
+        if (!solidB) {
+            sumMass += dr.v.y; sumX += px.v.y; sumY += py.v.y; sumZ += pz.v.y;
+        }
     }
     double acc[NPART] = {(double) sumMass, (double) sumX, (double) sumY, (double) sumZ, 0, 0, 0, 0};
     blockReduceStore(acc, v.partials + NPART*(long long) blockIdx.x);
@@ -684,6 +902,16 @@ template <typename T>
 struct Launcher {
     typedef typename ComputeOf<T>::type R;
 
+    // The paired 16-bit kernel serves lattices with an even nx unless LBM_B200_PAIRED16=0 in the environment.
+    static bool pairedKernels() {
+        static int enabled = -1;
+        if (enabled < 0) {
+            const char* e = std::getenv("LBM_B200_PAIRED16");
+            enabled = (e != nullptr && e[0] == '0') ? 0 : 1;
+        }
+        return enabled == 1;
+    }
+
     // The persistent grid of a kernel variant: one wave of resident blocks (blocks per SM of this variant times
     // the SMs), so that every block processes the same number of tiles in one wave.
     template <bool S, bool RE, bool FL>
@@ -698,8 +926,28 @@ struct Launcher {
         }
         return (int) std::max(1LL, std::min((long long) blocks, v.numTiles));
     }
+    template <bool S, bool RE>
+    static int pairGrid(const FluidView& v) {
+        static int blocks = 0;
+        if (blocks == 0) {
+            int perSM = 0, device = 0, sms = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, streamCollidePairKernel<T, S, RE>, THREADS, 0);
+            cudaGetDevice(&device);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+            blocks = std::max(1, perSM)*std::max(1, sms);
+        }
+        long long tiles = (long long) ((v.nx + PAIR_TX - 1)/PAIR_TX)*v.tilesY*v.nz;
+        return (int) std::max(1LL, std::min((long long) blocks, tiles));
+    }
     template <bool S, bool RE, bool FL>
     static int dense(const void* A, void* B, const FluidView& v, int remove, long long step, int maxGrid, cudaStream_t s) {
+        if constexpr (sizeof(T) == 2 && !FL) {
+            if (v.nx%2 == 0 && pairedKernels()) {
+                int grid = std::min(maxGrid, pairGrid<S, RE>(v));
+                streamCollidePairKernel<T, S, RE><<<grid, THREADS, 0, s>>>((const T*) A, (T*) B, v, remove, step);
+                return grid;
+            }
+        }
         int grid = std::min(maxGrid, residentGrid<S, RE, FL>(v));
         streamCollideKernel<T, R, S, RE, FL><<<grid, THREADS, 0, s>>>((const T*) A, (T*) B, v, remove, step);
         return grid;
@@ -729,6 +977,10 @@ struct Launcher {
         probe(streamCollideKernel<T, R, false, false, true>);
         probe(streamCollideKernel<T, R, true, true, true>);
         probe(streamCollideKernel<T, R, true, false, false>);
+        if constexpr (sizeof(T) == 2) {
+            probe(streamCollidePairKernel<T, false, false>);
+            probe(streamCollidePairKernel<T, true, true>);
+        }
         return best;
     }
     static void bounceBack(void* B, const int* wall, int numWall, const FluidView& v, double* partials, int grid, cudaStream_t s) {

@@ -115,22 +115,20 @@ template <> struct Storage<__nv_bfloat16> {
     }
 };
 
-// Dither words of the stores of one node and step: the MurmurHash3 32-bit finaliser (Appleby) of the node
-// and step mixed together seeds a xorshift32 stream (Marsaglia 2003, shifts 13, 17, 5); each word serves two
-// stores (low and high halves).
+// Dither words of the stores of one node and step: the MurmurHash3 32-bit finaliser (Appleby) of the node and
+// step mixed together; word k is that hash times an odd constant, a bijection of the hash, so each word is uniform
+// when the hash is (one multiply per word).  Each word serves two stores (low and high halves).
 struct Dither {
-    uint32_t state;
+    uint32_t hash;
     static __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
         h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
         return h;
     }
     __device__ __forceinline__ Dither(long long node, long long step) {
-        uint32_t h = fmix32((uint32_t) node ^ fmix32((uint32_t) step + 0x9E3779B9u*(uint32_t) ((unsigned long long) node >> 32)));
-        state = h ? h : 0x6A09E667u;
+        hash = fmix32((uint32_t) node ^ fmix32((uint32_t) step + 0x9E3779B9u*(uint32_t) ((unsigned long long) node >> 32)));
     }
-    __device__ __forceinline__ uint32_t next() {
-        state ^= state << 13; state ^= state >> 17; state ^= state << 5;
-        return state;
+    template <int k> __device__ __forceinline__ uint32_t word() const {
+        return hash*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) k);
     }
 };
 

@@ -357,6 +357,45 @@ def evaluate(net, cases, shape, inlet, tolerance=1e-6, max_steps=300000):
     return rows
 
 
+def conv_benchmark(shape=(128, 64, 64), widths=(16, 32, 64, 160), batch=2, repeats=5):
+    """Device time (CUDA events) of the forward and weight-gradient convolutions of every layer shape of the U-Net at
+    `shape` and `batch`: per layer the FLOPs (2 x voxels x 27 cin x cout per pass) and the TFLOP/s reached."""
+    nx, ny, nz = shape
+    layers, c = [], IN_CHANNELS
+    for level, w in enumerate(widths):
+        s = 2**level
+        layers += [((nz//s, ny//s, nx//s), c, w), ((nz//s, ny//s, nx//s), w, w)]
+        c = w
+    for level in range(len(widths) - 2, -1, -1):
+        s = 2**level
+        layers += [((nz//s, ny//s, nx//s), widths[level + 1] + widths[level], widths[level]),
+                   ((nz//s, ny//s, nx//s), widths[level], widths[level])]
+    layers.append(((nz, ny, nx), widths[0], 16))
+    rows = []
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for (d, h, w), cin, cout in layers:
+        x = _volume(torch.randn((batch, cin, d, h, w), device='cuda').to(torch.bfloat16))
+        wt = (torch.randn((cout, 27, cin), device='cuda')*0.1).to(torch.bfloat16)
+        dy = _volume(torch.randn((batch, cout, d, h, w), device='cuda').to(torch.bfloat16))
+        flops = 2.0*batch*d*h*w*27*cin*cout
+        times = {}
+        for name, fn in (('forward', lambda: conv3d_forward(x, wt)), ('weight_grad', lambda: conv3d_weight_grad(x, dy))):
+            fn()
+            torch.cuda.synchronize()
+            start.record()
+            for _ in range(repeats):
+                fn()
+            stop.record()
+            torch.cuda.synchronize()
+            times[name] = start.elapsed_time(stop)/repeats
+        rows.append({'volume': [d, h, w], 'cin': cin, 'cout': cout, 'gflop': flops/1e9,
+                     'forward_ms': times['forward'], 'forward_tflops': flops/(times['forward']*1e-3)/1e12,
+                     'weight_grad_ms': times['weight_grad'],
+                     'weight_grad_tflops': flops/(times['weight_grad']*1e-3)/1e12})
+    conv_status()
+    return rows
+
+
 def main(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument('--train', type=int, default=2000)
@@ -398,9 +437,10 @@ def main(argv=None):
               'steps_ratio_total': float(sum(r['cold_steps'] for r in rows)/max(1, sum(r['warm_steps'] for r in rows))),
               'final_velocity_error_max': float(errors.max()), 'final_velocity_error_mean': float(errors.mean()),
               'cases': rows}
+    report['conv_benchmark'] = conv_benchmark(shape, tuple(int(w) for w in args.widths.split(',')), args.batch)
     with open(args.out, 'w') as f:
         json.dump(report, f)
-    log(json.dumps({k: v for k, v in report.items() if k not in ('cases', 'loss_history')}))
+    log(json.dumps({k: v for k, v in report.items() if k not in ('cases', 'loss_history', 'conv_benchmark')}))
     return report
 
 
