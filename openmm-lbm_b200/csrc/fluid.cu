@@ -185,9 +185,16 @@ __device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2{__fmul2_rn(a.v, 
 __device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return F2{__ffma2_rn(a.v, b.v, c.v)}; }
 __device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2{__ffma2_rn(b.v, make_float2(-1.0f, -1.0f), a.v)}; }
 
-template <typename T> struct Pair16;
-template <> struct Pair16<__half> {
-    static __device__ __forceinline__ F2 decode(uint32_t w) {
+// Words of two x-adjacent nodes of one direction: a 32-bit word for 16-bit storage (stochastic rounding on store),
+// a float2 for FP32 storage.  left(l, c) is the pair (x0 - 1, x0) from the word to the left and this one, right(c, r)
+// the pair (x0 + 1, x0 + 2).
+template <typename T> struct PairIO;
+template <> struct PairIO<__half> {
+    typedef uint32_t Word;
+    static constexpr float scale = kHalfScale;
+    static __device__ __forceinline__ Word left(Word l, Word c) { return __byte_perm(l, c, 0x5432); }
+    static __device__ __forceinline__ Word right(Word c, Word r) { return __byte_perm(c, r, 0x5432); }
+    static __device__ __forceinline__ F2 decode(Word w) {
         __half2 h = *reinterpret_cast<__half2*>(&w);
         return F2{__half22float2(h)};
     }
@@ -197,10 +204,13 @@ template <> struct Pair16<__half> {
         asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
         return r;
     }
-    static constexpr float scale = kHalfScale;
 };
-template <> struct Pair16<__nv_bfloat16> {
-    static __device__ __forceinline__ F2 decode(uint32_t w) {
+template <> struct PairIO<__nv_bfloat16> {
+    typedef uint32_t Word;
+    static constexpr float scale = 1.0f;
+    static __device__ __forceinline__ Word left(Word l, Word c) { return __byte_perm(l, c, 0x5432); }
+    static __device__ __forceinline__ Word right(Word c, Word r) { return __byte_perm(c, r, 0x5432); }
+    static __device__ __forceinline__ F2 decode(Word w) {
         return F2{make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xFFFF0000u))};
     }
     static constexpr uint32_t ditherMask = 0xFFFFu;
@@ -209,43 +219,92 @@ template <> struct Pair16<__nv_bfloat16> {
         asm("cvt.rz.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
         return r;
     }
-    static constexpr float scale = 1.0f;
+};
+template <> struct PairIO<float> {
+    typedef float2 Word;
+    static __device__ __forceinline__ Word left(Word l, Word c) { return make_float2(l.y, c.x); }
+    static __device__ __forceinline__ Word right(Word c, Word r) { return make_float2(c.y, r.x); }
+    static __device__ __forceinline__ F2 decode(Word w) { return F2{w}; }
 };
 
-// Stochastic rounding of a pair of FP32 values (two nodes, one direction) to 16 bits, packed in one word.
-template <typename T>
-__device__ __forceinline__ uint32_t ditherPack(F2 value, uint32_t da, uint32_t db) {
-    float a = __uint_as_float(__float_as_uint(value.v.x) + (da & Pair16<T>::ditherMask));
-    float b = __uint_as_float(__float_as_uint(value.v.y) + (db & Pair16<T>::ditherMask));
-    return Pair16<T>::pack(a, b);
+// Factor from a deviation to the stored value of direction q.
+template <typename T, int q> __device__ __forceinline__ constexpr float storeScale() {
+    if constexpr (sizeof(T) == 2)
+        return PairIO<T>::scale*storeFactorOf(q);
+    else
+        return 1.0f;
 }
 
 constexpr int PAIR_TX = 64;         // nodes per tile row: 2 per lane
 
-// Stores the 16-bit pair of a direction, leaving the half of a solid node untouched (as the one-node kernel does).
-template <bool SOLID>
-__device__ __forceinline__ void storePairWord(uint32_t* p, uint32_t w, bool solidA, bool solidB) {
-    if (SOLID && (solidA || solidB)) {
-        unsigned short* h = reinterpret_cast<unsigned short*>(p);
-        if (!solidA)
-            h[0] = (unsigned short) (w & 0xFFFFu);
-        if (!solidB)
-            h[1] = (unsigned short) (w >> 16);
-        return;
+// Stores the pair `value` (stored units) of one direction; the half of a solid node stays untouched (as in the
+// one-node kernel).  16-bit storage rounds stochastically with the dither words da, db of the two nodes.
+template <typename T, bool SOLID>
+__device__ __forceinline__ void storePair(typename PairIO<T>::Word* p, F2 value, uint32_t da, uint32_t db, bool solidA,
+                                          bool solidB) {
+    if constexpr (sizeof(T) == 2) {
+        float a = __uint_as_float(__float_as_uint(value.v.x) + (da & PairIO<T>::ditherMask));
+        float b = __uint_as_float(__float_as_uint(value.v.y) + (db & PairIO<T>::ditherMask));
+        uint32_t w = PairIO<T>::pack(a, b);
+        if (SOLID && (solidA || solidB)) {
+            unsigned short* h = reinterpret_cast<unsigned short*>(p);
+            if (!solidA)
+                h[0] = (unsigned short) (w & 0xFFFFu);
+            if (!solidB)
+                h[1] = (unsigned short) (w >> 16);
+            return;
+        }
+        *p = w;
     }
-    *p = w;
+    else {
+        if (SOLID && (solidA || solidB)) {
+            float* h = reinterpret_cast<float*>(p);
+            if (!solidA)
+                h[0] = value.v.x;
+            if (!solidB)
+                h[1] = value.v.y;
+            return;
+        }
+        *p = value.v;
+    }
 }
 
-template <typename T, bool SOLID, bool REACT>
-__global__ void __launch_bounds__(THREADS, 2)
+// Ghost-mode parts of direction q for a pair of nodes, without the weight: sums over the odd and the even modes
+// k = 10..18 of e_k(c_q) a_k.
+template <int q>
+__device__ __forceinline__ void ghostSums2(const F2 a[15], F2& even, F2& odd) {
+    even = f2(0.0f);
+    odd = f2(0.0f);
+    staticFor<9>([&](auto kc) {
+        constexpr int k = decltype(kc)::value + 10;
+        constexpr float m = (float) modeValue(k, q);
+        if (m != 0.0f) {
+            if (k <= 15)
+                odd = fma2(f2(m), a[k-4], odd);
+            else
+                even = fma2(f2(m), a[k-4], even);
+        }
+    });
+}
+
+#ifndef LBM_PAIR_MIN_BLOCKS
+#define LBM_PAIR_MIN_BLOCKS 2
+#endif
+
+// The dense step with two x-adjacent nodes per thread (nx even), the arithmetic of both in packed FP32 pairs.
+template <typename T, bool SOLID, bool REACT, bool FLUCT>
+__global__ void __launch_bounds__(THREADS, LBM_PAIR_MIN_BLOCKS)
 streamCollidePairKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int remove, long long step) {
+    typedef typename PairIO<T>::Word Word;
+    constexpr bool dithered = sizeof(T) == 2;
     const int lane = threadIdx.x%32, warp = threadIdx.x/32;
     const unsigned N = (unsigned) v.n;
     const int nx = v.nx, ny = v.ny, nz = v.nz;
-    const uint32_t* __restrict__ a32 = reinterpret_cast<const uint32_t*>(A);
-    uint32_t* __restrict__ b32 = reinterpret_cast<uint32_t*>(B);
+    const Word* __restrict__ aw = reinterpret_cast<const Word*>(A);
+    Word* __restrict__ bw = reinterpret_cast<Word*>(B);
     const unsigned halfN = N/2;                       // words per direction plane (N is even)
-    const float om1 = 1.0f - (float) v.omega;
+    const float om = (float) v.omega, om1 = 1.0f - om;
+    const float mu = (float) v.mu, stressFactor = om*(2.0f - om);
     const F2 gx = f2((float) v.g[0]), gy = f2((float) v.g[1]), gz = f2((float) v.g[2]);
     F2 nux0 = f2(0.0f), nuy0 = f2(0.0f), nuz0 = f2(0.0f);
     if (remove) {
@@ -283,15 +342,15 @@ streamCollidePairKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v,
             constexpr int q = decltype(qc)::value;
             constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
             const unsigned base = ((unsigned) zs[1-cz]*ny + ys[1-cy])*nx;
-            const uint32_t* plane = a32 + (size_t) q*halfN;
-            uint32_t w;
+            const Word* plane = aw + (size_t) q*halfN;
+            Word w;
             if (cx == 0)
                 w = __ldg(plane + (base + x0)/2);
             else if (cx == 1)
-                w = __byte_perm(__ldg(plane + (base + xl)/2), __ldg(plane + (base + x0)/2), 0x5432);
+                w = PairIO<T>::left(__ldg(plane + (base + xl)/2), __ldg(plane + (base + x0)/2));
             else
-                w = __byte_perm(__ldg(plane + (base + x0)/2), __ldg(plane + (base + xr)/2), 0x5432);
-            r[q] = Pair16<T>::decode(w);
+                w = PairIO<T>::right(__ldg(plane + (base + x0)/2), __ldg(plane + (base + xr)/2));
+            r[q] = PairIO<T>::decode(w);
         });
         // Moments (deviations), the storage factors folded into the FMAs.
         F2 dr = f2(Storage<T>::template scale<0>())*r[0];
@@ -312,7 +371,7 @@ streamCollidePairKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v,
         const F2 rho = dr + f2(1.0f);
         const F2 inv = F2{make_float2(__fdividef(1.0f, rho.v.x), __fdividef(1.0f, rho.v.y))};
         const F2 ninv = F2{make_float2(-inv.v.x, -inv.v.y)};
-        const F2 dr3 = fma2(dr, f2(-1.0f/3.0f), f2(0.0f));
+        const F2 dr3 = dr*f2(-1.0f/3.0f);
         // Pi_neq = S2 - dr/3 - j j/rho.
         const F2 jxi = jx*ninv, jyi = jy*ninv;
         const F2 pxx = fma2(jx, jxi, sxx + dr3), pyy = fma2(jy, jyi, syy + dr3), pzz = fma2(jz, jz*ninv, szz + dr3);
@@ -337,22 +396,49 @@ streamCollidePairKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v,
         const F2 uu = fma2(uz, uz, fma2(uy, uy, ux*ux)), uf = fma2(uz, Fz, fma2(uy, Fy, ux*Fx));
         const F2 px = jx + Fx, py = jy + Fy, pz = jz + Fz;
         const F2 s45 = f2(om1*4.5f), s9 = f2(om1*9.0f);
-        const F2 qxx = s45*pxx, qyy = s45*pyy, qzz = s45*pzz, qxy = s9*pxy, qxz = s9*pxz, qyz = s9*pyz;
+        F2 qxx = s45*pxx, qyy = s45*pyy, qzz = s45*pzz, qxy = s9*pxy, qxz = s9*pxz, qyz = s9*pyz;
+        // Fluctuations: the amplitudes a_k = phi_k r_k/sqrt(b_k) of the 15 non-conserved modes of each node (Philox
+        // normals of the node and step), the stress modes merged into Q, the ghost modes added per direction.
+        F2 a[15];
+        if (FLUCT) {
+            float rnA[15], rnB[15];
+            philoxNormals<float, 15>(v.seed, PurposeFluid, node, step, rnA);
+            philoxNormals<float, 15>(v.seed, PurposeFluid, node + 1, step, rnB);
+            const float stressA = sqrtf(mu*rho.v.x*stressFactor), stressB = sqrtf(mu*rho.v.y*stressFactor);
+            const float ghostA = sqrtf(mu*rho.v.x), ghostB = sqrtf(mu*rho.v.y);
+#pragma unroll
+            for (int k = 4; k < 19; k++) {
+                const float norm = (float) invSqrtModeNorm(k);
+                a[k-4] = F2{make_float2(rnA[k-4]*(k < 10 ? stressA : ghostA)*norm, rnB[k-4]*(k < 10 ? stressB : ghostB)*norm)};
+            }
+            qxx = qxx + a[0]; qyy = qyy + a[1]; qzz = qzz + a[2];
+            qxy = qxy + a[3]; qxz = qxz + a[4]; qyz = qyz + a[5];
+        }
         const F2 qtr = (qxx + qyy + qzz)*f2(1.0f/3.0f);
         const F2 base = fma2(fma2(rho, uu, uf), f2(-1.5f), dr);
         // Dither words of the two nodes (the hash of collideNode's Dither, per node).
-        const uint32_t hashA = Dither::fmix32(node ^ stepHash), hashB = Dither::fmix32((node + 1) ^ stepHash);
-        uint32_t* outPlane = b32 + node/2;
+        uint32_t hashA = 0, hashB = 0;
+        if (dithered) {
+            hashA = Dither::fmix32(node ^ stepHash);
+            hashB = Dither::fmix32((node + 1) ^ stepHash);
+        }
+        Word* outPlane = bw + node/2;
         {
-            constexpr float k0 = Pair16<T>::scale*storeFactorOf(0);
-            const F2 value = (base - qtr)*f2(k0/3.0f);
-            storePairWord<SOLID>(outPlane, ditherPack<T>(value, hashA*0x9E3779B1u, hashB*0x9E3779B1u), solidA, solidB);
+            F2 value = (base - qtr)*f2(1.0f/3.0f);
+            if (FLUCT) {
+                F2 e, o;
+                ghostSums2<0>(a, e, o);
+                value = fma2(e, f2(wOf<float>(0)), value);
+            }
+            storePair<T, SOLID>(outPlane, value*f2(storeScale<T, 0>()), hashA*0x9E3779B1u, hashB*0x9E3779B1u,
+                                solidA, solidB);
         }
         staticFor<9>([&](auto pc) {
             constexpr int p = decltype(pc)::value;
             constexpr int q = 2*p + 1;
             constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
-            constexpr float k = Pair16<T>::scale*storeFactorOf(q);
+            constexpr float k = storeScale<T, q>();
+            constexpr float w = wOf<float>(q);
             F2 cu = f2(0), cf = f2(0), cp = f2(0);
             if (cx != 0) { cu = fma2(f2((float) cx), ux, cu); cf = fma2(f2((float) cx), Fx, cf); cp = fma2(f2((float) cx), px, cp); }
             if (cy != 0) { cu = fma2(f2((float) cy), uy, cu); cf = fma2(f2((float) cy), Fy, cf); cp = fma2(f2((float) cy), py, cp); }
@@ -364,14 +450,23 @@ streamCollidePairKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v,
             if (cx*cy != 0) cqc = fma2(f2((float) (cx*cy)), qxy, cqc);
             if (cx*cz != 0) cqc = fma2(f2((float) (cx*cz)), qxz, cqc);
             if (cy*cz != 0) cqc = fma2(f2((float) (cy*cz)), qyz, cqc);
-            // even and odd in storage units: k w_q (...) and k 3 w_q c.(j + F).
-            const F2 even = fma2(cu*fma2(rho, cu, cf), f2(4.5f), base + cqc)*f2(k*wOf<float>(q));
-            const F2 odd = cp*f2(k*oddOf<float>(q));
-            const uint32_t wa = hashA*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
-            const uint32_t wb = hashB*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
-            storePairWord<SOLID>(outPlane + (size_t) q*halfN, ditherPack<T>(even + odd, wa, wb), solidA, solidB);
-            storePairWord<SOLID>(outPlane + (size_t) (q + 1)*halfN, ditherPack<T>(even - odd, wa >> 16, wb >> 16),
-                                 solidA, solidB);
+            // even and odd in stored units: k w (...) and k 3 w c.(j + F), plus k w times the ghost sums.
+            F2 evenRaw = fma2(cu*fma2(rho, cu, cf), f2(4.5f), base + cqc);
+            F2 odd = cp*f2(k*oddOf<float>(q));
+            if (FLUCT) {
+                F2 e, o;
+                ghostSums2<q>(a, e, o);
+                evenRaw = evenRaw + e;
+                odd = fma2(o, f2(k*w), odd);
+            }
+            const F2 even = evenRaw*f2(k*w);
+            uint32_t wa = 0, wb = 0;
+            if (dithered) {
+                wa = hashA*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
+                wb = hashB*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
+            }
+            storePair<T, SOLID>(outPlane + (size_t) q*halfN, even + odd, wa, wb, solidA, solidB);
+            storePair<T, SOLID>(outPlane + (size_t) (q + 1)*halfN, even - odd, wa >> 16, wb >> 16, solidA, solidB);
         });
         if (!solidA) {
             sumMass += dr.v.x; sumX += px.v.x; sumY += py.v.x; sumZ += pz.v.x;
@@ -902,12 +997,25 @@ template <typename T>
 struct Launcher {
     typedef typename ComputeOf<T>::type R;
 
-    // The paired 16-bit kernel serves lattices with an even nx unless LBM_B200_PAIRED16=0 in the environment.
+    // The paired kernel serves FP32 and 16-bit storage on lattices with an even nx (measured at 256^3, FP32: 0.596
+    // against 0.677 ms per launch with fluctuations, 0.464 against 0.482 ms without).  LBM_B200_PAIRED16 = 0 and
+    // LBM_B200_PAIRED32 = 0 in the environment select the one-node kernel instead (for comparisons).
+    static int pairChoice(const char* name) {
+        const char* e = std::getenv(name);
+        return e == nullptr ? -1 : (e[0] == '0' ? 0 : 1);
+    }
+    template <bool FL>
     static bool pairedKernels() {
-        static int enabled = -1;
-        if (enabled < 0) {
-            const char* e = std::getenv("LBM_B200_PAIRED16");
-            enabled = (e != nullptr && e[0] == '0') ? 0 : 1;
+        static int enabled = -2;
+        if (enabled == -2) {
+            if (sizeof(T) == 2) {
+                int c = pairChoice("LBM_B200_PAIRED16");
+                enabled = c == 0 ? 0 : 1;
+            }
+            else {
+                int c = pairChoice("LBM_B200_PAIRED32");
+                enabled = c == 0 ? 0 : 1;
+            }
         }
         return enabled == 1;
     }
@@ -926,12 +1034,12 @@ struct Launcher {
         }
         return (int) std::max(1LL, std::min((long long) blocks, v.numTiles));
     }
-    template <bool S, bool RE>
+    template <bool S, bool RE, bool FL>
     static int pairGrid(const FluidView& v) {
         static int blocks = 0;
         if (blocks == 0) {
             int perSM = 0, device = 0, sms = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, streamCollidePairKernel<T, S, RE>, THREADS, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, streamCollidePairKernel<T, S, RE, FL>, THREADS, 0);
             cudaGetDevice(&device);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
             blocks = std::max(1, perSM)*std::max(1, sms);
@@ -941,10 +1049,10 @@ struct Launcher {
     }
     template <bool S, bool RE, bool FL>
     static int dense(const void* A, void* B, const FluidView& v, int remove, long long step, int maxGrid, cudaStream_t s) {
-        if constexpr (sizeof(T) == 2 && !FL) {
-            if (v.nx%2 == 0 && pairedKernels()) {
-                int grid = std::min(maxGrid, pairGrid<S, RE>(v));
-                streamCollidePairKernel<T, S, RE><<<grid, THREADS, 0, s>>>((const T*) A, (T*) B, v, remove, step);
+        if constexpr (sizeof(T) <= 4) {
+            if (v.nx%2 == 0 && pairedKernels<FL>()) {
+                int grid = std::min(maxGrid, pairGrid<S, RE, FL>(v));
+                streamCollidePairKernel<T, S, RE, FL><<<grid, THREADS, 0, s>>>((const T*) A, (T*) B, v, remove, step);
                 return grid;
             }
         }
@@ -977,9 +1085,10 @@ struct Launcher {
         probe(streamCollideKernel<T, R, false, false, true>);
         probe(streamCollideKernel<T, R, true, true, true>);
         probe(streamCollideKernel<T, R, true, false, false>);
-        if constexpr (sizeof(T) == 2) {
-            probe(streamCollidePairKernel<T, false, false>);
-            probe(streamCollidePairKernel<T, true, true>);
+        if constexpr (sizeof(T) <= 4) {
+            probe(streamCollidePairKernel<T, false, false, false>);
+            probe(streamCollidePairKernel<T, false, true, true>);
+            probe(streamCollidePairKernel<T, true, true, true>);
         }
         return best;
     }
