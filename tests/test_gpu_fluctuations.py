@@ -67,8 +67,9 @@ def vacf(record, lags):
     return np.stack([(record[:t]*record[lag:lag + t]).sum(axis=2).mean(axis=1)/3 for lag in lags], axis=1)
 
 
-def test_fluid_and_bead_temperatures():
-    context, force = free_beads(properties={'Precision': 'single'})
+@pytest.mark.parametrize('precision', ['single', 'half'])
+def test_fluid_and_bead_temperatures(precision):
+    context, force = free_beads(properties={'Precision': precision})
     context.integrator.step(1000)
     fluid, beads = [], []
     for _ in range(200):
