@@ -291,31 +291,179 @@ __device__ __forceinline__ void ghostSums2(const F2 a[15], F2& even, F2& odd) {
 #define LBM_PAIR_MIN_BLOCKS 2
 #endif
 
-// The dense step with two x-adjacent nodes per thread (nx even), the arithmetic of both in packed FP32 pairs.
+// Per-launch constants of the paired kernels.
+struct PairConstants {
+    float om1, mu, stressFactor;
+    F2 gx, gy, gz, nux0, nuy0, nuz0;
+    uint32_t stepHash;
+};
+
+__device__ __forceinline__ PairConstants pairConstants(const FluidView& v, int remove, long long step) {
+    PairConstants c;
+    const float om = (float) v.omega;
+    c.om1 = 1.0f - om;
+    c.mu = (float) v.mu;
+    c.stressFactor = om*(2.0f - om);
+    c.gx = f2((float) v.g[0]);
+    c.gy = f2((float) v.g[1]);
+    c.gz = f2((float) v.g[2]);
+    c.nux0 = c.nuy0 = c.nuz0 = f2(0.0f);
+    if (remove) {
+        c.nux0 = f2(-(float) v.stats->ucm[0]);
+        c.nuy0 = f2(-(float) v.stats->ucm[1]);
+        c.nuz0 = f2(-(float) v.stats->ucm[2]);
+    }
+    c.stepHash = Dither::fmix32((uint32_t) step + 0x9E3779B9u*(uint32_t) ((unsigned long long) step >> 32));
+    return c;
+}
+
+// The collision of the x-adjacent nodes `node` and `node + 1` from their pulled words r (stored units): stores the
+// 19 post-collision words at outPlane + q halfN (word index node/2) and adds the pair's mass and momentum to sums.
+// reactA, reactB flag nodes whose reaction force the coupling left in v.reaction.
+template <typename T, bool SOLID, bool REACT, bool FLUCT>
+__device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& v, const PairConstants& c, int remove,
+                                            long long step, unsigned node, bool solidA, bool solidB, bool reactA,
+                                            bool reactB, typename PairIO<T>::Word* outPlane, unsigned halfN,
+                                            float (&sums)[4]) {
+    constexpr bool dithered = sizeof(T) == 2;
+    // Moments (deviations), the storage factors folded into the FMAs.
+    F2 dr = f2(Storage<T>::template scale<0>())*r[0];
+    F2 jx = f2(0), jy = f2(0), jz = f2(0), sxx = f2(0), syy = f2(0), szz = f2(0), sxy = f2(0), sxz = f2(0), syz = f2(0);
+    staticFor<9>([&](auto pc) {
+        constexpr int q = 2*decltype(pc)::value + 1;
+        constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+        constexpr float s = Storage<T>::template scale<q>();
+        const F2 S = r[q] + r[q+1], D = r[q] - r[q+1];
+        dr = fma2(f2(s), S, dr);
+        if (cx != 0) { jx = fma2(f2(cx*s), D, jx); sxx = fma2(f2(s), S, sxx); }
+        if (cy != 0) { jy = fma2(f2(cy*s), D, jy); syy = fma2(f2(s), S, syy); }
+        if (cz != 0) { jz = fma2(f2(cz*s), D, jz); szz = fma2(f2(s), S, szz); }
+        if (cx*cy != 0) sxy = fma2(f2(cx*cy*s), S, sxy);
+        if (cx*cz != 0) sxz = fma2(f2(cx*cz*s), S, sxz);
+        if (cy*cz != 0) syz = fma2(f2(cy*cz*s), S, syz);
+    });
+    const F2 rho = dr + f2(1.0f);
+    const F2 inv = F2{make_float2(__fdividef(1.0f, rho.v.x), __fdividef(1.0f, rho.v.y))};
+    const F2 ninv = F2{make_float2(-inv.v.x, -inv.v.y)};
+    const F2 dr3 = dr*f2(-1.0f/3.0f);
+    // Pi_neq = S2 - dr/3 - j j/rho.
+    const F2 jxi = jx*ninv, jyi = jy*ninv;
+    const F2 pxx = fma2(jx, jxi, sxx + dr3), pyy = fma2(jy, jyi, syy + dr3), pzz = fma2(jz, jz*ninv, szz + dr3);
+    const F2 pxy = fma2(jy, jxi, sxy), pxz = fma2(jz, jxi, sxz), pyz = fma2(jz, jyi, syz);
+    if (remove) {
+        jx = fma2(rho, c.nux0, jx);
+        jy = fma2(rho, c.nuy0, jy);
+        jz = fma2(rho, c.nuz0, jz);
+    }
+    F2 Fx = rho*c.gx, Fy = rho*c.gy, Fz = rho*c.gz;
+    if (REACT) {
+        const float* rp = reinterpret_cast<const float*>(v.reaction) + 4*(size_t) node;
+        if (reactA) {
+            Fx.v.x += rp[0]; Fy.v.x += rp[1]; Fz.v.x += rp[2];
+        }
+        if (reactB) {
+            Fx.v.y += rp[4]; Fy.v.y += rp[5]; Fz.v.y += rp[6];
+        }
+    }
+    const F2 ux = fma2(Fx, f2(0.5f), jx)*inv, uy = fma2(Fy, f2(0.5f), jy)*inv, uz = fma2(Fz, f2(0.5f), jz)*inv;
+    const F2 uu = fma2(uz, uz, fma2(uy, uy, ux*ux)), uf = fma2(uz, Fz, fma2(uy, Fy, ux*Fx));
+    const F2 px = jx + Fx, py = jy + Fy, pz = jz + Fz;
+    const F2 s45 = f2(c.om1*4.5f), s9 = f2(c.om1*9.0f);
+    F2 qxx = s45*pxx, qyy = s45*pyy, qzz = s45*pzz, qxy = s9*pxy, qxz = s9*pxz, qyz = s9*pyz;
+    // Fluctuations: the amplitudes a_k = phi_k r_k/sqrt(b_k) of the 15 non-conserved modes of each node (Philox
+    // normals of the node and step), the stress modes merged into Q, the ghost modes added per direction.
+    F2 a[15];
+    if (FLUCT) {
+        float rnA[15], rnB[15];
+        philoxNormals<float, 15>(v.seed, PurposeFluid, node, step, rnA);
+        philoxNormals<float, 15>(v.seed, PurposeFluid, node + 1, step, rnB);
+        const float stressA = sqrtf(c.mu*rho.v.x*c.stressFactor), stressB = sqrtf(c.mu*rho.v.y*c.stressFactor);
+        const float ghostA = sqrtf(c.mu*rho.v.x), ghostB = sqrtf(c.mu*rho.v.y);
+#pragma unroll
+        for (int k = 4; k < 19; k++) {
+            const float norm = (float) invSqrtModeNorm(k);
+            a[k-4] = F2{make_float2(rnA[k-4]*(k < 10 ? stressA : ghostA)*norm, rnB[k-4]*(k < 10 ? stressB : ghostB)*norm)};
+        }
+        qxx = qxx + a[0]; qyy = qyy + a[1]; qzz = qzz + a[2];
+        qxy = qxy + a[3]; qxz = qxz + a[4]; qyz = qyz + a[5];
+    }
+    const F2 qtr = (qxx + qyy + qzz)*f2(1.0f/3.0f);
+    const F2 base = fma2(fma2(rho, uu, uf), f2(-1.5f), dr);
+    // Dither words of the two nodes (the hash of collideNode's Dither, per node).
+    uint32_t hashA = 0, hashB = 0;
+    if (dithered) {
+        hashA = Dither::fmix32(node ^ c.stepHash);
+        hashB = Dither::fmix32((node + 1) ^ c.stepHash);
+    }
+    {
+        F2 value = (base - qtr)*f2(1.0f/3.0f);
+        if (FLUCT) {
+            F2 e, o;
+            ghostSums2<0>(a, e, o);
+            value = fma2(e, f2(wOf<float>(0)), value);
+        }
+        storePair<T, SOLID>(outPlane, value*f2(storeScale<T, 0>()), hashA*0x9E3779B1u, hashB*0x9E3779B1u,
+                            solidA, solidB);
+    }
+    staticFor<9>([&](auto pc) {
+        constexpr int p = decltype(pc)::value;
+        constexpr int q = 2*p + 1;
+        constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+        constexpr float k = storeScale<T, q>();
+        constexpr float w = wOf<float>(q);
+        F2 cu = f2(0), cf = f2(0), cp = f2(0);
+        if (cx != 0) { cu = fma2(f2((float) cx), ux, cu); cf = fma2(f2((float) cx), Fx, cf); cp = fma2(f2((float) cx), px, cp); }
+        if (cy != 0) { cu = fma2(f2((float) cy), uy, cu); cf = fma2(f2((float) cy), Fy, cf); cp = fma2(f2((float) cy), py, cp); }
+        if (cz != 0) { cu = fma2(f2((float) cz), uz, cu); cf = fma2(f2((float) cz), Fz, cf); cp = fma2(f2((float) cz), pz, cp); }
+        F2 cqc = f2(0) - qtr;
+        if (cx != 0) cqc = cqc + qxx;
+        if (cy != 0) cqc = cqc + qyy;
+        if (cz != 0) cqc = cqc + qzz;
+        if (cx*cy != 0) cqc = fma2(f2((float) (cx*cy)), qxy, cqc);
+        if (cx*cz != 0) cqc = fma2(f2((float) (cx*cz)), qxz, cqc);
+        if (cy*cz != 0) cqc = fma2(f2((float) (cy*cz)), qyz, cqc);
+        // even and odd in stored units: k w (...) and k 3 w c.(j + F), plus k w times the ghost sums.
+        F2 evenRaw = fma2(cu*fma2(rho, cu, cf), f2(4.5f), base + cqc);
+        F2 odd = cp*f2(k*oddOf<float>(q));
+        if (FLUCT) {
+            F2 e, o;
+            ghostSums2<q>(a, e, o);
+            evenRaw = evenRaw + e;
+            odd = fma2(o, f2(k*w), odd);
+        }
+        const F2 even = evenRaw*f2(k*w);
+        uint32_t wa = 0, wb = 0;
+        if (dithered) {
+            wa = hashA*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
+            wb = hashB*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
+        }
+        storePair<T, SOLID>(outPlane + (size_t) q*halfN, even + odd, wa, wb, solidA, solidB);
+        storePair<T, SOLID>(outPlane + (size_t) (q + 1)*halfN, even - odd, wa >> 16, wb >> 16, solidA, solidB);
+    });
+    if (!solidA) {
+        sums[0] += dr.v.x; sums[1] += px.v.x; sums[2] += py.v.x; sums[3] += pz.v.x;
+    }
+    if (!solidB) {
+        sums[0] += dr.v.y; sums[1] += px.v.y; sums[2] += py.v.y; sums[3] += pz.v.y;
+    }
+}
+
+// The dense step with two x-adjacent nodes per thread (nx even), the arithmetic of both in packed FP32 pairs; each
+// thread loads its pulled words from global memory.
 template <typename T, bool SOLID, bool REACT, bool FLUCT>
 __global__ void __launch_bounds__(THREADS, LBM_PAIR_MIN_BLOCKS)
 streamCollidePairKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int remove, long long step) {
     typedef typename PairIO<T>::Word Word;
-    constexpr bool dithered = sizeof(T) == 2;
     const int lane = threadIdx.x%32, warp = threadIdx.x/32;
     const unsigned N = (unsigned) v.n;
     const int nx = v.nx, ny = v.ny, nz = v.nz;
     const Word* __restrict__ aw = reinterpret_cast<const Word*>(A);
     Word* __restrict__ bw = reinterpret_cast<Word*>(B);
     const unsigned halfN = N/2;                       // words per direction plane (N is even)
-    const float om = (float) v.omega, om1 = 1.0f - om;
-    const float mu = (float) v.mu, stressFactor = om*(2.0f - om);
-    const F2 gx = f2((float) v.g[0]), gy = f2((float) v.g[1]), gz = f2((float) v.g[2]);
-    F2 nux0 = f2(0.0f), nuy0 = f2(0.0f), nuz0 = f2(0.0f);
-    if (remove) {
-        nux0 = f2(-(float) v.stats->ucm[0]);
-        nuy0 = f2(-(float) v.stats->ucm[1]);
-        nuz0 = f2(-(float) v.stats->ucm[2]);
-    }
-    float sumMass = 0, sumX = 0, sumY = 0, sumZ = 0;
+    const PairConstants c = pairConstants(v, remove, step);
+    float sums[4] = {0, 0, 0, 0};
     const int tilesX = (nx + PAIR_TX - 1)/PAIR_TX, tilesY = v.tilesY;
     const unsigned numTiles = (unsigned) tilesX*tilesY*nz, stride = gridDim.x;
-    const uint32_t stepHash = Dither::fmix32((uint32_t) step + 0x9E3779B9u*(uint32_t) ((unsigned long long) step >> 32));
     for (unsigned t = blockIdx.x; t < numTiles; t += stride) {
         const int tx = (int) (t%tilesX);
         const unsigned rr = t/tilesX;
@@ -352,130 +500,16 @@ streamCollidePairKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v,
                 w = PairIO<T>::right(__ldg(plane + (base + x0)/2), __ldg(plane + (base + xr)/2));
             r[q] = PairIO<T>::decode(w);
         });
-        // Moments (deviations), the storage factors folded into the FMAs.
-        F2 dr = f2(Storage<T>::template scale<0>())*r[0];
-        F2 jx = f2(0), jy = f2(0), jz = f2(0), sxx = f2(0), syy = f2(0), szz = f2(0), sxy = f2(0), sxz = f2(0), syz = f2(0);
-        staticFor<9>([&](auto pc) {
-            constexpr int q = 2*decltype(pc)::value + 1;
-            constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
-            constexpr float s = Storage<T>::template scale<q>();
-            const F2 S = r[q] + r[q+1], D = r[q] - r[q+1];
-            dr = fma2(f2(s), S, dr);
-            if (cx != 0) { jx = fma2(f2(cx*s), D, jx); sxx = fma2(f2(s), S, sxx); }
-            if (cy != 0) { jy = fma2(f2(cy*s), D, jy); syy = fma2(f2(s), S, syy); }
-            if (cz != 0) { jz = fma2(f2(cz*s), D, jz); szz = fma2(f2(s), S, szz); }
-            if (cx*cy != 0) sxy = fma2(f2(cx*cy*s), S, sxy);
-            if (cx*cz != 0) sxz = fma2(f2(cx*cz*s), S, sxz);
-            if (cy*cz != 0) syz = fma2(f2(cy*cz*s), S, syz);
-        });
-        const F2 rho = dr + f2(1.0f);
-        const F2 inv = F2{make_float2(__fdividef(1.0f, rho.v.x), __fdividef(1.0f, rho.v.y))};
-        const F2 ninv = F2{make_float2(-inv.v.x, -inv.v.y)};
-        const F2 dr3 = dr*f2(-1.0f/3.0f);
-        // Pi_neq = S2 - dr/3 - j j/rho.
-        const F2 jxi = jx*ninv, jyi = jy*ninv;
-        const F2 pxx = fma2(jx, jxi, sxx + dr3), pyy = fma2(jy, jyi, syy + dr3), pzz = fma2(jz, jz*ninv, szz + dr3);
-        const F2 pxy = fma2(jy, jxi, sxy), pxz = fma2(jz, jxi, sxz), pyz = fma2(jz, jyi, syz);
-        if (remove) {
-            jx = fma2(rho, nux0, jx);
-            jy = fma2(rho, nuy0, jy);
-            jz = fma2(rho, nuz0, jz);
-        }
-        F2 Fx = rho*gx, Fy = rho*gy, Fz = rho*gz;
+        bool reactA = false, reactB = false;
         if (REACT) {
             uint32_t word = __ldg(&v.reactMask[(size_t) row*v.wordsPerRow + (x0 >> 5)]);
-            const float* rp = reinterpret_cast<const float*>(v.reaction) + 4*(size_t) node;
-            if ((word >> (x0 & 31)) & 1u) {
-                Fx.v.x += rp[0]; Fy.v.x += rp[1]; Fz.v.x += rp[2];
-            }
-            if ((word >> ((x0 + 1) & 31)) & 1u) {
-                Fx.v.y += rp[4]; Fy.v.y += rp[5]; Fz.v.y += rp[6];
-            }
+            reactA = (word >> (x0 & 31)) & 1u;
+            reactB = (word >> ((x0 + 1) & 31)) & 1u;
         }
-        const F2 ux = fma2(Fx, f2(0.5f), jx)*inv, uy = fma2(Fy, f2(0.5f), jy)*inv, uz = fma2(Fz, f2(0.5f), jz)*inv;
-        const F2 uu = fma2(uz, uz, fma2(uy, uy, ux*ux)), uf = fma2(uz, Fz, fma2(uy, Fy, ux*Fx));
-        const F2 px = jx + Fx, py = jy + Fy, pz = jz + Fz;
-        const F2 s45 = f2(om1*4.5f), s9 = f2(om1*9.0f);
-        F2 qxx = s45*pxx, qyy = s45*pyy, qzz = s45*pzz, qxy = s9*pxy, qxz = s9*pxz, qyz = s9*pyz;
-        // Fluctuations: the amplitudes a_k = phi_k r_k/sqrt(b_k) of the 15 non-conserved modes of each node (Philox
-        // normals of the node and step), the stress modes merged into Q, the ghost modes added per direction.
-        F2 a[15];
-        if (FLUCT) {
-            float rnA[15], rnB[15];
-            philoxNormals<float, 15>(v.seed, PurposeFluid, node, step, rnA);
-            philoxNormals<float, 15>(v.seed, PurposeFluid, node + 1, step, rnB);
-            const float stressA = sqrtf(mu*rho.v.x*stressFactor), stressB = sqrtf(mu*rho.v.y*stressFactor);
-            const float ghostA = sqrtf(mu*rho.v.x), ghostB = sqrtf(mu*rho.v.y);
-#pragma unroll
-            for (int k = 4; k < 19; k++) {
-                const float norm = (float) invSqrtModeNorm(k);
-                a[k-4] = F2{make_float2(rnA[k-4]*(k < 10 ? stressA : ghostA)*norm, rnB[k-4]*(k < 10 ? stressB : ghostB)*norm)};
-            }
-            qxx = qxx + a[0]; qyy = qyy + a[1]; qzz = qzz + a[2];
-            qxy = qxy + a[3]; qxz = qxz + a[4]; qyz = qyz + a[5];
-        }
-        const F2 qtr = (qxx + qyy + qzz)*f2(1.0f/3.0f);
-        const F2 base = fma2(fma2(rho, uu, uf), f2(-1.5f), dr);
-        // Dither words of the two nodes (the hash of collideNode's Dither, per node).
-        uint32_t hashA = 0, hashB = 0;
-        if (dithered) {
-            hashA = Dither::fmix32(node ^ stepHash);
-            hashB = Dither::fmix32((node + 1) ^ stepHash);
-        }
-        Word* outPlane = bw + node/2;
-        {
-            F2 value = (base - qtr)*f2(1.0f/3.0f);
-            if (FLUCT) {
-                F2 e, o;
-                ghostSums2<0>(a, e, o);
-                value = fma2(e, f2(wOf<float>(0)), value);
-            }
-            storePair<T, SOLID>(outPlane, value*f2(storeScale<T, 0>()), hashA*0x9E3779B1u, hashB*0x9E3779B1u,
-                                solidA, solidB);
-        }
-        staticFor<9>([&](auto pc) {
-            constexpr int p = decltype(pc)::value;
-            constexpr int q = 2*p + 1;
-            constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
-            constexpr float k = storeScale<T, q>();
-            constexpr float w = wOf<float>(q);
-            F2 cu = f2(0), cf = f2(0), cp = f2(0);
-            if (cx != 0) { cu = fma2(f2((float) cx), ux, cu); cf = fma2(f2((float) cx), Fx, cf); cp = fma2(f2((float) cx), px, cp); }
-            if (cy != 0) { cu = fma2(f2((float) cy), uy, cu); cf = fma2(f2((float) cy), Fy, cf); cp = fma2(f2((float) cy), py, cp); }
-            if (cz != 0) { cu = fma2(f2((float) cz), uz, cu); cf = fma2(f2((float) cz), Fz, cf); cp = fma2(f2((float) cz), pz, cp); }
-            F2 cqc = f2(0) - qtr;
-            if (cx != 0) cqc = cqc + qxx;
-            if (cy != 0) cqc = cqc + qyy;
-            if (cz != 0) cqc = cqc + qzz;
-            if (cx*cy != 0) cqc = fma2(f2((float) (cx*cy)), qxy, cqc);
-            if (cx*cz != 0) cqc = fma2(f2((float) (cx*cz)), qxz, cqc);
-            if (cy*cz != 0) cqc = fma2(f2((float) (cy*cz)), qyz, cqc);
-            // even and odd in stored units: k w (...) and k 3 w c.(j + F), plus k w times the ghost sums.
-            F2 evenRaw = fma2(cu*fma2(rho, cu, cf), f2(4.5f), base + cqc);
-            F2 odd = cp*f2(k*oddOf<float>(q));
-            if (FLUCT) {
-                F2 e, o;
-                ghostSums2<q>(a, e, o);
-                evenRaw = evenRaw + e;
-                odd = fma2(o, f2(k*w), odd);
-            }
-            const F2 even = evenRaw*f2(k*w);
-            uint32_t wa = 0, wb = 0;
-            if (dithered) {
-                wa = hashA*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
-                wb = hashB*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
-            }
-            storePair<T, SOLID>(outPlane + (size_t) q*halfN, even + odd, wa, wb, solidA, solidB);
-            storePair<T, SOLID>(outPlane + (size_t) (q + 1)*halfN, even - odd, wa >> 16, wb >> 16, solidA, solidB);
-        });
-        if (!solidA) {
-            sumMass += dr.v.x; sumX += px.v.x; sumY += py.v.x; sumZ += pz.v.x;
-        }
-        if (!solidB) {
-            sumMass += dr.v.y; sumX += px.v.y; sumY += py.v.y; sumZ += pz.v.y;
-        }
+        collidePair<T, SOLID, REACT, FLUCT>(r, v, c, remove, step, node, solidA, solidB, reactA, reactB, bw + node/2,
+                                            halfN, sums);
     }
-    double acc[NPART] = {(double) sumMass, (double) sumX, (double) sumY, (double) sumZ, 0, 0, 0, 0};
+    double acc[NPART] = {(double) sums[0], (double) sums[1], (double) sums[2], (double) sums[3], 0, 0, 0, 0};
     blockReduceStore(acc, v.partials + NPART*(long long) blockIdx.x);
 }
 
