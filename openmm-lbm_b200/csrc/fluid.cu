@@ -198,11 +198,8 @@ template <> struct PairIO<__half> {
         __half2 h = *reinterpret_cast<__half2*>(&w);
         return F2{__half22float2(h)};
     }
-    static constexpr uint32_t ditherMask = 0x1FFFu;
-    static __device__ __forceinline__ uint32_t pack(float lo, float hi) {   // round toward zero (after the dither)
-        uint32_t r;
-        asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
-        return r;
+    static __device__ __forceinline__ uint32_t pack(float lo, float hi, uint32_t rbits) {
+        return stochasticHalf2(lo, hi, rbits);
     }
 };
 template <> struct PairIO<__nv_bfloat16> {
@@ -213,11 +210,8 @@ template <> struct PairIO<__nv_bfloat16> {
     static __device__ __forceinline__ F2 decode(Word w) {
         return F2{make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xFFFF0000u))};
     }
-    static constexpr uint32_t ditherMask = 0xFFFFu;
-    static __device__ __forceinline__ uint32_t pack(float lo, float hi) {
-        uint32_t r;
-        asm("cvt.rz.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
-        return r;
+    static __device__ __forceinline__ uint32_t pack(float lo, float hi, uint32_t rbits) {
+        return stochasticBf162(lo, hi, rbits);
     }
 };
 template <> struct PairIO<float> {
@@ -238,14 +232,13 @@ template <typename T, int q> __device__ __forceinline__ constexpr float storeSca
 constexpr int PAIR_TX = 64;         // nodes per tile row: 2 per lane
 
 // Stores the pair `value` (stored units) of one direction; the half of a solid node stays untouched (as in the
-// one-node kernel).  16-bit storage rounds stochastically with the dither words da, db of the two nodes.
+// one-node kernel).  16-bit storage rounds stochastically with the dither bits of the two nodes, node A's in the low
+// half of `dither` and node B's in the high half.
 template <typename T, bool SOLID>
-__device__ __forceinline__ void storePair(typename PairIO<T>::Word* p, F2 value, uint32_t da, uint32_t db, bool solidA,
+__device__ __forceinline__ void storePair(typename PairIO<T>::Word* p, F2 value, uint32_t dither, bool solidA,
                                           bool solidB) {
     if constexpr (sizeof(T) == 2) {
-        float a = __uint_as_float(__float_as_uint(value.v.x) + (da & PairIO<T>::ditherMask));
-        float b = __uint_as_float(__float_as_uint(value.v.y) + (db & PairIO<T>::ditherMask));
-        uint32_t w = PairIO<T>::pack(a, b);
+        uint32_t w = PairIO<T>::pack(value.v.x, value.v.y, dither);
         if (SOLID && (solidA || solidB)) {
             unsigned short* h = reinterpret_cast<unsigned short*>(p);
             if (!solidA)
@@ -402,8 +395,8 @@ __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& 
             ghostSums2<0>(a, e, o);
             value = fma2(e, f2(wOf<float>(0)), value);
         }
-        storePair<T, SOLID>(outPlane, value*f2(storeScale<T, 0>()), hashA*0x9E3779B1u, hashB*0x9E3779B1u,
-                            solidA, solidB);
+        storePair<T, SOLID>(outPlane, value*f2(storeScale<T, 0>()),
+                            __byte_perm(hashA*0x9E3779B1u, hashB*0x9E3779B1u, 0x5410), solidA, solidB);
     }
     staticFor<9>([&](auto pc) {
         constexpr int p = decltype(pc)::value;
@@ -437,8 +430,9 @@ __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& 
             wa = hashA*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
             wb = hashB*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
         }
-        storePair<T, SOLID>(outPlane + (size_t) q*halfN, even + odd, wa, wb, solidA, solidB);
-        storePair<T, SOLID>(outPlane + (size_t) (q + 1)*halfN, even - odd, wa >> 16, wb >> 16, solidA, solidB);
+        // Direction q takes the low halves of the nodes' words, q + 1 the high halves.
+        storePair<T, SOLID>(outPlane + (size_t) q*halfN, even + odd, __byte_perm(wa, wb, 0x5410), solidA, solidB);
+        storePair<T, SOLID>(outPlane + (size_t) (q + 1)*halfN, even - odd, __byte_perm(wa, wb, 0x7632), solidA, solidB);
     });
     if (!solidA) {
         sums[0] += dr.v.x; sums[1] += px.v.x; sums[2] += py.v.x; sums[3] += pz.v.x;
