@@ -208,6 +208,12 @@ LbmStatus lbm_kernel_launches(LbmKernel* kernel, long long* launches);
 /* Conjugate-gradient iterations of the last centred stencil drag solve (0 for the other coupling schemes). */
 LbmStatus lbm_solver_iterations(LbmKernel* kernel, int* iterations);
 
+/* Steps, since creation, whose centred stencil drag was solved by spreading and gathering on the lattice nodes
+   instead of through the explicit coupling matrix (a cell of the particle cell list or a row of the matrix over its
+   capacity, or LBM_B200_SPREAD_CG=1 in the environment).  No counterpart in the reference, whose solve is always the
+   spread-and-gather one (platforms/reference/src/ReferenceLBMKernels.cpp:726-901). */
+LbmStatus lbm_solver_fallback_steps(LbmKernel* kernel, long long* steps);
+
 /* The steady-state residual r = max_nodes |u - u_prev| / (interval max_nodes |u|) over the fluid nodes, in FP64 on the
    device, with u = j/rho of the current (post-stream) state and u_prev the velocities recorded by the previous call,
    which this call replaces; the first call records them and returns infinity.  Called every `interval` steps it is the

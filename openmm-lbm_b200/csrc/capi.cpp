@@ -218,6 +218,14 @@ LbmStatus lbm_solver_iterations(LbmKernel* kernel, int* iterations) {
     return LBM_OK;
 }
 
+LbmStatus lbm_solver_fallback_steps(LbmKernel* kernel, long long* steps) {
+    CHECK_HANDLE(kernel);
+    if (!steps)
+        return fail(LBM_ERR_INVALID_ARGUMENT, "lbm_solver_fallback_steps: null argument");
+    *steps = kernel->impl->solverFallbackSteps();
+    return LBM_OK;
+}
+
 LbmStatus lbm_steady_residual(LbmKernel* kernel, int interval, double* residual) {
     CHECK_HANDLE(kernel);
     if (!residual || interval <= 0)

@@ -22,6 +22,7 @@
 #include "radix_sort.cuh"
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -157,7 +158,7 @@ __device__ bool gridBarrier(unsigned* bar, int* status, unsigned& generation) {
         }
         else {
             long long polls = 0;
-            while (atomicAdd(&bar[1], 0u) != target) {
+            while (*((volatile unsigned*) &bar[1]) != target) {
                 if (++polls > (1LL << 26) || atomicAdd(status, 0) == LBM_ERR_DEVICE_TIMEOUT) {
                     atomicExch(status, LBM_ERR_DEVICE_TIMEOUT);
                     ok = false;
@@ -179,7 +180,7 @@ __device__ bool gridBarrier(unsigned* bar, int* status, unsigned& generation) {
 // Block sum of a record (thread values v) into partials[block]; after a grid barrier (by the caller) every block adds
 // the records of all blocks in block order, so every block gets the same result, bit for bit.
 __device__ void blockSumStore(double v[kPartial], double* partials) {
-    __shared__ double red[kThreads/32][kPartial];
+    __shared__ double red[32][kPartial];
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int k = 0; k < kPartial; k++)
         v[k] = warpSum(v[k]);
@@ -197,12 +198,18 @@ __device__ void blockSumStore(double v[kPartial], double* partials) {
 }
 
 __device__ void reducePartials(const double* partials, int count, double out[kPartial]) {
+    // Warp k sums component k over the blocks (lanes strided over the records, then a fixed tree), so every block
+    // gets the same result, bit for bit.  The records were written by other blocks before a grid barrier: loads bypass
+    // L1.
     __shared__ double total[kPartial];
-    if (threadIdx.x < kPartial) {
+    const int lane = threadIdx.x & 31;
+    for (int k = threadIdx.x >> 5; k < kPartial; k += blockDim.x >> 5) {
         double s = 0;
-        for (int b = 0; b < count; b++)
-            s += ((volatile const double*) partials)[kPartial*b + threadIdx.x];
-        total[threadIdx.x] = s;
+        for (int r = lane; r < count; r += 32)
+            s += __ldcg(partials + kPartial*r + k);
+        s = warpSum(s);
+        if (lane == 0)
+            total[k] = s;
     }
     __syncthreads();
     for (int k = 0; k < kPartial; k++)
@@ -442,6 +449,424 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
     }
 }
 
+// ------------------------------------------------------------------------------------------------------
+// Centred drag with a stencil through the explicit coupling matrix.
+//
+// The operator of the conjugate gradients, (1 + a) F_k/m_k + a sum_l K_kl F_l with K_kl = sum_n w_k(n) w_l(n)/rho(n)
+// over the fluid nodes n that the stencils of k and l share, is the same as the spread-and-gather of the kernel above
+// (spread w_l F_l onto the nodes, gather with w_k/rho).  K is sparse (a particle's stencil overlaps those of the
+// particles within one stencil width), so it is built once per step and every iteration is a sparse product over a few
+// dozen entries per particle instead of a pass over the lattice nodes of all stencils.
+//   cgBinKernel     per particle: the node indices and weights of its stencil on each axis and its cell (cells of
+//                   kCgCellEdge nodes, on the first stencil index), inserted into a fixed-capacity cell list; per
+//                   slot: w/rho
+//   cgRowsKernel    one warp per particle k: the particles of the neighbouring cells whose first stencil indices are
+//                   within a stencil width of k's on every axis, sorted by index (so that every row, and every sum
+//                   over it, has one order), and K_kl for each, a lane per entry
+//   centeredSparseKernel  the conjugate gradients (same start, preconditioner, stopping rule and per-component
+//                   iteration as the kernel above) in one cooperative launch, two grid barriers per iteration
+// Rows are stored entry-major (entry e of row k at e np + k), so that a thread per row reads them coalesced.  A cell
+// or a row over its capacity sets a flag; the host then runs the spread-and-gather kernel for that step.
+// ------------------------------------------------------------------------------------------------------
+
+constexpr int kCgCellEdge = 4;      // nodes per cell edge (no less than the widest stencil)
+constexpr int kCgCellCapacity = 64; // particles per cell
+constexpr int kCgRowCapacity = 128; // entries per row of K
+constexpr int kSolveThreads = 1024; // threads per block of the solve (one block per SM: few barrier arrivals)
+
+struct SparseCg {
+    int4* axisIndex;       // 3 per particle: the stencil's node indices on each axis (-1 past the width)
+    double2* axisWeight;   // 6 per particle: the stencil's weights on each axis, [2 axis + 0/1] = entries 0-1 / 2-3
+    int4* firstIndex;      // the first stencil index on each axis
+    int* cellOf;           // cell of each particle
+    unsigned* cellCount;   // particles per cell (cleared by the solve kernel)
+    int* cellList;         // kCgCellCapacity per cell
+    int* rowCount;         // entries per row
+    int* rowIndex;         // entry e of row k at e np + k: the column particle
+    double* rowValue;      // K_kl, same layout
+    double* Ap;            // A p, 3 per particle
+    int* overflow;         // nonzero: a cell or a row over its capacity
+    int cells[3];          // cells per axis
+};
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads)
+cgBinKernel(CouplingView c, const R* __restrict__ slotWeight, const typename Vec4<R>::type* __restrict__ slotU,
+            const double* __restrict__ pos, R* coef, SparseCg g) {
+    const long long total = (long long) c.np*c.slots;
+    for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x) {
+        double w = (double) slotWeight[t];
+        double rho = (double) slotU[t].w;
+        coef[t] = (R) (rho > 0 ? w/rho : 0.0);
+    }
+    const int size[3] = {c.nx, c.ny, c.nz};
+    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x) {
+        int cell[3], first[3];
+        for (int a = 0; a < 3; a++) {
+            int index[4];
+            double weight[4];
+            axisWeights(c.stencil, c.width, latticeCoordinate(pos[3*i+a], c.dx, size[a]), size[a], c.open[a] != 0,
+                        index, weight);
+            for (int k = c.width; k < 4; k++)
+                index[k] = -1;
+            g.axisIndex[3*i + a] = make_int4(index[0], index[1], index[2], index[3]);
+            for (int k = c.width; k < 4; k++)
+                weight[k] = 0.0;
+            g.axisWeight[6*i + 2*a] = make_double2(weight[0], weight[1]);
+            g.axisWeight[6*i + 2*a + 1] = make_double2(weight[2], weight[3]);
+            first[a] = index[0];
+            cell[a] = min(index[0]/kCgCellEdge, g.cells[a] - 1);
+        }
+        g.firstIndex[i] = make_int4(first[0], first[1], first[2], 0);
+        int key = cell[0] + g.cells[0]*(cell[1] + g.cells[1]*cell[2]);
+        g.cellOf[i] = key;
+        unsigned slot = atomicAdd(&g.cellCount[key], 1u);
+        if (slot < (unsigned) kCgCellCapacity)
+            g.cellList[(long long) key*kCgCellCapacity + slot] = i;
+        else
+            atomicExch(g.overflow, 1);
+    }
+}
+
+// Periodic distance of two lattice indices on an axis of n nodes.
+__device__ __forceinline__ int periodicDistance(int a, int b, int n) {
+    int d = abs(a - b);
+    return min(d, n - d);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads)
+cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
+    __shared__ int candidates[kThreads/32][kCgRowCapacity];
+    __shared__ int sorted[kThreads/32][kCgRowCapacity];
+    __shared__ double rowCoef[kThreads/32][64];
+    __shared__ int cellEnd[kThreads/32][32], cellStart[kThreads/32][32], cellId[kThreads/32][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int* list = candidates[warp];
+    const int firstWarp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
+    const int warps = (gridDim.x*blockDim.x) >> 5;
+    const int size[3] = {c.nx, c.ny, c.nz};
+    const int w = c.width, S = c.slots;
+    for (int k = firstWarp; k < c.np; k += warps) {
+        for (int s = lane; s < S; s += 32)
+            rowCoef[warp][s] = (double) coef[(long long) k*S + s];
+        const int4 fk = g.firstIndex[k];
+        const int key = g.cellOf[k];
+        const int home[3] = {key%g.cells[0], (key/g.cells[0])%g.cells[1], key/(g.cells[0]*g.cells[1])};
+        // Lane j < 27 takes the neighbouring cell (j%3 - 1, j/3%3 - 1, j/9 - 1); a cell that an axis with fewer than
+        // 3 cells reaches twice is taken once (by its first offset).
+        int cell = -1, members = 0;
+        if (lane < 27) {
+            const int off[3] = {lane%3 - 1, (lane/3)%3 - 1, lane/9 - 1};
+            bool first = true;
+            int cc[3];
+            for (int a = 0; a < 3; a++) {
+                const int n = g.cells[a];
+                cc[a] = ((home[a] + off[a])%n + n)%n;
+                for (int d = -1; d < off[a]; d++)
+                    first &= ((home[a] + d)%n + n)%n != cc[a];
+            }
+            if (first) {
+                cell = cc[0] + g.cells[0]*(cc[1] + g.cells[1]*cc[2]);
+                members = min((int) g.cellCount[cell], kCgCellCapacity);
+            }
+        }
+        // Exclusive scan of the member counts over the lanes.
+        int start = members;
+        for (int d = 1; d < 32; d *= 2) {
+            const int v = __shfl_up_sync(0xFFFFFFFFu, start, d);
+            if (lane >= d)
+                start += v;
+        }
+        const int total = __shfl_sync(0xFFFFFFFFu, start, 31);
+        cellEnd[warp][lane] = lane < 27 ? start : 0x7FFFFFFF;
+        cellStart[warp][lane] = start - members;
+        cellId[warp][lane] = cell;
+        __syncwarp();
+        int found = 0;     // the same in every lane
+        for (int base = 0; base < total; base += 32) {
+            const int e = base + lane;
+            int l = -1;
+            bool near = false;
+            if (e < total) {
+                // The cell holding member e: the first of the 27 whose running end exceeds e.
+                int lo = 0, hi = 26;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (cellEnd[warp][mid] > e)
+                        hi = mid;
+                    else
+                        lo = mid + 1;
+                }
+                l = g.cellList[(long long) cellId[warp][lo]*kCgCellCapacity + (e - cellStart[warp][lo])];
+                const int4 fl = g.firstIndex[l];
+                near = periodicDistance(fl.x, fk.x, size[0]) < c.width &&
+                       periodicDistance(fl.y, fk.y, size[1]) < c.width &&
+                       periodicDistance(fl.z, fk.z, size[2]) < c.width;
+            }
+            const unsigned ballot = __ballot_sync(0xFFFFFFFFu, near);
+            const int at = found + __popc(ballot & ((1u << lane) - 1u));
+            if (near && at < kCgRowCapacity)
+                list[at] = l;
+            found += __popc(ballot);
+        }
+        __syncwarp();
+        if (found > kCgRowCapacity) {
+            if (lane == 0)
+                atomicExch(g.overflow, 1);
+            found = kCgRowCapacity;
+        }
+        // Rank sort (particle indices are distinct).
+        for (int j = lane; j < found; j += 32) {
+            const int v = list[j];
+            int rank = 0;
+            for (int i = 0; i < found; i++)
+                rank += list[i] < v;
+            sorted[warp][rank] = v;
+        }
+        __syncwarp();
+        // K_kl = sum over k's slots (ix, iy, iz) of (w/rho)_k times l's weight at the same node, the product of l's
+        // axis weights at the entries with k's indices (on each axis the first such entry: later duplicates, at
+        // clamped open faces, have weight zero).  Lanes over the row's entries.
+        const int4 ik[3] = {g.axisIndex[3*k], g.axisIndex[3*k + 1], g.axisIndex[3*k + 2]};
+        for (int j = lane; j < found; j += 32) {
+            const int l = sorted[warp][j];
+            double shifted[3][4];
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const int4 il = g.axisIndex[3*l + a];
+                const double2 w01 = g.axisWeight[6*l + 2*a], w23 = g.axisWeight[6*l + 2*a + 1];
+                const int mine[4] = {ik[a].x, ik[a].y, ik[a].z, ik[a].w};
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    double v = 0.0;
+                    if (mine[i] >= 0) {
+                        if (il.w == mine[i]) v = w23.y;
+                        if (il.z == mine[i]) v = w23.x;
+                        if (il.y == mine[i]) v = w01.y;
+                        if (il.x == mine[i]) v = w01.x;
+                    }
+                    shifted[a][i] = v;
+                }
+            }
+            double K = 0;
+#pragma unroll
+            for (int iz = 0; iz < 4; iz++) {
+                if (iz >= w || shifted[2][iz] == 0.0)
+                    continue;
+#pragma unroll
+                for (int iy = 0; iy < 4; iy++) {
+                    if (iy >= w || shifted[1][iy] == 0.0)
+                        continue;
+                    const double wyz = shifted[1][iy]*shifted[2][iz];
+#pragma unroll
+                    for (int ix = 0; ix < 4; ix++)
+                        if (ix < w)
+                            K += rowCoef[warp][ix + w*(iy + w*iz)]*(shifted[0][ix]*wyz);
+                }
+            }
+            g.rowIndex[(long long) j*c.np + k] = l;
+            g.rowValue[(long long) j*c.np + k] = K;
+        }
+        if (lane == 0)
+            g.rowCount[k] = found;
+        __syncwarp();
+    }
+}
+
+// (K v)_k for the three components of v (thread per row; entries in row order).
+__device__ __forceinline__ void rowProduct(const SparseCg& g, int np, int k, const double* v, double out[3]) {
+    const int n = g.rowCount[k];
+    double s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll 4
+    for (int e = 0; e < n; e++) {
+        const int l = g.rowIndex[(long long) e*np + k];
+        const double K = g.rowValue[(long long) e*np + k];
+        s0 += K*v[3*l];
+        s1 += K*v[3*l+1];
+        s2 += K*v[3*l+2];
+    }
+    out[0] = s0;
+    out[1] = s1;
+    out[2] = s2;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kSolveThreads, 1)
+centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel, const double* __restrict__ fin,
+                     const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
+                     const typename Vec4<R>::type* __restrict__ slotU, long long step, int isStep, double tolerance,
+                     int maxIterations, CgBuffers b, SparseCg g, double* fout, R* reaction, uint32_t* mask,
+                     double* wall) {
+    typedef typename Vec4<R>::type V;
+    constexpr int G = 8;       // lanes per particle where a particle's slots are summed
+    const int lane = threadIdx.x & 31, sub = lane%G;
+    const int firstWarp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
+    const int warps = (gridDim.x*blockDim.x) >> 5;
+    const int firstThread = blockIdx.x*blockDim.x + threadIdx.x, threads = gridDim.x*blockDim.x;
+    // The rows of this block (a contiguous range, so that its threads read the entry-major rows coalesced).
+    const int rowBegin = (int) ((long long) c.np*blockIdx.x/gridDim.x);
+    const int rowEnd = (int) ((long long) c.np*(blockIdx.x + 1)/gridDim.x);
+    const int S = c.slots;
+    const double a = c.a;
+    unsigned generation = 0;
+    if (threadIdx.x == 0)
+        generation = *((volatile unsigned*) &b.barrier[1]);
+    // The cell list has been read (by the rows kernel): empty it for the next step.
+    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x)
+        g.cellCount[g.cellOf[i]] = 0u;
+    if (*((volatile int*) g.overflow) != 0)
+        return;
+    // Right-hand side, diagonal and the start F = rhs/diag (ReferenceLBMKernels.cpp:758-782, 839-840): 8 lanes per
+    // particle, 4 particles per warp.
+    for (int base = firstWarp*(32/G); base < c.np; base += warps*(32/G)) {
+        const int i = base + lane/G;
+        const bool active = i < c.np;
+        double u[3] = {0, 0, 0}, self = 0;
+        if (active)
+            for (int s = sub; s < S; s += G) {
+                long long t = (long long) i*S + s;
+                V su = slotU[t];
+                double w = (double) slotWeight[t];
+                if (su.w > 0) {
+                    u[0] += (double) su.x*w;
+                    u[1] += (double) su.y*w;
+                    u[2] += (double) su.z*w;
+                    self += w*w/(double) su.w;
+                }
+            }
+        for (int o = G/2; o > 0; o /= 2) {
+            for (int d = 0; d < 3; d++)
+                u[d] += __shfl_xor_sync(0xFFFFFFFFu, u[d], o);
+            self += __shfl_xor_sync(0xFFFFFFFFu, self, o);
+        }
+        if (!active || sub != 0)
+            continue;
+        double m = c.mass[i];
+        double xi[3] = {0, 0, 0};
+        if (c.randomForce)
+            particleNoise(c.seed, i, step, xi);
+        double diag = (1.0 + a)/m + a*self;
+        for (int d = 0; d < 3; d++) {
+            double known = vel[3*i+d]*(1.0/c.velocityScale) + fin[3*i+d]*(c.h/(m*c.forceScale));
+            double v = (known - u[d])*(-c.gamma*m);
+            if (c.randomForce)
+                v += xi[d]*sqrt(2.0*c.gamma*m*c.kT);
+            double rhs = v*(1.0/m);
+            b.rhs[3*i+d] = rhs;
+            b.F[3*i+d] = rhs*(1.0/diag);
+        }
+        b.diag[i] = diag;
+    }
+    if (!gridBarrier(b.barrier, b.status, generation))
+        return;
+    // r = rhs - A F, z = r/diag, p = z; r.z, the norm of the right-hand side and r.r per component.
+    double acc[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = rowBegin + threadIdx.x; i < rowEnd; i += blockDim.x) {
+        double g3[3];
+        rowProduct(g, c.np, i, b.F, g3);
+        double m = c.mass[i], diag = b.diag[i];
+        for (int d = 0; d < 3; d++) {
+            double AF = b.F[3*i+d]*((1.0 + a)/m) + g3[d]*a;
+            double rhs = b.rhs[3*i+d];
+            double r = rhs - AF;
+            double z = r*(1.0/diag);
+            b.r[3*i+d] = r;
+            b.z[3*i+d] = z;
+            b.p[3*i+d] = z;
+            acc[d] += r*z;
+            acc[3+d] += rhs*rhs;
+            acc[6+d] += r*r;
+        }
+    }
+    blockSumStore(acc, b.partials[1]);
+    if (!gridBarrier(b.barrier, b.status, generation))
+        return;
+    double tot[kPartial];
+    reducePartials(b.partials[1], gridDim.x, tot);
+    double rz[3] = {tot[0], tot[1], tot[2]}, norm[3] = {tot[3], tot[4], tot[5]}, residual[3] = {tot[6], tot[7], tot[8]};
+    double beta[3] = {0, 0, 0};
+    int iteration = 0;
+    bool failed = false;       // the same in every block: every decision comes from the same reduced sums
+    for (;; iteration++) {
+        bool converged = true;
+        for (int d = 0; d < 3; d++)
+            if (residual[d] > tolerance*tolerance*norm[d])
+                converged = false;
+        if (converged)
+            break;
+        if (iteration == maxIterations) {
+            if (firstWarp == 0 && lane == 0)
+                atomicExch(b.status, LBM_ERR_CG_NOT_CONVERGED);
+            failed = true;
+            break;
+        }
+        // p = z + beta p and A p = A z + beta A p (p = z at the first iteration), with p.Ap.
+        double acc3[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = rowBegin + threadIdx.x; i < rowEnd; i += blockDim.x) {
+            double g3[3];
+            rowProduct(g, c.np, i, b.z, g3);
+            double m = c.mass[i];
+            for (int d = 0; d < 3; d++) {
+                double z = b.z[3*i+d];
+                double Az = z*((1.0 + a)/m) + g3[d]*a;
+                double p = z, Ap = Az;
+                if (iteration > 0) {
+                    p = z + beta[d]*b.p[3*i+d];
+                    Ap = Az + beta[d]*g.Ap[3*i+d];
+                }
+                b.p[3*i+d] = p;
+                g.Ap[3*i+d] = Ap;
+                acc3[d] += p*Ap;
+            }
+        }
+        blockSumStore(acc3, b.partials[0]);
+        if (!gridBarrier(b.barrier, b.status, generation))
+            return;
+        reducePartials(b.partials[0], gridDim.x, tot);
+        double alpha[3];
+        for (int d = 0; d < 3; d++)
+            alpha[d] = (tot[d] > 0 ? rz[d]/tot[d] : 0.0);
+        double acc4[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = rowBegin + threadIdx.x; i < rowEnd; i += blockDim.x) {
+            double diag = b.diag[i];
+            for (int d = 0; d < 3; d++) {
+                b.F[3*i+d] += alpha[d]*b.p[3*i+d];
+                double r = b.r[3*i+d] - alpha[d]*g.Ap[3*i+d];
+                b.r[3*i+d] = r;
+                double z = r*(1.0/diag);
+                b.z[3*i+d] = z;
+                acc4[d] += r*z;
+                acc4[3+d] += r*r;
+            }
+        }
+        blockSumStore(acc4, b.partials[1]);
+        if (!gridBarrier(b.barrier, b.status, generation))
+            return;
+        reducePartials(b.partials[1], gridDim.x, tot);
+        for (int d = 0; d < 3; d++) {
+            beta[d] = (rz[d] > 0 ? tot[d]/rz[d] : 0.0);
+            rz[d] = tot[d];
+            residual[d] = tot[3+d];
+        }
+    }
+    if (firstWarp == 0 && lane == 0)
+        *b.iterations = iteration;
+    if (failed)
+        return;
+    // Forces and reactions (ReferenceLBMKernels.cpp:889-900): a thread per particle, then a thread per slot.
+    for (int i = firstThread; i < c.np; i += threads)
+        for (int d = 0; d < 3; d++)
+            fout[3*i+d] = b.F[3*i+d]*c.forceScale;
+    if (isStep)
+        for (long long t = firstThread; t < (long long) c.np*S; t += threads) {
+            const int i = (int) (t/S);
+            const double w = (double) slotWeight[t];
+            if (w != 0.0)
+                addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*b.F[3*i], -w*b.F[3*i+1], -w*b.F[3*i+2]);
+        }
+}
+
 // Clear the reaction of the slots of the last step (and their mask words).
 template <typename R>
 __global__ void clearReactionKernel(FluidView f, const int* slotNode, long long total, R* reaction, uint32_t* mask) {
@@ -524,6 +949,8 @@ struct CouplingEngine::Device {
     int* values[2] = {nullptr, nullptr};
     unsigned* hist = nullptr;
     CgBuffers cg;
+    SparseCg sparse;
+    int sparseGrid = 0;
     void* spread = nullptr;
     double* reflectWall = nullptr;
     int cgGrid = 0;
@@ -537,6 +964,7 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
           pinned(nullptr), dev(new Device()) {
     (void) g;
     std::memset(&dev->cg, 0, sizeof(CgBuffers));
+    std::memset(&dev->sparse, 0, sizeof(SparseCg));
     stencilSlots = widthOf(l.interpolation_stencil);
     stencilSlots = stencilSlots*stencilSlots*stencilSlots;
     bool f64 = storageType == LBM_STORAGE_F64;
@@ -601,6 +1029,34 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
                 CUDA_CHECK(cudaMalloc(&b.partials[k], sizeof(double)*kPartial*(size_t) dev->cgGrid));
             CUDA_CHECK(cudaMalloc(&dev->spread, 4*r*(size_t) f.numNodes()));
             CUDA_CHECK(cudaMemsetAsync(dev->spread, 0, 4*r*(size_t) f.numNodes(), stream));
+            // The explicit coupling matrix (centeredSparseKernel) and its cell list.
+            SparseCg& g = dev->sparse;
+            int size[3] = {l.nx, l.ny, l.nz};
+            long long cells = 1;
+            for (int a = 0; a < 3; a++) {
+                g.cells[a] = std::max(1, size[a]/kCgCellEdge);
+                cells *= g.cells[a];
+            }
+            CUDA_CHECK(cudaMalloc(&g.axisIndex, sizeof(int4)*3*(size_t) np));
+            CUDA_CHECK(cudaMalloc(&g.firstIndex, sizeof(int4)*(size_t) np));
+            CUDA_CHECK(cudaMalloc(&g.axisWeight, sizeof(double2)*6*(size_t) np));
+            CUDA_CHECK(cudaMalloc(&g.cellOf, sizeof(int)*(size_t) np));
+            CUDA_CHECK(cudaMalloc(&g.cellCount, sizeof(unsigned)*(size_t) cells));
+            CUDA_CHECK(cudaMemsetAsync(g.cellCount, 0, sizeof(unsigned)*(size_t) cells, stream));
+            CUDA_CHECK(cudaMalloc(&g.cellList, sizeof(int)*kCgCellCapacity*(size_t) cells));
+            CUDA_CHECK(cudaMalloc(&g.rowCount, sizeof(int)*(size_t) np));
+            CUDA_CHECK(cudaMalloc(&g.rowIndex, sizeof(int)*kCgRowCapacity*(size_t) np));
+            CUDA_CHECK(cudaMalloc(&g.rowValue, sizeof(double)*kCgRowCapacity*(size_t) np));
+            CUDA_CHECK(cudaMalloc(&g.Ap, v3));
+            g.overflow = statusDev + 2;
+            if (f64)
+                CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, centeredSparseKernel<double>, kSolveThreads, 0));
+            else
+                CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, centeredSparseKernel<float>, kSolveThreads, 0));
+            long long wantedSolve = ((long long) np*32 + kSolveThreads - 1)/kSolveThreads;
+            // No more blocks than the partial records hold (cgGrid of the 256-thread solve).
+            dev->sparseGrid = (int) std::max(1LL, std::min(std::min(wantedSolve, (long long) std::max(1, perSM)*sms),
+                                                          (long long) dev->cgGrid));
         }
         CUDA_CHECK(cudaMallocHost(&pinned, v3));
         CUDA_CHECK(cudaStreamSynchronize(stream));
@@ -631,6 +1087,9 @@ void CouplingEngine::release() {
         cudaFree(b.rhs); cudaFree(b.diag); cudaFree(b.F); cudaFree(b.r); cudaFree(b.z); cudaFree(b.p);
         cudaFree(b.partials[0]); cudaFree(b.partials[1]); cudaFree(b.barrier);
         cudaFree(dev->spread);
+        SparseCg& g = dev->sparse;
+        cudaFree(g.axisIndex); cudaFree(g.firstIndex); cudaFree(g.axisWeight); cudaFree(g.cellOf); cudaFree(g.cellCount); cudaFree(g.cellList);
+        cudaFree(g.rowCount); cudaFree(g.rowIndex); cudaFree(g.rowValue); cudaFree(g.Ap);
         delete dev;
         dev = nullptr;
     }
@@ -712,9 +1171,12 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
         return;
     }
     // Centred drag with a stencil: the conjugate gradients on the device (ReferenceLBMKernels.cpp:834-888, tolerance
-    // 1e-13 in double; 1e-5 with single-precision arithmetic, as the reference's GPU platforms in single precision).
+    // 1e-13 in double; 1e-5 with single-precision arithmetic, as the reference's GPU platforms in single precision),
+    // through the explicit coupling matrix; the spread-and-gather kernel serves a step whose cell list or matrix rows
+    // overflow their capacity (and every step with LBM_B200_SPREAD_CG=1 in the environment, for comparisons).
     CgBuffers b = dev->cg;
-    CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*2, stream));
+    SparseCg g = dev->sparse;
+    CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*3, stream));
     double tolerance = std::is_same<R, double>::value ? 1e-13 : 1e-5;
     int maxIterations = 1000;
     long long stepArg = step;
@@ -728,13 +1190,37 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     int* sn = dev->slotNode;
     FluidView fv = f;
     CouplingView cc = c;
-    void* args[] = {&fv, &cc, &vel, &fin, &sn, &sw, &su, &coef, &stepArg, &isStepArg, &tolerance, &maxIterations, &b,
-                    &spread, &fout, &reaction, &mask, &wall};
-    CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredStencilKernel<R>, dev->cgGrid, kThreads, args, 0, stream));
-    fluid.launches++;
-    int status[2] = {0, 0};
-    CUDA_CHECK(cudaMemcpyAsync(status, statusDev, sizeof(int)*2, cudaMemcpyDeviceToHost, stream));
-    CUDA_CHECK(cudaStreamSynchronize(stream));
+    const double* pos = posDev;
+    int status[3] = {0, 0, 0};
+    static const bool spreadOnly = [] {
+        const char* e = std::getenv("LBM_B200_SPREAD_CG");
+        return e != nullptr && e[0] == '1';
+    }();
+    if (!spreadOnly) {
+        long long total = (long long) np*c.slots;
+        int gridSlots = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
+        cgBinKernel<R><<<gridSlots, kThreads, 0, stream>>>(c, sw, su, pos, coef, g);
+        CUDA_CHECK(cudaGetLastError());
+        cgRowsKernel<R><<<warpGrid(np), kThreads, 0, stream>>>(c, coef, g);
+        CUDA_CHECK(cudaGetLastError());
+        void* sparseArgs[] = {&fv, &cc, &vel, &fin, &sn, &sw, &su, &stepArg, &isStepArg, &tolerance, &maxIterations, &b,
+                              &g, &fout, &reaction, &mask, &wall};
+        CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredSparseKernel<R>, dev->sparseGrid, kSolveThreads,
+                                               sparseArgs, 0, stream));
+        fluid.launches += 3;
+        CUDA_CHECK(cudaMemcpyAsync(status, statusDev, sizeof(int)*3, cudaMemcpyDeviceToHost, stream));
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+    }
+    if (spreadOnly || status[2] != 0) {
+        CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*3, stream));
+        void* args[] = {&fv, &cc, &vel, &fin, &sn, &sw, &su, &coef, &stepArg, &isStepArg, &tolerance, &maxIterations, &b,
+                        &spread, &fout, &reaction, &mask, &wall};
+        CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredStencilKernel<R>, dev->cgGrid, kThreads, args, 0, stream));
+        fluid.launches++;
+        CUDA_CHECK(cudaMemcpyAsync(status, statusDev, sizeof(int)*2, cudaMemcpyDeviceToHost, stream));
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+        spreadSteps++;
+    }
     lastIterations = status[1];
     if (status[0] == LBM_ERR_CG_NOT_CONVERGED)
         throw Error(LBM_ERR_CG_NOT_CONVERGED, "LBMForce: the centred drag with the interpolation stencil did not converge "

@@ -32,6 +32,7 @@ public:
     int numParticles() const { return np; }
     // Conjugate-gradient iterations of the last centred stencil solve.
     int lastIterations = 0;
+    long long spreadSteps = 0;   // steps whose centred drag ran the spread-and-gather solve
 private:
     struct Device;
     void release();

@@ -254,6 +254,10 @@ int B200Kernel::solverIterations() const {
     return coupling ? coupling->lastIterations : 0;
 }
 
+long long B200Kernel::solverFallbackSteps() const {
+    return coupling ? coupling->spreadSteps : 0;
+}
+
 void B200Kernel::getFluidState(double* state) {
     CUDA_CHECK(cudaSetDevice(device));
     fluid->getState(state);

@@ -34,6 +34,7 @@ public:
     cudaStream_t getStream() const { return stream; }
     FluidEngine& fluidEngine() { return *fluid; }
     int solverIterations() const;
+    long long solverFallbackSteps() const;
     void setFluidEquilibrium(const double* density, const double* velocity, bool onDevice, bool strain);
     long long steadySolve(long long firstStep, int interval, double tolerance, long long maxSteps, double* residual);
 private:

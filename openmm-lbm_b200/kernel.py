@@ -119,6 +119,18 @@ class B200Kernel:
         check(self.lib.lbm_set_fluid_equilibrium(self.handle, density.ctypes.data, velocity.ctypes.data, MEMORY_HOST,
                                                  int(strain)), self.lib)
 
+    def solver_iterations(self):
+        """Conjugate-gradient iterations of the last centred stencil drag solve."""
+        n = ctypes.c_int()
+        check(self.lib.lbm_solver_iterations(self.handle, ctypes.byref(n)), self.lib)
+        return n.value
+
+    def solver_fallback_steps(self):
+        """Steps whose centred stencil drag was solved by spread and gather on the nodes (capacity overflow)."""
+        n = ctypes.c_longlong()
+        check(self.lib.lbm_solver_fallback_steps(self.handle, ctypes.byref(n)), self.lib)
+        return n.value
+
     def get_fluid_mach_number(self):
         mach = ctypes.c_double()
         check(self.lib.lbm_get_fluid_mach_number(self.handle, ctypes.byref(mach)), self.lib)

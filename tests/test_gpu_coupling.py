@@ -17,8 +17,54 @@ def run_case(walls, drag, stencil, factory, props, temperature=0.0, steps=60):
     context.integrator.step(steps)
     out = (context.positions.copy(), context.velocities.copy(), force.getFluidState(context),
            force.getWallForce(context))
+    if factory is None and drag == 'Centered' and stencil != 'NearestNode':
+        # Every step solved through the explicit coupling matrix (4 particles: no cell or row over capacity).
+        assert context.kernel.solver_fallback_steps() == 0
     context.close()
     return out
+
+
+def cluster_case(count, spread, stencil, factory, props, seed=3):
+    """`count` particles of mass 100 within a cube of `spread` nm (lattice spacing 0.5 nm) in the middle of a 16^3
+    lattice, centred drag with friction 10/ps, a field and random velocities: more particles than a cell of the
+    explicit coupling matrix holds (64, cells of 4^3 nodes) or more overlapping stencils than a row holds (128)."""
+    import lbm_b200
+    system = lbm_b200.System()
+    system.setDefaultPeriodicBoxVectors((8, 0, 0), (0, 8, 0), (0, 0, 8))
+    force = LBMForce()
+    force.setGridSize(16, 16, 16)
+    for i in range(count):
+        system.addParticle(100.0)
+        force.addParticle(i)
+    system.addForce(lbm_b200.ExternalForce(lambda p: np.tile([3.0, -2.0, 1.0], (len(p), 1))))
+    system.addForce(force)
+    force.setDragScheme(LBMForce.Centered)
+    force.setInterpolationStencil(getattr(LBMForce, stencil))
+    force.setFriction(10.0)
+    force.setTemperature(0.0)
+    force.setFluidMomentumRemovalFrequency(0)
+    context = lbm_b200.Context(system, lbm_b200.VerletIntegrator(0.01), factory, props)
+    rng = np.random.default_rng(seed)
+    context.setPositions(4.55 + rng.uniform(0.0, spread, (count, 3)))
+    context.setVelocities(rng.normal(0.0, 0.5, (count, 3)))
+    return context, force
+
+
+@pytest.mark.parametrize('count,spread,stencil', [(80, 1.9, 'Keys'), (200, 3.4, 'Keys'), (160, 2.4, 'ThreePoint')])
+def test_crowded_centred_drag_agrees_with_oracle(count, spread, stencil):
+    """Crowded particles overflow the capacity of the explicit coupling matrix (a cell of 80 in 2^3 nm; 200 and 160
+    particles whose stencils overlap more than 128 others), so those steps take the spread-and-gather solve: both
+    solves give the oracle's trajectory (FP64, 1e-10)."""
+    results = []
+    for factory, props in ((OracleKernel, None), (None, {'Precision': 'double'})):
+        context, force = cluster_case(count, spread, stencil, factory, props)
+        context.integrator.step(10)
+        results.append((context.positions.copy(), context.velocities.copy(), force.getFluidState(context)))
+        if factory is None:
+            assert context.kernel.solver_fallback_steps() > 0
+        context.close()
+    for a, b, name in zip(results[0], results[1], ('positions', 'velocities', 'state')):
+        assert abs(b - a).max() <= 1e-10*max(1.0, abs(a).max()), name
 
 
 @pytest.mark.parametrize('walls,drag,stencil', COUPLING_CASES)
