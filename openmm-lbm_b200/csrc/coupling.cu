@@ -1,9 +1,10 @@
 // Particle coupling kernels of the B200 LBM force kernel (sm_100a).
 //
 // The coupling of the reference (platforms/reference/src/ReferenceLBMKernels.cpp:503-1018), on the device:
-//   stencilKernel         one thread per (particle, stencil slot): the node and weight of the slot
-//                         (LBMStencils::axisWeights, LBMStencils.h:73-95) and the moments of the node pulled from the
-//                         populations (density, momentum after the momentum removal; a solid node has rho = 0)
+//   stencilClaimKernel    one thread per (particle, stencil slot): the node and weight of the slot
+//                         (LBMStencils::axisWeights, LBMStencils.h:73-95); the first slot of each fluid node pulls the
+//                         node's moments from the populations (density, momentum after the momentum removal)
+//   stencilGatherKernel   the moments of every slot from its node (a solid node has rho = 0)
 //   explicitKernel        one warp per particle: explicit drag F = -gamma m (v - u) + sqrt(2 gamma m kT) xi with u
 //                         interpolated over the stencil (:503-553, :643-697), reaction -w F on the stencil nodes
 //   centeredNearestKernel the closed form of the centred drag per node (:555-641), after a stable radix sort of the
@@ -37,13 +38,41 @@ namespace {
 
 const int kThreads = 256;
 
-// One thread per (particle, slot).
+// The stencil pass: the axis indices and weights of each particle, then one thread per (particle, stencil slot) in
+// two passes: nodes, weights and the moments of each node once, then the moments of every slot.
+// One thread per particle: the node indices and weights of its stencil on each axis, and the first index on each.
+__global__ void stencilAxesKernel(CouplingView c, const double* __restrict__ pos, int4* axisIndex, double2* axisWeight,
+                                  int4* firstIndex) {
+    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x) {
+        int index[3][4];
+        double weight[3][4];
+        stencilAxes(c, pos, i, index, weight);
+        for (int a = 0; a < 3; a++) {
+            axisIndex[3*i + a] = make_int4(index[a][0], index[a][1], index[a][2], index[a][3]);
+            axisWeight[6*i + 2*a] = make_double2(weight[a][0], weight[a][1]);
+            axisWeight[6*i + 2*a + 1] = make_double2(weight[a][2], weight[a][3]);
+        }
+        firstIndex[i] = make_int4(index[0][0], index[1][0], index[2][0], 0);
+    }
+}
+
 template <typename T, typename R>
-__global__ void stencilKernel(const T* __restrict__ A, FluidView f, CouplingView c, const double* __restrict__ pos,
-                              int remove, int centred, int* slotNode, R* slotWeight, typename Vec4<R>::type* slotU) {
+__global__ void stencilClaimKernel(const T* __restrict__ A, FluidView f, CouplingView c, const int4* __restrict__ axisIndex,
+                                   const double2* __restrict__ axisWeight, int remove, int centred, int* slotNode,
+                                   R* slotWeight, unsigned* nodeStamp, unsigned stamp, typename Vec4<R>::type* nodeU) {
     long long total = (long long) c.np*c.slots;
     for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x)
-        stencilSlot<T, R>(A, f, c, pos, t, remove, centred, slotNode, slotWeight, slotU);
+        stencilClaimSlot<T, R>(A, f, c, axisIndex, axisWeight, t, remove, centred, slotNode, slotWeight, nodeStamp,
+                               stamp, nodeU);
+}
+
+template <typename R>
+__global__ void stencilGatherKernel(CouplingView c, const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
+                                    const unsigned* __restrict__ nodeStamp, unsigned stamp,
+                                    const typename Vec4<R>::type* __restrict__ nodeU, typename Vec4<R>::type* slotU) {
+    long long total = (long long) c.np*c.slots;
+    for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x)
+        stencilGatherSlot<R>(t, slotNode, slotWeight, nodeStamp, stamp, nodeU, slotU);
 }
 
 // One warp per particle.
@@ -457,9 +486,8 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
 // (spread w_l F_l onto the nodes, gather with w_k/rho).  K is sparse (a particle's stencil overlaps those of the
 // particles within one stencil width), so it is built once per step and every iteration is a sparse product over a few
 // dozen entries per particle instead of a pass over the lattice nodes of all stencils.
-//   cgBinKernel     per particle: the node indices and weights of its stencil on each axis and its cell (cells of
-//                   kCgCellEdge nodes, on the first stencil index), inserted into a fixed-capacity cell list; per
-//                   slot: w/rho
+//   cgBinKernel     per particle: its cell (cells of kCgCellEdge nodes, on the first stencil index of the stencil
+//                   pass), inserted into a fixed-capacity cell list; per slot: w/rho
 //   cgRowsKernel    one warp per particle k: the particles of the neighbouring cells whose first stencil indices are
 //                   within a stencil width of k's on every axis, sorted by index (so that every row, and every sum
 //                   over it, has one order), and K_kl for each, a lane per entry
@@ -491,33 +519,18 @@ struct SparseCg {
 
 template <typename R>
 __global__ void __launch_bounds__(kThreads)
-cgBinKernel(CouplingView c, const R* __restrict__ slotWeight, const typename Vec4<R>::type* __restrict__ slotU,
-            const double* __restrict__ pos, R* coef, SparseCg g) {
+cgBinKernel(CouplingView c, const R* __restrict__ slotWeight, const typename Vec4<R>::type* __restrict__ slotU, R* coef,
+            SparseCg g) {
     const long long total = (long long) c.np*c.slots;
     for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x) {
         double w = (double) slotWeight[t];
         double rho = (double) slotU[t].w;
         coef[t] = (R) (rho > 0 ? w/rho : 0.0);
     }
-    const int size[3] = {c.nx, c.ny, c.nz};
     for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x) {
-        int cell[3], first[3];
-        for (int a = 0; a < 3; a++) {
-            int index[4];
-            double weight[4];
-            axisWeights(c.stencil, c.width, latticeCoordinate(pos[3*i+a], c.dx, size[a]), size[a], c.open[a] != 0,
-                        index, weight);
-            for (int k = c.width; k < 4; k++)
-                index[k] = -1;
-            g.axisIndex[3*i + a] = make_int4(index[0], index[1], index[2], index[3]);
-            for (int k = c.width; k < 4; k++)
-                weight[k] = 0.0;
-            g.axisWeight[6*i + 2*a] = make_double2(weight[0], weight[1]);
-            g.axisWeight[6*i + 2*a + 1] = make_double2(weight[2], weight[3]);
-            first[a] = index[0];
-            cell[a] = min(index[0]/kCgCellEdge, g.cells[a] - 1);
-        }
-        g.firstIndex[i] = make_int4(first[0], first[1], first[2], 0);
+        const int4 first = g.firstIndex[i];
+        const int cell[3] = {min(first.x/kCgCellEdge, g.cells[0] - 1), min(first.y/kCgCellEdge, g.cells[1] - 1),
+                             min(first.z/kCgCellEdge, g.cells[2] - 1)};
         int key = cell[0] + g.cells[0]*(cell[1] + g.cells[1]*cell[2]);
         g.cellOf[i] = key;
         unsigned slot = atomicAdd(&g.cellCount[key], 1u);
@@ -952,6 +965,12 @@ struct CouplingEngine::Device {
     SparseCg sparse;
     int sparseGrid = 0;
     void* spread = nullptr;
+    int4* axisIndex = nullptr;      // per particle: 3, the stencil's node indices on each axis
+    double2* axisWeight = nullptr;  // per particle: 6, the stencil's weights on each axis
+    int4* firstIndex = nullptr;     // per particle: the first stencil index on each axis
+    unsigned* nodeStamp = nullptr;  // per node: the stamp of the last stencil pass that computed its moments
+    void* nodeU = nullptr;          // per node: 4 R, the moments of that pass
+    unsigned stamp = 0;
     double* reflectWall = nullptr;
     int cgGrid = 0;
     size_t histCount = 0;
@@ -994,6 +1013,12 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
         CUDA_CHECK(cudaMalloc(&dev->slotU, 4*r*slots));
         CUDA_CHECK(cudaMemsetAsync(dev->slotNode, 0, sizeof(int)*slots, stream));
         CUDA_CHECK(cudaMemsetAsync(dev->slotWeight, 0, r*slots, stream));
+        CUDA_CHECK(cudaMalloc(&dev->axisIndex, sizeof(int4)*3*(size_t) np));
+        CUDA_CHECK(cudaMalloc(&dev->axisWeight, sizeof(double2)*6*(size_t) np));
+        CUDA_CHECK(cudaMalloc(&dev->firstIndex, sizeof(int4)*(size_t) np));
+        CUDA_CHECK(cudaMalloc(&dev->nodeStamp, sizeof(unsigned)*(size_t) f.numNodes()));
+        CUDA_CHECK(cudaMemsetAsync(dev->nodeStamp, 0, sizeof(unsigned)*(size_t) f.numNodes(), stream));
+        CUDA_CHECK(cudaMalloc(&dev->nodeU, 4*r*(size_t) f.numNodes()));
         if (l.drag_scheme == LBM_DRAG_CENTERED && l.interpolation_stencil == LBM_STENCIL_NEAREST) {
             int blocks = (np + kSortItems - 1)/kSortItems;
             dev->histCount = (size_t) 256*blocks;
@@ -1037,9 +1062,9 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
                 g.cells[a] = std::max(1, size[a]/kCgCellEdge);
                 cells *= g.cells[a];
             }
-            CUDA_CHECK(cudaMalloc(&g.axisIndex, sizeof(int4)*3*(size_t) np));
-            CUDA_CHECK(cudaMalloc(&g.firstIndex, sizeof(int4)*(size_t) np));
-            CUDA_CHECK(cudaMalloc(&g.axisWeight, sizeof(double2)*6*(size_t) np));
+            g.axisIndex = dev->axisIndex;
+            g.axisWeight = dev->axisWeight;
+            g.firstIndex = dev->firstIndex;
             CUDA_CHECK(cudaMalloc(&g.cellOf, sizeof(int)*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.cellCount, sizeof(unsigned)*(size_t) cells));
             CUDA_CHECK(cudaMemsetAsync(g.cellCount, 0, sizeof(unsigned)*(size_t) cells, stream));
@@ -1078,6 +1103,8 @@ void CouplingEngine::release() {
     pinned = nullptr;
     if (dev) {
         cudaFree(dev->slotNode); cudaFree(dev->slotWeight); cudaFree(dev->slotU); cudaFree(dev->coef);
+        cudaFree(dev->nodeStamp); cudaFree(dev->nodeU);
+        cudaFree(dev->axisIndex); cudaFree(dev->axisWeight); cudaFree(dev->firstIndex);
         for (int k = 0; k < 2; k++) {
             cudaFree(dev->keys[k]);
             cudaFree(dev->values[k]);
@@ -1088,7 +1115,7 @@ void CouplingEngine::release() {
         cudaFree(b.partials[0]); cudaFree(b.partials[1]); cudaFree(b.barrier);
         cudaFree(dev->spread);
         SparseCg& g = dev->sparse;
-        cudaFree(g.axisIndex); cudaFree(g.firstIndex); cudaFree(g.axisWeight); cudaFree(g.cellOf); cudaFree(g.cellCount); cudaFree(g.cellList);
+        cudaFree(g.cellOf); cudaFree(g.cellCount); cudaFree(g.cellList);
         cudaFree(g.rowCount); cudaFree(g.rowIndex); cudaFree(g.rowValue); cudaFree(g.Ap);
         delete dev;
         dev = nullptr;
@@ -1130,11 +1157,17 @@ void CouplingEngine::reflect(const LbmParticleArrays* p, double wallMomentum[3])
 
 template <typename T, typename R>
 static void launchStencil(const void* A, const FluidView& f, const CouplingView& c, const double* pos, int remove, int centred,
-                          int* slotNode, void* slotWeight, void* slotU, cudaStream_t s) {
+                          int* slotNode, void* slotWeight, void* slotU, unsigned* nodeStamp, unsigned stamp,
+                          void* nodeU, int4* axisIndex, double2* axisWeight, int4* firstIndex, cudaStream_t s) {
+    typedef typename Vec4<R>::type V;
     long long total = (long long) c.np*c.slots;
     int grid = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
-    stencilKernel<T, R><<<grid, kThreads, 0, s>>>((const T*) A, f, c, pos, remove, centred, slotNode, (R*) slotWeight,
-                                                   (typename Vec4<R>::type*) slotU);
+    stencilAxesKernel<<<std::max(1, (c.np + kThreads - 1)/kThreads), kThreads, 0, s>>>(c, pos, axisIndex, axisWeight,
+                                                                                      firstIndex);
+    stencilClaimKernel<T, R><<<grid, kThreads, 0, s>>>((const T*) A, f, c, axisIndex, axisWeight, remove, centred,
+                                                        slotNode, (R*) slotWeight, nodeStamp, stamp, (V*) nodeU);
+    stencilGatherKernel<R><<<grid, kThreads, 0, s>>>(c, slotNode, (const R*) slotWeight, nodeStamp, stamp,
+                                                     (const V*) nodeU, (V*) slotU);
 }
 
 template <typename R>
@@ -1190,7 +1223,6 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     int* sn = dev->slotNode;
     FluidView fv = f;
     CouplingView cc = c;
-    const double* pos = posDev;
     int status[3] = {0, 0, 0};
     static const bool spreadOnly = [] {
         const char* e = std::getenv("LBM_B200_SPREAD_CG");
@@ -1199,7 +1231,7 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     if (!spreadOnly) {
         long long total = (long long) np*c.slots;
         int gridSlots = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
-        cgBinKernel<R><<<gridSlots, kThreads, 0, stream>>>(c, sw, su, pos, coef, g);
+        cgBinKernel<R><<<gridSlots, kThreads, 0, stream>>>(c, sw, su, coef, g);
         CUDA_CHECK(cudaGetLastError());
         cgRowsKernel<R><<<warpGrid(np), kThreads, 0, stream>>>(c, coef, g);
         CUDA_CHECK(cudaGetLastError());
@@ -1234,14 +1266,21 @@ void CouplingEngine::couple(long long step, bool isStep, bool remove) {
     CouplingView c = makeCouplingView(lattice, f, np, widthOf(lattice.interpolation_stencil), massDev);
     bool centred = lattice.drag_scheme == LBM_DRAG_CENTERED;
     const void* A = fluid.inputArray();
+    if (++dev->stamp == 0u) {     // the stamps wrapped around: no node may carry a stale stamp
+        CUDA_CHECK(cudaMemsetAsync(dev->nodeStamp, 0, sizeof(unsigned)*(size_t) f.n, stream));
+        dev->stamp = 1u;
+    }
+    unsigned* ns = dev->nodeStamp;
+    void* nu = dev->nodeU;
+    unsigned st = dev->stamp;
     switch (storageType) {
-    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
-    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
-    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
-    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, stream); break;
+    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, stream); break;
+    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, stream); break;
+    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, stream); break;
+    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, stream); break;
     }
     CUDA_CHECK(cudaGetLastError());
-    fluid.launches++;
+    fluid.launches += 3;
     if (isStep)
         CUDA_CHECK(cudaMemsetAsync(wallDev, 0, sizeof(double)*3, stream));
     if (storageType == LBM_STORAGE_F64)

@@ -145,11 +145,9 @@ __device__ void axisWeights(int stencil, int width, double s, int n, bool open, 
 
 // Density deviation and momentum of the post-stream populations of a node (pulled from the input array).
 template <typename T>
-__device__ void pullMoments(const T* A, const FluidView& f, long long node, double& dr, double& jx, double& jy, double& jz) {
+__device__ void pullMomentsAt(const T* A, const FluidView& f, int x, int y, int z, double& dr, double& jx, double& jy,
+                              double& jz) {
     typedef typename std::conditional<std::is_same<T, double>::value, double, float>::type R;
-    int x = (int) (node%f.nx);
-    long long r = node/f.nx;
-    int y = (int) (r%f.ny), z = (int) (r/f.ny);
     int xs[3] = {x == 0 ? f.nx-1 : x-1, x, x == f.nx-1 ? 0 : x+1};
     int ys[3] = {y == 0 ? f.ny-1 : y-1, y, y == f.ny-1 ? 0 : y+1};
     int zs[3] = {z == 0 ? f.nz-1 : z-1, z, z == f.nz-1 ? 0 : z+1};
@@ -165,6 +163,32 @@ __device__ void pullMoments(const T* A, const FluidView& f, long long node, doub
         c += cz*v;
     }
     dr = d; jx = a; jy = b; jz = c;
+}
+
+template <typename T>
+__device__ void pullMoments(const T* A, const FluidView& f, long long node, double& dr, double& jx, double& jy, double& jz) {
+    long long r = node/f.nx;
+    pullMomentsAt<T>(A, f, (int) (node%f.nx), (int) (r%f.ny), (int) (r/f.ny), dr, jx, jy, jz);
+}
+
+// The node indices and weights of particle i's stencil on each axis (entries past the width: index -1, weight 0).
+__device__ __forceinline__ void stencilAxes(const CouplingView& c, const double* __restrict__ pos, int i, int index[3][4],
+                                            double weight[3][4]) {
+    const int size[3] = {c.nx, c.ny, c.nz};
+    for (int a = 0; a < 3; a++) {
+        for (int k = 0; k < 4; k++) {
+            index[a][k] = -1;
+            weight[a][k] = 0.0;
+        }
+        double sc = latticeCoordinate(pos[3*i+a], c.dx, size[a]);
+        if (c.stencil == LBM_STENCIL_NEAREST) {
+            // nearestNode (ReferenceLBMKernels.cpp:973-983): periodic wrap on every axis.
+            index[a][0] = ((int) floor(sc + 0.5))%size[a];
+            weight[a][0] = 1.0;
+        }
+        else
+            axisWeights(c.stencil, c.width, sc, size[a], c.open[a] != 0, index[a], weight[a]);
+    }
 }
 
 // The node, weight and fluid velocity of stencil slot t = i*slots + s (particle i, slot s): the node and weight of
@@ -220,6 +244,67 @@ __device__ __forceinline__ void stencilSlot(const T* __restrict__ A, const Fluid
         uz = jz*(1.0/rho);
     }
     slotU[t] = Vec4<R>::make((R) ux, (R) uy, (R) uz, (R) rho);
+}
+
+// The node and weight of stencil slot t, as stencilSlot (from the particle's axis indices and weights, computed once
+// per particle by stencilAxes), with the moments computed once per node: the first slot of a fluid node to claim it in
+// this pass (nodeStamp[node] set to `stamp`) pulls the node's moments into nodeU[node]; stencilGatherSlot then copies
+// them to every slot of the node.  The moments of a node are the same for all its slots, and overlapping stencils
+// share most of their nodes.
+template <typename T, typename R>
+__device__ __forceinline__ void stencilClaimSlot(const T* __restrict__ A, const FluidView& f, const CouplingView& c,
+                                                 const int4* __restrict__ axisIndex,
+                                                 const double2* __restrict__ axisWeight, long long t, int remove,
+                                                 int centred, int* slotNode, R* slotWeight, unsigned* nodeStamp,
+                                                 unsigned stamp, typename Vec4<R>::type* nodeU) {
+    const int i = (int) (t/c.slots), s = (int) (t - (long long) i*c.slots);
+    const int sub[3] = {s%c.width, (s/c.width)%c.width, s/(c.width*c.width)};
+    int idx[3];
+    double w = 1.0;
+    for (int a = 0; a < 3; a++) {
+        const int4 ia = axisIndex[3*i + a];
+        const double2 wa = axisWeight[6*i + 2*a + sub[a]/2];
+        idx[a] = sub[a] == 0 ? ia.x : sub[a] == 1 ? ia.y : sub[a] == 2 ? ia.z : ia.w;
+        w *= (sub[a] & 1) ? wa.y : wa.x;
+    }
+    long long node = idx[0] + (long long) c.nx*(idx[1] + (long long) c.ny*idx[2]);
+    slotNode[t] = (int) node;
+    slotWeight[t] = (R) w;
+    if (w == 0.0)
+        return;
+    if (c.solidMask != nullptr) {
+        const long long row = idx[1] + (long long) c.ny*idx[2];
+        if ((__ldg(&c.solidMask[row*c.wordsPerRow + idx[0]/32]) >> (idx[0]%32)) & 1u)
+            return;
+    }
+    if (atomicExch(&nodeStamp[node], stamp) != stamp) {
+        double dr, jx, jy, jz;
+        pullMomentsAt<T>(A, f, idx[0], idx[1], idx[2], dr, jx, jy, jz);
+        double rho = 1.0 + dr;
+        if (remove) {
+            jx -= rho*f.stats->ucm[0];
+            jy -= rho*f.stats->ucm[1];
+            jz -= rho*f.stats->ucm[2];
+        }
+        if (centred) {
+            jx += c.h*rho*c.g[0];
+            jy += c.h*rho*c.g[1];
+            jz += c.h*rho*c.g[2];
+        }
+        nodeU[node] = Vec4<R>::make((R) (jx*(1.0/rho)), (R) (jy*(1.0/rho)), (R) (jz*(1.0/rho)), (R) rho);
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void stencilGatherSlot(long long t, const int* __restrict__ slotNode,
+                                                  const R* __restrict__ slotWeight, const unsigned* __restrict__ nodeStamp,
+                                                  unsigned stamp, const typename Vec4<R>::type* __restrict__ nodeU,
+                                                  typename Vec4<R>::type* slotU) {
+    const long long node = slotNode[t];
+    typename Vec4<R>::type u = Vec4<R>::make(0, 0, 0, 0);
+    if (slotWeight[t] != (R) 0 && nodeStamp[node] == stamp)
+        u = nodeU[node];
+    slotU[t] = u;
 }
 
 // Reaction (fx, fy, fz) on a node: added into the fluid's reaction buffer and the node flagged, or for a solid node
