@@ -493,7 +493,8 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
 //                   over it, has one order), and K_kl for each, a lane per entry
 //   centeredSparseKernel  the conjugate gradients (same start, preconditioner, stopping rule and per-component
 //                   iteration as the kernel above) in one cooperative launch, two grid barriers per iteration
-// Rows are stored entry-major (entry e of row k at e np + k), so that a thread per row reads them coalesced.  A cell
+// Rows are stored entry-major (entry e of row k at e np + k), so that the threads of consecutive rows read them
+// coalesced; two threads share a row in the products.  A cell
 // or a row over its capacity sets a flag; the host then runs the spread-and-gather kernel for that step.
 // ------------------------------------------------------------------------------------------------------
 
@@ -548,7 +549,7 @@ __device__ __forceinline__ int periodicDistance(int a, int b, int n) {
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
 cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
     __shared__ int candidates[kThreads/32][kCgRowCapacity];
     __shared__ int sorted[kThreads/32][kCgRowCapacity];
@@ -597,31 +598,45 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
         cellId[warp][lane] = cell;
         __syncwarp();
         int found = 0;     // the same in every lane
-        for (int base = 0; base < total; base += 32) {
-            const int e = base + lane;
-            int l = -1;
-            bool near = false;
-            if (e < total) {
-                // The cell holding member e: the first of the 27 whose running end exceeds e.
-                int lo = 0, hi = 26;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (cellEnd[warp][mid] > e)
-                        hi = mid;
-                    else
-                        lo = mid + 1;
+        // Four rounds of 32 members at a time, their loads issued together.
+        for (int base = 0; base < total; base += 128) {
+            int lq[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int e = base + 32*r + lane;
+                lq[r] = -1;
+                if (e < total) {
+                    // The cell holding member e: the first of the 27 whose running end exceeds e.
+                    int lo = 0, hi = 26;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (cellEnd[warp][mid] > e)
+                            hi = mid;
+                        else
+                            lo = mid + 1;
+                    }
+                    lq[r] = g.cellList[(long long) cellId[warp][lo]*kCgCellCapacity + (e - cellStart[warp][lo])];
                 }
-                l = g.cellList[(long long) cellId[warp][lo]*kCgCellCapacity + (e - cellStart[warp][lo])];
-                const int4 fl = g.firstIndex[l];
-                near = periodicDistance(fl.x, fk.x, size[0]) < c.width &&
-                       periodicDistance(fl.y, fk.y, size[1]) < c.width &&
-                       periodicDistance(fl.z, fk.z, size[2]) < c.width;
             }
-            const unsigned ballot = __ballot_sync(0xFFFFFFFFu, near);
-            const int at = found + __popc(ballot & ((1u << lane) - 1u));
-            if (near && at < kCgRowCapacity)
-                list[at] = l;
-            found += __popc(ballot);
+            bool nq[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                nq[r] = false;
+                if (lq[r] >= 0) {
+                    const int4 fl = g.firstIndex[lq[r]];
+                    nq[r] = periodicDistance(fl.x, fk.x, size[0]) < c.width &&
+                            periodicDistance(fl.y, fk.y, size[1]) < c.width &&
+                            periodicDistance(fl.z, fk.z, size[2]) < c.width;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const unsigned ballot = __ballot_sync(0xFFFFFFFFu, nq[r]);
+                const int at = found + __popc(ballot & ((1u << lane) - 1u));
+                if (nq[r] && at < kCgRowCapacity)
+                    list[at] = lq[r];
+                found += __popc(ballot);
+            }
         }
         __syncwarp();
         if (found > kCgRowCapacity) {
@@ -687,21 +702,24 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
     }
 }
 
-// (K v)_k for the three components of v (thread per row; entries in row order).
+// (K v)_k for the three components of v, by the two threads 2j, 2j + 1 of a row (the even and the odd entries, then
+// their sum), in both; k < 0: no row (the threads still take part in the exchange).  Called by every thread of the warp.
 __device__ __forceinline__ void rowProduct(const SparseCg& g, int np, int k, const double* v, double out[3]) {
-    const int n = g.rowCount[k];
     double s0 = 0, s1 = 0, s2 = 0;
+    if (k >= 0) {
+        const int n = g.rowCount[k];
 #pragma unroll 4
-    for (int e = 0; e < n; e++) {
-        const int l = g.rowIndex[(long long) e*np + k];
-        const double K = g.rowValue[(long long) e*np + k];
-        s0 += K*v[3*l];
-        s1 += K*v[3*l+1];
-        s2 += K*v[3*l+2];
+        for (int e = threadIdx.x & 1; e < n; e += 2) {
+            const int l = g.rowIndex[(long long) e*np + k];
+            const double K = g.rowValue[(long long) e*np + k];
+            s0 += K*v[3*l];
+            s1 += K*v[3*l+1];
+            s2 += K*v[3*l+2];
+        }
     }
-    out[0] = s0;
-    out[1] = s1;
-    out[2] = s2;
+    out[0] = s0 + __shfl_xor_sync(0xFFFFFFFFu, s0, 1);
+    out[1] = s1 + __shfl_xor_sync(0xFFFFFFFFu, s1, 1);
+    out[2] = s2 + __shfl_xor_sync(0xFFFFFFFFu, s2, 1);
 }
 
 template <typename R>
@@ -775,9 +793,12 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
         return;
     // r = rhs - A F, z = r/diag, p = z; r.z, the norm of the right-hand side and r.r per component.
     double acc[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int i = rowBegin + threadIdx.x; i < rowEnd; i += blockDim.x) {
+    for (int base = rowBegin; base < rowEnd; base += blockDim.x/2) {
+        const int i = base + threadIdx.x/2;
         double g3[3];
-        rowProduct(g, c.np, i, b.F, g3);
+        rowProduct(g, c.np, i < rowEnd ? i : -1, b.F, g3);
+        if (i >= rowEnd || (threadIdx.x & 1))
+            continue;
         double m = c.mass[i], diag = b.diag[i];
         for (int d = 0; d < 3; d++) {
             double AF = b.F[3*i+d]*((1.0 + a)/m) + g3[d]*a;
@@ -816,9 +837,12 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
         }
         // p = z + beta p and A p = A z + beta A p (p = z at the first iteration), with p.Ap.
         double acc3[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-        for (int i = rowBegin + threadIdx.x; i < rowEnd; i += blockDim.x) {
+        for (int base = rowBegin; base < rowEnd; base += blockDim.x/2) {
+            const int i = base + threadIdx.x/2;
             double g3[3];
-            rowProduct(g, c.np, i, b.z, g3);
+            rowProduct(g, c.np, i < rowEnd ? i : -1, b.z, g3);
+            if (i >= rowEnd || (threadIdx.x & 1))
+                continue;
             double m = c.mass[i];
             for (int d = 0; d < 3; d++) {
                 double z = b.z[3*i+d];
