@@ -908,11 +908,11 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
 template <typename R>
 __global__ void clearReactionKernel(FluidView f, const int* slotNode, long long total, R* reaction, uint32_t* mask) {
     for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x) {
-        long long node = slotNode[t];
-        *reinterpret_cast<typename Vec4<R>::type*>(reaction + 4*node) = Vec4<R>::make(0, 0, 0, 0);
-        long long row = node/f.nx;
-        int x = (int) (node - row*f.nx);
-        mask[row*f.wordsPerRow + x/32] = 0u;
+        const unsigned node = (unsigned) slotNode[t];
+        *reinterpret_cast<typename Vec4<R>::type*>(reaction + 4*(size_t) node) = Vec4<R>::make(0, 0, 0, 0);
+        const unsigned row = node/(unsigned) f.nx;
+        const int x = (int) (node - row*(unsigned) f.nx);
+        mask[(size_t) row*f.wordsPerRow + x/32] = 0u;
     }
 }
 

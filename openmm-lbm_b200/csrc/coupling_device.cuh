@@ -79,12 +79,13 @@ __device__ __forceinline__ void atomicAdd3(double* r, double x, double y, double
     atomicAdd(&r[2], z);
 }
 
+// Node indices are below 2^32 (the fluid checks it), so 32-bit division finds their rows.
 __device__ __forceinline__ bool isSolid(const uint32_t* mask, int wordsPerRow, int nx, long long node) {
     if (mask == nullptr)
         return false;
-    long long row = node/nx;
-    int x = (int) (node - row*nx);
-    return (__ldg(&mask[row*wordsPerRow + x/32]) >> (x%32)) & 1u;
+    const unsigned row = (unsigned) node/(unsigned) nx;
+    const int x = (int) ((unsigned) node - row*(unsigned) nx);
+    return (__ldg(&mask[(size_t) row*wordsPerRow + x/32]) >> (x%32)) & 1u;
 }
 
 // Lattice coordinate of a position along an axis, wrapped into [0, n) (ReferenceLBMKernels.cpp:978-979).
@@ -319,10 +320,10 @@ __device__ void addReaction(const FluidView& f, const CouplingView& c, R* reacti
         return;
     }
     atomicAdd3(reaction + 4*node, fx, fy, fz);
-    long long row = node/f.nx;
-    int x = (int) (node - row*f.nx);
+    const unsigned row = (unsigned) node/(unsigned) f.nx;
+    const int x = (int) ((unsigned) node - row*(unsigned) f.nx);
     uint32_t bit = 1u << (x%32);
-    uint32_t* word = &mask[row*f.wordsPerRow + x/32];
+    uint32_t* word = &mask[(size_t) row*f.wordsPerRow + x/32];
     if (!(*((volatile uint32_t*) word) & bit))
         atomicOr(word, bit);
 }
