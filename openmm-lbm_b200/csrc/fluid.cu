@@ -382,6 +382,18 @@ __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& 
     }
     const F2 qtr = (qxx + qyy + qzz)*f2(1.0f/3.0f);
     const F2 base = fma2(fma2(rho, uu, uf), f2(-1.5f), dr);
+    // The even part of direction q (before the weight), base - qtr + 4.5 (c.u)(rho c.u + c.F) + c.Q.c, as
+    // base - qtr + sum_{c_a != 0} P_aa + sum_{a < b} c_a c_b P_ab with the symmetric tensor
+    // P_aa = 4.5 u_a (rho u_a + F_a) + q_aa and P_ab = 4.5 (u_a (2 rho u_b + F_b) + u_b F_a) + q_ab: the axis
+    // directions take E_a = base - qtr + P_aa, the diagonal ones S_ab +- P_ab with S_ab = E_a + P_bb.
+    const F2 rho2 = rho + rho, base1 = base - qtr;
+    const F2 Ex = base1 + fma2(ux*fma2(rho, ux, Fx), f2(4.5f), qxx);
+    const F2 Pyy = fma2(uy*fma2(rho, uy, Fy), f2(4.5f), qyy), Pzz = fma2(uz*fma2(rho, uz, Fz), f2(4.5f), qzz);
+    const F2 Ey = base1 + Pyy, Ez = base1 + Pzz;
+    const F2 Pxy = fma2(fma2(ux, fma2(rho2, uy, Fy), uy*Fx), f2(4.5f), qxy);
+    const F2 Pxz = fma2(fma2(ux, fma2(rho2, uz, Fz), uz*Fx), f2(4.5f), qxz);
+    const F2 Pyz = fma2(fma2(uy, fma2(rho2, uz, Fz), uz*Fy), f2(4.5f), qyz);
+    const F2 Sxy = Ex + Pyy, Sxz = Ex + Pzz, Syz = Ey + Pzz;
     // Dither words of the two nodes (the hash of collideNode's Dither, per node).
     uint32_t hashA = 0, hashB = 0;
     if (dithered) {
@@ -404,20 +416,34 @@ __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& 
         constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
         constexpr float k = storeScale<T, q>();
         constexpr float w = wOf<float>(q);
-        F2 cu = f2(0), cf = f2(0), cp = f2(0);
-        if (cx != 0) { cu = fma2(f2((float) cx), ux, cu); cf = fma2(f2((float) cx), Fx, cf); cp = fma2(f2((float) cx), px, cp); }
-        if (cy != 0) { cu = fma2(f2((float) cy), uy, cu); cf = fma2(f2((float) cy), Fy, cf); cp = fma2(f2((float) cy), py, cp); }
-        if (cz != 0) { cu = fma2(f2((float) cz), uz, cu); cf = fma2(f2((float) cz), Fz, cf); cp = fma2(f2((float) cz), pz, cp); }
-        F2 cqc = f2(0) - qtr;
-        if (cx != 0) cqc = cqc + qxx;
-        if (cy != 0) cqc = cqc + qyy;
-        if (cz != 0) cqc = cqc + qzz;
-        if (cx*cy != 0) cqc = fma2(f2((float) (cx*cy)), qxy, cqc);
-        if (cx*cz != 0) cqc = fma2(f2((float) (cx*cz)), qxz, cqc);
-        if (cy*cz != 0) cqc = fma2(f2((float) (cy*cz)), qyz, cqc);
-        // even and odd in stored units: k w (...) and k 3 w c.(j + F), plus k w times the ghost sums.
-        F2 evenRaw = fma2(cu*fma2(rho, cu, cf), f2(4.5f), base + cqc);
-        F2 odd = cp*f2(k*oddOf<float>(q));
+        F2 evenRaw;
+        if constexpr (cy == 0 && cz == 0)
+            evenRaw = Ex;
+        else if constexpr (cx == 0 && cz == 0)
+            evenRaw = Ey;
+        else if constexpr (cx == 0 && cy == 0)
+            evenRaw = Ez;
+        else if constexpr (cz == 0)
+            evenRaw = cx*cy > 0 ? Sxy + Pxy : Sxy - Pxy;
+        else if constexpr (cy == 0)
+            evenRaw = cx*cz > 0 ? Sxz + Pxz : Sxz - Pxz;
+        else
+            evenRaw = cy*cz > 0 ? Syz + Pyz : Syz - Pyz;
+        // The odd part in stored units, k 3 w c.(j + F) (3 w rounded as oddOf).
+        constexpr float ko = k*oddOf<float>(q);
+        F2 odd;
+        if constexpr (cx != 0) {
+            odd = px*f2(cx*ko);
+            if constexpr (cy != 0) odd = fma2(py, f2(cy*ko), odd);
+            if constexpr (cz != 0) odd = fma2(pz, f2(cz*ko), odd);
+        }
+        else if constexpr (cy != 0) {
+            odd = py*f2(cy*ko);
+            if constexpr (cz != 0) odd = fma2(pz, f2(cz*ko), odd);
+        }
+        else
+            odd = pz*f2(cz*ko);
+        // Plus k w times the ghost sums with fluctuations; even in stored units is k w evenRaw.
         if (FLUCT) {
             F2 e, o;
             ghostSums2<q>(a, e, o);
