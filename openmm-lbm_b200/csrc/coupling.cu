@@ -553,7 +553,7 @@ __global__ void __launch_bounds__(kThreads, 4)
 cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
     __shared__ int candidates[kThreads/32][kCgRowCapacity];
     __shared__ int sorted[kThreads/32][kCgRowCapacity];
-    __shared__ double rowCoef[kThreads/32][64];
+    __shared__ R rowCoef[kThreads/32][64];
     __shared__ int cellEnd[kThreads/32][32], cellStart[kThreads/32][32], cellId[kThreads/32][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int* list = candidates[warp];
@@ -563,7 +563,7 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
     const int w = c.width, S = c.slots;
     for (int k = firstWarp; k < c.np; k += warps) {
         for (int s = lane; s < S; s += 32)
-            rowCoef[warp][s] = (double) coef[(long long) k*S + s];
+            rowCoef[warp][s] = coef[(long long) k*S + s];
         const int4 fk = g.firstIndex[k];
         const int key = g.cellOf[k];
         const int home[3] = {key%g.cells[0], (key/g.cells[0])%g.cells[1], key/(g.cells[0]*g.cells[1])};
@@ -659,7 +659,8 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
         const int4 ik[3] = {g.axisIndex[3*k], g.axisIndex[3*k + 1], g.axisIndex[3*k + 2]};
         for (int j = lane; j < found; j += 32) {
             const int l = sorted[warp][j];
-            double shifted[3][4];
+            // In the precision of the fluid's arithmetic (the slots' w/rho are stored in it).
+            R shifted[3][4];
 #pragma unroll
             for (int a = 0; a < 3; a++) {
                 const int4 il = g.axisIndex[3*l + a];
@@ -674,19 +675,19 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
                         if (il.y == mine[i]) v = w01.y;
                         if (il.x == mine[i]) v = w01.x;
                     }
-                    shifted[a][i] = v;
+                    shifted[a][i] = (R) v;
                 }
             }
-            double K = 0;
+            R K = 0;
 #pragma unroll
             for (int iz = 0; iz < 4; iz++) {
-                if (iz >= w || shifted[2][iz] == 0.0)
+                if (iz >= w || shifted[2][iz] == (R) 0)
                     continue;
 #pragma unroll
                 for (int iy = 0; iy < 4; iy++) {
-                    if (iy >= w || shifted[1][iy] == 0.0)
+                    if (iy >= w || shifted[1][iy] == (R) 0)
                         continue;
-                    const double wyz = shifted[1][iy]*shifted[2][iz];
+                    const R wyz = shifted[1][iy]*shifted[2][iz];
 #pragma unroll
                     for (int ix = 0; ix < 4; ix++)
                         if (ix < w)
@@ -694,7 +695,7 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
                 }
             }
             g.rowIndex[(long long) j*c.np + k] = l;
-            g.rowValue[(long long) j*c.np + k] = K;
+            g.rowValue[(long long) j*c.np + k] = (double) K;
         }
         if (lane == 0)
             g.rowCount[k] = found;
