@@ -509,7 +509,7 @@ struct SparseCg {
     int4* firstIndex;      // the first stencil index on each axis
     int* cellOf;           // cell of each particle
     unsigned* cellCount;   // particles per cell (cleared by the solve kernel)
-    int* cellList;         // kCgCellCapacity per cell
+    int4* cellList;        // kCgCellCapacity per cell: the particle and its first stencil index on each axis
     int* rowCount;         // entries per row
     int* rowIndex;         // entry e of row k at e np + k: the column particle
     double* rowValue;      // K_kl, same layout
@@ -536,7 +536,7 @@ cgBinKernel(CouplingView c, const R* __restrict__ slotWeight, const typename Vec
         g.cellOf[i] = key;
         unsigned slot = atomicAdd(&g.cellCount[key], 1u);
         if (slot < (unsigned) kCgCellCapacity)
-            g.cellList[(long long) key*kCgCellCapacity + slot] = i;
+            g.cellList[(long long) key*kCgCellCapacity + slot] = make_int4(i, first.x, first.y, first.z);
         else
             atomicExch(g.overflow, 1);
     }
@@ -601,10 +601,12 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
         // Four rounds of 32 members at a time, their loads issued together.
         for (int base = 0; base < total; base += 128) {
             int lq[4];
+            bool nq[4];
 #pragma unroll
             for (int r = 0; r < 4; r++) {
                 const int e = base + 32*r + lane;
                 lq[r] = -1;
+                nq[r] = false;
                 if (e < total) {
                     // The cell holding member e: the first of the 27 whose running end exceeds e.
                     int lo = 0, hi = 26;
@@ -615,18 +617,11 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
                         else
                             lo = mid + 1;
                     }
-                    lq[r] = g.cellList[(long long) cellId[warp][lo]*kCgCellCapacity + (e - cellStart[warp][lo])];
-                }
-            }
-            bool nq[4];
-#pragma unroll
-            for (int r = 0; r < 4; r++) {
-                nq[r] = false;
-                if (lq[r] >= 0) {
-                    const int4 fl = g.firstIndex[lq[r]];
-                    nq[r] = periodicDistance(fl.x, fk.x, size[0]) < c.width &&
-                            periodicDistance(fl.y, fk.y, size[1]) < c.width &&
-                            periodicDistance(fl.z, fk.z, size[2]) < c.width;
+                    const int4 m = g.cellList[(long long) cellId[warp][lo]*kCgCellCapacity + (e - cellStart[warp][lo])];
+                    lq[r] = m.x;
+                    nq[r] = periodicDistance(m.y, fk.x, size[0]) < c.width &&
+                            periodicDistance(m.z, fk.y, size[1]) < c.width &&
+                            periodicDistance(m.w, fk.z, size[2]) < c.width;
                 }
             }
 #pragma unroll
@@ -1093,7 +1088,7 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
             CUDA_CHECK(cudaMalloc(&g.cellOf, sizeof(int)*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.cellCount, sizeof(unsigned)*(size_t) cells));
             CUDA_CHECK(cudaMemsetAsync(g.cellCount, 0, sizeof(unsigned)*(size_t) cells, stream));
-            CUDA_CHECK(cudaMalloc(&g.cellList, sizeof(int)*kCgCellCapacity*(size_t) cells));
+            CUDA_CHECK(cudaMalloc(&g.cellList, sizeof(int4)*kCgCellCapacity*(size_t) cells));
             CUDA_CHECK(cudaMalloc(&g.rowCount, sizeof(int)*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.rowIndex, sizeof(int)*kCgRowCapacity*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.rowValue, sizeof(double)*kCgRowCapacity*(size_t) np));
