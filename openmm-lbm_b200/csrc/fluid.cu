@@ -280,8 +280,15 @@ __device__ __forceinline__ void ghostSums2(const F2 a[15], F2& even, F2& odd) {
     });
 }
 
+// Resident blocks of 256 threads per SM the paired kernel is compiled for: 3 for 16-bit storage without
+// fluctuations (it fits in 80 registers without spilling and waits on its loads, so more warps help: FP16 channel
+// step 0.584 -> 0.569 ms, BF16 0.581 -> 0.561 ms), 2 otherwise (FP32 storage at 3 blocks: channel step 0.722 ->
+// 0.852 ms, 256^3 0.473 -> 0.483 ms; the noise needs more registers).
 #ifndef LBM_PAIR_MIN_BLOCKS
 #define LBM_PAIR_MIN_BLOCKS 2
+#endif
+#ifndef LBM_PAIR_MIN_BLOCKS_16BIT
+#define LBM_PAIR_MIN_BLOCKS_16BIT 3
 #endif
 
 // Per-launch constants of the paired kernels.
@@ -471,7 +478,7 @@ __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& 
 // The dense step with two x-adjacent nodes per thread (nx even), the arithmetic of both in packed FP32 pairs; each
 // thread loads its pulled words from global memory.
 template <typename T, bool SOLID, bool REACT, bool FLUCT>
-__global__ void __launch_bounds__(THREADS, LBM_PAIR_MIN_BLOCKS)
+__global__ void __launch_bounds__(THREADS, (sizeof(T) == 2 && !FLUCT) ? LBM_PAIR_MIN_BLOCKS_16BIT : LBM_PAIR_MIN_BLOCKS)
 streamCollidePairKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int remove, long long step) {
     typedef typename PairIO<T>::Word Word;
     const int lane = threadIdx.x%32, warp = threadIdx.x/32;
