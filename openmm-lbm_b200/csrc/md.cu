@@ -1,11 +1,11 @@
 // Bead dynamics on the device (include/lbm_b200_md.h): the forces and the leapfrog integrator that OpenMM would
 // provide around the LBM force kernel in the benchmark configurations.  Harmonic bonds, and WCA or truncated
-// Lennard-Jones pairs found with a cell list: particles are sorted by cell (radix_sort.cuh), each cell's range in
-// the sorted order is recorded, and each particle visits the 27 cells around its own (a brute-force pass serves
-// boxes with fewer than 3 cells along an axis).
+// Lennard-Jones pairs found with a cell list: particles are binned by cell with atomics into fixed-capacity bins,
+// and each particle visits the 27 cells around its own, taking each cell's particles in index order (so every
+// force is summed in one order); a cell over its capacity is scanned over all particles instead (a brute-force pass
+// serves boxes with fewer than 3 cells along an axis).
 #include "lbm_internal.h"
 #include "lbm_b200_md.h"
-#include "radix_sort.cuh"
 #include <algorithm>
 #include <cmath>
 #include <string>
@@ -29,10 +29,13 @@ struct MdView {
     const double* invMass;
     const int* bondOffset;
     const int* bondPartner;
-    const int* cellStart;
-    const int* cellEnd;
-    const int* sorted;       // particle indices in cell order
+    const unsigned* cellKey;   // cell of each particle
+    const unsigned* binCount;  // particles per cell (cleared after each force pass)
+    const int* bins;           // binCapacity per cell: the particles of the cell, in arbitrary order
+    int binCapacity;
 };
+
+constexpr int kMaxBinCapacity = 16;
 
 __device__ __forceinline__ void minimumImage(const MdView& v, double d[3]) {
     for (int a = 0; a < 3; a++)
@@ -77,27 +80,28 @@ __device__ void bondForces(const MdView& v, const double* pos, int i, double f[3
     }
 }
 
-__global__ void cellKeysKernel(MdView v, const double* pos, unsigned* keys, int* values) {
+__global__ void binKernel(MdView v, const double* pos, unsigned* cellKey, unsigned* binCount, int* bins) {
     for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < v.n; i += gridDim.x*blockDim.x) {
         const double* x = &pos[3*i];
-        keys[i] = (unsigned) (cellOf(v, x, 0) + v.ncell[0]*(cellOf(v, x, 1) + v.ncell[1]*cellOf(v, x, 2)));
-        values[i] = i;
+        const unsigned key = (unsigned) (cellOf(v, x, 0) + v.ncell[0]*(cellOf(v, x, 1) + v.ncell[1]*cellOf(v, x, 2)));
+        cellKey[i] = key;
+        const unsigned slot = atomicAdd(&binCount[key], 1u);
+        if (slot < (unsigned) v.binCapacity)
+            bins[(size_t) key*v.binCapacity + slot] = i;
     }
 }
 
-__global__ void cellRangeKernel(int n, const unsigned* keys, int* cellStart, int* cellEnd, int clear) {
-    for (int k = blockIdx.x*blockDim.x + threadIdx.x; k < n; k += gridDim.x*blockDim.x) {
-        unsigned key = keys[k];
-        if (clear) {
-            cellStart[key] = 0;
-            cellEnd[key] = 0;
-            continue;
-        }
-        if (k == 0 || keys[k-1] != key)
-            cellStart[key] = k;
-        if (k == n-1 || keys[k+1] != key)
-            cellEnd[key] = k + 1;
-    }
+__global__ void clearBinsKernel(int n, const unsigned* cellKey, unsigned* binCount) {
+    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < n; i += gridDim.x*blockDim.x)
+        binCount[cellKey[i]] = 0u;
+}
+
+__device__ __forceinline__ void pairWith(const MdView& v, const double* pos, int i, const double* x, int j, double f[3]) {
+    if (j == i || bonded(v, i, j))
+        return;
+    double d[3] = {x[0] - pos[3*j], x[1] - pos[3*j+1], x[2] - pos[3*j+2]};
+    minimumImage(v, d);
+    pairForce(v, d, f);
 }
 
 __global__ void cellForceKernel(MdView v, const double* pos, double* forces) {
@@ -113,15 +117,27 @@ __global__ void cellForceKernel(MdView v, const double* pos, double* forces) {
                         int cx = (c[0] + dx + v.ncell[0])%v.ncell[0];
                         int cy = (c[1] + dy + v.ncell[1])%v.ncell[1];
                         int cz = (c[2] + dz + v.ncell[2])%v.ncell[2];
-                        long long cell = cx + (long long) v.ncell[0]*(cy + (long long) v.ncell[1]*cz);
-                        for (int k = v.cellStart[cell]; k < v.cellEnd[cell]; k++) {
-                            int j = v.sorted[k];
-                            if (j == i || bonded(v, i, j))
-                                continue;
-                            double d[3] = {x[0] - pos[3*j], x[1] - pos[3*j+1], x[2] - pos[3*j+2]};
-                            minimumImage(v, d);
-                            pairForce(v, d, f);
+                        unsigned cell = (unsigned) (cx + v.ncell[0]*(cy + v.ncell[1]*cz));
+                        const int count = (int) v.binCount[cell];
+                        if (count <= v.binCapacity) {
+                            // The cell's particles in index order (insertion sort of at most kMaxBinCapacity).
+                            int member[kMaxBinCapacity];
+                            for (int e = 0; e < count; e++) {
+                                int j = v.bins[(size_t) cell*v.binCapacity + e], p = e;
+                                while (p > 0 && member[p-1] > j) {
+                                    member[p] = member[p-1];
+                                    p--;
+                                }
+                                member[p] = j;
+                            }
+                            for (int e = 0; e < count; e++)
+                                pairWith(v, pos, i, x, member[e], f);
                         }
+                        else
+                            // Over capacity: every particle of the cell, found by scanning them all in index order.
+                            for (int j = 0; j < v.n; j++)
+                                if (v.cellKey[j] == cell)
+                                    pairWith(v, pos, i, x, j, f);
                     }
         }
         for (int a = 0; a < 3; a++)
@@ -184,15 +200,12 @@ struct MdEngine {
     double* invMass = nullptr;
     int* bondOffset = nullptr;
     int* bondPartner = nullptr;
-    int* cellStart = nullptr;
-    int* cellEnd = nullptr;
-    unsigned* keys[2] = {nullptr, nullptr};
-    int* values[2] = {nullptr, nullptr};
-    unsigned* hist = nullptr;
+    unsigned* cellKey = nullptr;
+    unsigned* binCount = nullptr;
+    int* bins = nullptr;
     double* scalar = nullptr;
     bool brute = true;
     long long ncells = 0;
-    int bits = 1;
     long long launches = 0;
 
     MdEngine(int n, const double* masses, const double box[3], int numBonds, const int* bonds, double k, double r0,
@@ -224,6 +237,17 @@ struct MdEngine {
         }
         if (pairType == LBM_PAIR_NONE)
             brute = true;
+        // Bin capacity: WCA cells (no smaller than 2^(1/6) sigma) hold few particles of a repulsive fluid; truncated
+        // Lennard-Jones cells (no smaller than the cutoff) hold a liquid's.  The bins stay under 2 GB: larger boxes
+        // take fewer, larger cells.
+        view.binCapacity = pairType == LBM_PAIR_WCA ? 8 : kMaxBinCapacity;
+        while (!brute && ncells*view.binCapacity*(long long) sizeof(int) > (2LL << 30)) {
+            int a = view.ncell[0] >= view.ncell[1] && view.ncell[0] >= view.ncell[2] ? 0 : (view.ncell[1] >= view.ncell[2] ? 1 : 2);
+            ncells /= view.ncell[a];
+            view.ncell[a] = std::max(3, view.ncell[a]/2);
+            view.cellSize[a] = box[a]/view.ncell[a];
+            ncells *= view.ncell[a];
+        }
         // Bonds as adjacency lists (CSR).
         std::vector<int> count(n + 1, 0), offset(n + 1, 0), partner(2*(size_t) numBonds);
         for (int b = 0; b < numBonds; b++) {
@@ -257,17 +281,10 @@ struct MdEngine {
                 CUDA_CHECK(cudaMemcpy(bondPartner, partner.data(), sizeof(int)*partner.size(), cudaMemcpyHostToDevice));
             CUDA_CHECK(cudaMalloc(&scalar, sizeof(double)*4));
             if (!brute) {
-                CUDA_CHECK(cudaMalloc(&cellStart, sizeof(int)*ncells));
-                CUDA_CHECK(cudaMalloc(&cellEnd, sizeof(int)*ncells));
-                CUDA_CHECK(cudaMemset(cellStart, 0, sizeof(int)*ncells));
-                CUDA_CHECK(cudaMemset(cellEnd, 0, sizeof(int)*ncells));
-                for (int b = 0; b < 2; b++) {
-                    CUDA_CHECK(cudaMalloc(&keys[b], sizeof(unsigned)*n));
-                    CUDA_CHECK(cudaMalloc(&values[b], sizeof(int)*n));
-                }
-                CUDA_CHECK(cudaMalloc(&hist, sizeof(unsigned)*256*(size_t) ((n + kSortItems - 1)/kSortItems)));
-                while (bits < 32 && (1LL << bits) < ncells)
-                    bits++;
+                CUDA_CHECK(cudaMalloc(&cellKey, sizeof(unsigned)*n));
+                CUDA_CHECK(cudaMalloc(&binCount, sizeof(unsigned)*ncells));
+                CUDA_CHECK(cudaMemset(binCount, 0, sizeof(unsigned)*ncells));
+                CUDA_CHECK(cudaMalloc(&bins, sizeof(int)*(size_t) ncells*view.binCapacity));
             }
         }
         catch (...) {
@@ -277,19 +294,17 @@ struct MdEngine {
         view.invMass = invMass;
         view.bondOffset = bondOffset;
         view.bondPartner = bondPartner;
-        view.cellStart = cellStart;
-        view.cellEnd = cellEnd;
+        view.cellKey = cellKey;
+        view.binCount = binCount;
+        view.bins = bins;
     }
     void release() {
-        cudaFree(invMass); cudaFree(bondOffset); cudaFree(bondPartner); cudaFree(cellStart); cudaFree(cellEnd);
-        for (int b = 0; b < 2; b++) {
-            cudaFree(keys[b]);
-            cudaFree(values[b]);
-        }
-        cudaFree(hist);
+        cudaFree(invMass); cudaFree(bondOffset); cudaFree(bondPartner); cudaFree(cellKey); cudaFree(binCount);
+        cudaFree(bins);
         cudaFree(scalar);
-        invMass = nullptr; bondOffset = bondPartner = cellStart = cellEnd = nullptr;
-        keys[0] = keys[1] = nullptr; values[0] = values[1] = nullptr; hist = nullptr; scalar = nullptr;
+        invMass = nullptr; bondOffset = bondPartner = bins = nullptr;
+        cellKey = binCount = nullptr;
+        scalar = nullptr;
     }
     ~MdEngine() { release(); }
 
@@ -302,16 +317,12 @@ struct MdEngine {
             launches++;
             return;
         }
-        cellKeysKernel<<<gridFor(n), 256, 0, s>>>(view, pos, keys[0], values[0]);
-        int cur = radixSortByKey(keys, values, hist, n, bits, s);
-        cellRangeKernel<<<gridFor(n), 256, 0, s>>>(n, keys[cur], cellStart, cellEnd, 0);
-        MdView v = view;
-        v.sorted = values[cur];
-        cellForceKernel<<<gridFor(n), 256, 0, s>>>(v, pos, out);
-        // Reset the ranges of the occupied cells, so that the next call starts from empty cells.
-        cellRangeKernel<<<gridFor(n), 256, 0, s>>>(n, keys[cur], cellStart, cellEnd, 1);
+        binKernel<<<gridFor(n), 256, 0, s>>>(view, pos, cellKey, binCount, bins);
+        cellForceKernel<<<gridFor(n), 256, 0, s>>>(view, pos, out);
+        // Empty the occupied bins, so that the next call starts from empty cells.
+        clearBinsKernel<<<gridFor(n), 256, 0, s>>>(n, cellKey, binCount);
         CUDA_CHECK(cudaGetLastError());
-        launches += 4 + 3*((bits + 7)/8);
+        launches += 3;
     }
 };
 
