@@ -186,14 +186,16 @@ __device__ bool gridBarrier(unsigned* bar, int* status, unsigned& generation) {
             atomicExch(&bar[1], target);
         }
         else {
+            // Poll with plain loads (an atomic per poll from every waiting block would queue behind one another at
+            // the word's L2 slice, and delay the release); look at the status word every 256 polls.
             long long polls = 0;
             while (*((volatile unsigned*) &bar[1]) != target) {
-                if (++polls > (1LL << 26) || atomicAdd(status, 0) == LBM_ERR_DEVICE_TIMEOUT) {
+                if (++polls > (1LL << 26) ||
+                    ((polls & 255) == 0 && *((volatile int*) status) == LBM_ERR_DEVICE_TIMEOUT)) {
                     atomicExch(status, LBM_ERR_DEVICE_TIMEOUT);
                     ok = false;
                     break;
                 }
-                __nanosleep(32);
             }
         }
         __threadfence();
