@@ -67,6 +67,16 @@ def test_crowded_centred_drag_agrees_with_oracle(count, spread, stencil):
         assert abs(b - a).max() <= 1e-10*max(1.0, abs(a).max()), name
 
 
+@pytest.mark.parametrize('stencil', ['Trilinear', 'ThreePoint', 'Keys'])
+def test_centred_stencil_at_open_faces_agrees_with_oracle(stencil):
+    """The centred drag with a stencil next to open x faces, where the stencil's indices are clamped to the last
+    node (repeated entries of weight zero): the coupling matrix matches the oracle's spread-and-gather solve."""
+    ref = run_case('faces', 'Centered', stencil, OracleKernel, None)
+    got = run_case('faces', 'Centered', stencil, None, {'Precision': 'double'})
+    for a, b, name in zip(ref, got, ('positions', 'velocities', 'state', 'wall')):
+        assert abs(b - a).max() <= 1e-10*max(1.0, abs(a).max()), name
+
+
 @pytest.mark.parametrize('walls,drag,stencil', COUPLING_CASES)
 def test_coupling_agrees_with_oracle_double(walls, drag, stencil):
     ref = run_case(walls, drag, stencil, OracleKernel, None)
