@@ -496,8 +496,8 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
 //   centeredSparseKernel  the conjugate gradients (same start, preconditioner, stopping rule and per-component
 //                   iteration as the kernel above) in one cooperative launch, two grid barriers per iteration
 // Rows are stored entry-major (entry e of row k at e np + k), so that the threads of consecutive rows read them
-// coalesced; two threads share a row in the products.  A cell
-// or a row over its capacity sets a flag; the host then runs the spread-and-gather kernel for that step.
+// coalesced; two threads share a row in the products.  A cell or a row over its capacity sets a flag; the host then
+// runs the spread-and-gather kernel for that step.
 // ------------------------------------------------------------------------------------------------------
 
 constexpr int kCgCellEdge = 4;      // nodes per cell edge (no less than the widest stencil)
