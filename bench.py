@@ -520,6 +520,33 @@ def run_b200(args, w, rank, world, device):
     }
 
 
+def plain_fluid_record(args, w, rank, world, device):
+    """The dense step of the plain fluid of the same lattice (no particles, no fluctuations, the same storage), timed
+    like the main record: its MLUPS and the roofline fraction of its dense kernel."""
+    import copy
+    plain = Workload(n=w.n, coupled=False, fluctuations=False, seed=w.seed)
+    sub = copy.copy(args)
+    sub.observables = False
+    r = run_b200(sub, plain, rank, world, device)
+    return {'workload': plain.name(), 'value': r['value'], 'unit': 'MLUPS', 'ms_per_step': r['ms_per_step'],
+            'dense_kernel_ms': r['roofline']['avg_launch_ms'], 'roofline_frac': r['roofline']['frac'],
+            'achieved_gbs': r['roofline']['achieved'], 'peak_gbs': r['roofline']['peak'],
+            'gpu_launches': r['gpu_launches'], 'clocks': r['clocks']}
+
+
+def host_description():
+    """The host's logical core count and CPU model (the CPU baseline runs on one of these cores)."""
+    model = 'unknown'
+    try:
+        for line in open('/proc/cpuinfo'):
+            if line.startswith('model name'):
+                model = line.split(':', 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {'nproc': os.cpu_count(), 'cpu_model': model, 'threads_used': 1}
+
+
 def metric_name(w):
     return 'MLUPS (fluid nodes x lattice steps / s) of the %s lattice step' % ('coupled' if w.coupled else 'fluid')
 
@@ -645,7 +672,10 @@ def main():
     parser.add_argument('--size', type=int, default=0, help='lattice edge in x (smaller cases for profiling)')
     parser.add_argument('--no-fluctuations', action='store_true')
     parser.add_argument('--no-cpu-baseline', action='store_true')
-    parser.add_argument('--observables', action='store_true', help='fluid and bead temperatures after the run')
+    parser.add_argument('--no-observables', dest='observables', action='store_false',
+                        help='skip the fluid and bead temperatures after the run')
+    parser.add_argument('--no-plain-fluid', action='store_true',
+                        help='skip the record of the plain fluid (no particles, no fluctuations) of the same size')
     parser.add_argument('--graph-steps', type=int, default=10, help='batch: lattice steps per CUDA graph')
     parser.add_argument('--replicas', type=int, default=256, help='batch: number of replicas')
     parser.add_argument('--separate', action='store_true', help='batch: also time the replicas as separate kernels')
@@ -673,7 +703,8 @@ def main():
             'value': value, 'unit': 'MLUPS', 'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': dt*1e3, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
             'data': 'synthetic', 'config': {'workload': w.name(), 'sample': sample},
-            'cpu_baseline': {'value': value, 'unit': 'MLUPS', 'cores': 1, 'kind': kind, 'sample': sample},
+            'cpu_baseline': {'value': value, 'unit': 'MLUPS', 'cores': 1, 'kind': kind, 'sample': sample,
+                             'host': host_description()},
             'e2e': {'value': value, 'unit': 'MLUPS', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}))
         return
     if args.impl == 'reference':
@@ -689,7 +720,8 @@ def main():
             'ms_per_step': dt*1e3, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
             'data': 'synthetic', 'config': {'workload': w.name(), 'sample': sample.name()},
             'cpu_baseline': {'value': value, 'unit': 'MLUPS', 'cores': 1, 'kind': kind,
-                             'sample': 'per step, %s (the same per-node and per-bead work)' % sample.name()},
+                             'sample': 'per step, %s (the same per-node and per-bead work)' % sample.name(),
+                             'host': host_description()},
             'e2e': {'value': value, 'unit': 'MLUPS', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}))
         return
     if world > 1:
@@ -704,11 +736,14 @@ def main():
             result['cpu_baseline'] = {'value': value, 'unit': 'MLUPS', 'cores': 1, 'kind': kind, 'sample': sample}
     else:
         result = run_b200(args, w, rank, world, local)
+        if args.workload == 'coupled' and not args.no_plain_fluid:
+            result['plain_fluid'] = plain_fluid_record(args, w, rank, world, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != 'batch':
         sample = w.sample(min(w.shape[0], 128))
         value, kind, dt = run_cpu(args, sample, 2, 1)
         result['cpu_baseline'] = {'value': value, 'unit': 'MLUPS', 'cores': 1, 'kind': kind,
-                                  'sample': 'two timed steps after one warm-up of %s' % sample.name()}
+                                  'sample': 'two timed steps after one warm-up of %s' % sample.name(),
+                                  'host': host_description()}
     if rank == 0:
         print(json.dumps(result))
     if world > 1:

@@ -214,6 +214,13 @@ LbmStatus lbm_solver_iterations(LbmKernel* kernel, int* iterations);
    spread-and-gather one (platforms/reference/src/ReferenceLBMKernels.cpp:726-901). */
 LbmStatus lbm_solver_fallback_steps(LbmKernel* kernel, long long* steps);
 
+/* Limits of the centred stencil drag's conjugate gradients, for tests of their failure paths: at most max_iterations
+   iterations (then LBM_ERR_CG_NOT_CONVERGED, as ReferenceLBMKernels.cpp:864-866 after 1000), and barrier_polls polls
+   of a block waiting at a grid barrier of the cooperative solve (then LBM_ERR_DEVICE_TIMEOUT).  A failed solve leaves
+   no reaction on the fluid and the step can be evaluated again.  0 restores a default (1000 iterations, 2^26 polls).
+   No counterpart in the reference, whose cap is fixed and whose solve has no device-side wait. */
+LbmStatus lbm_set_solver_limits(LbmKernel* kernel, int max_iterations, long long barrier_polls);
+
 /* The steady-state residual r = max_nodes |u - u_prev| / (interval max_nodes |u|) over the fluid nodes, in FP64 on the
    device, with u = j/rho of the current (post-stream) state and u_prev the velocities recorded by the previous call,
    which this call replaces; the first call records them and returns infinity.  Called every `interval` steps it is the

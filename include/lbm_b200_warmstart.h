@@ -30,6 +30,12 @@ LbmStatus lbm_conv3d_weight_grad(const void* x, const void* dy, float* dw, int b
  * LBM_ERR_DEVICE_TIMEOUT if a wait for the tensor cores gave up (its results are not valid). */
 LbmStatus lbm_conv3d_status(void* stream);
 
+/* Polls of the bounded waits for the tensor cores on the current device, for tests of the timeout path: a wait that
+ * runs out of polls makes its convolution leave (after the tensor cores finish the stage in flight) and the next
+ * lbm_conv3d_status return LBM_ERR_DEVICE_TIMEOUT.  0 makes every wait give up at once; a negative value restores the
+ * default (2^24 polls).  No counterpart in the reference. */
+LbmStatus lbm_conv3d_set_wait_limit(long long polls);
+
 #ifdef __cplusplus
 }
 #endif

@@ -103,6 +103,7 @@ SIGNATURES = {
     'lbm_dense_kernel_time': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong), _D]),
     'lbm_kernel_launches': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     'lbm_solver_iterations': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
+    'lbm_set_solver_limits': (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_longlong]),
     'lbm_solver_fallback_steps': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     'lbm_steady_residual': (ctypes.c_int, [_P, ctypes.c_int, _D]),
     'lbm_steady_solve': (ctypes.c_int, [_P, ctypes.c_longlong, ctypes.c_int, ctypes.c_double, ctypes.c_longlong,

@@ -218,6 +218,11 @@ LbmStatus lbm_solver_iterations(LbmKernel* kernel, int* iterations) {
     return LBM_OK;
 }
 
+LbmStatus lbm_set_solver_limits(LbmKernel* kernel, int max_iterations, long long barrier_polls) {
+    CHECK_HANDLE(kernel);
+    return guard([&] { kernel->impl->setSolverLimits(max_iterations, barrier_polls); });
+}
+
 LbmStatus lbm_solver_fallback_steps(LbmKernel* kernel, long long* steps) {
     CHECK_HANDLE(kernel);
     if (!steps)

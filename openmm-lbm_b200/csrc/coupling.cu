@@ -168,15 +168,18 @@ struct CgBuffers {
     unsigned* barrier;     // [0] arrival count, [1] generation
     int* status;           // 0 ok, LBM_ERR_CG_NOT_CONVERGED, LBM_ERR_DEVICE_TIMEOUT
     int* iterations;
+    long long pollLimit;   // polls of a waiting block before it gives up (kDefaultBarrierPolls)
 };
 
-// Grid barrier for a cooperative launch (all blocks resident), with a bounded spin: after about 2^26 polls the
+// Grid barrier for a cooperative launch (all blocks resident), with a bounded spin: after b.pollLimit polls the
 // waiting block gives up, records a timeout in the status word and returns false; every block then leaves the
-// solve at its next barrier.
-__device__ bool gridBarrier(unsigned* bar, int* status, unsigned& generation) {
+// solve at its next barrier.  Thread 0 takes the decision for its block (its own wait and the status word), so
+// all threads of a block return the same value and leave together.
+__device__ bool gridBarrier(unsigned* bar, int* status, unsigned& generation, long long pollLimit) {
+    __shared__ int okShared;
     __syncthreads();
-    bool ok = true;
     if (threadIdx.x == 0) {
+        bool ok = true;
         unsigned target = generation + 1;
         __threadfence();
         unsigned arrived = atomicAdd(&bar[0], 1u);
@@ -190,7 +193,7 @@ __device__ bool gridBarrier(unsigned* bar, int* status, unsigned& generation) {
             // the word's L2 slice, and delay the release); look at the status word every 256 polls.
             long long polls = 0;
             while (*((volatile unsigned*) &bar[1]) != target) {
-                if (++polls > (1LL << 26) ||
+                if (++polls > pollLimit ||
                     ((polls & 255) == 0 && *((volatile int*) status) == LBM_ERR_DEVICE_TIMEOUT)) {
                     atomicExch(status, LBM_ERR_DEVICE_TIMEOUT);
                     ok = false;
@@ -200,12 +203,10 @@ __device__ bool gridBarrier(unsigned* bar, int* status, unsigned& generation) {
         }
         __threadfence();
         generation = target;
+        okShared = ok && *((volatile int*) status) != LBM_ERR_DEVICE_TIMEOUT;
     }
-    __shared__ int okShared;
-    if (threadIdx.x == 0)
-        okShared = ok;
     __syncthreads();
-    return okShared != 0 && *((volatile int*) status) != LBM_ERR_DEVICE_TIMEOUT;
+    return okShared != 0;
 }
 
 // Block sum of a record (thread values v) into partials[block]; after a grid barrier (by the caller) every block adds
@@ -347,7 +348,7 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
                 atomicAdd3(spread + 4*(long long) slotNode[t], w*F[0], w*F[1], w*F[2]);
         }
     }
-    if (!gridBarrier(b.barrier, b.status, generation))
+    if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
         return;
     // r = rhs - A F, z = r/diag, p = z; r.z, the norm of the right-hand side and r.r per component.
     double acc[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -371,7 +372,7 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
         }
     }
     blockSumStore(acc, b.partials[1]);
-    if (!gridBarrier(b.barrier, b.status, generation))
+    if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
         return;
     for (int i = firstWarp; i < c.np; i += warps)
         clearSpread(i);
@@ -397,13 +398,13 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
         // The spread buffer was cleared by every block before the last barrier (the clearing of the start comes
         // before the barrier at the top of the first iteration's spread below).
         if (clearBeforeSpread) {
-            if (!gridBarrier(b.barrier, b.status, generation))
+            if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
                 return;
             clearBeforeSpread = false;
         }
         for (int i = firstWarp; i < c.np; i += warps)
             spreadP(i, b.p);
-        if (!gridBarrier(b.barrier, b.status, generation))
+        if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
             return;
         double acc3[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int i = firstWarp; i < c.np; i += warps) {
@@ -420,7 +421,7 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
             }
         }
         blockSumStore(acc3, b.partials[0]);
-        if (!gridBarrier(b.barrier, b.status, generation))
+        if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
             return;
         reducePartials(b.partials[0], gridDim.x, tot);
         double alpha[3];
@@ -443,7 +444,7 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
             }
         }
         blockSumStore(acc4, b.partials[1]);
-        if (!gridBarrier(b.barrier, b.status, generation))
+        if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
             return;
         reducePartials(b.partials[1], gridDim.x, tot);
         double beta[3];
@@ -787,7 +788,7 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
         }
         b.diag[i] = diag;
     }
-    if (!gridBarrier(b.barrier, b.status, generation))
+    if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
         return;
     // r = rhs - A F, z = r/diag, p = z; r.z, the norm of the right-hand side and r.r per component.
     double acc[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -812,7 +813,7 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
         }
     }
     blockSumStore(acc, b.partials[1]);
-    if (!gridBarrier(b.barrier, b.status, generation))
+    if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
         return;
     double tot[kPartial];
     reducePartials(b.partials[1], gridDim.x, tot);
@@ -856,7 +857,7 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
             }
         }
         blockSumStore(acc3, b.partials[0]);
-        if (!gridBarrier(b.barrier, b.status, generation))
+        if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
             return;
         reducePartials(b.partials[0], gridDim.x, tot);
         double alpha[3];
@@ -876,7 +877,7 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
             }
         }
         blockSumStore(acc4, b.partials[1]);
-        if (!gridBarrier(b.barrier, b.status, generation))
+        if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
             return;
         reducePartials(b.partials[1], gridDim.x, tot);
         for (int d = 0; d < 3; d++) {
@@ -1061,6 +1062,7 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
             CUDA_CHECK(cudaMalloc(&dev->coef, r*slots));
             b.status = statusDev;
             b.iterations = statusDev + 1;
+            b.pollLimit = kDefaultBarrierPolls;
             CUDA_CHECK(cudaMalloc(&b.barrier, sizeof(unsigned)*2));
             CUDA_CHECK(cudaMemsetAsync(b.barrier, 0, sizeof(unsigned)*2, stream));
             int device = 0, sms = 0, perSM = 0;
@@ -1233,7 +1235,8 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     SparseCg g = dev->sparse;
     CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*3, stream));
     double tolerance = std::is_same<R, double>::value ? 1e-13 : 1e-5;
-    int maxIterations = 1000;
+    int maxIterations = cgMaxIterations;
+    b.pollLimit = barrierPollLimit;
     long long stepArg = step;
     int isStepArg = isStep ? 1 : 0;
     R* spread = (R*) dev->spread;
@@ -1278,9 +1281,21 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     lastIterations = status[1];
     if (status[0] == LBM_ERR_CG_NOT_CONVERGED)
         throw Error(LBM_ERR_CG_NOT_CONVERGED, "LBMForce: the centred drag with the interpolation stencil did not converge "
-                    "in 1000 iterations of the conjugate gradients");
-    if (status[0] == LBM_ERR_DEVICE_TIMEOUT)
+                    "in " + std::to_string(maxIterations) + " iterations of the conjugate gradients");
+    if (status[0] == LBM_ERR_DEVICE_TIMEOUT) {
+        // The blocks left the solve at different barriers, so the arrival count holds a partial count: start the
+        // barrier of the next solve from zero.
+        CUDA_CHECK(cudaMemsetAsync(b.barrier, 0, sizeof(unsigned)*2, stream));
+        CUDA_CHECK(cudaStreamSynchronize(stream));
         throw Error(LBM_ERR_DEVICE_TIMEOUT, "LBMForce: a grid barrier of the conjugate gradients timed out");
+    }
+}
+
+void CouplingEngine::setSolverLimits(int maxIterations, long long barrierPolls) {
+    if (maxIterations < 0 || barrierPolls < 0)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_set_solver_limits: the limits must not be negative");
+    cgMaxIterations = maxIterations > 0 ? maxIterations : kDefaultCgIterations;
+    barrierPollLimit = barrierPolls > 0 ? barrierPolls : kDefaultBarrierPolls;
 }
 
 void CouplingEngine::couple(long long step, bool isStep, bool remove) {

@@ -9,6 +9,11 @@ namespace lbm {
 
 struct CouplingView;
 
+// Limits of the centred stencil drag's conjugate gradients: the iteration cap of the reference
+// (ReferenceLBMKernels.cpp:864-866) and the polls after which a block waiting at a grid barrier gives up.
+constexpr int kDefaultCgIterations = 1000;
+constexpr long long kDefaultBarrierPolls = 1LL << 26;
+
 class CouplingEngine {
 public:
     CouplingEngine(const LbmLatticeParameters& lattice, FluidEngine& fluid, const Geometry& geometry, int numParticles,
@@ -33,6 +38,8 @@ public:
     // Conjugate-gradient iterations of the last centred stencil solve.
     int lastIterations = 0;
     long long spreadSteps = 0;   // steps whose centred drag ran the spread-and-gather solve
+    // Lower limits make the failure paths reachable in tests; 0 restores a default.
+    void setSolverLimits(int maxIterations, long long barrierPolls);
 private:
     struct Device;
     void release();
@@ -50,6 +57,8 @@ private:
     double* pinned;            // pinned staging for host particle arrays
     Device* dev;               // slot, sort and solver buffers
     int stencilSlots;
+    int cgMaxIterations = kDefaultCgIterations;
+    long long barrierPollLimit = kDefaultBarrierPolls;
 };
 
 } // namespace lbm

@@ -330,9 +330,7 @@ __device__ void addReaction(const FluidView& f, const CouplingView& c, R* reacti
 
 // Three normals of particle i for step `step` (Philox, purpose 2), in double.
 __device__ __forceinline__ void particleNoise(uint32_t seed, int i, long long step, double xi[3]) {
-    double v[4];
-    boxMuller(philoxBlock(seed, PurposeParticle, i, step, 0), v);
-    xi[0] = v[0]; xi[1] = v[1]; xi[2] = v[2];
+    philoxNormals<double, 3>(seed, PurposeParticle, i, step, xi);
 }
 
 __device__ __forceinline__ double warpSum(double v) {

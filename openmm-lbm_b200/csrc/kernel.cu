@@ -46,6 +46,10 @@ B200Kernel::B200Kernel(const LbmLatticeParameters& l, const LbmOptions& options,
     for (int i = 0; i < np; i++)
         if (!(masses[i] > 0))
             throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: coupled particles must have a positive mass");
+    // The coupling keeps the node of each stencil slot as a 32-bit signed index (and the solid nodes are ints at the
+    // interface), so a lattice with coupled particles is limited to 2^31 - 1 nodes; the fluid alone goes to 2^32.
+    if (np > 0 && n > 2147483647LL)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: a lattice with coupled particles may have at most 2^31 - 1 nodes");
     CUDA_CHECK(cudaSetDevice(device));
     if (options.stream != nullptr)
         stream = (cudaStream_t) options.stream;
@@ -256,6 +260,13 @@ int B200Kernel::solverIterations() const {
 
 long long B200Kernel::solverFallbackSteps() const {
     return coupling ? coupling->spreadSteps : 0;
+}
+
+void B200Kernel::setSolverLimits(int maxIterations, long long barrierPolls) {
+    if (maxIterations < 0 || barrierPolls < 0)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_set_solver_limits: the limits must not be negative");
+    if (coupling)
+        coupling->setSolverLimits(maxIterations, barrierPolls);
 }
 
 void B200Kernel::getFluidState(double* state) {

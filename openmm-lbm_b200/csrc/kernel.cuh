@@ -35,6 +35,7 @@ public:
     FluidEngine& fluidEngine() { return *fluid; }
     int solverIterations() const;
     long long solverFallbackSteps() const;
+    void setSolverLimits(int maxIterations, long long barrierPolls);
     void setFluidEquilibrium(const double* density, const double* velocity, bool onDevice, bool strain);
     long long steadySolve(long long firstStep, int interval, double tolerance, long long maxSteps, double* residual);
 private:

@@ -52,8 +52,9 @@ void computeLatticeParameters(const LbmForceDescription& force, const double box
     if (l.nx <= 0 || l.ny <= 0 || l.nz <= 0)
         throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: the grid size must be set to positive values with setGridSize()");
 
-    // Nodes and populations are indexed with 64-bit integers on the device, so the only limit is memory;
-    // the reference's 2^31 node limit (LBMForceImpl.cpp:56-78) comes from its 32-bit indexing.
+    // The reference's 2^31 node limit (LBMForceImpl.cpp:56-78) comes from its 32-bit indexing.  The dense kernels
+    // here index nodes with 32-bit unsigned integers, so the fluid may have up to 2^32 nodes (lbm_create checks it);
+    // a lattice with coupled particles stays below 2^31 nodes, because the coupling keeps signed 32-bit node indices.
 
     // The lattice spans the periodic box with cubic cells (:80-92).
     l.dx = box[0]/l.nx;

@@ -1,5 +1,5 @@
 // Device helpers of the B200 LBM kernels: the D3Q19 velocity set, storage conversion of the population
-// deviations, the Philox4x32-10 counter-based generator and the collision algebra.
+// deviations, the Philox4x32 counter-based generator and the collision algebra.
 //
 // The algebra is that of the reference's D3Q19 class (openmmapi/include/internal/D3Q19.h): equilibrium
 // deviation (:55), regularized non-equilibrium part (:116), Guo forcing (:127) and the Lulli et al.
@@ -168,18 +168,27 @@ template <> __device__ __forceinline__ void storeq<__nv_bfloat16, float>(__nv_bf
 }
 
 // ------------------------------------------------------------------------------------------------------
-// Philox4x32-10 (Salmon, Moraes, Dror and Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11),
-// with the published multipliers 0xD2511F53, 0xCD9E8D57 and Weyl increments 0x9E3779B9, 0xBB67AE85.
-// The normal number m of (purpose, index, step) comes from the counter (index, step low, step high,
-// purpose*256 + m/4) and the key (seed, 0x4C424D32): lanes (0,1) and (2,3) of the output are Box-Muller
-// pairs, u = (x + 1/2) 2^-32, r = sqrt(-2 ln u_a), normals r cos(2 pi (u_b - 1/2)) and r sin(2 pi (u_b - 1/2)).
+// Philox4x32 (Salmon, Moraes, Dror and Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11) with the
+// published multipliers 0xD2511F53, 0xCD9E8D57 and Weyl increments 0x9E3779B9, 0xBB67AE85, and kPhiloxRounds = 7
+// rounds: the smallest round count that the paper reports to pass the BigCrush battery (10 is its default, with a
+// safety margin); the thermal noise of the fluid takes about half the instructions of the fluctuating dense step.
+//
+// Normal number m of (purpose, index, step): block b is Philox of the counter (index, step low, step high,
+// purpose*256 + b) under the key (seed, 0x4C424D32); word k of the draw is lane k%4 of block k/4.  The normals come in
+// Box-Muller pairs i = m/2, two pairs per three words: pair i takes the radius word w_a, a = 3(m/4) + i%2, with
+// u = (w_a + 1/2) 2^-32 and r = sqrt(-2 ln u), and the 16-bit half h of word 3(m/4) + 2 (the low half for even i,
+// the high half for odd i), with the angle t = 2 pi ((h + 1/2) 2^-16 - 1/2); normal m is r cos t (m even) or r sin t
+// (m odd).  15 normals take 3 blocks, 19 take 4, 3 take 1.
 // ------------------------------------------------------------------------------------------------------
 
 enum { PurposeFluid = 0, PurposeBoundary = 1, PurposeParticle = 2 };
 
-__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+constexpr int kPhiloxRounds = 7;
+
+template <int ROUNDS>
+__device__ __forceinline__ uint4 philox4x32(uint4 c, uint32_t k0, uint32_t k1) {
 #pragma unroll
-    for (int round = 0; round < 10; round++) {
+    for (int round = 0; round < ROUNDS; round++) {
         uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u*c.x;
         uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u*c.z;
         c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
@@ -192,54 +201,56 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1
 __device__ __forceinline__ uint4 philoxBlock(uint32_t seed, int purpose, long long index, long long step, int block) {
     uint4 c = make_uint4((uint32_t) index, (uint32_t) step, (uint32_t) ((unsigned long long) step >> 32),
                          (uint32_t) (purpose*256 + block));
-    return philox4x32_10(c, seed, 0x4C424D32u);
+    return philox4x32<kPhiloxRounds>(c, seed, 0x4C424D32u);
 }
 
-// Four normals from one Philox block, in the compute precision R.  Angles are taken in (-pi, pi):
-// normals r cos(2 pi (u_b - 1/2)) and r sin(2 pi (u_b - 1/2)).
-__device__ __forceinline__ void boxMuller(uint4 x, float out[4]) {
-    const float scale = 2.3283064365386963e-10f;        // 2^-32
+// One Box-Muller pair from a 32-bit radius word and a 16-bit angle half-word, in the compute precision.
+__device__ __forceinline__ void boxMullerPair(uint32_t a, uint32_t h, float& n0, float& n1) {
     const float below1 = 0.99999994f;                   // 1 - 2^-24: keeps log(u) < 0 after rounding to float
-    float ua = fminf(fmaf((float) x.x, scale, 0.5f*scale), below1), ub = fmaf((float) x.y, scale, 0.5f*scale);
-    float uc = fminf(fmaf((float) x.z, scale, 0.5f*scale), below1), ud = fmaf((float) x.w, scale, 0.5f*scale);
+    const float u = fminf(fmaf((float) a, 2.3283064365386963e-10f, 1.1641532182693481e-10f), below1);
+    const float t = fmaf((float) h, 9.587379924285257e-05f, -3.1415447166901718f);   // 2 pi ((h + 1/2)/2^16 - 1/2)
 #ifdef LBM_ACCURATE_FLOAT_NORMALS
-    float r0 = sqrtf(-2.0f*logf(ua)), r1 = sqrtf(-2.0f*logf(uc));
-    float s0, c0, s1, c1;
-    sincospif(2.0f*ub - 1.0f, &s0, &c0);
-    sincospif(2.0f*ud - 1.0f, &s1, &c1);
+    const float r = sqrtf(-2.0f*logf(u));
+    float s, c;
+    sincosf(t, &s, &c);
 #else
     // Hardware approximations (MUFU): -2 ln u = -2 ln2 log2(u), and sin/cos of an angle in (-pi, pi), where their
     // absolute error is about 2^-21.
-    float r0 = sqrtf(fmaxf(-1.3862943611198906f*__log2f(ua), 0.0f));
-    float r1 = sqrtf(fmaxf(-1.3862943611198906f*__log2f(uc), 0.0f));
-    float s0, c0, s1, c1;
-    __sincosf(6.283185307179586f*(ub - 0.5f), &s0, &c0);
-    __sincosf(6.283185307179586f*(ud - 0.5f), &s1, &c1);
+    const float r = sqrtf(fmaxf(-1.3862943611198906f*__log2f(u), 0.0f));
+    float s, c;
+    __sincosf(t, &s, &c);
 #endif
-    out[0] = r0*c0; out[1] = r0*s0; out[2] = r1*c1; out[3] = r1*s1;
+    n0 = r*c;
+    n1 = r*s;
 }
-__device__ __forceinline__ void boxMuller(uint4 x, double out[4]) {
-    const double scale = 2.3283064365386963e-10;
-    double ua = ((double) x.x + 0.5)*scale, ub = ((double) x.y + 0.5)*scale;
-    double uc = ((double) x.z + 0.5)*scale, ud = ((double) x.w + 0.5)*scale;
-    double r0 = sqrt(-2.0*log(ua)), r1 = sqrt(-2.0*log(uc));
-    double s0, c0, s1, c1;
-    sincospi(2.0*ub - 1.0, &s0, &c0);
-    sincospi(2.0*ud - 1.0, &s1, &c1);
-    out[0] = r0*c0; out[1] = r0*s0; out[2] = r1*c1; out[3] = r1*s1;
+__device__ __forceinline__ void boxMullerPair(uint32_t a, uint32_t h, double& n0, double& n1) {
+    const double u = ((double) a + 0.5)*2.3283064365386963e-10;
+    const double v = ((double) h + 0.5)*1.52587890625e-05;
+    const double r = sqrt(-2.0*log(u));
+    double s, c;
+    sincospi(2.0*v - 1.0, &s, &c);
+    n0 = r*c;
+    n1 = r*s;
 }
 
-// The first `count` normals (count <= 20) of (purpose, index, step).
+// The first COUNT normals (COUNT <= 20) of (purpose, index, step).
 template <typename R, int COUNT>
 __device__ __forceinline__ void philoxNormals(uint32_t seed, int purpose, long long index, long long step, R* out) {
+    constexpr int PAIRS = (COUNT + 1)/2, GROUPS = (PAIRS + 1)/2, BLOCKS = (3*GROUPS + 3)/4;
+    uint32_t w[4*BLOCKS];
 #pragma unroll
-    for (int b = 0; b < (COUNT + 3)/4; b++) {
-        R v[4];
-        boxMuller(philoxBlock(seed, purpose, index, step, b), v);
+    for (int b = 0; b < BLOCKS; b++) {
+        const uint4 x = philoxBlock(seed, purpose, index, step, b);
+        w[4*b] = x.x; w[4*b+1] = x.y; w[4*b+2] = x.z; w[4*b+3] = x.w;
+    }
 #pragma unroll
-        for (int l = 0; l < 4; l++)
-            if (4*b + l < COUNT)
-                out[4*b + l] = v[l];
+    for (int i = 0; i < PAIRS; i++) {
+        const uint32_t angles = w[3*(i/2) + 2];
+        R n0, n1;
+        boxMullerPair(w[3*(i/2) + i%2], (i%2) ? (angles >> 16) : (angles & 0xFFFFu), n0, n1);
+        out[2*i] = n0;
+        if (2*i + 1 < COUNT)
+            out[2*i + 1] = n1;
     }
 }
 

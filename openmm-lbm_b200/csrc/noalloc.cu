@@ -32,20 +32,47 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double noallocPartials[kMaxChunks*kRecord];
 
 std::mutex setupMutex;
-double* partialsAddress[kMaxDevices] = {nullptr};
+struct ScratchEntry {
+    void* context;      // the context whose module gave `address`
+    double* address;
+};
+ScratchEntry scratch[kMaxDevices] = {};
 
-// The device address of the scratch on the current device, looked up once per device with that device current.
+// The current CUDA context (CUcontext), through the driver entry point that the runtime hands out, so that the
+// library needs no link to the driver library; nullptr if there is none yet or the entry point is unavailable.
+void* currentContext() {
+    typedef int (*CtxGetCurrent)(void**);
+    static CtxGetCurrent getCurrent = [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult found;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &found) != cudaSuccess ||
+                found != cudaDriverEntryPointSuccess)
+            fn = nullptr;
+        return (CtxGetCurrent) fn;
+    }();
+    void* context = nullptr;
+    if (getCurrent == nullptr || getCurrent(&context) != 0)
+        return nullptr;
+    return context;
+}
+
+// The device address of the scratch on the current device, looked up with that device current: once per device, and
+// again whenever the device's context is not the one of the last lookup (after cudaDeviceReset the runtime creates a
+// new context, whose copy of the array may sit elsewhere).
 double* scratchAddress(int device) {
     std::lock_guard<std::mutex> lock(setupMutex);
-    if (partialsAddress[device] == nullptr) {
+    ScratchEntry& entry = scratch[device];
+    void* context = currentContext();
+    if (entry.address == nullptr || context == nullptr || context != entry.context) {
         void* ptr = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&ptr, noallocPartials);
         if (e != cudaSuccess)
             throw Error(LBM_ERR_CUDA, std::string("lbm_fluid_moments_noalloc: cudaGetSymbolAddress failed: ") +
                         cudaGetErrorString(e));
-        partialsAddress[device] = static_cast<double*>(ptr);
+        entry.address = static_cast<double*>(ptr);
+        entry.context = currentContext();     // the lookup made the context current if it was not yet
     }
-    return partialsAddress[device];
+    return entry.address;
 }
 
 // One block per chunk: the sums over the chunk's fluid nodes (deviations [q*N + node]) in a fixed order.

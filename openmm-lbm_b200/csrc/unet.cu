@@ -29,6 +29,9 @@ constexpr int kChunk = 64;                     // BF16 per stage row
 constexpr long long kSpinLimit = 1LL << 24;    // polls of an mbarrier before giving up
 
 __device__ int convStatus;
+// Polls of the waits for the tensor cores (kSpinLimit unless lbm_conv3d_set_wait_limit lowered it).  The drain of a
+// stage whose wait gave up always uses kSpinLimit.
+__device__ long long convWaitPolls = kSpinLimit;
 
 __device__ __forceinline__ uint32_t smemAddr(const void* p) {
     return (uint32_t) __cvta_generic_to_shared(p);
@@ -63,8 +66,8 @@ __device__ __forceinline__ void commitTo(uint32_t mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(mbar) : "memory");
 }
 
-__device__ __forceinline__ bool waitParity(uint32_t mbar, uint32_t parity) {
-    for (long long i = 0; i < kSpinLimit; i++) {
+__device__ __forceinline__ bool waitParity(uint32_t mbar, uint32_t parity, long long limit) {
+    for (long long i = 0; i < limit; i++) {
         uint32_t done;
         asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
                      "selp.b32 %0, 1, 0, P1;\n\t}" : "=r"(done) : "r"(mbar), "r"(parity) : "memory");
@@ -136,8 +139,9 @@ __device__ __forceinline__ void releaseStage(const Stage& st, uint32_t ncols) {
 }
 
 // One stage: the tiles are in shared memory; thread 0 issues the four K = 16 MMAs and commits; all threads wait.
-// Returns false (for every thread) if the wait gave up.
-__device__ __forceinline__ bool runStage(const Stage& st, uint32_t idesc, int stage) {
+// Returns false (for every thread) if the wait gave up; the caller then drains the stage (drainStage) before it
+// frees the tensor memory that the MMAs may still be writing.
+__device__ __forceinline__ bool runStage(const Stage& st, uint32_t idesc, int stage, long long limit) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -147,8 +151,15 @@ __device__ __forceinline__ bool runStage(const Stage& st, uint32_t idesc, int st
             mmaBf16(st.tmem, smemDescriptor(a + 32*j), smemDescriptor(b + 32*j), idesc, (stage > 0 || j > 0) ? 1u : 0u);
         commitTo(st.mbar);
     }
-    bool ok = waitParity(st.mbar, (uint32_t) (stage & 1));
+    bool ok = waitParity(st.mbar, (uint32_t) (stage & 1), limit);
     return __syncthreads_and(ok) != 0;
+}
+
+// After a wait that gave up: wait once more, with the full limit, for the MMAs of that stage (the only ones in flight),
+// so that the tensor memory and the shared-memory tiles are released only when the tensor cores are done with them.
+__device__ __forceinline__ void drainStage(const Stage& st, int stage) {
+    waitParity(st.mbar, (uint32_t) (stage & 1), kSpinLimit);
+    __syncthreads();
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -171,7 +182,9 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
         vy = (int) (r%H); r /= H;
         vz = (int) (r%D); vn = (int) (r/D);
     }
+    const long long limit = convWaitPolls;
     bool ok = true;
+    int failedStage = -1;
     for (int c = 0; c < stages && ok; c++) {
         for (int kv = 0; kv < 8; kv++) {
             int k = c*kChunk + kv*8;
@@ -191,8 +204,12 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
                 val = __ldg(reinterpret_cast<const uint4*>(w + (long long) row*K + k));
             *reinterpret_cast<uint4*>(st.tileB + swizzled(row, kv)) = val;
         }
-        ok = runStage(st, idesc, c);
+        ok = runStage(st, idesc, c, limit);
+        if (!ok)
+            failedStage = c;
     }
+    if (!ok)
+        drainStage(st, failedStage);
     fenceAfterSync();
     if (ok) {
         const int row = warp*32 + lane;
@@ -230,6 +247,7 @@ convWeightGradKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* _
     const long long stagesTotal = (M + kChunk - 1)/kChunk;
     const uint32_t idesc = instrDescriptor(nt);
     const int col = tid%kChunk, half = tid/kChunk;       // this thread's voxel column and row-group parity
+    const long long limit = convWaitPolls;
     bool ok = true;
     int stage = 0;
     for (long long c = blockIdx.z; c < stagesTotal && ok; c += gridDim.z, stage++) {
@@ -267,7 +285,9 @@ convWeightGradKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* _
             for (int i = 0; i < 8; i++)
                 *reinterpret_cast<__nv_bfloat16*>(st.tileB + swizzled(8*g + i, col >> 3) + colOffset) = e[i];
         }
-        ok = runStage(st, idesc, stage);
+        ok = runStage(st, idesc, stage, limit);
+        if (!ok)
+            drainStage(st, stage);
     }
     fenceAfterSync();
     if (ok && stage > 0) {
@@ -367,6 +387,12 @@ LbmStatus lbm_conv3d_status(void* stream) {
         return (LbmStatus) status;
     }
     return LBM_OK;
+}
+
+LbmStatus lbm_conv3d_set_wait_limit(long long polls) {
+    long long value = polls >= 0 ? polls : kSpinLimit;
+    cudaError_t e = cudaMemcpyToSymbol(convWaitPolls, &value, sizeof(long long));
+    return e == cudaSuccess ? LBM_OK : launchError(e);
 }
 
 } // extern "C"

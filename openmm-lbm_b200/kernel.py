@@ -125,6 +125,10 @@ class B200Kernel:
         check(self.lib.lbm_solver_iterations(self.handle, ctypes.byref(n)), self.lib)
         return n.value
 
+    def set_solver_limits(self, max_iterations=0, barrier_polls=0):
+        """Iteration cap and barrier poll limit of the centred stencil drag's solve (0 restores the default)."""
+        check(self.lib.lbm_set_solver_limits(self.handle, int(max_iterations), int(barrier_polls)), self.lib)
+
     def solver_fallback_steps(self):
         """Steps whose centred stencil drag was solved by spread and gather on the nodes (capacity overflow)."""
         n = ctypes.c_longlong()

@@ -35,6 +35,7 @@ _SIGNATURES = {
                                               ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                               ctypes.c_void_p]),
     'lbm_conv3d_status': (ctypes.c_int, [ctypes.c_void_p]),
+    'lbm_conv3d_set_wait_limit': (ctypes.c_int, [ctypes.c_longlong]),
 }
 
 INLET_SCALE = 0.02

@@ -118,12 +118,13 @@ static double seq_gaussian(OracleKernel* k) {
     return r*cos(angle);
 }
 
-/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): 10 rounds of two 32x32->64 multiplications with the
-   published multipliers and Weyl key increments. */
-void oracle_philox4x32_10(const uint32_t counter[4], const uint32_t key[2], uint32_t out[4]) {
+/* Philox4x32 (Salmon, Moraes, Dror, Shaw, SC'11) with `rounds` rounds of two 32x32->64 multiplications with the
+   published multipliers and Weyl key increments; 10 rounds is the published Philox4x32-10 (its known answers pin this
+   function), 7 the round count of the normal numbers below. */
+void oracle_philox4x32(const uint32_t counter[4], const uint32_t key[2], int rounds, uint32_t out[4]) {
     uint32_t c0 = counter[0], c1 = counter[1], c2 = counter[2], c3 = counter[3];
     uint32_t k0 = key[0], k1 = key[1];
-    for (int round = 0; round < 10; round++) {
+    for (int round = 0; round < rounds; round++) {
         uint64_t p0 = (uint64_t) 0xD2511F53u*c0;
         uint64_t p1 = (uint64_t) 0xCD9E8D57u*c2;
         uint32_t hi0 = (uint32_t) (p0 >> 32), lo0 = (uint32_t) p0;
@@ -138,22 +139,37 @@ void oracle_philox4x32_10(const uint32_t counter[4], const uint32_t key[2], uint
     out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
-/* The counter of normal number m of (purpose, index, step): counter = (index, step low, step high,
-   purpose*256 + m/4), key = (seed, 0x4C424D32).  Lanes (0,1) and (2,3) of the output are Box-Muller
-   pairs: u = (x + 1/2) 2^-32, r = sqrt(-2 ln u_a), normals r cos(2 pi (u_b - 1/2)) and r sin(2 pi (u_b - 1/2)). */
-double oracle_philox_normal(uint32_t seed, int purpose, long long index, long long step, int m) {
+void oracle_philox4x32_10(const uint32_t counter[4], const uint32_t key[2], uint32_t out[4]) {
+    oracle_philox4x32(counter, key, 10, out);
+}
+
+#define ORACLE_PHILOX_ROUNDS 7
+
+/* Word k of the draw of (purpose, index, step): lane k%4 of Philox4x32-7 of the counter (index, step low, step high,
+   purpose*256 + k/4) under the key (seed, 0x4C424D32). */
+static uint32_t philox_word(uint32_t seed, int purpose, long long index, long long step, int k) {
     uint32_t counter[4] = {(uint32_t) index, (uint32_t) step, (uint32_t) ((unsigned long long) step >> 32),
-                           (uint32_t) (purpose*256 + m/4)};
+                           (uint32_t) (purpose*256 + k/4)};
     uint32_t key[2] = {seed, 0x4C424D32u};
     uint32_t x[4];
-    oracle_philox4x32_10(counter, key, x);
-    int lane = m%4;
-    uint32_t a = x[lane < 2 ? 0 : 2], b = x[lane < 2 ? 1 : 3];
-    double ua = ((double) a + 0.5)*(1.0/4294967296.0);
-    double ub = ((double) b + 0.5)*(1.0/4294967296.0);
-    double r = sqrt(-2.0*log(ua));
-    double angle = 6.283185307179586476925287*(ub - 0.5);
-    return (lane%2 == 0 ? r*cos(angle) : r*sin(angle));
+    oracle_philox4x32(counter, key, ORACLE_PHILOX_ROUNDS, x);
+    return x[k%4];
+}
+
+/* Normal number m of (purpose, index, step).  Box-Muller pairs i = m/2, two pairs per three words: the radius word
+   a = 3(m/4) + i%2 gives u = (w_a + 1/2) 2^-32 and r = sqrt(-2 ln u); the 16-bit half h of word 3(m/4) + 2 (low half
+   for even i, high half for odd i) gives the angle t = 2 pi ((h + 1/2) 2^-16 - 1/2); normal m is r cos t for even m,
+   r sin t for odd m. */
+double oracle_philox_normal(uint32_t seed, int purpose, long long index, long long step, int m) {
+    int pair = m/2, group = m/4;
+    uint32_t a = philox_word(seed, purpose, index, step, 3*group + pair%2);
+    uint32_t angles = philox_word(seed, purpose, index, step, 3*group + 2);
+    uint32_t h = (pair%2) ? (angles >> 16) : (angles & 0xFFFFu);
+    double u = ((double) a + 0.5)*(1.0/4294967296.0);
+    double v = ((double) h + 0.5)*(1.0/65536.0);
+    double r = sqrt(-2.0*log(u));
+    double angle = 6.283185307179586476925287*(v - 0.5);
+    return (m%2 == 0 ? r*cos(angle) : r*sin(angle));
 }
 
 /* ------------------------------------------------------------------------------------------------ */

@@ -11,7 +11,7 @@
  *     turned into normals by the Box-Muller transform of ReferenceLBMKernels.cpp:1052-1064 and drawn in
  *     the reference's order (particles, then the nodes of the collision, then the boundary nodes), so
  *     that the oracle and the shimmed reference agree bit for bit also with noise;
- *   ORACLE_RANDOM_PHILOX: the counter-based Philox4x32-10 normals of the CUDA kernels (lbm_philox_*),
+ *   ORACLE_RANDOM_PHILOX: the counter-based Philox4x32-7 normals of the CUDA kernels (lbm_device.cuh),
  *     one counter per (purpose, node or particle, step), so that the oracle and the GPU agree to
  *     rounding also with noise.
  */
@@ -45,6 +45,7 @@ LbmStatus oracle_get_fluid_state(OracleKernel* kernel, double* state);
 LbmStatus oracle_set_fluid_state(OracleKernel* kernel, const double* state);
 
 /* Building blocks exposed for the tests. */
+void oracle_philox4x32(const uint32_t counter[4], const uint32_t key[2], int rounds, uint32_t out[4]);
 void oracle_philox4x32_10(const uint32_t counter[4], const uint32_t key[2], uint32_t out[4]);
 /* Normal number m (0-based) of a purpose/index/step, in double (the Philox scheme of the kernels). */
 double oracle_philox_normal(uint32_t seed, int purpose, long long index, long long step, int m);

@@ -56,7 +56,7 @@ COUPLING_CASES = ([(walls, drag, 'NearestNode') for walls in (False, True, 'face
                    for stencil in ('Trilinear', 'ThreePoint', 'Keys')])
 
 
-def coupling_case(walls, drag, stencil, kernel_factory=None, properties=None, temperature=0.0, seed=0):
+def coupling_case(walls, drag, stencil, kernel_factory=None, properties=None, temperature=0.0, seed=0, removal=0):
     """test_coupling_agrees_with_reference (TestLBMForce.py:573-635): 4 particles of mass 100 on an 8^3 lattice,
     friction 10/ps, a constant external field and a soft pair force, explicit or centred drag, every stencil,
     with the wall plane j = 0 or open faces along x."""
@@ -77,7 +77,7 @@ def coupling_case(walls, drag, stencil, kernel_factory=None, properties=None, te
     force.setFriction(10.0)
     force.setTemperature(temperature)
     force.setRandomNumberSeed(seed)
-    force.setFluidMomentumRemovalFrequency(0)
+    force.setFluidMomentumRemovalFrequency(removal)
     if walls == 'faces':
         force.setFaceBoundary(LBMForce.XMin, LBMForce.Velocity)
         force.setFaceBoundary(LBMForce.XMax, LBMForce.Density)
@@ -212,3 +212,49 @@ def channel_startup_profile(nz, tau, g, t, terms=4001):
     u -= (4*g*h*h/(nu*np.pi**3*n**3)*np.sin(n*np.pi*s/h)*np.exp(-nu*n*n*np.pi**2*t/(h*h))).sum(axis=0)
     u[0] = u[-1] = 0.0
     return u
+
+
+def step_with_repeated_evaluation(context):
+    """One integration step whose force evaluation is repeated before the step count advances, as the GPU platforms
+    of OpenMM do when they enlarge their neighbour list (ReferenceLBMKernels.cpp:341-365): returns the coupled forces of
+    both evaluations; the step integrates with the first."""
+    p, v, f = context._coupled_arrays(np.zeros_like(context.positions))
+    context.kernel.begin_step(context.step_count, p, v, f)
+    if v is not None:
+        context.velocities[context.coupled] = v
+    first = context._forces()
+    again = context._forces()
+    dt = context.integrator.step_size
+    context.velocities += dt*first/context.masses[:, None]
+    context.positions += dt*context.velocities
+    context.step_count += 1
+    return first, again
+
+
+def evaluation_sequence(context):
+    """The force evaluations of the kernel's evaluation rules (ReferenceLBMKernels.cpp:341-401), in order: before the
+    first step (no coupling force yet), between steps (the next step's forces, twice), a step with a repeated
+    evaluation (the same forces again), and between steps after more steps; then the state.  Returns a dict of
+    arrays."""
+    out = {'before_first_step': context.getForces()}
+    context.integrator.step(2)
+    out['between_steps'] = context.getForces()
+    out['between_steps_again'] = context.getForces()
+    out['step_first_evaluation'], out['step_repeated_evaluation'] = step_with_repeated_evaluation(context)
+    context.integrator.step(2)
+    out['between_steps_later'] = context.getForces()
+    context.integrator.step(1)
+    out['positions'] = context.positions.copy()
+    out['velocities'] = context.velocities.copy()
+    return out
+
+
+# The cases of the evaluation-sequence fixture: (walls, drag, stencil); momentum removal every 2 steps (none with open
+# faces, where it is not allowed), so that the next-step forces of odd and even step counts differ in the removal.
+EVALUATION_CASES = [(False, 'Explicit', 'NearestNode'), (True, 'Explicit', 'Keys'), (False, 'Centered', 'NearestNode'),
+                    (True, 'Centered', 'ThreePoint'), ('faces', 'Centered', 'Keys'), ('faces', 'Explicit', 'Trilinear')]
+
+
+def evaluation_case(walls, drag, stencil, kernel_factory=None, properties=None, temperature=0.0):
+    return coupling_case(walls, drag, stencil, kernel_factory, properties, temperature=temperature, seed=5,
+                         removal=0 if walls == 'faces' else 2)

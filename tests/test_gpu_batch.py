@@ -3,6 +3,7 @@ fluctuating fluids, tau 0.7, kT = 1e-4, distinct Philox seeds; Lennard-Jones bea
 mass 1; three-point stencil, explicit drag 0.8; lattice units dx = 1 nm, dt = 1 ps, rho0 = 1 Da/nm^3) on small lattices
 of uneven sizes:
 
+- pathwise against the CPU oracle (its Philox mode and its bead forces), FP64 and FP32;
 - pathwise: each replica of a batch follows a B200Kernel with the same lattice parameters and the bead dynamics of
   the benchmark (BeadDynamics), step for step, within 1e-9 relative in FP64 over 30 steps (the bead pair forces are
   summed in another order, and the chaotic bead dynamics amplify the last bits);
@@ -75,6 +76,52 @@ def run_separately(lattice, positions, steps):
     kernel.close()
     md.close()
     return out
+
+
+def run_oracle(lattice, positions, steps):
+    """One replica on the CPU oracle (Philox mode: the same random numbers as the device), its Lennard-Jones bead
+    forces from the oracle's bead forces, and the leapfrog of a VerletIntegrator with the lattice time step."""
+    from oracle import OracleKernel, md_forces
+    n = lattice.nx
+    count = len(positions)
+    masses = np.ones(count)
+    kernel = OracleKernel(lattice, masses, [])
+    pos = np.array(positions, dtype=np.float64)
+    vel = np.zeros_like(pos)
+    box = np.array([n, n, n], dtype=np.float64)
+    for s in range(steps):
+        kernel.begin_step(s, pos, vel, np.zeros_like(pos))
+        frc = md_forces(pos, box, np.zeros((0, 2), dtype=np.int32), 0.0, 1.0, 'lj', SIGMA, KT, CUTOFF)
+        kernel.execute(s, pos, vel, frc)
+        vel += frc/masses[:, None]
+        pos += vel
+    out = kernel.get_fluid_state(), pos, vel
+    kernel.close()
+    return out
+
+
+@pytest.mark.parametrize('precision,steps,tolerance', [('double', 30, 1e-9), ('single', 10, 1e-5)])
+def test_batch_follows_oracle(precision, steps, tolerance):
+    """Each replica of a batch of the batching configuration (fluctuating fluid, three-point stencil, explicit drag,
+    Lennard-Jones beads) follows the CPU oracle path by path: FP64 within 1e-9 over 30 steps (the bead pair forces
+    are summed in another order and the bead dynamics amplify the last bits), FP32 storage within 1e-5 over 10."""
+    sizes, beads = [12, 16, 10, 14], [20, 35, 8, 26]
+    lattices, positions = make_replicas(sizes, beads, seed=99)
+    batch = ReplicaBatch(lattices, beads, np.ones(sum(beads)), np.concatenate(positions), pair=('lj', SIGMA, KT, CUTOFF),
+                         precision=precision)
+    batch.step(steps)
+    pos, vel = batch.particles_state()
+    offsets = np.concatenate([[0], np.cumsum(beads)])
+    for r, n in enumerate(sizes):
+        state, ref_pos, ref_vel = run_oracle(lattices[r], positions[r], steps)
+        got = batch.fluid_state(r)
+        assert abs(got - state).max() <= tolerance*abs(state).max(), r
+        b = slice(offsets[r], offsets[r+1])
+        d = pos[b] - ref_pos
+        d -= n*np.round(d/n)
+        assert abs(d).max() <= tolerance*abs(ref_pos).max(), r
+        assert abs(vel[b] - ref_vel).max() <= tolerance*abs(ref_vel).max(), r
+    batch.close()
 
 
 def test_batch_follows_separate_kernels():

@@ -69,10 +69,16 @@ def vacf(record, lags):
 
 @pytest.mark.parametrize('precision', ['single', 'half'])
 def test_fluid_and_bead_temperatures(precision):
+    """400 snapshots 20 steps apart after 1000 steps, in 20 blocks.  The standard error comes from the spread of the
+    block means, so the bound is the two-sided 99.9 % quantile of Student's t with 19 degrees of freedom (3.88) times
+    that error, not a normal 3 sigma."""
+    from scipy.stats import t as student
+    blocks = 20
+    bound = student.ppf(0.9995, blocks - 1)
     context, force = free_beads(properties={'Precision': precision})
     context.integrator.step(1000)
     fluid, beads = [], []
-    for _ in range(200):
+    for _ in range(400):
         context.integrator.step(20)
         density, velocity = force.getFluidFields(context)
         u = velocity - (velocity*density[:, None]).sum(axis=0)/density.sum()
@@ -80,9 +86,9 @@ def test_fluid_and_bead_temperatures(precision):
         beads.append(MASS*(context.velocities**2).sum(axis=1).mean()/3)
     context.close()
     for name, samples in (('fluid', fluid), ('beads', beads)):
-        mean, err = block_mean(samples)
+        mean, err = block_mean(samples, blocks)
         print('%s temperature %.4f +- %.4f kT' % (name, mean/KT, err/KT))
-        assert abs(mean/KT - 1) <= max(3*err/KT, 0.02), name
+        assert abs(mean/KT - 1) <= max(bound*err/KT, 0.02), name
 
 
 def test_bead_velocity_autocorrelation_agrees_with_oracle():

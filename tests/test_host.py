@@ -100,3 +100,23 @@ def test_kernel_calls_fail_cleanly_without_a_device():
     with pytest.raises(lbm_b200.LbmError) as error:
         lbm_b200.B200Kernel(lattice_of(force, box=(2.0, 2.0, 2.0)), [], [])
     assert error.value.status == 5
+
+
+def test_coupled_lattice_above_2_31_nodes_is_rejected():
+    """The coupling keeps 32-bit signed node indices: lbm_create refuses a lattice of 2^31 nodes or more with coupled
+    particles (before it touches a device), while the same lattice without particles passes that check."""
+    import ctypes
+    from lbm_b200.abi import LBM_ERR_INVALID_ARGUMENT, LbmOptions, STORAGE, dptr
+    lib = load_library()
+    force = LBMForce()
+    force.setGridSize(8, 8, 8)
+    lattice = lattice_of(force)
+    lattice.nx, lattice.ny, lattice.nz = 1291, 1291, 1291          # 2.15e9 nodes
+    options = LbmOptions(STORAGE['half'], 0, None)
+    masses = np.ones(1)
+    handle = ctypes.c_void_p()
+    status = lib.lbm_create(ctypes.byref(lattice), ctypes.byref(options), 1, dptr(masses), 0, None,
+                            ctypes.byref(handle))
+    assert status == LBM_ERR_INVALID_ARGUMENT
+    assert '2^31 - 1 nodes' in lib.lbm_last_error().decode()
+    assert not handle.value

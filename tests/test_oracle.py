@@ -7,11 +7,13 @@ import os
 import numpy as np
 import pytest
 
-from cases import COUPLING_CASES, FLUID_WALLS, coupling_case, fluid_case
+from cases import (COUPLING_CASES, EVALUATION_CASES, FLUID_WALLS, coupling_case, evaluation_case, evaluation_sequence,
+                   fluid_case)
 import oracle
 from oracle import OracleKernel
 
 GOLDEN = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'reference_cases.npz'))
+SEQUENCES = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'evaluation_sequences.npz'))
 
 
 def sequential(lattice, masses, solid):
@@ -39,6 +41,19 @@ def test_oracle_coupling_matches_reference_golden(walls, drag, stencil):
         ref = GOLDEN[key + '_' + name]
         # TestLBMForce.py:633-635.
         assert abs(value - ref).max() <= 1e-10*max(1.0, abs(ref).max()), name
+
+
+@pytest.mark.parametrize('walls,drag,stencil', EVALUATION_CASES)
+def test_oracle_evaluation_rules_match_reference_golden(walls, drag, stencil):
+    """The evaluation rules (ReferenceLBMKernels.cpp:341-401): no coupling force before the first step, the next
+    step's forces between steps (with the momentum removal of that step), the same forces on a repeated evaluation,
+    and a run that queries between steps ends where the reference's does."""
+    context, force = evaluation_case(walls, drag, stencil, sequential)
+    got = evaluation_sequence(context)
+    for name, value in got.items():
+        ref = SEQUENCES['%s_%s_%s_%s' % (walls, drag, stencil, name)]
+        assert abs(value - ref).max() <= 1e-10*max(1.0, abs(ref).max()), name
+    assert (got['step_repeated_evaluation'] == got['step_first_evaluation']).all()
 
 
 @pytest.mark.skipif(not oracle.reference_available(), reason='the reference build (oracle/_ref) is absent')
