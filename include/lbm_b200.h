@@ -214,6 +214,41 @@ LbmStatus lbm_solver_iterations(LbmKernel* kernel, int* iterations);
    spread-and-gather one (platforms/reference/src/ReferenceLBMKernels.cpp:726-901). */
 LbmStatus lbm_solver_fallback_steps(LbmKernel* kernel, long long* steps);
 
+/*
+ * The particle buffers of an OpenMM CUDA-platform Context (OpenMM's CudaContext: getPosq(), getPosqCorrection(),
+ * getVelm(), getLongForceBuffer(), getAtomIndexArray()), on the handle's device, for an OpenMM platform kernel that
+ * drives this library without copying the particles through host memory.  They are what the reference's CUDA kernels
+ * read and write (platforms/common/src/kernels/lbmCoupling.cc:12-16, 47-54, 148-171, 2043-2053).  Atoms are in the
+ * platform's storage order, which OpenMM changes when it reorders them: atom_index[j] is the System index of the atom
+ * stored at slot j.
+ */
+enum { LBM_OPENMM_SINGLE = 0, LBM_OPENMM_MIXED = 1, LBM_OPENMM_DOUBLE = 2 };   /* the Context's "Precision" */
+typedef struct LbmOpenMMBuffers {
+    const void* posq;              /* float4 (single, mixed) or double4 (double): x, y, z (nm) and the charge */
+    const void* posq_correction;   /* mixed: float4 added to posq for the full position; NULL otherwise */
+    void* velm;                    /* float4 (single) or double4 (mixed, double): v (nm/ps) and 1/mass */
+    long long* force;              /* fixed-point forces in units of 2^-32 kJ/mol/nm, [k*padded_num_atoms + j] */
+    const int* atom_index;         /* [num_atoms] */
+    int num_atoms, padded_num_atoms;
+    int precision;                 /* LBM_OPENMM_* */
+} LbmOpenMMBuffers;
+
+/* The coupled particles as System indices, in coupling order (LBMLatticeParameters::particles, LBMKernels.h:61), and
+   the number of atoms of the System; once, before the first lbm_begin_step_openmm / lbm_execute_openmm.  No
+   counterpart call in the reference, whose CUDA kernel builds the same index (couplingIndex, lbmCoupling.cc:12-16). */
+LbmStatus lbm_set_coupled_atoms(LbmKernel* kernel, int num_atoms, int num_coupled, const int* particles);
+
+/* CalcLBMForceKernel::beginStep (LBMKernels.h:119) on the buffers of an OpenMM Context: the reflection at the walls
+   reverses the velocities of the coupled atoms in velm (reflectParticles, lbmCoupling.cc:148-171). */
+LbmStatus lbm_begin_step_openmm(LbmKernel* kernel, long long step_count, const LbmOpenMMBuffers* buffers);
+
+/* CalcLBMForceKernel::execute (LBMKernels.h:128) on the buffers of an OpenMM Context: the coupling forces are added
+   to the fixed-point force buffer as (long long) (F 2^32) (applyCouplingForces, lbmCoupling.cc:2043-2053).  With the
+   centred drag the other forces of the coupled atoms are read from that buffer first (times 2^-32), so the call must
+   come after every other force of the step, as the reference's post-computation (CommonLBMKernels.cpp:115-126). */
+LbmStatus lbm_execute_openmm(LbmKernel* kernel, long long step_count, const LbmOpenMMBuffers* buffers,
+                             int include_forces, int include_energy, double* energy);
+
 /* Limits of the centred stencil drag's conjugate gradients, for tests of their failure paths: at most max_iterations
    iterations (then LBM_ERR_CG_NOT_CONVERGED, as ReferenceLBMKernels.cpp:864-866 after 1000), and barrier_polls polls
    of a block waiting at a grid barrier of the cooperative solve (then LBM_ERR_DEVICE_TIMEOUT).  A failed solve leaves

@@ -31,6 +31,16 @@ class LbmError(RuntimeError):
         self.status = status
 
 
+class LbmOpenMMBuffers(ctypes.Structure):
+    """The particle buffers of an OpenMM CUDA-platform Context (device pointers)."""
+    _fields_ = [('posq', ctypes.c_void_p), ('posq_correction', ctypes.c_void_p), ('velm', ctypes.c_void_p),
+                ('force', ctypes.c_void_p), ('atom_index', ctypes.c_void_p), ('num_atoms', ctypes.c_int),
+                ('padded_num_atoms', ctypes.c_int), ('precision', ctypes.c_int)]
+
+
+OPENMM_PRECISION = {'single': 0, 'mixed': 1, 'double': 2}
+
+
 class LbmLatticeParameters(ctypes.Structure):
     _fields_ = [('nx', ctypes.c_int), ('ny', ctypes.c_int), ('nz', ctypes.c_int),
                 ('dx', ctypes.c_double), ('dt', ctypes.c_double), ('density', ctypes.c_double),
@@ -103,6 +113,10 @@ SIGNATURES = {
     'lbm_dense_kernel_time': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong), _D]),
     'lbm_kernel_launches': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     'lbm_solver_iterations': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
+    'lbm_set_coupled_atoms': (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    'lbm_begin_step_openmm': (ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(LbmOpenMMBuffers)]),
+    'lbm_execute_openmm': (ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(LbmOpenMMBuffers), ctypes.c_int,
+                                          ctypes.c_int, _D]),
     'lbm_set_solver_limits': (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_longlong]),
     'lbm_solver_fallback_steps': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     'lbm_steady_residual': (ctypes.c_int, [_P, ctypes.c_int, _D]),

@@ -218,6 +218,27 @@ LbmStatus lbm_solver_iterations(LbmKernel* kernel, int* iterations) {
     return LBM_OK;
 }
 
+LbmStatus lbm_set_coupled_atoms(LbmKernel* kernel, int num_atoms, int num_coupled, const int* particles) {
+    CHECK_HANDLE(kernel);
+    return guard([&] { kernel->impl->setCoupledAtoms(num_atoms, num_coupled, particles); });
+}
+
+LbmStatus lbm_begin_step_openmm(LbmKernel* kernel, long long step_count, const LbmOpenMMBuffers* buffers) {
+    CHECK_HANDLE(kernel);
+    return guard([&] { kernel->impl->beginStepOpenMM(step_count, buffers); });
+}
+
+LbmStatus lbm_execute_openmm(LbmKernel* kernel, long long step_count, const LbmOpenMMBuffers* buffers,
+                             int include_forces, int include_energy, double* energy) {
+    CHECK_HANDLE(kernel);
+    (void) include_energy;
+    return guard([&] {
+        double e = kernel->impl->executeOpenMM(step_count, buffers, include_forces != 0);
+        if (energy)
+            *energy = e;
+    });
+}
+
 LbmStatus lbm_set_solver_limits(LbmKernel* kernel, int max_iterations, long long barrier_polls) {
     CHECK_HANDLE(kernel);
     return guard([&] { kernel->impl->setSolverLimits(max_iterations, barrier_polls); });

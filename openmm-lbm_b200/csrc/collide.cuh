@@ -215,8 +215,8 @@ __device__ __forceinline__ void collideNode(const T* __restrict__ A, T* __restri
     if (FLUCT) {
         R rn[15];
         philoxNormals<R, 15>(k.seed, PurposeFluid, node, step, rn);
-        R ghost = sqrt(k.mu*rho);
-        modeAmplitudes<R>(rn, sqrt(k.mu*rho*k.stressFactor), ghost, a);
+        R ghost = noiseSqrt(k.mu*rho);
+        modeAmplitudes<R>(rn, noiseSqrt(k.mu*rho*k.stressFactor), ghost, a);
         qxx += a[0]; qyy += a[1]; qzz += a[2];
         qxy += a[3]; qxz += a[4]; qyz += a[5];
     }

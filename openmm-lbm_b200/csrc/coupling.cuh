@@ -38,6 +38,8 @@ public:
     // Conjugate-gradient iterations of the last centred stencil solve.
     int lastIterations = 0;
     long long spreadSteps = 0;   // steps whose centred drag ran the spread-and-gather solve
+    // The coupling forces of the last evaluation (kJ/mol/nm, 3 doubles per particle in coupling order, device memory).
+    const double* couplingForces() const { return forceOutDev; }
     // Lower limits make the failure paths reachable in tests; 0 restores a default.
     void setSolverLimits(int maxIterations, long long barrierPolls);
 private:

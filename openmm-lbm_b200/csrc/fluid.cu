@@ -377,8 +377,8 @@ __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& 
         float rnA[15], rnB[15];
         philoxNormals<float, 15>(v.seed, PurposeFluid, node, step, rnA);
         philoxNormals<float, 15>(v.seed, PurposeFluid, node + 1, step, rnB);
-        const float stressA = sqrtf(c.mu*rho.v.x*c.stressFactor), stressB = sqrtf(c.mu*rho.v.y*c.stressFactor);
-        const float ghostA = sqrtf(c.mu*rho.v.x), ghostB = sqrtf(c.mu*rho.v.y);
+        const float stressA = approxSqrt(c.mu*rho.v.x*c.stressFactor), stressB = approxSqrt(c.mu*rho.v.y*c.stressFactor);
+        const float ghostA = approxSqrt(c.mu*rho.v.x), ghostB = approxSqrt(c.mu*rho.v.y);
 #pragma unroll
         for (int k = 4; k < 19; k++) {
             const float norm = (float) invSqrtModeNorm(k);

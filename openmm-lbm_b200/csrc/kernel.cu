@@ -1,6 +1,7 @@
 // Host object of the B200 LBM force kernel (see kernel.cuh).
 #include "kernel.cuh"
 #include "coupling.cuh"
+#include "openmm_buffers.cuh"
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -79,6 +80,8 @@ B200Kernel::B200Kernel(const LbmLatticeParameters& l, const LbmOptions& options,
 }
 
 B200Kernel::~B200Kernel() {
+    cudaFree(couplingIndexDev);
+    cudaFree(stageDev);
     coupling.reset();
     fluid.reset();
     if (ownStream && stream != nullptr)
@@ -104,6 +107,12 @@ double B200Kernel::execute(long long stepCount, const LbmParticleArrays* particl
     CUDA_CHECK(cudaSetDevice(device));
     if (numParticles > 0 && particles == nullptr)
         throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_execute: the particle arrays are missing");
+    if (evaluate(stepCount, particles, includeForces))
+        coupling->addForces(particles);
+    return 0.0;
+}
+
+bool B200Kernel::evaluate(long long stepCount, const LbmParticleArrays* particles, bool includeForces) {
     bool repeatedStep = (stepForcesCurrent && stepCount == stepIndex-1);
     if (stepPending) {
         stepPending = false;
@@ -111,8 +120,73 @@ double B200Kernel::execute(long long stepCount, const LbmParticleArrays* particl
     }
     else if (includeForces && numParticles > 0 && stepCount > 0 && !repeatedStep)
         computeNextStepForces(stepCount, particles);
-    if (includeForces && numParticles > 0)
-        coupling->addForces(particles);
+    return includeForces && numParticles > 0;
+}
+
+// The OpenMM Context interface.  couplingIndex[atom] is built once from the coupled particles' System indices; every
+// call gathers the coupled atoms from the Context's buffers (the storage order changes when OpenMM reorders the atoms)
+// into device arrays in coupling order, and writes back what the reference's CUDA kernels write: the reflected
+// velocities, and the coupling forces in fixed point.
+void B200Kernel::setCoupledAtoms(int numAtoms, int numCoupled, const int* particles) {
+    CUDA_CHECK(cudaSetDevice(device));
+    if (numAtoms < 0 || numCoupled != numParticles || (numCoupled > 0 && particles == nullptr))
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_set_coupled_atoms: the coupled particles differ from lbm_create()");
+    std::vector<int> index(std::max(1, numAtoms), -1);
+    for (int i = 0; i < numCoupled; i++) {
+        if (particles[i] < 0 || particles[i] >= numAtoms || index[particles[i]] >= 0)
+            throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_set_coupled_atoms: a particle index is out of range or repeated");
+        index[particles[i]] = i;
+    }
+    cudaFree(couplingIndexDev);
+    couplingIndexDev = nullptr;
+    CUDA_CHECK(cudaMalloc(&couplingIndexDev, sizeof(int)*index.size()));
+    CUDA_CHECK(cudaMemcpy(couplingIndexDev, index.data(), sizeof(int)*index.size(), cudaMemcpyHostToDevice));
+    if (stageDev == nullptr)
+        CUDA_CHECK(cudaMalloc(&stageDev, sizeof(double)*9*(size_t) std::max(1, numParticles)));
+    openmmAtoms = numAtoms;
+}
+
+LbmParticleArrays B200Kernel::stagingArrays() {
+    LbmParticleArrays a;
+    a.positions = stageDev;
+    a.velocities = stageDev + 3*(size_t) numParticles;
+    a.forces = stageDev + 6*(size_t) numParticles;
+    a.memory = LBM_MEMORY_DEVICE;
+    return a;
+}
+
+void B200Kernel::beginStepOpenMM(long long stepCount, const LbmOpenMMBuffers* buffers) {
+    CUDA_CHECK(cudaSetDevice(device));
+    if (numParticles == 0) {
+        beginStep(stepCount, nullptr);
+        return;
+    }
+    if (couplingIndexDev == nullptr)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_begin_step_openmm: call lbm_set_coupled_atoms() first");
+    validateOpenMMBuffers(buffers, openmmAtoms);
+    LbmParticleArrays a = stagingArrays();
+    bool reflects = !geometry.solidNodes.empty();
+    if (reflects)
+        gatherOpenMM(*buffers, couplingIndexDev, a.positions, a.velocities, nullptr, false, stream);
+    beginStep(stepCount, &a);
+    if (reflects)
+        scatterVelocitiesOpenMM(*buffers, couplingIndexDev, a.velocities, stream);
+}
+
+double B200Kernel::executeOpenMM(long long stepCount, const LbmOpenMMBuffers* buffers, bool includeForces) {
+    CUDA_CHECK(cudaSetDevice(device));
+    if (numParticles == 0) {
+        evaluate(stepCount, nullptr, includeForces);
+        return 0.0;
+    }
+    if (couplingIndexDev == nullptr)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_execute_openmm: call lbm_set_coupled_atoms() first");
+    validateOpenMMBuffers(buffers, openmmAtoms);
+    LbmParticleArrays a = stagingArrays();
+    gatherOpenMM(*buffers, couplingIndexDev, a.positions, a.velocities, a.forces,
+                 lattice.drag_scheme == LBM_DRAG_CENTERED, stream);
+    if (evaluate(stepCount, &a, includeForces))
+        addForcesFixedPoint(*buffers, couplingIndexDev, coupling->couplingForces(), stream);
     return 0.0;
 }
 

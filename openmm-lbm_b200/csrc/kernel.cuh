@@ -36,9 +36,16 @@ public:
     int solverIterations() const;
     long long solverFallbackSteps() const;
     void setSolverLimits(int maxIterations, long long barrierPolls);
+    // The OpenMM Context interface: coupled atoms as System indices, then beginStep/execute on its buffers.
+    void setCoupledAtoms(int numAtoms, int numCoupled, const int* particles);
+    void beginStepOpenMM(long long stepCount, const LbmOpenMMBuffers* buffers);
+    double executeOpenMM(long long stepCount, const LbmOpenMMBuffers* buffers, bool includeForces);
     void setFluidEquilibrium(const double* density, const double* velocity, bool onDevice, bool strain);
     long long steadySolve(long long firstStep, int interval, double tolerance, long long maxSteps, double* residual);
 private:
+    // The evaluation rules of execute(); returns whether the coupling forces are to be added to the caller's forces.
+    bool evaluate(long long stepCount, const LbmParticleArrays* particles, bool includeForces);
+    LbmParticleArrays stagingArrays();
     void advanceFluid(const LbmParticleArrays* particles);
     void computeNextStepForces(long long stepCount, const LbmParticleArrays* particles);
     void checkMachNumber();
@@ -53,6 +60,11 @@ private:
     bool stepPending, stepForcesCurrent, stepWallValid;
     long long stepIndex;
     double hostWallMomentum[3];     // reflection at the walls and reactions on solid nodes, Da nm/ps
+    // The OpenMM Context interface: couplingIndex[atom] (-1 for an atom that is not coupled) and the coupled atoms'
+    // positions, velocities and other forces gathered into coupling order (device memory).
+    int openmmAtoms = 0;
+    int* couplingIndexDev = nullptr;
+    double* stageDev = nullptr;
 };
 
 } // namespace lbm

@@ -204,6 +204,19 @@ __device__ __forceinline__ uint4 philoxBlock(uint32_t seed, int purpose, long lo
     return philox4x32<kPhiloxRounds>(c, seed, 0x4C424D32u);
 }
 
+// Square root by the hardware approximation (sqrt.approx.f32: one special-function instruction, relative error of
+// order 2^-23) for the amplitudes of the thermal noise, where the IEEE-rounded sqrtf would take a multi-instruction
+// sequence; x >= 0.
+__device__ __forceinline__ float approxSqrt(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// The square root of a noise amplitude in the compute precision: the approximation in float, IEEE in double.
+__device__ __forceinline__ float noiseSqrt(float x) { return approxSqrt(x); }
+__device__ __forceinline__ double noiseSqrt(double x) { return sqrt(x); }
+
 // One Box-Muller pair from a 32-bit radius word and a 16-bit angle half-word, in the compute precision.
 __device__ __forceinline__ void boxMullerPair(uint32_t a, uint32_t h, float& n0, float& n1) {
     const float below1 = 0.99999994f;                   // 1 - 2^-24: keeps log(u) < 0 after rounding to float
@@ -216,7 +229,7 @@ __device__ __forceinline__ void boxMullerPair(uint32_t a, uint32_t h, float& n0,
 #else
     // Hardware approximations (MUFU): -2 ln u = -2 ln2 log2(u), and sin/cos of an angle in (-pi, pi), where their
     // absolute error is about 2^-21.
-    const float r = sqrtf(fmaxf(-1.3862943611198906f*__log2f(u), 0.0f));
+    const float r = approxSqrt(fmaxf(-1.3862943611198906f*__log2f(u), 0.0f));
     float s, c;
     __sincosf(t, &s, &c);
 #endif

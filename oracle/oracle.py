@@ -17,6 +17,7 @@ from lbm_b200.abi import LbmLatticeParameters, LbmParticleArrays, MEMORY_HOST, c
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_PATH = os.path.join(HERE, '_ref', 'libref_lbm.so')
+ADAPTER_PATH = os.path.join(HERE, '_ref', 'libadapter_lbm.so')
 ORACLE_PATH = os.path.join(HERE, 'liblbm_oracle.so')
 
 RANDOM_SEQUENTIAL, RANDOM_PHILOX = 0, 1
@@ -42,8 +43,11 @@ class _Lib:
             'get_fluid_state': (ctypes.c_int, [P, D]),
             'set_fluid_state': (ctypes.c_int, [P, D]),
         }
-        if prefix == 'refdrv_':
+        if prefix in ('refdrv_', 'adapterdrv_'):
             sig['create'] = (ctypes.c_int, [LP, ctypes.c_int, D, ctypes.c_int, I, ctypes.POINTER(P)])
+            sig['create_with_storage'] = (ctypes.c_int, [LP, ctypes.c_int, D, ctypes.c_int, I, ctypes.c_int,
+                                                         ctypes.POINTER(P)])
+            sig['get_fluid_fields_halo'] = (ctypes.c_int, [P, D, D])
             sig['copy_parameters'] = (ctypes.c_int, [P, LP, ctypes.c_int, I])
             sig['create_checkpoint'] = (ctypes.c_int, [P, P, ctypes.POINTER(ctypes.c_size_t)])
             sig['load_checkpoint'] = (ctypes.c_int, [P, P, ctypes.c_size_t])
@@ -71,9 +75,11 @@ class _Lib:
 
 
 def library(kind):
-    """'reference' (oracle/_ref) or 'oracle' (the C restatement)."""
+    """'reference' (oracle/_ref), 'adapter' (the B200 platform kernel through the same driver) or 'oracle' (the C
+    restatement)."""
     if kind not in _libs:
-        path, prefix = (REF_PATH, 'refdrv_') if kind == 'reference' else (ORACLE_PATH, 'oracle_')
+        path, prefix = {'reference': (REF_PATH, 'refdrv_'), 'adapter': (ADAPTER_PATH, 'adapterdrv_'),
+                        'oracle': (ORACLE_PATH, 'oracle_')}[kind]
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         _libs[kind] = _Lib(path, prefix)
@@ -82,6 +88,10 @@ def library(kind):
 
 def reference_available():
     return os.path.exists(REF_PATH)
+
+
+def adapter_available():
+    return os.path.exists(ADAPTER_PATH)
 
 
 class _CpuKernel:
@@ -180,6 +190,38 @@ class ReferenceKernel(_CpuKernel):
     def load_checkpoint(self, data):
         buf = ctypes.create_string_buffer(data, len(data))
         self.lib.check(self.lib.load_checkpoint(self.handle, buf, len(data)))
+
+
+class AdapterKernel(ReferenceKernel):
+    """The project's B200 platform kernel (openmm-lbm_b200/openmm/B200LBMKernels.cpp, CalcLBMForceKernel over
+    liblbm_b200.so), created by its kernel factory and driven through OpenMM's kernel interface by the same driver as
+    the reference's kernel (oracle/_ref/libadapter_lbm.so; a GPU is needed).  storage: 'double', 'single', 'half' or
+    'bfloat16'."""
+
+    name = 'B200 adapter'
+
+    def __init__(self, lattice, masses, solid_nodes, storage='double'):
+        from lbm_b200.abi import STORAGE
+        lib = library('adapter')
+        masses = np.ascontiguousarray(masses, dtype=np.float64)
+        self.solid = np.ascontiguousarray(solid_nodes, dtype=np.int32)
+        h = ctypes.c_void_p()
+        lat = lattice.copy()
+        lib.check(lib.create_with_storage(ctypes.byref(lat), len(masses), dptr(masses), len(self.solid),
+                                          self.solid.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), STORAGE[storage],
+                                          ctypes.byref(h)))
+        _CpuKernel.__init__(self, lib, h, lattice, len(masses))
+
+
+def fields_with_halo(kernel):
+    """getFluidFields() with the halo of a ReferenceKernel or AdapterKernel: density and velocity on the lattice
+    extended by one node on every side, (nz + 2, ny + 2, nx + 2) and (nz + 2, ny + 2, nx + 2, 3)."""
+    l = kernel.lattice
+    shape = (l.nz + 2, l.ny + 2, l.nx + 2)
+    d = np.zeros(shape)
+    v = np.zeros(shape + (3,))
+    kernel.lib.check(kernel.lib.get_fluid_fields_halo(kernel.handle, dptr(d), dptr(v)))
+    return d, v
 
 
 class OracleKernel(_CpuKernel):

@@ -3,6 +3,11 @@
  * kernel, ReferenceCalcLBMForceKernel (platforms/reference/src/ReferenceLBMKernels.cpp), compiled
  * unmodified from the reference sources against the minimal OpenMM shim in oracle/shim/.
  *
+ * Compiled with LBM_DRIVER_ADAPTER it drives instead the B200 platform kernel of this project
+ * (openmm-lbm_b200/openmm/, CalcLBMForceKernel over liblbm_b200.so), created by its kernel factory,
+ * with the entry points prefixed adapterdrv_: the same harness then runs the reference's kernel and
+ * the drop-in through the same OpenMM interface.
+ *
  * Only the tests, the smoke check and the CPU-baseline leg of the benchmark use this file; it is the
  * checker, never the product.  It exposes the entry points of include/lbm_b200.h with the prefix
  * refdrv_ and host particle arrays only, so that the same Python harness can drive the reference,
@@ -15,7 +20,14 @@
  */
 #include "LBMForce.h"
 #include "LBMKernels.h"
+#ifdef LBM_DRIVER_ADAPTER
+#include "B200LBMKernelFactory.h"
+#include "B200LBMKernels.h"
+#define DRV(name) adapterdrv_##name
+#else
 #include "ReferenceLBMKernels.h"
+#define DRV(name) refdrv_##name
+#endif
 #include "openmm/internal/ContextImpl.h"
 #include "openmm/reference/ReferencePlatform.h"
 #include "lbm_b200.h"
@@ -40,7 +52,7 @@ struct RefKernel {
     ContextImpl context;
     ReferencePlatform::PlatformData data;
     std::vector<Vec3> positions, velocities, forces;
-    ReferenceCalcLBMForceKernel* kernel;
+    CalcLBMForceKernel* kernel;
     int numParticles;
     long long numNodes;
     RefKernel() : kernel(NULL), numParticles(0), numNodes(0) {
@@ -71,7 +83,10 @@ LBMLatticeParameters toLattice(const LbmLatticeParameters* in, int numParticles,
     l.nx = in->nx; l.ny = in->ny; l.nz = in->nz;
     l.procs[0] = l.procs[1] = l.procs[2] = 1;
     l.particleCopiesCheck = false;
-    l.densityHaloExchange = l.velocityHaloExchange = false;
+    // The density halo is exchanged and the velocity halo is not, so that getFluidFields() with the halo shows both
+    // kinds of halo node (one domain: no exchange takes place).
+    l.densityHaloExchange = true;
+    l.velocityHaloExchange = false;
     l.dx = in->dx; l.dt = in->dt; l.density = in->density;
     l.tau = in->tau; l.omega = in->omega;
     l.initialVelocity = Vec3(in->initial_velocity[0], in->initial_velocity[1], in->initial_velocity[2]);
@@ -117,12 +132,22 @@ LbmStatus fail(const std::exception& e) {
 
 extern "C" {
 
-const char* refdrv_last_error(void) {
+LbmStatus DRV(create_with_storage)(const LbmLatticeParameters* lattice, int num_particles, const double* masses,
+                                   int num_solid, const int* solid, int storage, RefKernel** out);
+
+const char* DRV(last_error)(void) {
     return lastError.c_str();
 }
 
-LbmStatus refdrv_create(const LbmLatticeParameters* lattice, int num_particles, const double* masses,
-                        int num_solid, const int* solid, RefKernel** out) {
+LbmStatus DRV(create)(const LbmLatticeParameters* lattice, int num_particles, const double* masses,
+                      int num_solid, const int* solid, RefKernel** out) {
+    return DRV(create_with_storage)(lattice, num_particles, masses, num_solid, solid, LBM_STORAGE_F64, out);
+}
+
+/* The storage type matters only for the B200 platform kernel (the reference's Reference kernel stores doubles). */
+LbmStatus DRV(create_with_storage)(const LbmLatticeParameters* lattice, int num_particles, const double* masses,
+                                   int num_solid, const int* solid, int storage, RefKernel** out) {
+    (void) storage;
     GUARD_BEGIN
     RefKernel* k = new RefKernel();
     k->numParticles = num_particles;
@@ -132,7 +157,14 @@ LbmStatus refdrv_create(const LbmLatticeParameters* lattice, int num_particles, 
     k->positions.resize(num_particles);
     k->velocities.resize(num_particles);
     k->forces.resize(num_particles);
+#ifdef LBM_DRIVER_ADAPTER
+    // The B200 platform kernel, created by its factory for a platform that keeps the particles in host vectors.
+    LBMPlugin::B200LBMKernelFactory factory(storage);
+    k->kernel = dynamic_cast<CalcLBMForceKernel*>(factory.createKernelImpl(CalcLBMForceKernel::Name(), k->platform,
+                                                                           k->context));
+#else
     k->kernel = new ReferenceCalcLBMForceKernel("CalcLBMForce", k->platform);
+#endif
     LBMLatticeParameters l = toLattice(lattice, num_particles, num_solid, solid);
     // The Reference kernel never reads the LBMForce object it is given (its parameters come in l).
     alignas(LBMForce) static char forceStorage[sizeof(LBMForce)];
@@ -148,11 +180,11 @@ LbmStatus refdrv_create(const LbmLatticeParameters* lattice, int num_particles, 
     GUARD_END
 }
 
-void refdrv_destroy(RefKernel* k) {
+void DRV(destroy)(RefKernel* k) {
     delete k;
 }
 
-LbmStatus refdrv_begin_step(RefKernel* k, long long step, const LbmParticleArrays* p) {
+LbmStatus DRV(begin_step)(RefKernel* k, long long step, const LbmParticleArrays* p) {
     GUARD_BEGIN
     k->context.setStepCount(step);
     if (k->numParticles > 0)
@@ -163,7 +195,7 @@ LbmStatus refdrv_begin_step(RefKernel* k, long long step, const LbmParticleArray
     GUARD_END
 }
 
-LbmStatus refdrv_execute(RefKernel* k, long long step, const LbmParticleArrays* p, int include_forces,
+LbmStatus DRV(execute)(RefKernel* k, long long step, const LbmParticleArrays* p, int include_forces,
                          int include_energy, double* energy) {
     GUARD_BEGIN
     k->context.setStepCount(step);
@@ -177,13 +209,13 @@ LbmStatus refdrv_execute(RefKernel* k, long long step, const LbmParticleArrays* 
     GUARD_END
 }
 
-LbmStatus refdrv_copy_parameters(RefKernel* k, const LbmLatticeParameters* lattice, int num_solid, const int* solid) {
+LbmStatus DRV(copy_parameters)(RefKernel* k, const LbmLatticeParameters* lattice, int num_solid, const int* solid) {
     GUARD_BEGIN
     k->kernel->copyParametersToContext(k->context, toLattice(lattice, k->numParticles, num_solid, solid));
     GUARD_END
 }
 
-LbmStatus refdrv_get_fluid_fields(RefKernel* k, double* density, double* velocity) {
+LbmStatus DRV(get_fluid_fields)(RefKernel* k, double* density, double* velocity) {
     GUARD_BEGIN
     std::vector<double> d;
     std::vector<Vec3> v;
@@ -196,13 +228,27 @@ LbmStatus refdrv_get_fluid_fields(RefKernel* k, double* density, double* velocit
     GUARD_END
 }
 
-LbmStatus refdrv_get_fluid_mach_number(RefKernel* k, double* mach) {
+/* getFluidFields() with the halo: (nx + 2)(ny + 2)(nz + 2) values, i fastest, NaN where the kernel gives none. */
+LbmStatus DRV(get_fluid_fields_halo)(RefKernel* k, double* density, double* velocity) {
+    GUARD_BEGIN
+    std::vector<double> d;
+    std::vector<Vec3> v;
+    k->kernel->getFluidFields(k->context, d, v, true);
+    for (size_t i = 0; i < d.size(); i++) {
+        density[i] = d[i];
+        for (int a = 0; a < 3; a++)
+            velocity[3*i+a] = v[i][a];
+    }
+    GUARD_END
+}
+
+LbmStatus DRV(get_fluid_mach_number)(RefKernel* k, double* mach) {
     GUARD_BEGIN
     *mach = k->kernel->getFluidMachNumber(k->context);
     GUARD_END
 }
 
-LbmStatus refdrv_get_wall_force(RefKernel* k, double* force) {
+LbmStatus DRV(get_wall_force)(RefKernel* k, double* force) {
     GUARD_BEGIN
     Vec3 f = k->kernel->getWallForce(k->context);
     for (int a = 0; a < 3; a++)
@@ -210,7 +256,7 @@ LbmStatus refdrv_get_wall_force(RefKernel* k, double* force) {
     GUARD_END
 }
 
-LbmStatus refdrv_get_fluid_state(RefKernel* k, double* state) {
+LbmStatus DRV(get_fluid_state)(RefKernel* k, double* state) {
     GUARD_BEGIN
     std::vector<double> s;
     k->kernel->getFluidState(k->context, s);
@@ -218,7 +264,7 @@ LbmStatus refdrv_get_fluid_state(RefKernel* k, double* state) {
     GUARD_END
 }
 
-LbmStatus refdrv_set_fluid_state(RefKernel* k, const double* state) {
+LbmStatus DRV(set_fluid_state)(RefKernel* k, const double* state) {
     GUARD_BEGIN
     std::vector<double> s(state, state + LBM_NUM_VELOCITIES*k->numNodes);
     k->kernel->setFluidState(k->context, s);
@@ -226,7 +272,7 @@ LbmStatus refdrv_set_fluid_state(RefKernel* k, const double* state) {
 }
 
 /* The checkpoint of the reference kernel, as bytes: the first call with buffer == NULL gives the size. */
-LbmStatus refdrv_create_checkpoint(RefKernel* k, void* buffer, size_t* bytes) {
+LbmStatus DRV(create_checkpoint)(RefKernel* k, void* buffer, size_t* bytes) {
     GUARD_BEGIN
     std::stringstream stream;
     k->kernel->createCheckpoint(k->context, stream);
@@ -240,7 +286,7 @@ LbmStatus refdrv_create_checkpoint(RefKernel* k, void* buffer, size_t* bytes) {
     GUARD_END
 }
 
-LbmStatus refdrv_load_checkpoint(RefKernel* k, const void* buffer, size_t bytes) {
+LbmStatus DRV(load_checkpoint)(RefKernel* k, const void* buffer, size_t bytes) {
     GUARD_BEGIN
     std::stringstream stream(std::string((const char*) buffer, bytes));
     k->kernel->loadCheckpoint(k->context, stream);
