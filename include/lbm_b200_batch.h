@@ -2,9 +2,9 @@
  * coupled particles, advanced together on one device.
  *
  * No counterpart in the reference: its examples run seed ensembles as one OpenMM Context per replica, looping in
- * Python (examples/cocomo).  Here every phase of a lattice step (bead pair forces, stencil and explicit drag, the
- * dense stream-collide kernel, the per-replica sums, the reaction clear and the leapfrog of the beads) is one
- * persistent launch over all replicas, and a run of steps is captured once in a CUDA graph and replayed.  Each
+ * Python (examples/cocomo).  Here a run of steps of all replicas (bead pair forces, stencil and explicit drag, the
+ * dense stream-collide step, the per-replica sums, the reaction clear and the leapfrog of the beads) is one
+ * persistent cooperative launch, captured once in a CUDA graph and replayed (lbm_batch_set_persistent).  Each
  * replica follows the step of a kernel created by lbm_create with the same lattice parameters, driven as an OpenMM
  * VerletIntegrator step would drive it: beginStep, the bead forces, execute (explicit drag and the fluid step), and
  * the leapfrog v += dt F/m, x += dt v with the lattice time step.
@@ -61,8 +61,20 @@ LbmStatus lbm_batch_get_fluid_state(LbmBatch* batch, int replica, double* state)
  * u = j/rho + g/2 and <u> the mass-weighted mean, and the bead temperature sum m v^2/(3 n) of the current velocities. */
 LbmStatus lbm_batch_temperatures(LbmBatch* batch, double* fluid_kT, double* bead_kT);
 
+/* The form of a step: enable != 0 (the default) runs graph_steps steps in one persistent cooperative launch, captured
+ * once in a CUDA graph and replayed -- the phases of a step (bead pair forces, stencil slots and the clear of the
+ * previous reactions; explicit drag, reaction and leapfrog; the dense step with the per-replica sums) separated by
+ * bounded grid barriers; enable = 0 launches the seven phase kernels of a step one after another (each replica then
+ * computes the same step; the form exists for comparisons).  A grid barrier that waits more than the poll limit
+ * gives up: that launch stops incomplete and the next call that synchronizes (lbm_batch_get_particles,
+ * lbm_batch_get_fluid_state, lbm_batch_temperatures) returns LBM_ERR_DEVICE_TIMEOUT.
+ * lbm_batch_set_barrier_polls sets that limit (0: the default 2^26 polls; a low value makes the timeout reachable in
+ * tests). */
+LbmStatus lbm_batch_set_persistent(LbmBatch* batch, int enable);
+LbmStatus lbm_batch_set_barrier_polls(LbmBatch* batch, long long polls);
+
 /* Total nodes of all replicas, lattice steps taken, kernels launched so far, the block size of the dense kernel and
- * the steps per CUDA graph. */
+ * the steps per CUDA graph (one launch per graph_steps steps in the persistent form). */
 LbmStatus lbm_batch_info(LbmBatch* batch, long long* total_nodes, long long* steps, long long* launches,
                          int* threads_per_block, int* graph_steps);
 

@@ -6,6 +6,8 @@
     harness  System / Context / VerletIntegrator: the OpenMM call order that drives the kernel
     md       BeadDynamics: bead forces and the leapfrog on the device (the benchmark's stand-in for OpenMM)
     batch    ReplicaBatch: many independent periodic replicas with their beads, advanced together
+    reporters  saveCheckpoint / loadCheckpoint and the reference's reporters (checkpoints, temperature, VTK files),
+             with a Simulation driver that calls them as OpenMM's does
 """
 from .batch import ReplicaBatch  # noqa: F401
 from .abi import LbmError, LbmLatticeParameters, load_library  # noqa: F401
@@ -13,3 +15,5 @@ from .force import LBMForce  # noqa: F401
 from .harness import Context, ExternalForce, PairForce, System, VerletIntegrator  # noqa: F401
 from .kernel import B200Kernel  # noqa: F401
 from .md import BeadDynamics, random_walk_chains  # noqa: F401
+from .reporters import (LBMCheckpointReporter, LBMTemperatureReporter, LBMVTKReporter, Simulation,  # noqa: F401
+                        loadCheckpoint, saveCheckpoint)

@@ -28,6 +28,8 @@ _SIGNATURES = {
     'lbm_batch_set_velocities': (ctypes.c_int, [_P, _D]),
     'lbm_batch_get_fluid_state': (ctypes.c_int, [_P, ctypes.c_int, _D]),
     'lbm_batch_temperatures': (ctypes.c_int, [_P, _D, _D]),
+    'lbm_batch_set_persistent': (ctypes.c_int, [_P, ctypes.c_int]),
+    'lbm_batch_set_barrier_polls': (ctypes.c_int, [_P, ctypes.c_longlong]),
     'lbm_batch_info': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                                       ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int),
                                       ctypes.POINTER(ctypes.c_int)]),
@@ -114,6 +116,14 @@ class ReplicaBatch:
         beads = np.zeros(self.num_replicas)
         check(self.lib.lbm_batch_temperatures(self.handle, _dp(fluid), _dp(beads)), self.lib)
         return fluid, beads
+
+    def set_persistent(self, enable=True):
+        """One persistent launch per graph_steps steps (True, the default) or the seven phase kernels of a step."""
+        check(self.lib.lbm_batch_set_persistent(self.handle, int(enable)), self.lib)
+
+    def set_barrier_polls(self, polls=0):
+        """Poll limit of the persistent step's grid barriers (0: the default)."""
+        check(self.lib.lbm_batch_set_barrier_polls(self.handle, int(polls)), self.lib)
 
     def info(self):
         nodes, steps, launches = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()

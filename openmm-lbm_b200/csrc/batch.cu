@@ -18,6 +18,7 @@
 #include "lbm_b200_md.h"
 #include "collide.cuh"
 #include "coupling_device.cuh"
+#include "grid_barrier.cuh"
 #include "lbm_internal.h"
 #include <algorithm>
 #include <cmath>
@@ -318,6 +319,221 @@ __global__ void batchGatherKernel(const T* __restrict__ A, FluidView f, double* 
     }
 }
 
+// ------------------------------------------------------------------------------------------------------------------
+// The persistent step: `steps` lattice steps of every replica in one cooperative launch (every block resident), the
+// phases of a step separated by bounded grid barriers (grid_barrier.cuh):
+//
+//   phase 1  bead pair forces (blocks over replicas), stencil slots of every bead (threads over slots), and the clear
+//            of the reactions of the previous step (their slot nodes are kept in the other half of slotNode)
+//   phase 2  explicit drag of every bead and its reaction on the fluid (warps over beads), then the bead's leapfrog
+//   phase 3  the dense step of every replica (work items of BT nodes); the last block to finish a replica's items
+//            reduces its per-warp sums in a fixed order (the mass, momentum and removal velocity of the next step)
+//
+// The reaction buffers and slot nodes alternate between steps (buffer step & 1), so that the clear of step s - 1 and
+// the slots of step s share phase 1.  A replica computes what the seven-kernel step computes, in the same order of
+// floating-point operations.  A barrier that times out sets LBM_ERR_DEVICE_TIMEOUT in the status word and every
+// block leaves the launch.
+// ------------------------------------------------------------------------------------------------------------------
+
+struct PersistentArgs {
+    const FluidView* views[2];     // the replicas' views with reaction buffer 0 / 1
+    const CouplingView* cviews;
+    const ReplicaTable* table;
+    const int* itemReplica;
+    const int* particleReplica;
+    int numReplicas, numItems, totalParticles, slots, coupled, steps;
+    PairParams pair;
+    void* pop[2];                  // populations: the launch starts from pop[cur]
+    int cur;
+    double* partials;              // 4 per warp of every item
+    int* replicaDone;              // items of the current step finished, per replica
+    BatchClock* clock;
+    double *pos, *vel, *fpair, *fdrag, *invMass, *wall;
+    int* slotNode[2];
+    void* slotWeight;
+    void* slotU;
+    unsigned* barrier;
+    int* status;
+    long long pollLimit;
+};
+
+// Sums of replica r's items (the body of batchFinishKernel for one replica, by the whole block), in the same order.
+__device__ __forceinline__ void finishReplica(const PersistentArgs& a, int r, int warpsPerItem) {
+    __shared__ double red[16][4];
+    const int lane = threadIdx.x%32, warp = threadIdx.x/32;
+    const ReplicaTable& rt = a.table[r];
+    size_t begin = (size_t) rt.firstItem*warpsPerItem, count = (size_t) rt.numItems*warpsPerItem;
+    double acc[4] = {0, 0, 0, 0};
+    for (size_t i = threadIdx.x; i < count; i += blockDim.x)
+        for (int k = 0; k < 4; k++)
+            acc[k] += __ldcg(&a.partials[4*(begin + i) + k]);
+    for (int k = 0; k < 4; k++)
+        acc[k] = warpReduceSum(acc[k]);
+    if (lane == 0)
+        for (int k = 0; k < 4; k++)
+            red[warp][k] = acc[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double total[4] = {0, 0, 0, 0};
+        for (int w = 0; w < (int) blockDim.x/32; w++)
+            for (int k = 0; k < 4; k++)
+                total[k] += red[w][k];
+        StepStats* st = a.views[0][r].stats;
+        st->mass = total[0];
+        double mass = a.views[0][r].numFluid + total[0];
+        for (int k = 0; k < 3; k++) {
+            st->momentum[k] = total[1+k];
+            st->ucm[k] = total[1+k]/mass;
+        }
+        a.replicaDone[r] = 0;
+    }
+    __syncthreads();
+}
+
+template <typename T, typename R, bool FLUCT, int BT>
+__global__ void __launch_bounds__(BT, batchMinBlocks<R, BT>())
+batchPersistentKernel(PersistentArgs a) {
+    typedef typename Vec4<R>::type V;
+    __shared__ int lastShared;
+    const int lane = threadIdx.x%32, warp = threadIdx.x/32;
+    const long long step0 = a.clock->step;
+    const long long totalSlots = (long long) a.totalParticles*a.slots;
+    const int threads = gridDim.x*blockDim.x, firstThread = blockIdx.x*blockDim.x + threadIdx.x;
+    const int warps = threads >> 5, firstWarp = firstThread >> 5;
+    R* slotWeight = (R*) a.slotWeight;
+    V* slotU = (V*) a.slotU;
+    for (int s = 0; s < a.steps; s++) {
+        const long long step = step0 + s;
+        const int buf = (int) (step & 1);
+        const FluidView* views = a.views[buf];
+        const T* A = (const T*) a.pop[(a.cur + s) & 1];
+        T* B = (T*) a.pop[(a.cur + s + 1) & 1];
+        if (a.coupled) {
+            // Phase 1: pair forces, stencil slots, clear of the previous step's reactions.
+            for (int r = blockIdx.x; r < a.numReplicas; r += gridDim.x) {
+                const ReplicaTable& rt = a.table[r];
+                const double* x = a.pos + 3*(size_t) rt.firstParticle;
+                double* out = a.fpair + 3*(size_t) rt.firstParticle;
+                for (int i = threadIdx.x; i < rt.numParticles; i += blockDim.x) {
+                    double f[3] = {0, 0, 0};
+                    if (a.pair.type != LBM_PAIR_NONE)
+                        for (int j = 0; j < rt.numParticles; j++) {
+                            if (j == i)
+                                continue;
+                            double d[3];
+                            for (int k = 0; k < 3; k++) {
+                                d[k] = x[3*i+k] - x[3*j+k];
+                                d[k] -= rt.box[k]*rint(d[k]/rt.box[k]);
+                            }
+                            double r2 = d[0]*d[0] + d[1]*d[1] + d[2]*d[2];
+                            if (r2 >= a.pair.rc2 || r2 == 0.0)
+                                continue;
+                            double s2 = a.pair.sigma2/r2, s6 = s2*s2*s2;
+                            double scale = 24.0*a.pair.eps*s6*(2.0*s6 - 1.0)/r2;
+                            for (int k = 0; k < 3; k++)
+                                f[k] += scale*d[k];
+                        }
+                    for (int k = 0; k < 3; k++)
+                        out[3*i+k] = f[k];
+                }
+            }
+            int* nodes = a.slotNode[buf];
+            const int* oldNodes = a.slotNode[1 - buf];
+            const FluidView* oldViews = a.views[1 - buf];
+            for (long long t = firstThread; t < totalSlots; t += threads) {
+                const int p = (int) (t/a.slots), sl = (int) (t - (long long) p*a.slots);
+                const int r = a.particleReplica[p];
+                const ReplicaTable& rt = a.table[r];
+                const int p0 = rt.firstParticle, i = p - p0;
+                const int remove = rt.removeFrequency > 0 && step%rt.removeFrequency == 0;
+                const size_t so = (size_t) p0*a.slots;
+                // The clear of slot t of the previous step (reaction buffer 1 - buf).
+                const FluidView& of = oldViews[r];
+                const long long node = oldNodes[t];
+                R* reaction = (R*) const_cast<void*>(of.reaction);
+                *reinterpret_cast<V*>(reaction + 4*node) = Vec4<R>::make(0, 0, 0, 0);
+                const long long row = node/of.nx;
+                const int xx = (int) (node - row*of.nx);
+                const_cast<uint32_t*>(of.reactMask)[row*of.wordsPerRow + xx/32] = 0u;
+                stencilSlot<T, R, true>(A + (size_t) 19*rt.nodeOffset, views[r], a.cviews[r], a.pos + 3*(size_t) p0,
+                                  (long long) i*a.slots + sl, remove, 0, nodes + so, slotWeight + so, slotU + so);
+            }
+            if (!gridSync(a.barrier, a.status, a.pollLimit))
+                return;
+            // Phase 2: explicit drag and reaction, then the leapfrog of the bead (v += dt F/m, x += dt v).
+            for (int p = firstWarp; p < a.totalParticles; p += warps) {
+                const int r = a.particleReplica[p];
+                const ReplicaTable& rt = a.table[r];
+                const FluidView& f = views[r];
+                const int p0 = rt.firstParticle;
+                const size_t so = (size_t) p0*a.slots;
+                explicitParticle<R, true>(f, a.cviews[r], a.vel + 3*(size_t) p0, nodes + so, slotWeight + so, slotU + so, p - p0,
+                                    lane, step, 1, a.fdrag + 3*(size_t) p0, (R*) const_cast<void*>(f.reaction),
+                                    const_cast<uint32_t*>(f.reactMask), a.wall);
+                __syncwarp();
+                if (lane < 3) {
+                    const size_t k = 3*(size_t) p + lane;
+                    const double force = a.fpair[k] + a.fdrag[k];
+                    const double v = a.vel[k] + rt.dt*force*a.invMass[p];
+                    a.vel[k] = v;
+                    a.pos[k] += rt.dt*v;
+                }
+            }
+            if (!gridSync(a.barrier, a.status, a.pollLimit))
+                return;
+        }
+        // Phase 3: the dense step; the last block of a replica reduces its sums.
+        for (int w = blockIdx.x; w < a.numItems; w += gridDim.x) {
+            const int r = a.itemReplica[w];
+            const FluidView& v = views[r];
+            const ReplicaTable& rt = a.table[r];
+            const int remove = rt.removeFrequency > 0 && step%rt.removeFrequency == 0;
+            const CollideConstants<R> k = collideConstants<R>(v.omega, v.g, v.stats->ucm, remove, v.mu, v.seed);
+            const unsigned N = rt.numNodes;
+            const unsigned local = (unsigned) (w - rt.firstItem)*BT + threadIdx.x;
+            R sm = 0, sx = 0, sy = 0, sz = 0;
+            if (local < N) {
+                const int nx = v.nx, ny = v.ny, nz = v.nz;
+                const unsigned row = local/(unsigned) nx;
+                const int x = (int) (local - row*nx);
+                const int y = (int) (row%ny), z = (int) (row/ny);
+                R ex = 0, ey = 0, ez = 0;
+                if (a.coupled) {
+                    uint32_t word = __ldcg(&v.reactMask[(size_t) row*v.wordsPerRow + x/32]);
+                    if ((word >> (x%32)) & 1u) {
+                        const R* rp = reinterpret_cast<const R*>(v.reaction) + 4*(size_t) local;
+                        ex = __ldcg(rp);
+                        ey = __ldcg(rp + 1);
+                        ez = __ldcg(rp + 2);
+                    }
+                }
+                const size_t base = (size_t) 19*rt.nodeOffset;
+                collideNode<T, R, FLUCT, true>(A + base, B + base, N, local, x, y, z, nx, ny, nz, k, ex, ey, ez, step, sm,
+                                               sx, sy, sz);
+            }
+            double s0 = warpReduceSum((double) sm), s1 = warpReduceSum((double) sx);
+            double s2 = warpReduceSum((double) sy), s3 = warpReduceSum((double) sz);
+            if (lane == 0) {
+                double* out = a.partials + 4*((size_t) w*(BT/32) + warp);
+                out[0] = s0; out[1] = s1; out[2] = s2; out[3] = s3;
+                __threadfence();
+            }
+            __syncthreads();
+            if (threadIdx.x == 0)
+                lastShared = atomicAdd(&a.replicaDone[r], 1) == rt.numItems - 1;
+            __syncthreads();
+            if (lastShared) {
+                __threadfence();
+                finishReplica(a, r, BT/32);
+            }
+        }
+        if (!gridSync(a.barrier, a.status, a.pollLimit))
+            return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        a.clock->step = step0 + a.steps;
+}
+
 int stencilWidth(int stencil) {
     switch (stencil) {
     case LBM_STENCIL_TRILINEAR: return 2;
@@ -341,8 +557,13 @@ public:
     void getFluidState(int replica, double* state);
     void temperatures(double* fluidKT, double* beadKT);
     void info(long long* totalNodes, long long* steps, long long* launchCount, int* threads, int* graphSteps);
+    void setPersistent(bool enable);
+    void setBarrierPolls(long long polls);
 private:
     template <typename T> void launchStep();
+    template <typename T, int BT> void launchPersistent(int steps);
+    void launchPersistentAny(int steps);
+    void checkStatus();
     template <typename T, int BT> void launchDense(const void* A, void* B);
     void launchDenseAny(const void* A, void* B);
     template <typename T, int BT> int denseGrid();
@@ -377,6 +598,14 @@ private:
     void *slotWeightDev, *slotUDev;
     cudaGraphExec_t graphExec;
     int graphCur;
+    // The persistent step (batchPersistentKernel): the reaction buffers, masks and slot nodes come in two halves
+    // (buffer step & 1), viewsDev holds the replicas' views for both, and the grid barrier its counter and status.
+    bool persistent;
+    unsigned maskWordsTotal;
+    int* replicaDoneDev;
+    unsigned* barrierDev;
+    int* statusDev;
+    long long barrierPolls;
 };
 
 BatchEngine::BatchEngine(int nr, const LbmLatticeParameters* ls, const int* np, const double* masses,
@@ -388,7 +617,8 @@ BatchEngine::BatchEngine(int nr, const LbmLatticeParameters* ls, const int* np, 
           reactionDev(nullptr), maskDev(nullptr), particleReplicaDev(nullptr), posDev(nullptr), velDev(nullptr),
           fpairDev(nullptr), fdragDev(nullptr), invMassDev(nullptr), massDev(nullptr), cellMassDev(nullptr),
           wallDev(nullptr), cellEnergyDev(nullptr), slotNodeDev(nullptr), slotWeightDev(nullptr), slotUDev(nullptr),
-          graphExec(nullptr), graphCur(0) {
+          graphExec(nullptr), graphCur(0), persistent(true), maskWordsTotal(0), replicaDoneDev(nullptr),
+          barrierDev(nullptr), statusDev(nullptr), barrierPolls(1LL << 26) {
     pop[0] = pop[1] = nullptr;
     if (nr <= 0 || ls == nullptr || np == nullptr)
         throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_batch_create: no replicas");
@@ -466,12 +696,19 @@ BatchEngine::BatchEngine(int nr, const LbmLatticeParameters* ls, const int* np, 
         CUDA_CHECK(cudaMemsetAsync(clockDev, 0, sizeof(BatchClock), stream));
         CUDA_CHECK(cudaMalloc(&wallDev, sizeof(double)*4));
         CUDA_CHECK(cudaMemsetAsync(wallDev, 0, sizeof(double)*4, stream));
+        maskWordsTotal = maskWords;
         if (coupled) {
-            CUDA_CHECK(cudaMalloc(&reactionDev, 4*e*(size_t) totalNodes));
-            CUDA_CHECK(cudaMemsetAsync(reactionDev, 0, 4*e*(size_t) totalNodes, stream));
-            CUDA_CHECK(cudaMalloc(&maskDev, sizeof(uint32_t)*(size_t) maskWords));
-            CUDA_CHECK(cudaMemsetAsync(maskDev, 0, sizeof(uint32_t)*(size_t) maskWords, stream));
+            // Two halves (the reactions of even and odd steps in the persistent step).
+            CUDA_CHECK(cudaMalloc(&reactionDev, 2*4*e*(size_t) totalNodes));
+            CUDA_CHECK(cudaMemsetAsync(reactionDev, 0, 2*4*e*(size_t) totalNodes, stream));
+            CUDA_CHECK(cudaMalloc(&maskDev, 2*sizeof(uint32_t)*(size_t) maskWords));
+            CUDA_CHECK(cudaMemsetAsync(maskDev, 0, 2*sizeof(uint32_t)*(size_t) maskWords, stream));
         }
+        CUDA_CHECK(cudaMalloc(&replicaDoneDev, sizeof(int)*nr));
+        CUDA_CHECK(cudaMemsetAsync(replicaDoneDev, 0, sizeof(int)*nr, stream));
+        CUDA_CHECK(cudaMalloc(&statusDev, sizeof(int)*2));
+        CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*2, stream));
+        barrierDev = reinterpret_cast<unsigned*>(statusDev + 1);
         // Views of the replicas.
         std::vector<CouplingView> cviews(nr);
         std::vector<double> cellMass(nr);
@@ -524,8 +761,16 @@ BatchEngine::BatchEngine(int nr, const LbmLatticeParameters* ls, const int* np, 
                 particleReplica[p] = r;
             }
         }
-        CUDA_CHECK(cudaMalloc(&viewsDev, sizeof(FluidView)*nr));
-        CUDA_CHECK(cudaMemcpy(viewsDev, viewsHost.data(), sizeof(FluidView)*nr, cudaMemcpyHostToDevice));
+        // The views of the second half of the reaction buffers follow those of the first.
+        std::vector<FluidView> views2 = viewsHost;
+        for (int r = 0; r < nr; r++)
+            if (coupled) {
+                views2[r].reaction = (const char*) viewsHost[r].reaction + 4*e*(size_t) totalNodes;
+                views2[r].reactMask = viewsHost[r].reactMask + maskWords;
+            }
+        views2.insert(views2.begin(), viewsHost.begin(), viewsHost.end());
+        CUDA_CHECK(cudaMalloc(&viewsDev, sizeof(FluidView)*2*nr));
+        CUDA_CHECK(cudaMemcpy(viewsDev, views2.data(), sizeof(FluidView)*2*nr, cudaMemcpyHostToDevice));
         CUDA_CHECK(cudaMalloc(&cviewsDev, sizeof(CouplingView)*nr));
         CUDA_CHECK(cudaMemcpy(cviewsDev, cviews.data(), sizeof(CouplingView)*nr, cudaMemcpyHostToDevice));
         CUDA_CHECK(cudaMalloc(&cellEnergyDev, sizeof(double)*nr));
@@ -541,8 +786,8 @@ BatchEngine::BatchEngine(int nr, const LbmLatticeParameters* ls, const int* np, 
         if (totalParticles > 0)
             CUDA_CHECK(cudaMemcpy(posDev, positions, sizeof(double)*3*(size_t) totalParticles, cudaMemcpyHostToDevice));
         size_t ns = (size_t) std::max(1, totalParticles)*slots;
-        CUDA_CHECK(cudaMalloc(&slotNodeDev, sizeof(int)*ns));
-        CUDA_CHECK(cudaMemsetAsync(slotNodeDev, 0, sizeof(int)*ns, stream));
+        CUDA_CHECK(cudaMalloc(&slotNodeDev, 2*sizeof(int)*ns));
+        CUDA_CHECK(cudaMemsetAsync(slotNodeDev, 0, 2*sizeof(int)*ns, stream));
         CUDA_CHECK(cudaMalloc(&slotWeightDev, e*ns));
         CUDA_CHECK(cudaMalloc(&slotUDev, 4*e*ns));
         CUDA_CHECK(cudaMalloc(&tableDev, sizeof(ReplicaTable)*nr));
@@ -571,7 +816,7 @@ void BatchEngine::release() {
     releaseGraph();
     void* ptrs[] = {pop[0], pop[1], viewsDev, cviewsDev, tableDev, statsDev, clockDev, itemReplicaDev, partialsDev,
                     reactionDev, maskDev, particleReplicaDev, posDev, velDev, fpairDev, fdragDev, invMassDev, massDev,
-                    cellMassDev, wallDev, cellEnergyDev, slotNodeDev, slotWeightDev, slotUDev};
+                    cellMassDev, wallDev, cellEnergyDev, slotNodeDev, slotWeightDev, slotUDev, replicaDoneDev, statusDev};
     for (void* p : ptrs)
         cudaFree(p);
     pop[0] = pop[1] = nullptr;
@@ -579,6 +824,7 @@ void BatchEngine::release() {
     itemReplicaDev = nullptr; partialsDev = nullptr; reactionDev = nullptr; maskDev = nullptr; particleReplicaDev = nullptr;
     posDev = velDev = fpairDev = fdragDev = invMassDev = massDev = cellMassDev = wallDev = cellEnergyDev = nullptr;
     slotNodeDev = nullptr; slotWeightDev = slotUDev = nullptr;
+    replicaDoneDev = nullptr; statusDev = nullptr; barrierDev = nullptr;
     if (ownStream && stream)
         cudaStreamDestroy(stream);
     stream = nullptr;
@@ -682,10 +928,149 @@ void BatchEngine::launchStep() {
     cur = 1 - cur;
 }
 
+template <typename T, int BT>
+void BatchEngine::launchPersistent(int steps) {
+    typedef T R;
+    // Every block must be resident (the grid barriers): the grid is the occupancy of this variant times the SMs.
+    int perSM = 0;
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &perSM, fluctuate ? batchPersistentKernel<T, R, true, BT> : batchPersistentKernel<T, R, false, BT>, BT, 0));
+    if (perSM < 1)
+        throw Error(LBM_ERR_NOT_SUPPORTED, "lbm_batch_step: the persistent step does not fit on a multiprocessor");
+    PersistentArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.views[0] = viewsDev;
+    a.views[1] = viewsDev + numReplicas;
+    a.cviews = cviewsDev;
+    a.table = tableDev;
+    a.itemReplica = itemReplicaDev;
+    a.particleReplica = particleReplicaDev;
+    a.numReplicas = numReplicas;
+    a.numItems = numItems;
+    a.totalParticles = totalParticles;
+    a.slots = slots;
+    a.coupled = coupled ? 1 : 0;
+    a.steps = steps;
+    a.pair = pairParams;
+    a.pop[0] = pop[0];
+    a.pop[1] = pop[1];
+    a.cur = cur;
+    a.partials = partialsDev;
+    a.replicaDone = replicaDoneDev;
+    a.clock = clockDev;
+    a.pos = posDev; a.vel = velDev; a.fpair = fpairDev; a.fdrag = fdragDev; a.invMass = invMassDev; a.wall = wallDev;
+    a.slotNode[0] = slotNodeDev;
+    a.slotNode[1] = slotNodeDev + (size_t) std::max(1, totalParticles)*slots;
+    a.slotWeight = slotWeightDev;
+    a.slotU = slotUDev;
+    a.barrier = barrierDev;
+    a.status = statusDev;
+    a.pollLimit = barrierPolls;
+    int grid = perSM*sms;
+    void* args[] = {&a};
+    CUDA_CHECK(cudaMemsetAsync(barrierDev, 0, sizeof(unsigned), stream));
+    CUDA_CHECK(cudaLaunchCooperativeKernel(fluctuate ? (const void*) batchPersistentKernel<T, R, true, BT> :
+                                           (const void*) batchPersistentKernel<T, R, false, BT>,
+                                           grid, BT, args, 0, stream));
+    launches++;
+    cur = (cur + steps) & 1;
+}
+
+void BatchEngine::launchPersistentAny(int steps) {
+    bool f64 = storage == LBM_STORAGE_F64;
+    switch (threads) {
+    case 128: f64 ? launchPersistent<double, 128>(steps) : launchPersistent<float, 128>(steps); break;
+    case 512: f64 ? launchPersistent<double, 512>(steps) : launchPersistent<float, 512>(steps); break;
+    default: f64 ? launchPersistent<double, 256>(steps) : launchPersistent<float, 256>(steps); break;
+    }
+}
+
+// A timed-out grid barrier of the persistent step leaves LBM_ERR_DEVICE_TIMEOUT in the status word: reported (and
+// cleared) by the next call that synchronizes.
+void BatchEngine::checkStatus() {
+    int status = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&status, statusDev, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (status != 0) {
+        // The blocks left the launch at different points: the item counters of the per-replica sums and the reaction
+        // buffers may hold partial values.  Clear them, so that later steps start from a consistent state.
+        CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int), stream));
+        CUDA_CHECK(cudaMemsetAsync(replicaDoneDev, 0, sizeof(int)*numReplicas, stream));
+        if (coupled) {
+            size_t e = storage == LBM_STORAGE_F64 ? 8 : 4;
+            CUDA_CHECK(cudaMemsetAsync(reactionDev, 0, 2*4*e*(size_t) totalNodes, stream));
+            CUDA_CHECK(cudaMemsetAsync(maskDev, 0, 2*sizeof(uint32_t)*(size_t) maskWordsTotal, stream));
+        }
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+        throw Error((LbmStatus) status, "lbm_batch: a grid barrier of the persistent step timed out; the steps of that "
+                    "launch are incomplete");
+    }
+}
+
+void BatchEngine::setPersistent(bool enable) {
+    CUDA_CHECK(cudaSetDevice(device));
+    if (enable == persistent)
+        return;
+    releaseGraph();
+    // The two step forms keep the reactions of a step in different halves of the buffers: start from clean ones (a
+    // step's reactions are not needed after it).
+    size_t e = storage == LBM_STORAGE_F64 ? 8 : 4;
+    if (coupled) {
+        CUDA_CHECK(cudaMemsetAsync(reactionDev, 0, 2*4*e*(size_t) totalNodes, stream));
+        CUDA_CHECK(cudaMemsetAsync(maskDev, 0, 2*sizeof(uint32_t)*(size_t) maskWordsTotal, stream));
+    }
+    persistent = enable;
+}
+
+void BatchEngine::setBarrierPolls(long long polls) {
+    if (polls < 0)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_batch_set_barrier_polls: the limit must not be negative");
+    barrierPolls = polls > 0 ? polls : (1LL << 26);
+    releaseGraph();
+}
+
 void BatchEngine::step(int steps) {
     CUDA_CHECK(cudaSetDevice(device));
     if (steps < 0)
         throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_batch_step: negative step count");
+    if (persistent) {
+        // graphSteps steps per launch, captured once into a graph (the launch and the clear of its barrier) and
+        // replayed; the rest in one direct launch.  graphSteps is even, so a replay leaves the populations in the
+        // buffer where it found them.
+        int s = 0;
+        if (steps >= graphSteps && graphExec == nullptr) {
+            int start = cur;
+            long long launches0 = launches;
+            cudaGraph_t graph = nullptr;
+            CUDA_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                launchPersistentAny(graphSteps);
+            }
+            catch (...) {
+                cudaStreamEndCapture(stream, &graph);
+                if (graph)
+                    cudaGraphDestroy(graph);
+                cur = start;
+                throw;
+            }
+            CUDA_CHECK(cudaStreamEndCapture(stream, &graph));
+            cudaError_t e = cudaGraphInstantiate(&graphExec, graph, 0);
+            cudaGraphDestroy(graph);
+            CUDA_CHECK(e);
+            cur = start;
+            graphCur = start;
+            launches = launches0;
+        }
+        if (graphExec != nullptr && cur == graphCur)
+            for (; s + graphSteps <= steps; s += graphSteps) {
+                CUDA_CHECK(cudaGraphLaunch(graphExec, stream));
+                launches++;
+            }
+        if (s < steps)
+            launchPersistentAny(steps - s);
+        stepsTaken += steps;
+        return;
+    }
     long long perStep = coupled ? 7 : 2;
     if (steps >= graphSteps && graphExec == nullptr) {
         // Capture graphSteps steps (an even number, so that the populations end in the buffer they started in).
@@ -769,6 +1154,7 @@ int BatchEngine::autotune(int newGraphSteps, double* denseMs) {
 
 void BatchEngine::getParticles(double* positions, double* velocities) {
     CUDA_CHECK(cudaSetDevice(device));
+    checkStatus();
     size_t v3 = sizeof(double)*3*(size_t) totalParticles;
     if (positions && totalParticles)
         CUDA_CHECK(cudaMemcpyAsync(positions, posDev, v3, cudaMemcpyDeviceToHost, stream));
@@ -785,6 +1171,8 @@ void BatchEngine::setVelocities(const double* velocities) {
 }
 
 void BatchEngine::getFluidState(int r, double* state) {
+    CUDA_CHECK(cudaSetDevice(device));
+    checkStatus();
     CUDA_CHECK(cudaSetDevice(device));
     if (r < 0 || r >= numReplicas)
         throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_batch_get_fluid_state: no such replica");
@@ -808,6 +1196,8 @@ void BatchEngine::getFluidState(int r, double* state) {
 }
 
 void BatchEngine::temperatures(double* fluidKT, double* beadKT) {
+    CUDA_CHECK(cudaSetDevice(device));
+    checkStatus();
     CUDA_CHECK(cudaSetDevice(device));
     double* out = nullptr;
     CUDA_CHECK(cudaMalloc(&out, sizeof(double)*2*numReplicas));
@@ -940,6 +1330,18 @@ LbmStatus lbm_batch_get_fluid_state(LbmBatch* batch, int replica, double* state)
 LbmStatus lbm_batch_temperatures(LbmBatch* batch, double* fluid_kT, double* bead_kT) {
     if (!batch) return nullBatch();
     return batchGuard([&] { batch->impl->temperatures(fluid_kT, bead_kT); });
+}
+
+LbmStatus lbm_batch_set_persistent(LbmBatch* batch, int enable) {
+    if (!batch)
+        return nullBatch();
+    return batchGuard([&] { batch->impl->setPersistent(enable != 0); });
+}
+
+LbmStatus lbm_batch_set_barrier_polls(LbmBatch* batch, long long polls) {
+    if (!batch)
+        return nullBatch();
+    return batchGuard([&] { batch->impl->setBarrierPolls(polls); });
 }
 
 LbmStatus lbm_batch_info(LbmBatch* batch, long long* total_nodes, long long* steps, long long* launches,

@@ -173,7 +173,8 @@ __device__ __forceinline__ CollideConstants<R> collideConstants(double omega, co
 // an nx x ny x nz lattice of N nodes.  The node's mass and momentum deviations after the collision are added to the
 // sums: the collision conserves mass and gives the momentum j + F (the fluctuation modes carry neither), so they are
 // dr and j + F, equal to the sums of the stored values up to the rounding of the stores.
-template <typename T, typename R, bool FLUCT>
+// COHERENT: A was written by the same launch (a persistent kernel), so it is read through L2, not the read-only path.
+template <typename T, typename R, bool FLUCT, bool COHERENT = false>
 __device__ __forceinline__ void collideNode(const T* __restrict__ A, T* __restrict__ B, unsigned N, unsigned node,
                                             int x, int y, int z, int nx, int ny, int nz, const CollideConstants<R>& k,
                                             R ex, R ey, R ez, long long step, R& sumMass, R& sumX, R& sumY, R& sumZ) {
@@ -189,7 +190,10 @@ __device__ __forceinline__ void collideNode(const T* __restrict__ A, T* __restri
         constexpr int q = decltype(qc)::value;
         constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
         const unsigned src = node + ox[1-cx] + oy[1-cy] + oz[1-cz];
-        r[q] = Storage<T>::template raw<q>(A + ((size_t) q*N + src));
+        if constexpr (COHERENT)
+            r[q] = Storage<T>::template rawCoherent<q>(A + ((size_t) q*N + src));
+        else
+            r[q] = Storage<T>::template raw<q>(A + ((size_t) q*N + src));
     });
     Moments<R> m = momentsOfRaw<T, R>(r);
     R rho = R(1) + m.dr, inv = reciprocal(rho);

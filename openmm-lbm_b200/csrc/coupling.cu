@@ -19,6 +19,7 @@
 // reaction only where there is one.
 #include "coupling.cuh"
 #include "coupling_device.cuh"
+#include "grid_barrier.cuh"
 #include "lbm_device.cuh"
 #include "radix_sort.cuh"
 #include <algorithm>
@@ -165,49 +166,11 @@ struct CgBuffers {
     double* z;             // holds A p between the product and the update
     double* p;
     double* partials[2];   // kPartial doubles per block, two buffers used alternately
-    unsigned* barrier;     // [0] arrival count, [1] generation
+    unsigned* barrier;     // arrivals at the grid barriers of the launch (cleared before it, with the status words)
     int* status;           // 0 ok, LBM_ERR_CG_NOT_CONVERGED, LBM_ERR_DEVICE_TIMEOUT
     int* iterations;
     long long pollLimit;   // polls of a waiting block before it gives up (kDefaultBarrierPolls)
 };
-
-// Grid barrier for a cooperative launch (all blocks resident), with a bounded spin: after b.pollLimit polls the
-// waiting block gives up, records a timeout in the status word and returns false; every block then leaves the
-// solve at its next barrier.  Thread 0 takes the decision for its block (its own wait and the status word), so
-// all threads of a block return the same value and leave together.
-__device__ bool gridBarrier(unsigned* bar, int* status, unsigned& generation, long long pollLimit) {
-    __shared__ int okShared;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        bool ok = true;
-        unsigned target = generation + 1;
-        __threadfence();
-        unsigned arrived = atomicAdd(&bar[0], 1u);
-        if (arrived == gridDim.x - 1) {
-            bar[0] = 0;
-            __threadfence();
-            atomicExch(&bar[1], target);
-        }
-        else {
-            // Poll with plain loads (an atomic per poll from every waiting block would queue behind one another at
-            // the word's L2 slice, and delay the release); look at the status word every 256 polls.
-            long long polls = 0;
-            while (*((volatile unsigned*) &bar[1]) != target) {
-                if (++polls > pollLimit ||
-                    ((polls & 255) == 0 && *((volatile int*) status) == LBM_ERR_DEVICE_TIMEOUT)) {
-                    atomicExch(status, LBM_ERR_DEVICE_TIMEOUT);
-                    ok = false;
-                    break;
-                }
-            }
-        }
-        __threadfence();
-        generation = target;
-        okShared = ok && *((volatile int*) status) != LBM_ERR_DEVICE_TIMEOUT;
-    }
-    __syncthreads();
-    return okShared != 0;
-}
 
 // Block sum of a record (thread values v) into partials[block]; after a grid barrier (by the caller) every block adds
 // the records of all blocks in block order, so every block gets the same result, bit for bit.
@@ -265,9 +228,6 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
     const int warps = (gridDim.x*blockDim.x) >> 5;
     const int S = c.slots;
     const double a = c.a;
-    unsigned generation = 0;
-    if (threadIdx.x == 0)
-        generation = *((volatile unsigned*) &b.barrier[1]);
     // spread(n) += w p_i on the stencil nodes of particle i.
     auto spreadP = [&](int i, const double* p) {
         double p0 = p[3*i], p1 = p[3*i+1], p2 = p[3*i+2];
@@ -348,7 +308,7 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
                 atomicAdd3(spread + 4*(long long) slotNode[t], w*F[0], w*F[1], w*F[2]);
         }
     }
-    if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
+    if (!gridSync(b.barrier, b.status, b.pollLimit))
         return;
     // r = rhs - A F, z = r/diag, p = z; r.z, the norm of the right-hand side and r.r per component.
     double acc[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -372,7 +332,7 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
         }
     }
     blockSumStore(acc, b.partials[1]);
-    if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
+    if (!gridSync(b.barrier, b.status, b.pollLimit))
         return;
     for (int i = firstWarp; i < c.np; i += warps)
         clearSpread(i);
@@ -398,13 +358,13 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
         // The spread buffer was cleared by every block before the last barrier (the clearing of the start comes
         // before the barrier at the top of the first iteration's spread below).
         if (clearBeforeSpread) {
-            if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
+            if (!gridSync(b.barrier, b.status, b.pollLimit))
                 return;
             clearBeforeSpread = false;
         }
         for (int i = firstWarp; i < c.np; i += warps)
             spreadP(i, b.p);
-        if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
+        if (!gridSync(b.barrier, b.status, b.pollLimit))
             return;
         double acc3[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int i = firstWarp; i < c.np; i += warps) {
@@ -421,7 +381,7 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
             }
         }
         blockSumStore(acc3, b.partials[0]);
-        if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
+        if (!gridSync(b.barrier, b.status, b.pollLimit))
             return;
         reducePartials(b.partials[0], gridDim.x, tot);
         double alpha[3];
@@ -444,7 +404,7 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
             }
         }
         blockSumStore(acc4, b.partials[1]);
-        if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
+        if (!gridSync(b.barrier, b.status, b.pollLimit))
             return;
         reducePartials(b.partials[1], gridDim.x, tot);
         double beta[3];
@@ -739,9 +699,6 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
     const int rowEnd = (int) ((long long) c.np*(blockIdx.x + 1)/gridDim.x);
     const int S = c.slots;
     const double a = c.a;
-    unsigned generation = 0;
-    if (threadIdx.x == 0)
-        generation = *((volatile unsigned*) &b.barrier[1]);
     // The cell list has been read (by the rows kernel): empty it for the next step.
     for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x)
         g.cellCount[g.cellOf[i]] = 0u;
@@ -788,7 +745,7 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
         }
         b.diag[i] = diag;
     }
-    if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
+    if (!gridSync(b.barrier, b.status, b.pollLimit))
         return;
     // r = rhs - A F, z = r/diag, p = z; r.z, the norm of the right-hand side and r.r per component.
     double acc[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -813,7 +770,7 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
         }
     }
     blockSumStore(acc, b.partials[1]);
-    if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
+    if (!gridSync(b.barrier, b.status, b.pollLimit))
         return;
     double tot[kPartial];
     reducePartials(b.partials[1], gridDim.x, tot);
@@ -857,7 +814,7 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
             }
         }
         blockSumStore(acc3, b.partials[0]);
-        if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
+        if (!gridSync(b.barrier, b.status, b.pollLimit))
             return;
         reducePartials(b.partials[0], gridDim.x, tot);
         double alpha[3];
@@ -877,7 +834,7 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
             }
         }
         blockSumStore(acc4, b.partials[1]);
-        if (!gridBarrier(b.barrier, b.status, generation, b.pollLimit))
+        if (!gridSync(b.barrier, b.status, b.pollLimit))
             return;
         reducePartials(b.partials[1], gridDim.x, tot);
         for (int d = 0; d < 3; d++) {
@@ -1063,8 +1020,9 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
             b.status = statusDev;
             b.iterations = statusDev + 1;
             b.pollLimit = kDefaultBarrierPolls;
-            CUDA_CHECK(cudaMalloc(&b.barrier, sizeof(unsigned)*2));
-            CUDA_CHECK(cudaMemsetAsync(b.barrier, 0, sizeof(unsigned)*2, stream));
+            // The arrival counter of the grid barriers is statusDev[3]: the memset of the status words before every
+            // cooperative launch clears it too.
+            b.barrier = reinterpret_cast<unsigned*>(statusDev + 3);
             int device = 0, sms = 0, perSM = 0;
             CUDA_CHECK(cudaGetDevice(&device));
             CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
@@ -1136,7 +1094,7 @@ void CouplingEngine::release() {
         cudaFree(dev->hist);
         CgBuffers& b = dev->cg;
         cudaFree(b.rhs); cudaFree(b.diag); cudaFree(b.F); cudaFree(b.r); cudaFree(b.z); cudaFree(b.p);
-        cudaFree(b.partials[0]); cudaFree(b.partials[1]); cudaFree(b.barrier);
+        cudaFree(b.partials[0]); cudaFree(b.partials[1]);
         cudaFree(dev->spread);
         SparseCg& g = dev->sparse;
         cudaFree(g.cellOf); cudaFree(g.cellCount); cudaFree(g.cellList);
@@ -1233,7 +1191,7 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     // overflow their capacity (and every step with LBM_B200_SPREAD_CG=1 in the environment, for comparisons).
     CgBuffers b = dev->cg;
     SparseCg g = dev->sparse;
-    CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*3, stream));
+    CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, stream));
     double tolerance = std::is_same<R, double>::value ? 1e-13 : 1e-5;
     int maxIterations = cgMaxIterations;
     b.pollLimit = barrierPollLimit;
@@ -1269,7 +1227,7 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
         CUDA_CHECK(cudaStreamSynchronize(stream));
     }
     if (spreadOnly || status[2] != 0) {
-        CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*3, stream));
+        CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, stream));
         void* args[] = {&fv, &cc, &vel, &fin, &sn, &sw, &su, &coef, &stepArg, &isStepArg, &tolerance, &maxIterations, &b,
                         &spread, &fout, &reaction, &mask, &wall};
         CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredStencilKernel<R>, dev->cgGrid, kThreads, args, 0, stream));
@@ -1282,13 +1240,10 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     if (status[0] == LBM_ERR_CG_NOT_CONVERGED)
         throw Error(LBM_ERR_CG_NOT_CONVERGED, "LBMForce: the centred drag with the interpolation stencil did not converge "
                     "in " + std::to_string(maxIterations) + " iterations of the conjugate gradients");
-    if (status[0] == LBM_ERR_DEVICE_TIMEOUT) {
-        // The blocks left the solve at different barriers, so the arrival count holds a partial count: start the
-        // barrier of the next solve from zero.
-        CUDA_CHECK(cudaMemsetAsync(b.barrier, 0, sizeof(unsigned)*2, stream));
-        CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (status[0] == LBM_ERR_DEVICE_TIMEOUT)
+        // The blocks left the solve at different barriers; the arrival counter holds a partial count, which the
+        // memset before the next cooperative launch clears.
         throw Error(LBM_ERR_DEVICE_TIMEOUT, "LBMForce: a grid barrier of the conjugate gradients timed out");
-    }
 }
 
 void CouplingEngine::setSolverLimits(int maxIterations, long long barrierPolls) {

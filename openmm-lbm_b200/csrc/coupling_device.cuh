@@ -69,6 +69,19 @@ template <> struct Vec4<double> {
     static __device__ __forceinline__ double4 make(double a, double b, double c, double d) { return make_double4(a, b, c, d); }
 };
 
+// Loads of a slot's 4-vector through the read-only path (data of an earlier launch) or through L2 (data written by the
+// same launch); double4 as two double2.
+__device__ __forceinline__ float4 loadReadOnly(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ double4 loadReadOnly(const double4* p) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 loadCoherent(const float4* p) { return __ldcg(p); }
+__device__ __forceinline__ double4 loadCoherent(const double4* p) {
+    const double2 a = __ldcg(reinterpret_cast<const double2*>(p)), b = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
 // r[0..2] += (x, y, z): one vector atomic for float (sm_90 and later), three for double.
 __device__ __forceinline__ void atomicAdd3(float* r, double x, double y, double z) {
     atomicAdd(reinterpret_cast<float4*>(r), make_float4((float) x, (float) y, (float) z, 0.0f));
@@ -196,18 +209,22 @@ __device__ __forceinline__ void stencilAxes(const CouplingView& c, const double*
 // the slot (LBMStencils::axisWeights, LBMStencils.h:73-95) and the moments of the node pulled from the populations
 // (density, momentum after the momentum removal; a solid node has rho = 0).  centred: the velocity is
 // u~ = (j + h rho g)/rho (ReferenceLBMKernels.cpp:622, 773); explicit: u = j/rho (:539, :672).
-template <typename T, typename R>
+template <typename T, typename R, bool COHERENT = false>
 __device__ __forceinline__ void stencilSlot(const T* __restrict__ A, const FluidView& f, const CouplingView& c,
-                                            const double* __restrict__ pos, long long t, int remove, int centred,
+                                            const double* __restrict__ posIn, long long t, int remove, int centred,
                                             int* slotNode, R* slotWeight, typename Vec4<R>::type* slotU) {
+    // COHERENT: the positions were written by the same launch (a persistent kernel): read them through L2.
     int i = (int) (t/c.slots), s = (int) (t%c.slots);
+    double pos[3];
+    for (int a = 0; a < 3; a++)
+        pos[a] = COHERENT ? __ldcg(&posIn[3*i+a]) : posIn[3*i+a];
     int size[3] = {c.nx, c.ny, c.nz};
     int idx[3];
     double w = 1.0;
     if (c.stencil == LBM_STENCIL_NEAREST) {
         // nearestNode (ReferenceLBMKernels.cpp:973-983): periodic wrap on every axis.
         for (int a = 0; a < 3; a++) {
-            double sc = latticeCoordinate(pos[3*i+a], c.dx, size[a]);
+            double sc = latticeCoordinate(pos[a], c.dx, size[a]);
             idx[a] = ((int) floor(sc + 0.5))%size[a];
         }
     }
@@ -216,7 +233,7 @@ __device__ __forceinline__ void stencilSlot(const T* __restrict__ A, const Fluid
         for (int a = 0; a < 3; a++) {
             int index[4];
             double weight[4];
-            axisWeights(c.stencil, c.width, latticeCoordinate(pos[3*i+a], c.dx, size[a]), size[a], c.open[a] != 0,
+            axisWeights(c.stencil, c.width, latticeCoordinate(pos[a], c.dx, size[a]), size[a], c.open[a] != 0,
                         index, weight);
             idx[a] = index[sub[a]];
             w *= weight[sub[a]];
@@ -343,18 +360,24 @@ __device__ __forceinline__ double warpSum(double v) {
 // Explicit drag of particle i, nearest node or stencil (ReferenceLBMKernels.cpp:503-553, 643-697), by one warp (the
 // lanes over the stencil slots): F = -gamma m (v - u) + sqrt(2 gamma m kT) xi with u interpolated over the stencil,
 // written to fout; on a lattice step the reaction -w F goes to the stencil nodes.
-template <typename R>
-__device__ __forceinline__ void explicitParticle(const FluidView& f, const CouplingView& c, const double* __restrict__ vel,
-                                                 const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
-                                                 const typename Vec4<R>::type* __restrict__ slotU, int i, int lane,
+template <typename R, bool COHERENT = false>
+__device__ __forceinline__ void explicitParticle(const FluidView& f, const CouplingView& c, const double* vel,
+                                                 const int* slotNode, const R* slotWeight,
+                                                 const typename Vec4<R>::type* slotU, int i, int lane,
                                                  long long step, int isStep, double* fout, R* reaction, uint32_t* mask,
                                                  double* wall) {
+    // COHERENT: the slots and velocities were written by the same launch (a persistent kernel): loads through L2.
+    typedef typename Vec4<R>::type V;
+    auto slotU_ = [&](long long t) { if constexpr (COHERENT) return loadCoherent(slotU + t); else return loadReadOnly(slotU + t); };
+    auto weight_ = [&](long long t) { if constexpr (COHERENT) return __ldcg(slotWeight + t); else return __ldg(slotWeight + t); };
+    auto node_ = [&](long long t) { if constexpr (COHERENT) return __ldcg(slotNode + t); else return __ldg(slotNode + t); };
+    auto vel_ = [&](int k) { if constexpr (COHERENT) return __ldcg(vel + k); else return __ldg(vel + k); };
     double u[3] = {0, 0, 0};
     for (int s = lane; s < c.slots; s += 32) {
         long long t = (long long) i*c.slots + s;
-        typename Vec4<R>::type su = slotU[t];
+        V su = slotU_(t);
         if (su.w > 0) {
-            double w = (double) slotWeight[t];
+            double w = (double) weight_(t);
             u[0] += (double) su.x*w;
             u[1] += (double) su.y*w;
             u[2] += (double) su.z*w;
@@ -368,7 +391,7 @@ __device__ __forceinline__ void explicitParticle(const FluidView& f, const Coupl
         particleNoise(c.seed, i, step, xi);
     double F[3];
     for (int a = 0; a < 3; a++) {
-        double v = vel[3*i+a]*(1.0/c.velocityScale);
+        double v = vel_(3*i+a)*(1.0/c.velocityScale);
         F[a] = (v - u[a])*(-c.gamma*m);
         if (c.randomForce)
             F[a] += xi[a]*sqrt(2.0*c.gamma*m*c.kT);
@@ -379,9 +402,9 @@ __device__ __forceinline__ void explicitParticle(const FluidView& f, const Coupl
     if (isStep)
         for (int s = lane; s < c.slots; s += 32) {
             long long t = (long long) i*c.slots + s;
-            double w = (double) slotWeight[t];
+            double w = (double) weight_(t);
             if (w != 0.0)
-                addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*F[0], -w*F[1], -w*F[2]);
+                addReaction<R>(f, c, reaction, mask, wall, node_(t), -w*F[0], -w*F[1], -w*F[2]);
         }
 }
 

@@ -320,24 +320,60 @@ __device__ __forceinline__ PairConstants pairConstants(const FluidView& v, int r
 // The collision of the x-adjacent nodes `node` and `node + 1` from their pulled words r (stored units): stores the
 // 19 post-collision words at outPlane + q halfN (word index node/2) and adds the pair's mass and momentum to sums.
 // reactA, reactB flag nodes whose reaction force the coupling left in v.reaction.
+// hi + t as the rounded sum hi and its exact rounding error, added to lo (Knuth's TwoSum: six rounded operations, valid
+// whatever the magnitudes; the packed intrinsics are never re-associated by the compiler).
+__device__ __forceinline__ void twoSumInto(F2& hi, F2& lo, F2 t) {
+    const F2 s = hi + t;
+    const F2 bb = s - hi;
+    lo = lo + ((hi - (s - bb)) + (t - bb));
+    hi = s;
+}
+
+// How the paired kernel carries the momentum in two floats (hi + lo).  In FP32 arithmetic the momentum sums and
+// j + F are rounded every step, and a flow accelerated by a small force drifts by the accumulated rounding (2.5e-4 of
+// u after 20,000 steps of the precision channel, against FP64, in the column emulation tests/channel_column.py and on
+// the GPU): with level 2 the momentum sums and j + F are formed with their rounding errors, and the odd part of every
+// direction adds the errors' share before the rounded momentum (1.6e-5 in the emulation, 2.6e-5 on the GPU).  Level 1
+// compensates j + F only: the decoded values of 16-bit storage are multiples of a coarse quantum, so their momentum
+// sums are exact or nearly so in FP32.  A fluctuating fluid takes level 0: its thermal noise dwarfs the drift, and the
+// extra arithmetic would slow its instruction-bound kernel by 18%.
+#ifndef LBM_COMPENSATED_16BIT
+#define LBM_COMPENSATED_16BIT 1
+#endif
+template <typename T, bool FLUCT> LBM_HD constexpr int compensationLevel() {
+    return FLUCT ? 0 : (sizeof(T) == 4 ? 2 : LBM_COMPENSATED_16BIT);
+}
+
 template <typename T, bool SOLID, bool REACT, bool FLUCT>
 __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& v, const PairConstants& c, int remove,
                                             long long step, unsigned node, bool solidA, bool solidB, bool reactA,
                                             bool reactB, typename PairIO<T>::Word* outPlane, unsigned halfN,
                                             float (&sums)[4]) {
     constexpr bool dithered = sizeof(T) == 2;
-    // Moments (deviations), the storage factors folded into the FMAs.
+    constexpr int level = compensationLevel<T, FLUCT>();
+    constexpr bool comp = level >= 1, compSums = level >= 2;
+    // Moments (deviations), the storage factors folded into the FMAs.  With comp the momentum is summed with its
+    // rounding errors in jxl, jyl, jzl (the terms cx s D are exact: s is a power of two).
     F2 dr = f2(Storage<T>::template scale<0>())*r[0];
     F2 jx = f2(0), jy = f2(0), jz = f2(0), sxx = f2(0), syy = f2(0), szz = f2(0), sxy = f2(0), sxz = f2(0), syz = f2(0);
+    F2 jxl = f2(0), jyl = f2(0), jzl = f2(0);
     staticFor<9>([&](auto pc) {
         constexpr int q = 2*decltype(pc)::value + 1;
         constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
         constexpr float s = Storage<T>::template scale<q>();
         const F2 S = r[q] + r[q+1], D = r[q] - r[q+1];
         dr = fma2(f2(s), S, dr);
-        if (cx != 0) { jx = fma2(f2(cx*s), D, jx); sxx = fma2(f2(s), S, sxx); }
-        if (cy != 0) { jy = fma2(f2(cy*s), D, jy); syy = fma2(f2(s), S, syy); }
-        if (cz != 0) { jz = fma2(f2(cz*s), D, jz); szz = fma2(f2(s), S, szz); }
+        if constexpr (compSums) {
+            // The first term of each component (q = 1, 3, 5) starts the sum exactly.
+            if (cx != 0) { if (q == 1) jx = D*f2(cx*s); else twoSumInto(jx, jxl, D*f2(cx*s)); sxx = fma2(f2(s), S, sxx); }
+            if (cy != 0) { if (q == 3) jy = D*f2(cy*s); else twoSumInto(jy, jyl, D*f2(cy*s)); syy = fma2(f2(s), S, syy); }
+            if (cz != 0) { if (q == 5) jz = D*f2(cz*s); else twoSumInto(jz, jzl, D*f2(cz*s)); szz = fma2(f2(s), S, szz); }
+        }
+        else {
+            if (cx != 0) { jx = fma2(f2(cx*s), D, jx); sxx = fma2(f2(s), S, sxx); }
+            if (cy != 0) { jy = fma2(f2(cy*s), D, jy); syy = fma2(f2(s), S, syy); }
+            if (cz != 0) { jz = fma2(f2(cz*s), D, jz); szz = fma2(f2(s), S, szz); }
+        }
         if (cx*cy != 0) sxy = fma2(f2(cx*cy*s), S, sxy);
         if (cx*cz != 0) sxz = fma2(f2(cx*cz*s), S, sxz);
         if (cy*cz != 0) syz = fma2(f2(cy*cz*s), S, syz);
@@ -351,9 +387,16 @@ __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& 
     const F2 pxx = fma2(jx, jxi, sxx + dr3), pyy = fma2(jy, jyi, syy + dr3), pzz = fma2(jz, jz*ninv, szz + dr3);
     const F2 pxy = fma2(jy, jxi, sxy), pxz = fma2(jz, jxi, sxz), pyz = fma2(jz, jyi, syz);
     if (remove) {
-        jx = fma2(rho, c.nux0, jx);
-        jy = fma2(rho, c.nuy0, jy);
-        jz = fma2(rho, c.nuz0, jz);
+        if constexpr (compSums) {
+            twoSumInto(jx, jxl, rho*c.nux0);
+            twoSumInto(jy, jyl, rho*c.nuy0);
+            twoSumInto(jz, jzl, rho*c.nuz0);
+        }
+        else {
+            jx = fma2(rho, c.nux0, jx);
+            jy = fma2(rho, c.nuy0, jy);
+            jz = fma2(rho, c.nuz0, jz);
+        }
     }
     F2 Fx = rho*c.gx, Fy = rho*c.gy, Fz = rho*c.gz;
     if (REACT) {
@@ -367,7 +410,19 @@ __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& 
     }
     const F2 ux = fma2(Fx, f2(0.5f), jx)*inv, uy = fma2(Fy, f2(0.5f), jy)*inv, uz = fma2(Fz, f2(0.5f), jz)*inv;
     const F2 uu = fma2(uz, uz, fma2(uy, uy, ux*ux)), uf = fma2(uz, Fz, fma2(uy, Fy, ux*Fx));
-    const F2 px = jx + Fx, py = jy + Fy, pz = jz + Fz;
+    // The momentum after the force, p = j + F, and with comp its low part (the rounding error of the sum and that of
+    // the momentum sums).
+    F2 px = jx, py = jy, pz = jz, pxl = jxl, pyl = jyl, pzl = jzl;
+    if constexpr (comp) {
+        twoSumInto(px, pxl, Fx);
+        twoSumInto(py, pyl, Fy);
+        twoSumInto(pz, pzl, Fz);
+    }
+    else {
+        px = jx + Fx;
+        py = jy + Fy;
+        pz = jz + Fz;
+    }
     const F2 s45 = f2(c.om1*4.5f), s9 = f2(c.om1*9.0f);
     F2 qxx = s45*pxx, qyy = s45*pyy, qzz = s45*pzz, qxy = s9*pxy, qxz = s9*pxz, qyz = s9*pyz;
     // Fluctuations: the amplitudes a_k = phi_k r_k/sqrt(b_k) of the 15 non-conserved modes of each node (Philox
@@ -436,10 +491,19 @@ __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& 
             evenRaw = cx*cz > 0 ? Sxz + Pxz : Sxz - Pxz;
         else
             evenRaw = cy*cz > 0 ? Syz + Pyz : Syz - Pyz;
-        // The odd part in stored units, k 3 w c.(j + F) (3 w rounded as oddOf).
+        // The odd part in stored units, k 3 w c.(j + F) (3 w rounded as oddOf); with comp the low parts of j + F come
+        // first in the FMA chain, so that the high parts are added to their contribution and rounded once.
         constexpr float ko = k*oddOf<float>(q);
-        F2 odd;
-        if constexpr (cx != 0) {
+        F2 odd = f2(0.0f);
+        if constexpr (comp) {
+            if constexpr (cx != 0) odd = fma2(pxl, f2(cx*ko), odd);
+            if constexpr (cy != 0) odd = fma2(pyl, f2(cy*ko), odd);
+            if constexpr (cz != 0) odd = fma2(pzl, f2(cz*ko), odd);
+            if constexpr (cx != 0) odd = fma2(px, f2(cx*ko), odd);
+            if constexpr (cy != 0) odd = fma2(py, f2(cy*ko), odd);
+            if constexpr (cz != 0) odd = fma2(pz, f2(cz*ko), odd);
+        }
+        else if constexpr (cx != 0) {
             odd = px*f2(cx*ko);
             if constexpr (cy != 0) odd = fma2(py, f2(cy*ko), odd);
             if constexpr (cz != 0) odd = fma2(pz, f2(cz*ko), odd);

@@ -77,6 +77,8 @@ template <typename T> struct Storage;
 template <> struct Storage<double> {
     template <int q> static LBM_HD constexpr double scale() { return 1.0; }
     template <int q> static __device__ __forceinline__ double raw(const double* p) { return __ldg(p); }
+    // The load of data that the same launch writes (persistent kernels): through L2, never the read-only path.
+    template <int q> static __device__ __forceinline__ double rawCoherent(const double* p) { return __ldcg(p); }
     template <int q> static __device__ __forceinline__ double storeOne(double* p, double v, uint32_t) { *p = v; return v; }
     template <int q> static __device__ __forceinline__ void storePair(double* pa, double* pb, double a, double b, uint32_t,
                                                                       double& ra, double& rb) {
@@ -86,6 +88,7 @@ template <> struct Storage<double> {
 template <> struct Storage<float> {
     template <int q> static LBM_HD constexpr float scale() { return 1.0f; }
     template <int q> static __device__ __forceinline__ float raw(const float* p) { return __ldg(p); }
+    template <int q> static __device__ __forceinline__ float rawCoherent(const float* p) { return __ldcg(p); }
     template <int q> static __device__ __forceinline__ float storeOne(float* p, float v, uint32_t) { *p = v; return v; }
     template <int q> static __device__ __forceinline__ void storePair(float* pa, float* pb, float a, float b, uint32_t,
                                                                       float& ra, float& rb) {

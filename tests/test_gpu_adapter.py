@@ -98,3 +98,26 @@ def test_adapter_checkpoint_restarts_bit_for_bit():
     got = force.getFluidState(context), context.positions.copy()
     context.close()
     assert (got[0] == expected[0]).all() and (got[1] == expected[1]).all()
+
+
+def test_checkpoint_reporter_and_load_continue_bit_for_bit(tmp_path):
+    """saveCheckpoint / loadCheckpoint (python/openmmlbm.i:513-586) and LBMCheckpointReporter on the B200 kernel: a
+    run rebuilt from the reporter's last file continues as the uninterrupted run, bit for bit."""
+    import lbm_b200
+    path = os.path.join(str(tmp_path), 'run.chk')
+    context, force = coupling_case(True, 'Centered', 'Keys', None, {'Precision': 'single'}, temperature=300.0)
+    simulation = lbm_b200.Simulation(context)
+    simulation.reporters.append(lbm_b200.LBMCheckpointReporter(path, 6, force))
+    simulation.step(12)
+    simulation.reporters = []
+    simulation.step(6)
+    expected = force.getFluidState(context), context.positions.copy(), context.velocities.copy()
+    context.close()
+    context, force = coupling_case(True, 'Centered', 'Keys', None, {'Precision': 'single'}, temperature=300.0)
+    lbm_b200.loadCheckpoint(path, context, force)
+    assert context.getStepCount() == 12
+    context.integrator.step(6)
+    got = force.getFluidState(context), context.positions.copy(), context.velocities.copy()
+    context.close()
+    for a, b in zip(expected, got):
+        assert (a == b).all()

@@ -142,25 +142,73 @@ def test_batch_follows_separate_kernels():
     batch.close()
 
 
-def test_graph_replay_equals_direct_launches():
+@pytest.mark.parametrize('persistent', [True, False])
+def test_graph_replay_equals_direct_launches(persistent):
+    """The persistent step runs graph_steps steps per launch: 25 + 15 steps with graphs of 10 steps are two graph
+    replays and two direct launches (the 15 start at an odd step, off the graph's buffer parity), with graphs of 1000
+    steps two direct launches; the seven-kernel form launches 7 kernels per step.  Every way gives the same run."""
     sizes, beads = [16, 20, 12], [30, 50, 10]
     lattices, positions = make_replicas(sizes, beads, seed=7)
     runs = []
     for graph_steps in (10, 1000):
         batch = ReplicaBatch(lattices, beads, np.ones(sum(beads)), np.concatenate(positions),
                              pair=('lj', SIGMA, KT, CUTOFF), precision='double')
+        batch.set_persistent(persistent)
         batch.autotune(graph_steps)
         launches = batch.info()['launches']
         batch.step(25)
         batch.step(15)
         info = batch.info()
-        assert info['steps'] == 40 and info['launches'] - launches == 7*40
+        expected = ({10: 4, 1000: 2}[graph_steps] if persistent else 7*40)
+        assert info['steps'] == 40 and info['launches'] - launches == expected
         runs.append((batch.fluid_state(1), batch.particles_state()[1]))
         batch.close()
     (state_a, vel_a), (state_b, vel_b) = runs
     # The reactions of beads that share a node are added with atomics, in any order.
     assert abs(state_a - state_b).max() <= 1e-12*abs(state_a).max()
     assert abs(vel_a - vel_b).max() <= 1e-12*abs(vel_a).max()
+
+
+@pytest.mark.parametrize('precision', ['double', 'single'])
+def test_persistent_step_equals_phase_kernels(precision):
+    """The persistent step (phases separated by grid barriers, per-replica sums by the last block of each replica,
+    double-buffered reactions) computes what the seven phase kernels compute (reactions summed with atomics in any
+    order: 1e-12 in FP64, 1e-6 in FP32, over 30 steps of the chaotic bead dynamics)."""
+    sizes, beads = [12, 17, 14, 9], [25, 40, 30, 6]
+    lattices, positions = make_replicas(sizes, beads, seed=13)
+    runs = []
+    for persistent in (True, False):
+        batch = ReplicaBatch(lattices, beads, np.ones(sum(beads)), np.concatenate(positions),
+                             pair=('lj', SIGMA, KT, CUTOFF), precision=precision)
+        batch.set_persistent(persistent)
+        batch.autotune(10)
+        batch.step(30)
+        runs.append([batch.fluid_state(r) for r in range(len(sizes))] + list(batch.particles_state()))
+        batch.close()
+    tol = 1e-12 if precision == 'double' else 1e-6
+    for a, b in zip(*runs):
+        assert abs(a - b).max() <= tol*abs(a).max()
+
+
+def test_persistent_barrier_timeout_is_reported():
+    """A poll limit of one makes the blocks that wait at a grid barrier of the persistent step give up: the launch
+    stops, the next synchronizing call reports LBM_ERR_DEVICE_TIMEOUT, and with the default limit the batch steps
+    again (the fluid temperature of every replica stays finite)."""
+    from lbm_b200.abi import LBM_ERR_DEVICE_TIMEOUT, LbmError
+    sizes, beads = [16, 20, 12], [30, 50, 10]
+    lattices, positions = make_replicas(sizes, beads, seed=5)
+    batch = ReplicaBatch(lattices, beads, np.ones(sum(beads)), np.concatenate(positions),
+                         pair=('lj', SIGMA, KT, CUTOFF), precision='single')
+    batch.set_barrier_polls(1)
+    batch.step(4)
+    with pytest.raises(LbmError) as failure:
+        batch.particles_state()
+    assert failure.value.status == LBM_ERR_DEVICE_TIMEOUT
+    batch.set_barrier_polls(0)
+    batch.step(6)
+    fluid, _ = batch.temperatures()
+    batch.close()
+    assert np.isfinite(fluid).all()
 
 
 @pytest.mark.parametrize('precision', ['single', 'double'])
