@@ -2,7 +2,8 @@
 stream-collide kernel.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload coupled|fluid|channel|batch] [--precision double|single|half|bfloat16] [--size EDGE]
+                    [--workload coupled|fluid|channel|batch|warmstart] [--precision double|single|half|bfloat16]
+                    [--size EDGE]
                     [--graph-steps G] [--replicas R] [--separate]
 
 Workload "coupled" (default, the scale configuration): a 256^3 periodic fluctuating D3Q19 fluid (tau 0.6, kT 1e-4 in
@@ -14,7 +15,10 @@ fluid) and the leapfrog of the beads, all on the device.  "fluid": the fluid alo
 precision configuration, a 384x384x192 Poiseuille channel between bounce-back planes (g_x 5e-7, tau 0.55), for the
 MLUPS of each storage format.  "batch": the batching configuration, 256 periodic fluctuating replicas of uneven sizes
 with Lennard-Jones beads, every phase one launch over all replicas, G steps per CUDA graph (--separate also times the
-replicas as separate kernels).
+replicas as separate kernels).  The default run also reports the plain fluid of the same lattice ("plain_fluid") and,
+when openmm-lbm_b200/warmstart_net/weights.pt exists, the metric's time-to-steady part ("warm_start": held-out obstacle
+channels solved to the residual 1e-6 from rest and from the learned warm start); "warmstart" runs that alone, on
+--steps channels.
 
 value = fluid nodes x steps / device time (MLUPS).  e2e = the same metric through the C ABI with the beads' positions
 and velocities in pinned host memory: copied to the device before and back after every step.  With N > 1 (torchrun,
@@ -534,6 +538,30 @@ def plain_fluid_record(args, w, rank, world, device):
             'gpu_launches': r['gpu_launches'], 'clocks': r['clocks']}
 
 
+WARMSTART_WEIGHTS = os.path.join(PACKAGE, 'warmstart_net', 'weights.pt')
+
+
+def warm_start_record(cases, first_seed=300001):
+    """The metric's time-to-steady part: `cases` obstacle channels (128x64x64, seeds the network never saw) solved to
+    the steady residual 1e-6 from rest and from the learned warm start (openmm-lbm_b200/warmstart_net/weights.pt), one
+    solve at a time; value = total cold wall time / total warm wall time (the prediction included)."""
+    load_package()
+    from lbm_b200 import warmstart
+    net = warmstart.load_network(WARMSTART_WEIGHTS)
+    rows = warmstart.time_to_steady(net, list(range(first_seed, first_seed + cases)))
+    cold = sum(r['cold_seconds'] for r in rows)
+    warm = sum(r['warm_seconds'] for r in rows)
+    return {'metric': 'time to steady state (residual 1e-6) from rest / from the learned warm start',
+            'value': cold/warm, 'unit': 'x', 'cases': len(rows),
+            'workload': '128x64x64 obstacle channel, 5-20 spheres of radius 4-10, Velocity inlet 0.02, Density outlet, '
+                        'tau 0.6, FP32 (held-out seeds %d..%d)' % (first_seed, first_seed + cases - 1),
+            'cold_seconds_mean': cold/len(rows), 'warm_seconds_mean': warm/len(rows),
+            'cold_steps_mean': float(np.mean([r['cold_steps'] for r in rows])),
+            'warm_steps_mean': float(np.mean([r['warm_steps'] for r in rows])),
+            'speedup_per_case': [round(r['speedup'], 3) for r in rows],
+            'final_velocity_error_max': float(max(r['final_velocity_error'] for r in rows))}
+
+
 def host_description():
     """The host's logical core count and CPU model (the CPU baseline runs on one of these cores)."""
     model = 'unknown'
@@ -667,7 +695,7 @@ def main():
     parser.add_argument('--steps', type=int, default=30)
     parser.add_argument('--warmup', type=int, default=5)
     parser.add_argument('--impl', default='b200', choices=['b200', 'reference'])
-    parser.add_argument('--workload', default='coupled', choices=['coupled', 'fluid', 'channel', 'batch'])
+    parser.add_argument('--workload', default='coupled', choices=['coupled', 'fluid', 'channel', 'batch', 'warmstart'])
     parser.add_argument('--precision', default='single', choices=list(STORAGE_BYTES))
     parser.add_argument('--size', type=int, default=0, help='lattice edge in x (smaller cases for profiling)')
     parser.add_argument('--no-fluctuations', action='store_true')
@@ -676,6 +704,8 @@ def main():
                         help='skip the fluid and bead temperatures after the run')
     parser.add_argument('--no-plain-fluid', action='store_true',
                         help='skip the record of the plain fluid (no particles, no fluctuations) of the same size')
+    parser.add_argument('--warm-start-cases', type=int, default=4,
+                        help='held-out channels of the time-to-steady record (0: none)')
     parser.add_argument('--graph-steps', type=int, default=10, help='batch: lattice steps per CUDA graph')
     parser.add_argument('--replicas', type=int, default=256, help='batch: number of replicas')
     parser.add_argument('--separate', action='store_true', help='batch: also time the replicas as separate kernels')
@@ -684,6 +714,14 @@ def main():
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     local = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.workload == 'warmstart':
+        # The learned warm start alone: time to the steady residual from rest and from the network's prediction.
+        if rank == 0:
+            record = warm_start_record(max(1, args.steps))
+            record.update({'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup, 'higher_is_better': True,
+                           'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic obstacle channels'})
+            print(json.dumps(record))
+        return
     if args.workload == 'channel':
         base = ChannelWorkload()
     elif args.workload == 'batch':
@@ -738,6 +776,8 @@ def main():
         result = run_b200(args, w, rank, world, local)
         if args.workload == 'coupled' and not args.no_plain_fluid:
             result['plain_fluid'] = plain_fluid_record(args, w, rank, world, local)
+        if args.workload == 'coupled' and rank == 0 and args.warm_start_cases > 0 and os.path.exists(WARMSTART_WEIGHTS):
+            result['warm_start'] = warm_start_record(args.warm_start_cases)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != 'batch':
         sample = w.sample(min(w.shape[0], 128))
         value, kind, dt = run_cpu(args, sample, 2, 1)

@@ -323,16 +323,19 @@ __global__ void batchGatherKernel(const T* __restrict__ A, FluidView f, double* 
 // The persistent step: `steps` lattice steps of every replica in one cooperative launch (every block resident), the
 // phases of a step separated by bounded grid barriers (grid_barrier.cuh):
 //
-//   phase 1  bead pair forces (blocks over replicas), stencil slots of every bead (threads over slots), and the clear
-//            of the reactions of the previous step (their slot nodes are kept in the other half of slotNode)
-//   phase 2  explicit drag of every bead and its reaction on the fluid (warps over beads), then the bead's leapfrog
-//   phase 3  the dense step of every replica (work items of BT nodes); the last block to finish a replica's items
-//            reduces its per-warp sums in a fixed order (the mass, momentum and removal velocity of the next step)
+//   phase 1  the sums of the previous step per replica (blocks over replicas: mass, momentum and the velocity that this
+//            step's momentum removal subtracts), bead pair forces (blocks over replicas), stencil slots of every bead
+//            (threads over slots) with the nodes' j/rho before the removal, and the clear of the previous step's
+//            reactions (their slot nodes are kept in the other half of slotNode)
+//   phase 2  explicit drag of every bead (the removal applied to the interpolated velocity: sum w (j/rho - ucm) =
+//            sum w j/rho - ucm sum w) and its reaction on the fluid (warps over beads), then the bead's leapfrog
+//   phase 3  the dense step of every replica (work items of BT nodes), per-warp partial sums
 //
+// After the last step a final phase forms the last step's sums, so that the statistics are complete between launches.
 // The reaction buffers and slot nodes alternate between steps (buffer step & 1), so that the clear of step s - 1 and
-// the slots of step s share phase 1.  A replica computes what the seven-kernel step computes, in the same order of
-// floating-point operations.  A barrier that times out sets LBM_ERR_DEVICE_TIMEOUT in the status word and every
-// block leaves the launch.
+// the slots of step s share phase 1.  A replica computes what the seven-kernel step computes, up to the rounding of
+// the removal's form.  A barrier that times out sets LBM_ERR_DEVICE_TIMEOUT in the status word and every block leaves
+// the launch.
 // ------------------------------------------------------------------------------------------------------------------
 
 struct PersistentArgs {
@@ -346,7 +349,6 @@ struct PersistentArgs {
     void* pop[2];                  // populations: the launch starts from pop[cur]
     int cur;
     double* partials;              // 4 per warp of every item
-    int* replicaDone;              // items of the current step finished, per replica
     BatchClock* clock;
     double *pos, *vel, *fpair, *fdrag, *invMass, *wall;
     int* slotNode[2];
@@ -385,7 +387,6 @@ __device__ __forceinline__ void finishReplica(const PersistentArgs& a, int r, in
             st->momentum[k] = total[1+k];
             st->ucm[k] = total[1+k]/mass;
         }
-        a.replicaDone[r] = 0;
     }
     __syncthreads();
 }
@@ -394,7 +395,6 @@ template <typename T, typename R, bool FLUCT, int BT>
 __global__ void __launch_bounds__(BT, batchMinBlocks<R, BT>())
 batchPersistentKernel(PersistentArgs a) {
     typedef typename Vec4<R>::type V;
-    __shared__ int lastShared;
     const int lane = threadIdx.x%32, warp = threadIdx.x/32;
     const long long step0 = a.clock->step;
     const long long totalSlots = (long long) a.totalParticles*a.slots;
@@ -408,8 +408,11 @@ batchPersistentKernel(PersistentArgs a) {
         const FluidView* views = a.views[buf];
         const T* A = (const T*) a.pop[(a.cur + s) & 1];
         T* B = (T*) a.pop[(a.cur + s + 1) & 1];
+        // Phase 1.  The sums of the previous step (those of the launch's first step are complete already).
+        if (s > 0)
+            for (int r = blockIdx.x; r < a.numReplicas; r += gridDim.x)
+                finishReplica(a, r, BT/32);
         if (a.coupled) {
-            // Phase 1: pair forces, stencil slots, clear of the previous step's reactions.
             for (int r = blockIdx.x; r < a.numReplicas; r += gridDim.x) {
                 const ReplicaTable& rt = a.table[r];
                 const double* x = a.pos + 3*(size_t) rt.firstParticle;
@@ -422,7 +425,7 @@ batchPersistentKernel(PersistentArgs a) {
                                 continue;
                             double d[3];
                             for (int k = 0; k < 3; k++) {
-                                d[k] = x[3*i+k] - x[3*j+k];
+                                d[k] = __ldcg(&x[3*i+k]) - __ldcg(&x[3*j+k]);
                                 d[k] -= rt.box[k]*rint(d[k]/rt.box[k]);
                             }
                             double r2 = d[0]*d[0] + d[1]*d[1] + d[2]*d[2];
@@ -445,35 +448,40 @@ batchPersistentKernel(PersistentArgs a) {
                 const int r = a.particleReplica[p];
                 const ReplicaTable& rt = a.table[r];
                 const int p0 = rt.firstParticle, i = p - p0;
-                const int remove = rt.removeFrequency > 0 && step%rt.removeFrequency == 0;
                 const size_t so = (size_t) p0*a.slots;
                 // The clear of slot t of the previous step (reaction buffer 1 - buf).
                 const FluidView& of = oldViews[r];
-                const long long node = oldNodes[t];
+                const long long node = __ldcg(&oldNodes[t]);
                 R* reaction = (R*) const_cast<void*>(of.reaction);
                 *reinterpret_cast<V*>(reaction + 4*node) = Vec4<R>::make(0, 0, 0, 0);
                 const long long row = node/of.nx;
                 const int xx = (int) (node - row*of.nx);
                 const_cast<uint32_t*>(of.reactMask)[row*of.wordsPerRow + xx/32] = 0u;
+                // The slot with the nodes' j/rho before the removal (applied in phase 2).
                 stencilSlot<T, R, true>(A + (size_t) 19*rt.nodeOffset, views[r], a.cviews[r], a.pos + 3*(size_t) p0,
-                                  (long long) i*a.slots + sl, remove, 0, nodes + so, slotWeight + so, slotU + so);
+                                        (long long) i*a.slots + sl, 0, 0, nodes + so, slotWeight + so, slotU + so);
             }
-            if (!gridSync(a.barrier, a.status, a.pollLimit))
-                return;
+        }
+        if (!gridSync(a.barrier, a.status, a.pollLimit))
+            return;
+        if (a.coupled) {
             // Phase 2: explicit drag and reaction, then the leapfrog of the bead (v += dt F/m, x += dt v).
+            int* nodes = a.slotNode[buf];
             for (int p = firstWarp; p < a.totalParticles; p += warps) {
                 const int r = a.particleReplica[p];
                 const ReplicaTable& rt = a.table[r];
                 const FluidView& f = views[r];
                 const int p0 = rt.firstParticle;
                 const size_t so = (size_t) p0*a.slots;
-                explicitParticle<R, true>(f, a.cviews[r], a.vel + 3*(size_t) p0, nodes + so, slotWeight + so, slotU + so, p - p0,
-                                    lane, step, 1, a.fdrag + 3*(size_t) p0, (R*) const_cast<void*>(f.reaction),
-                                    const_cast<uint32_t*>(f.reactMask), a.wall);
+                const bool remove = rt.removeFrequency > 0 && step%rt.removeFrequency == 0;
+                explicitParticle<R, true>(f, a.cviews[r], a.vel + 3*(size_t) p0, nodes + so, slotWeight + so, slotU + so,
+                                          p - p0, lane, step, 1, a.fdrag + 3*(size_t) p0,
+                                          (R*) const_cast<void*>(f.reaction), const_cast<uint32_t*>(f.reactMask), a.wall,
+                                          remove ? f.stats->ucm : nullptr);
                 __syncwarp();
                 if (lane < 3) {
                     const size_t k = 3*(size_t) p + lane;
-                    const double force = a.fpair[k] + a.fdrag[k];
+                    const double force = __ldcg(&a.fpair[k]) + a.fdrag[k];
                     const double v = a.vel[k] + rt.dt*force*a.invMass[p];
                     a.vel[k] = v;
                     a.pos[k] += rt.dt*v;
@@ -482,13 +490,15 @@ batchPersistentKernel(PersistentArgs a) {
             if (!gridSync(a.barrier, a.status, a.pollLimit))
                 return;
         }
-        // Phase 3: the dense step; the last block of a replica reduces its sums.
+        // Phase 3: the dense step, per-warp partial sums (formed into the replica's sums in the next phase 1).
         for (int w = blockIdx.x; w < a.numItems; w += gridDim.x) {
             const int r = a.itemReplica[w];
             const FluidView& v = views[r];
             const ReplicaTable& rt = a.table[r];
             const int remove = rt.removeFrequency > 0 && step%rt.removeFrequency == 0;
-            const CollideConstants<R> k = collideConstants<R>(v.omega, v.g, v.stats->ucm, remove, v.mu, v.seed);
+            // The removal velocity of this step, written by phase 1 of this launch: read through L2.
+            const double ucm[3] = {__ldcg(&v.stats->ucm[0]), __ldcg(&v.stats->ucm[1]), __ldcg(&v.stats->ucm[2])};
+            const CollideConstants<R> k = collideConstants<R>(v.omega, v.g, ucm, remove, v.mu, v.seed);
             const unsigned N = rt.numNodes;
             const unsigned local = (unsigned) (w - rt.firstItem)*BT + threadIdx.x;
             R sm = 0, sx = 0, sy = 0, sz = 0;
@@ -516,20 +526,14 @@ batchPersistentKernel(PersistentArgs a) {
             if (lane == 0) {
                 double* out = a.partials + 4*((size_t) w*(BT/32) + warp);
                 out[0] = s0; out[1] = s1; out[2] = s2; out[3] = s3;
-                __threadfence();
-            }
-            __syncthreads();
-            if (threadIdx.x == 0)
-                lastShared = atomicAdd(&a.replicaDone[r], 1) == rt.numItems - 1;
-            __syncthreads();
-            if (lastShared) {
-                __threadfence();
-                finishReplica(a, r, BT/32);
             }
         }
         if (!gridSync(a.barrier, a.status, a.pollLimit))
             return;
     }
+    // The sums of the last step.
+    for (int r = blockIdx.x; r < a.numReplicas; r += gridDim.x)
+        finishReplica(a, r, BT/32);
     if (blockIdx.x == 0 && threadIdx.x == 0)
         a.clock->step = step0 + a.steps;
 }
@@ -602,7 +606,6 @@ private:
     // (buffer step & 1), viewsDev holds the replicas' views for both, and the grid barrier its counter and status.
     bool persistent;
     unsigned maskWordsTotal;
-    int* replicaDoneDev;
     unsigned* barrierDev;
     int* statusDev;
     long long barrierPolls;
@@ -617,8 +620,7 @@ BatchEngine::BatchEngine(int nr, const LbmLatticeParameters* ls, const int* np, 
           reactionDev(nullptr), maskDev(nullptr), particleReplicaDev(nullptr), posDev(nullptr), velDev(nullptr),
           fpairDev(nullptr), fdragDev(nullptr), invMassDev(nullptr), massDev(nullptr), cellMassDev(nullptr),
           wallDev(nullptr), cellEnergyDev(nullptr), slotNodeDev(nullptr), slotWeightDev(nullptr), slotUDev(nullptr),
-          graphExec(nullptr), graphCur(0), persistent(true), maskWordsTotal(0), replicaDoneDev(nullptr),
-          barrierDev(nullptr), statusDev(nullptr), barrierPolls(1LL << 26) {
+          graphExec(nullptr), graphCur(0), persistent(true), maskWordsTotal(0), barrierDev(nullptr), statusDev(nullptr), barrierPolls(1LL << 26) {
     pop[0] = pop[1] = nullptr;
     if (nr <= 0 || ls == nullptr || np == nullptr)
         throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_batch_create: no replicas");
@@ -704,8 +706,6 @@ BatchEngine::BatchEngine(int nr, const LbmLatticeParameters* ls, const int* np, 
             CUDA_CHECK(cudaMalloc(&maskDev, 2*sizeof(uint32_t)*(size_t) maskWords));
             CUDA_CHECK(cudaMemsetAsync(maskDev, 0, 2*sizeof(uint32_t)*(size_t) maskWords, stream));
         }
-        CUDA_CHECK(cudaMalloc(&replicaDoneDev, sizeof(int)*nr));
-        CUDA_CHECK(cudaMemsetAsync(replicaDoneDev, 0, sizeof(int)*nr, stream));
         CUDA_CHECK(cudaMalloc(&statusDev, sizeof(int)*2));
         CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*2, stream));
         barrierDev = reinterpret_cast<unsigned*>(statusDev + 1);
@@ -816,7 +816,7 @@ void BatchEngine::release() {
     releaseGraph();
     void* ptrs[] = {pop[0], pop[1], viewsDev, cviewsDev, tableDev, statsDev, clockDev, itemReplicaDev, partialsDev,
                     reactionDev, maskDev, particleReplicaDev, posDev, velDev, fpairDev, fdragDev, invMassDev, massDev,
-                    cellMassDev, wallDev, cellEnergyDev, slotNodeDev, slotWeightDev, slotUDev, replicaDoneDev, statusDev};
+                    cellMassDev, wallDev, cellEnergyDev, slotNodeDev, slotWeightDev, slotUDev, statusDev};
     for (void* p : ptrs)
         cudaFree(p);
     pop[0] = pop[1] = nullptr;
@@ -824,7 +824,7 @@ void BatchEngine::release() {
     itemReplicaDev = nullptr; partialsDev = nullptr; reactionDev = nullptr; maskDev = nullptr; particleReplicaDev = nullptr;
     posDev = velDev = fpairDev = fdragDev = invMassDev = massDev = cellMassDev = wallDev = cellEnergyDev = nullptr;
     slotNodeDev = nullptr; slotWeightDev = slotUDev = nullptr;
-    replicaDoneDev = nullptr; statusDev = nullptr; barrierDev = nullptr;
+    statusDev = nullptr; barrierDev = nullptr;
     if (ownStream && stream)
         cudaStreamDestroy(stream);
     stream = nullptr;
@@ -956,7 +956,6 @@ void BatchEngine::launchPersistent(int steps) {
     a.pop[1] = pop[1];
     a.cur = cur;
     a.partials = partialsDev;
-    a.replicaDone = replicaDoneDev;
     a.clock = clockDev;
     a.pos = posDev; a.vel = velDev; a.fpair = fpairDev; a.fdrag = fdragDev; a.invMass = invMassDev; a.wall = wallDev;
     a.slotNode[0] = slotNodeDev;
@@ -992,10 +991,9 @@ void BatchEngine::checkStatus() {
     CUDA_CHECK(cudaMemcpyAsync(&status, statusDev, sizeof(int), cudaMemcpyDeviceToHost, stream));
     CUDA_CHECK(cudaStreamSynchronize(stream));
     if (status != 0) {
-        // The blocks left the launch at different points: the item counters of the per-replica sums and the reaction
-        // buffers may hold partial values.  Clear them, so that later steps start from a consistent state.
+        // The blocks left the launch at different points: the reaction buffers may hold partial values.  Clear them,
+        // so that later steps start from a consistent state.
         CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int), stream));
-        CUDA_CHECK(cudaMemsetAsync(replicaDoneDev, 0, sizeof(int)*numReplicas, stream));
         if (coupled) {
             size_t e = storage == LBM_STORAGE_F64 ? 8 : 4;
             CUDA_CHECK(cudaMemsetAsync(reactionDev, 0, 2*4*e*(size_t) totalNodes, stream));

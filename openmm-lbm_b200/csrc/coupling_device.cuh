@@ -365,14 +365,17 @@ __device__ __forceinline__ void explicitParticle(const FluidView& f, const Coupl
                                                  const int* slotNode, const R* slotWeight,
                                                  const typename Vec4<R>::type* slotU, int i, int lane,
                                                  long long step, int isStep, double* fout, R* reaction, uint32_t* mask,
-                                                 double* wall) {
+                                                 double* wall, const double* removal = nullptr) {
     // COHERENT: the slots and velocities were written by the same launch (a persistent kernel): loads through L2.
+    // removal: the velocity that this step's momentum removal subtracts from every node, where the slots hold the
+    // nodes' j/rho before the removal (the persistent batch step); (j - rho ucm)/rho = j/rho - ucm, so the fluid
+    // velocity at the particle is sum w j/rho - ucm sum w over the fluid slots.
     typedef typename Vec4<R>::type V;
     auto slotU_ = [&](long long t) { if constexpr (COHERENT) return loadCoherent(slotU + t); else return loadReadOnly(slotU + t); };
     auto weight_ = [&](long long t) { if constexpr (COHERENT) return __ldcg(slotWeight + t); else return __ldg(slotWeight + t); };
     auto node_ = [&](long long t) { if constexpr (COHERENT) return __ldcg(slotNode + t); else return __ldg(slotNode + t); };
     auto vel_ = [&](int k) { if constexpr (COHERENT) return __ldcg(vel + k); else return __ldg(vel + k); };
-    double u[3] = {0, 0, 0};
+    double u[3] = {0, 0, 0}, wsum = 0;
     for (int s = lane; s < c.slots; s += 32) {
         long long t = (long long) i*c.slots + s;
         V su = slotU_(t);
@@ -381,10 +384,16 @@ __device__ __forceinline__ void explicitParticle(const FluidView& f, const Coupl
             u[0] += (double) su.x*w;
             u[1] += (double) su.y*w;
             u[2] += (double) su.z*w;
+            wsum += w;
         }
     }
     for (int a = 0; a < 3; a++)
         u[a] = warpSum(u[a]);
+    if (removal != nullptr) {
+        wsum = warpSum(wsum);
+        for (int a = 0; a < 3; a++)
+            u[a] -= __ldcg(&removal[a])*wsum;
+    }
     double m = c.mass[i];
     double xi[3] = {0, 0, 0};
     if (c.randomForce)

@@ -1,9 +1,10 @@
 // Bead dynamics on the device (include/lbm_b200_md.h): the forces and the leapfrog integrator that OpenMM would
 // provide around the LBM force kernel in the benchmark configurations.  Harmonic bonds, and WCA or truncated
 // Lennard-Jones pairs found with a cell list: particles are binned by cell with atomics into fixed-capacity bins,
-// and each particle visits the 27 cells around its own, taking each cell's particles in index order (so every
-// force is summed in one order); a cell over its capacity is scanned over all particles instead (a brute-force pass
-// serves boxes with fewer than 3 cells along an axis).
+// and one warp per particle visits the 27 cells around its own (a lane per cell, taking the cell's particles in index
+// order, and a lane for the bonds), the lanes' forces summed by a fixed shuffle tree (so every force is summed in one
+// order); a cell over its capacity is scanned over all particles instead (a brute-force pass serves boxes with fewer
+// than 3 cells along an axis).
 #include "lbm_internal.h"
 #include "lbm_b200_md.h"
 #include <algorithm>
@@ -21,6 +22,7 @@ namespace {
 struct MdView {
     int n;
     double box[3];
+    double invBox[3];
     int ncell[3];
     double cellSize[3];
     double k, r0;
@@ -37,9 +39,11 @@ struct MdView {
 
 constexpr int kMaxBinCapacity = 16;
 
+// Minimum image.  d/box is taken as d*(1/box): the two differ by an ulp at most, which can move rint() only for a
+// separation of half a box, far beyond every cutoff and bond length (the box holds at least 3 cells of the cutoff).
 __device__ __forceinline__ void minimumImage(const MdView& v, double d[3]) {
     for (int a = 0; a < 3; a++)
-        d[a] -= v.box[a]*rint(d[a]/v.box[a]);
+        d[a] -= v.box[a]*rint(d[a]*v.invBox[a]);
 }
 
 __device__ __forceinline__ int cellOf(const MdView& v, const double* x, int a) {
@@ -104,44 +108,47 @@ __device__ __forceinline__ void pairWith(const MdView& v, const double* pos, int
     pairForce(v, d, f);
 }
 
-__global__ void cellForceKernel(MdView v, const double* pos, double* forces) {
-    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < v.n; i += gridDim.x*blockDim.x) {
+// The same forces with one warp per particle, for latency: lane c < 27 takes the neighbouring cell c (its members in
+// index order), lane 27 the bonds, and the lanes' forces are summed by a fixed shuffle tree.
+__global__ void __launch_bounds__(256) cellForceWarpKernel(MdView v, const double* pos, double* forces) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x*blockDim.x) >> 5;
+    for (int i = (blockIdx.x*blockDim.x + threadIdx.x) >> 5; i < v.n; i += warps) {
         double f[3] = {0, 0, 0};
-        bondForces(v, pos, i, f);
-        if (v.pairType != LBM_PAIR_NONE) {
-            const double* x = &pos[3*i];
-            int c[3] = {cellOf(v, x, 0), cellOf(v, x, 1), cellOf(v, x, 2)};
-            for (int dz = -1; dz <= 1; dz++)
-                for (int dy = -1; dy <= 1; dy++)
-                    for (int dx = -1; dx <= 1; dx++) {
-                        int cx = (c[0] + dx + v.ncell[0])%v.ncell[0];
-                        int cy = (c[1] + dy + v.ncell[1])%v.ncell[1];
-                        int cz = (c[2] + dz + v.ncell[2])%v.ncell[2];
-                        unsigned cell = (unsigned) (cx + v.ncell[0]*(cy + v.ncell[1]*cz));
-                        const int count = (int) v.binCount[cell];
-                        if (count <= v.binCapacity) {
-                            // The cell's particles in index order (insertion sort of at most kMaxBinCapacity).
-                            int member[kMaxBinCapacity];
-                            for (int e = 0; e < count; e++) {
-                                int j = v.bins[(size_t) cell*v.binCapacity + e], p = e;
-                                while (p > 0 && member[p-1] > j) {
-                                    member[p] = member[p-1];
-                                    p--;
-                                }
-                                member[p] = j;
-                            }
-                            for (int e = 0; e < count; e++)
-                                pairWith(v, pos, i, x, member[e], f);
-                        }
-                        else
-                            // Over capacity: every particle of the cell, found by scanning them all in index order.
-                            for (int j = 0; j < v.n; j++)
-                                if (v.cellKey[j] == cell)
-                                    pairWith(v, pos, i, x, j, f);
+        const double x[3] = {pos[3*i], pos[3*i+1], pos[3*i+2]};
+        if (lane == 27)
+            bondForces(v, pos, i, f);
+        else if (lane < 27 && v.pairType != LBM_PAIR_NONE) {
+            const int c[3] = {cellOf(v, x, 0), cellOf(v, x, 1), cellOf(v, x, 2)};
+            const int cx = (c[0] + lane%3 - 1 + v.ncell[0])%v.ncell[0];
+            const int cy = (c[1] + (lane/3)%3 - 1 + v.ncell[1])%v.ncell[1];
+            const int cz = (c[2] + lane/9 - 1 + v.ncell[2])%v.ncell[2];
+            const unsigned cell = (unsigned) (cx + v.ncell[0]*(cy + v.ncell[1]*cz));
+            const int count = (int) v.binCount[cell];
+            if (count <= v.binCapacity) {
+                int member[kMaxBinCapacity];
+                for (int e = 0; e < count; e++) {
+                    int j = v.bins[(size_t) cell*v.binCapacity + e], p = e;
+                    while (p > 0 && member[p-1] > j) {
+                        member[p] = member[p-1];
+                        p--;
                     }
+                    member[p] = j;
+                }
+                for (int e = 0; e < count; e++)
+                    pairWith(v, pos, i, x, member[e], f);
+            }
+            else
+                for (int j = 0; j < v.n; j++)
+                    if (v.cellKey[j] == cell)
+                        pairWith(v, pos, i, x, j, f);
         }
         for (int a = 0; a < 3; a++)
-            forces[3*i+a] = f[a];
+            for (int o = 16; o > 0; o >>= 1)
+                f[a] += __shfl_down_sync(0xffffffffu, f[a], o);
+        if (lane == 0)
+            for (int a = 0; a < 3; a++)
+                forces[3*i+a] = f[a];
     }
 }
 
@@ -217,8 +224,10 @@ struct MdEngine {
         CUDA_CHECK(cudaSetDevice(device));
         view = MdView();
         view.n = n;
-        for (int a = 0; a < 3; a++)
+        for (int a = 0; a < 3; a++) {
             view.box[a] = box[a];
+            view.invBox[a] = 1.0/box[a];
+        }
         view.k = k;
         view.r0 = r0;
         view.pairType = pairType;
@@ -318,7 +327,7 @@ struct MdEngine {
             return;
         }
         binKernel<<<gridFor(n), 256, 0, s>>>(view, pos, cellKey, binCount, bins);
-        cellForceKernel<<<gridFor(n), 256, 0, s>>>(view, pos, out);
+        cellForceWarpKernel<<<gridFor(32LL*n), 256, 0, s>>>(view, pos, out);
         // Empty the occupied bins, so that the next call starts from empty cells.
         clearBinsKernel<<<gridFor(n), 256, 0, s>>>(n, cellKey, binCount);
         CUDA_CHECK(cudaGetLastError());

@@ -12,7 +12,8 @@ spheres of radius U[4, 10] with centres uniform in the interior (x in [12, nx - 
 cross-section), all in lattice units.  Network input channels: the solid mask, the inlet velocity / 0.02, and the
 coordinates x/nx, y/ny, z/nz (zero padding to 8); outputs: u/u_in and (rho - 1)/rho_scale.
 
-    python openmm-lbm_b200/warmstart_experiment.py --train 2000 --test 200 --epochs 8 --out report.json
+The network that bench.py's time-to-steady measurement loads is trained by openmm-lbm_b200/warmstart_net/train.py,
+which writes it beside itself (weights.pt).
 """
 import argparse
 import ctypes
@@ -397,6 +398,37 @@ def conv_benchmark(shape=(128, 64, 64), widths=(16, 32, 64, 160), batch=2, repea
     return rows
 
 
+def save_network(net, path):
+    """The network's weights (BF16, the precision the convolutions use), biases, output standardisation and widths."""
+    torch.save({'widths': list(net.widths),
+                'weights': [w.detach().to(torch.bfloat16).cpu() for w in net.weights],
+                'biases': [b.detach().float().cpu() for b in net.biases],
+                'rho_scale': float(net.rho_scale), 'out_mean': net.out_mean.cpu(), 'out_std': net.out_std.cpu()}, path)
+
+
+def load_network(path):
+    """A WarmStartNet on the GPU with the weights that save_network wrote."""
+    data = torch.load(path, map_location='cpu')
+    net = WarmStartNet(widths=tuple(data['widths']))
+    with torch.no_grad():
+        for p, w in zip(net.weights, data['weights']):
+            p.copy_(w.float())
+        for p, b in zip(net.biases, data['biases']):
+            p.copy_(b)
+        net.rho_scale.fill_(data['rho_scale'])
+        net.out_mean.copy_(data['out_mean'])
+        net.out_std.copy_(data['out_std'])
+    return net.cuda()
+
+
+def time_to_steady(net, seeds, shape=(128, 64, 64), inlet=0.02, tolerance=1e-6, radius=(4.0, 10.0)):
+    """Held-out channels solved to the steady residual `tolerance` from rest and from the network's prediction, one
+    after the other: per case the wall time (the prediction included) and the steps of each, and the warm solve's
+    final velocity error against the cold one."""
+    cases = solve_cases(seeds, shape, inlet, float(net.rho_scale), threads=1, tolerance=tolerance, radius=radius)
+    return evaluate(net, cases, shape, inlet, tolerance=tolerance)
+
+
 def main(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument('--train', type=int, default=2000)
@@ -408,6 +440,8 @@ def main(argv=None):
     p.add_argument('--threads', type=int, default=4, help='concurrent solves of the training data')
     p.add_argument('--radius', default='4,10', help='sphere radii range')
     p.add_argument('--out', default='warmstart_report.json')
+    p.add_argument('--save', default='', help='write the trained network (save_network) to this path')
+    p.add_argument('--no-conv-benchmark', action='store_true')
     args = p.parse_args(argv)
     shape = tuple(int(a) for a in args.shape.split('x'))
     inlet = 0.02
@@ -426,6 +460,8 @@ def main(argv=None):
     t1 = time.perf_counter()
     history = train(net, train_cases, args.epochs, args.batch, log=log)
     t_train = time.perf_counter() - t1
+    if args.save:
+        save_network(net, args.save)
     rows = evaluate(net, test_cases, shape, inlet)
     speedups = np.array([r['speedup'] for r in rows])
     errors = np.array([r['final_velocity_error'] for r in rows])
@@ -438,7 +474,8 @@ def main(argv=None):
               'steps_ratio_total': float(sum(r['cold_steps'] for r in rows)/max(1, sum(r['warm_steps'] for r in rows))),
               'final_velocity_error_max': float(errors.max()), 'final_velocity_error_mean': float(errors.mean()),
               'cases': rows}
-    report['conv_benchmark'] = conv_benchmark(shape, tuple(int(w) for w in args.widths.split(',')), args.batch)
+    if not args.no_conv_benchmark:
+        report['conv_benchmark'] = conv_benchmark(shape, tuple(int(w) for w in args.widths.split(',')), args.batch)
     with open(args.out, 'w') as f:
         json.dump(report, f)
     log(json.dumps({k: v for k, v in report.items() if k not in ('cases', 'loss_history', 'conv_benchmark')}))

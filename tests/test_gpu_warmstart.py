@@ -112,5 +112,24 @@ def test_trained_network_speeds_up_steady_solves():
     cold = sum(r['cold_steps'] for r in rows)
     warm = sum(r['warm_steps'] for r in rows)
     print('steps cold %d warm %d; final velocity errors %s' % (cold, warm, [round(r['final_velocity_error'], 6) for r in rows]))
-    assert warm < cold
+    # The stated margin: at least 15% fewer steps in all (measured on B200: 17,300 against 24,400, 29% fewer).
+    assert warm <= 0.85*cold
+    assert max(r['final_velocity_error'] for r in rows) <= 5e-3
+
+
+@pytest.mark.skipif(not __import__('os').path.exists(__import__('os').path.join(
+    __import__('os').path.dirname(ws.__file__), 'warmstart_net', 'weights.pt')), reason='the trained network is not committed')
+def test_committed_network_speeds_up_held_out_channels():
+    """The committed network of the 128x64x64 obstacle channel (openmm-lbm_b200/warmstart_net/train.py) on two
+    channels it never saw: both reach the steady residual 1e-6 faster than from rest, in total at least 1.3 times
+    faster in wall time, and end within 5e-3 of the cold solves' fields."""
+    import os
+    net = ws.load_network(os.path.join(os.path.dirname(ws.__file__), 'warmstart_net', 'weights.pt'))
+    rows = ws.time_to_steady(net, [400001, 400002])
+    cold = sum(r['cold_seconds'] for r in rows)
+    warm = sum(r['warm_seconds'] for r in rows)
+    print('held-out: cold %.2f s warm %.2f s (%.2fx), steps %s' % (cold, warm, cold/warm,
+                                                                  [(r['cold_steps'], r['warm_steps']) for r in rows]))
+    assert all(r['warm_steps'] < r['cold_steps'] for r in rows)
+    assert cold >= 1.3*warm
     assert max(r['final_velocity_error'] for r in rows) <= 5e-3
