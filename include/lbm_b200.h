@@ -184,11 +184,31 @@ LbmStatus lbm_get_wall_force(LbmKernel* kernel, double force[3]);
 LbmStatus lbm_get_fluid_state(LbmKernel* kernel, double* state);
 LbmStatus lbm_set_fluid_state(LbmKernel* kernel, const double* state);
 
-/* CalcLBMForceKernel::createCheckpoint / loadCheckpoint (LBMKernels.h:170-174): a byte image of the
-   kernel state (populations in the storage type, random key, wall momentum, step bookkeeping). */
+/* CalcLBMForceKernel::createCheckpoint / loadCheckpoint (LBMKernels.h:170-174).  The checkpoint is the kernel
+   stream of the reference's GPU platforms (CommonCalcLBMForceKernel::createCheckpoint, CommonLBMKernels.cpp:
+   2019-2058), which the reference's CUDA kernel reads, followed by a trailer of this kernel that the reference
+   ignores:
+     int element size E (8 for double and mixed precision, 4 for single); int flags[2] = {numbers drawn for the
+     next step, fluid advanced}; the populations f_q - w_q, 19*N values of E bytes, [q*N + node]; with coupled
+     particles P > 0, P float4 of drawn numbers and 3*P values of E bytes of particle wall momentum (SoA); 3*max(1,
+     solid nodes) values of E bytes of wall momentum (SoA); with boundary nodes B > 0 (regularized walls, open
+     faces), 3*B values of E bytes (SoA);
+     the trailer: the tag "B200LBM1", the exact step statistics and evaluation state, and, when the populations of
+     FP64 storage were written with E = 4, their raw storage bytes.
+   This kernel writes no drawn numbers (flags[0] = 0: its random numbers are a function of the seed, the step and
+   the particle or node) and puts the wall momentum of the last step, less the static part that a reader adds, into
+   the first wall entry.  A checkpoint with its trailer restarts this kernel bit for bit; one without it (written
+   by the reference's CUDA kernel) restores the populations, the wall momentum and the flag "fluid advanced", and
+   the next step draws new random numbers.  A checkpoint of another element size is rejected with "LBMForce: the
+   checkpoint was written with a different precision". */
 LbmStatus lbm_checkpoint_size(LbmKernel* kernel, size_t* bytes);
 LbmStatus lbm_create_checkpoint(LbmKernel* kernel, void* buffer, size_t bytes);
 LbmStatus lbm_load_checkpoint(LbmKernel* kernel, const void* buffer, size_t bytes);
+/* The element size E of the checkpoint stream (4 or 8), as the platform's precision gives it: 8 for double and
+   mixed, 4 for single.  The default is 8 with FP64 storage and 4 otherwise. */
+LbmStatus lbm_set_checkpoint_element_size(LbmKernel* kernel, int element_size);
+/* The sizes of the two parts of the checkpoint: the reference's stream and the trailer. */
+LbmStatus lbm_checkpoint_layout(LbmKernel* kernel, size_t* stream_bytes, size_t* trailer_bytes);
 
 /* Number of device nodes N = nx*ny*nz and the storage type actually used. */
 LbmStatus lbm_get_info(LbmKernel* kernel, long long* num_nodes, int* storage);

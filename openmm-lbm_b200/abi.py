@@ -107,6 +107,8 @@ SIGNATURES = {
     'lbm_checkpoint_size': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_size_t)]),
     'lbm_create_checkpoint': (ctypes.c_int, [_P, _P, ctypes.c_size_t]),
     'lbm_load_checkpoint': (ctypes.c_int, [_P, _P, ctypes.c_size_t]),
+    'lbm_set_checkpoint_element_size': (ctypes.c_int, [_P, ctypes.c_int]),
+    'lbm_checkpoint_layout': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
     'lbm_get_info': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]),
     'lbm_get_stream': (_P, [_P]),
     'lbm_profile_dense_kernel': (ctypes.c_int, [_P, ctypes.c_int]),

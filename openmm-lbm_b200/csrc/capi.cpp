@@ -183,6 +183,18 @@ LbmStatus lbm_load_checkpoint(LbmKernel* kernel, const void* buffer, size_t byte
     return guard([&] { kernel->impl->loadCheckpoint(buffer, bytes); });
 }
 
+LbmStatus lbm_set_checkpoint_element_size(LbmKernel* kernel, int element_size) {
+    CHECK_HANDLE(kernel);
+    return guard([&] { kernel->impl->setCheckpointElementSize(element_size); });
+}
+
+LbmStatus lbm_checkpoint_layout(LbmKernel* kernel, size_t* stream_bytes, size_t* trailer_bytes) {
+    CHECK_HANDLE(kernel);
+    if (!stream_bytes || !trailer_bytes)
+        return fail(LBM_ERR_INVALID_ARGUMENT, "lbm_checkpoint_layout: null argument");
+    return guard([&] { kernel->impl->checkpointLayout(*stream_bytes, *trailer_bytes); });
+}
+
 LbmStatus lbm_get_info(LbmKernel* kernel, long long* num_nodes, int* storage) {
     CHECK_HANDLE(kernel);
     if (num_nodes)

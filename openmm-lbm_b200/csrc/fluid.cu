@@ -1551,23 +1551,39 @@ StepStats FluidEngine::readStats() {
 }
 
 void FluidEngine::getState(double* host) {
+    getStateByDirection([&](int q, const double* values) {
+        std::memcpy(host + (size_t) q*view.n, values, sizeof(double)*view.n);
+    });
+}
+
+void FluidEngine::getStateByDirection(const std::function<void(int, const double*)>& sink) {
     if (stagingDev == nullptr)
         CUDA_CHECK(cudaMalloc(&stagingDev, sizeof(double)*4*(size_t) view.n));
+    std::vector<double> plane((size_t) view.n);
     for (int q = 0; q < 19; q++) {
         dispatchStorage(storageType, [&](auto L) { decltype(L)::gather(pop[cur], q, view, (double*) stagingDev, stream); });
         CUDA_CHECK(cudaGetLastError());
-        CUDA_CHECK(cudaMemcpyAsync(host + (size_t) q*view.n, stagingDev, sizeof(double)*view.n, cudaMemcpyDeviceToHost, stream));
+        CUDA_CHECK(cudaMemcpyAsync(plane.data(), stagingDev, sizeof(double)*view.n, cudaMemcpyDeviceToHost, stream));
         CUDA_CHECK(cudaStreamSynchronize(stream));
+        sink(q, plane.data());
     }
 }
 
 void FluidEngine::setState(const double* host) {
+    setStateByDirection([&](int q, double* values) {
+        std::memcpy(values, host + (size_t) q*view.n, sizeof(double)*view.n);
+    });
+}
+
+void FluidEngine::setStateByDirection(const std::function<void(int, double*)>& source) {
     if (stagingDev == nullptr)
         CUDA_CHECK(cudaMalloc(&stagingDev, sizeof(double)*4*(size_t) view.n));
     int* changedDev = reinterpret_cast<int*>(partialsDev);
     CUDA_CHECK(cudaMemsetAsync(changedDev, 0, sizeof(int), stream));
+    std::vector<double> plane((size_t) view.n);
     for (int q = 0; q < 19; q++) {
-        CUDA_CHECK(cudaMemcpyAsync(stagingDev, host + (size_t) q*view.n, sizeof(double)*view.n, cudaMemcpyHostToDevice, stream));
+        source(q, plane.data());
+        CUDA_CHECK(cudaMemcpyAsync(stagingDev, plane.data(), sizeof(double)*view.n, cudaMemcpyHostToDevice, stream));
         dispatchStorage(storageType, [&](auto L) {
             decltype(L)::scatter(pop[cur], pop[1-cur], q, view, (const double*) stagingDev, changedDev, stream);
         });

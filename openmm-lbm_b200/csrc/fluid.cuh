@@ -13,6 +13,7 @@
 
 #include "lbm_internal.h"
 #include <cuda_runtime.h>
+#include <functional>
 #include <vector>
 
 namespace lbm {
@@ -56,6 +57,9 @@ public:
     // Populations as deviations [q*N + node] in double, from or to host memory (the reference's state layout).
     void getState(double* host);
     void setState(const double* host);
+    // The state one direction q at a time, each plane f_q(x) of view.n doubles in node order (getState's layout).
+    void getStateByDirection(const std::function<void(int, const double*)>& sink);
+    void setStateByDirection(const std::function<void(int, double*)>& source);
     // One lattice step: stream+collide (with momentum removal when `remove`), bounce-back, boundaries and the
     // reduction of the step statistics.  The coupling reaction is read from the reaction buffers when `react`.
     void step(long long stepIndex, bool remove, bool react);

@@ -93,4 +93,28 @@ void buildGeometry(const LbmLatticeParameters& l, int numSolid, const int* solid
     }
 }
 
+// The static part of the wall momentum of a step, -2 c_q w_q for every link from a solid node into the fluid, which
+// the reference's GPU kernels keep apart from the momentum that they store per wall entry (CommonLBMKernels.cpp:
+// 297-311 for bounce-back, :356-366 for the solid directions of the boundary nodes; added back at :1932 and :1938).  A bounce-back link is stored
+// here from its fluid side (bit q of x where x + c_q is solid), so the link from the solid node has velocity -c_q.
+void staticWallMomentum(const LbmLatticeParameters& l, const Geometry& g, double momentum[3]) {
+    momentum[0] = momentum[1] = momentum[2] = 0;
+    auto weight = [](int q) { return q == 0 ? 1.0/3.0 : q < 7 ? 1.0/18.0 : 1.0/36.0; };
+    if (l.wall_scheme == LBM_WALL_BOUNCEBACK)
+        for (size_t i = 0; i < g.wallNodes.size(); i++)
+            for (int q = 1; q < 19; q++)
+                if (g.wallLinks[i] & (1<<q)) {
+                    momentum[0] += 2.0*kCx[q]*weight(q);
+                    momentum[1] += 2.0*kCy[q]*weight(q);
+                    momentum[2] += 2.0*kCz[q]*weight(q);
+                }
+    for (size_t b = 0; b < g.boundaryNodes.size(); b++)
+        for (int q = 1; q < 19; q++)
+            if (g.solidBits[b] & (1<<q)) {
+                momentum[0] -= 2.0*kCx[q]*weight(q);
+                momentum[1] -= 2.0*kCy[q]*weight(q);
+                momentum[2] -= 2.0*kCz[q]*weight(q);
+            }
+}
+
 } // namespace lbm

@@ -2,10 +2,12 @@
 #include "kernel.cuh"
 #include "coupling.cuh"
 #include "openmm_buffers.cuh"
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
 #include <sstream>
+#include <vector>
 
 namespace lbm {
 
@@ -14,25 +16,64 @@ namespace lbm {
 
 namespace {
 
-const uint64_t kCheckpointMagic = 0x314B43423230304CULL;   // "L002BCK1"
-const int kCheckpointVersion = 1;
+// The trailer that follows the reference's kernel stream in a checkpoint: what a bitwise restart needs beyond it.
+const char kTrailerTag[8] = {'B', '2', '0', '0', 'L', 'B', 'M', '1'};
+const int kTrailerVersion = 1;
 
-struct CheckpointHeader {
-    uint64_t magic;
+struct CheckpointTrailer {
+    char tag[8];
     int version, storage;
     int nx, ny, nz, numParticles;
-    int stepForcesCurrent, stepWallValid, pad[2];
+    int stepWallValid, rawPopulations;    // rawPopulations: the raw storage bytes follow the trailer
     long long stepIndex;
     double hostWall[3];
     StepStats stats;
 };
+
+// Element counts of the arrays of the reference's kernel stream (CommonLBMKernels.cpp:251, 378, 401, 666, 723).
+struct StreamLayout {
+    size_t populations, particles, solidEntries, boundaryNodes;
+    size_t bytes(size_t elementSize) const {
+        size_t b = 3*sizeof(int) + populations*elementSize;
+        if (particles > 0)
+            b += 16*particles + 3*particles*elementSize;
+        b += 3*solidEntries*elementSize;
+        if (boundaryNodes > 0)
+            b += 3*boundaryNodes*elementSize;
+        return b;
+    }
+};
+
+void putValue(char*& out, int elementSize, double value) {
+    if (elementSize == 8)
+        std::memcpy(out, &value, 8);
+    else {
+        float f = (float) value;
+        std::memcpy(out, &f, 4);
+    }
+    out += elementSize;
+}
+
+double getValue(const char*& in, int elementSize) {
+    double value;
+    if (elementSize == 8)
+        std::memcpy(&value, in, 8);
+    else {
+        float f;
+        std::memcpy(&f, in, 4);
+        value = f;
+    }
+    in += elementSize;
+    return value;
+}
 
 } // namespace
 
 B200Kernel::B200Kernel(const LbmLatticeParameters& l, const LbmOptions& options, int np, const double* masses,
                        int numSolid, const int* solid)
         : lattice(l), stream(nullptr), ownStream(false), device(options.device), numParticles(np), stepPending(false),
-          stepForcesCurrent(false), stepWallValid(false), stepIndex(0) {
+          stepForcesCurrent(false), stepWallValid(false), stepIndex(0),
+          checkpointElementSize(options.storage == LBM_STORAGE_F64 ? 8 : 4) {
     hostWallMomentum[0] = hostWallMomentum[1] = hostWallMomentum[2] = 0;
     if (l.nx <= 0 || l.ny <= 0 || l.nz <= 0)
         throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: the grid size must be set to positive values with setGridSize()");
@@ -72,6 +113,7 @@ B200Kernel::B200Kernel(const LbmLatticeParameters& l, const LbmOptions& options,
             throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: a solid node is listed more than once");
     if ((long long) geometry.solidNodes.size() == n)
         throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: all lattice nodes are solid");
+    staticWallMomentum(lattice, geometry, staticWall);
     fluid.reset(new FluidEngine(lattice, options.storage, geometry, stream));
     if (np > 0) {
         fluid->enableReaction();
@@ -355,53 +397,171 @@ void B200Kernel::setFluidState(const double* state) {
     stepForcesCurrent = false;
 }
 
-size_t B200Kernel::checkpointSize() {
-    return sizeof(CheckpointHeader) + fluid->stateBytes();
+// The checkpoint (LBMKernels.h:170-174): the kernel stream of the reference's GPU platforms (CommonLBMKernels.cpp:
+// 2019-2058), then this kernel's trailer.  With one domain the reference stores one wall entry per solid node and one
+// boundary entry per boundary node; only the sums of the entries matter to its readers (getWallForce,
+// CommonLBMKernels.cpp:1918-1945), so the dynamic wall momentum goes into the first wall entry.
+void B200Kernel::setCheckpointElementSize(int elementSize) {
+    if (elementSize != 4 && elementSize != 8)
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_set_checkpoint_element_size: the element size must be 4 or 8");
+    checkpointElementSize = elementSize;
 }
 
-// createCheckpoint / loadCheckpoint (LBMKernels.h:170-174): the populations in the storage type and pull
-// layout, the step statistics (the sums of the next momentum removal), the wall momentum and the evaluation
-// state.  The random numbers are a function of the seed and the step, so no generator state is saved.
+bool B200Kernel::rawPopulationsInTrailer() const {
+    return fluid->storage() == LBM_STORAGE_F64 && checkpointElementSize == 4;
+}
+
+double B200Kernel::wallMomentumScale() const {
+    return lattice.density*lattice.dx*lattice.dx*lattice.dx*lattice.dx/lattice.dt;
+}
+
+static StreamLayout streamLayout(long long numNodes, int numParticles, const Geometry& g) {
+    StreamLayout s;
+    s.populations = 19*(size_t) numNodes;
+    s.particles = (size_t) numParticles;
+    s.solidEntries = std::max<size_t>(1, g.solidNodes.size());
+    s.boundaryNodes = g.boundaryNodes.size();
+    return s;
+}
+
+void B200Kernel::checkpointLayout(size_t& streamBytes, size_t& trailerBytes) {
+    streamBytes = streamLayout(numNodes(), numParticles, geometry).bytes(checkpointElementSize);
+    trailerBytes = sizeof(CheckpointTrailer) + (rawPopulationsInTrailer() ? fluid->stateBytes() : 0);
+}
+
+size_t B200Kernel::checkpointSize() {
+    size_t streamBytes, trailerBytes;
+    checkpointLayout(streamBytes, trailerBytes);
+    return streamBytes + trailerBytes;
+}
+
 void B200Kernel::createCheckpoint(void* buffer, size_t bytes) {
     CUDA_CHECK(cudaSetDevice(device));
     if (bytes < checkpointSize())
         throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_create_checkpoint: the buffer is too small");
-    CheckpointHeader h;
+    const int e = checkpointElementSize;
+    const long long n = numNodes();
+    StreamLayout layout = streamLayout(n, numParticles, geometry);
+    char* out = (char*) buffer;
+    int head[3] = {e, 0, stepWallValid ? 1 : 0};
+    std::memcpy(out, head, sizeof(head));
+    out += sizeof(head);
+    fluid->getStateByDirection([&](int q, const double* values) {
+        char* plane = out + (size_t) q*n*e;
+        for (long long x = 0; x < n; x++)
+            putValue(plane, e, values[x]);
+    });
+    out += layout.populations*e;
+    if (numParticles > 0) {
+        std::memset(out, 0, 16*layout.particles + 3*layout.particles*e);
+        out += 16*layout.particles + 3*layout.particles*e;
+    }
+    // The wall momentum of the last step in lattice units, without the static part that the reader adds.
+    double wall[3] = {0, 0, 0};
+    StepStats stats = fluid->readStats();
+    if (!geometry.solidNodes.empty() && stepWallValid) {
+        double reaction[3] = {0, 0, 0};
+        if (coupling)
+            coupling->reactionWallMomentum(reaction);
+        for (int a = 0; a < 3; a++)
+            wall[a] = hostWallMomentum[a]/wallMomentumScale() + stats.wall[a] + reaction[a] - staticWall[a];
+    }
+    for (int a = 0; a < 3; a++)
+        for (size_t i = 0; i < layout.solidEntries; i++)
+            putValue(out, e, i == 0 ? wall[a] : 0.0);
+    if (layout.boundaryNodes > 0) {
+        std::memset(out, 0, 3*layout.boundaryNodes*e);
+        out += 3*layout.boundaryNodes*e;
+    }
+    CheckpointTrailer h;
     std::memset(&h, 0, sizeof(h));
-    h.magic = kCheckpointMagic;
-    h.version = kCheckpointVersion;
+    std::memcpy(h.tag, kTrailerTag, sizeof(kTrailerTag));
+    h.version = kTrailerVersion;
     h.storage = fluid->storage();
     h.nx = lattice.nx; h.ny = lattice.ny; h.nz = lattice.nz;
     h.numParticles = numParticles;
-    h.stepForcesCurrent = 0;
     h.stepWallValid = stepWallValid;
+    h.rawPopulations = rawPopulationsInTrailer() ? 1 : 0;
     h.stepIndex = stepIndex;
     for (int a = 0; a < 3; a++)
         h.hostWall[a] = hostWallMomentum[a];
-    h.stats = fluid->readStats();
-    std::memcpy(buffer, &h, sizeof(h));
-    fluid->copyStateOut((char*) buffer + sizeof(h));
+    h.stats = stats;
+    std::memcpy(out, &h, sizeof(h));
+    out += sizeof(h);
+    if (h.rawPopulations)
+        fluid->copyStateOut(out);
 }
 
 void B200Kernel::loadCheckpoint(const void* buffer, size_t bytes) {
     CUDA_CHECK(cudaSetDevice(device));
-    if (bytes < sizeof(CheckpointHeader))
+    const char* in = (const char*) buffer;
+    int head[3];
+    if (bytes < sizeof(head))
         throw Error(LBM_ERR_CHECKPOINT, "LBMForce: the checkpoint is truncated");
-    CheckpointHeader h;
-    std::memcpy(&h, buffer, sizeof(h));
-    if (h.magic != kCheckpointMagic || h.version != kCheckpointVersion)
-        throw Error(LBM_ERR_CHECKPOINT, "LBMForce: the checkpoint was not written by this kernel");
-    if (h.storage != fluid->storage() || h.nx != lattice.nx || h.ny != lattice.ny || h.nz != lattice.nz ||
-            h.numParticles != numParticles)
-        throw Error(LBM_ERR_CHECKPOINT, "LBMForce: the checkpoint belongs to another lattice, precision or set of particles");
-    if (bytes < checkpointSize())
+    std::memcpy(head, in, sizeof(head));
+    const int e = head[0];
+    if (e != checkpointElementSize)
+        throw Error(LBM_ERR_CHECKPOINT, "LBMForce: the checkpoint was written with a different precision");
+    const long long n = numNodes();
+    StreamLayout layout = streamLayout(n, numParticles, geometry);
+    size_t streamBytes = layout.bytes(e);
+    if (bytes < streamBytes)
         throw Error(LBM_ERR_CHECKPOINT, "LBMForce: the checkpoint is truncated");
-    fluid->copyStateIn((const char*) buffer + sizeof(h));
-    fluid->restoreStats(h.stats);
+    // This kernel's trailer, when it describes this kernel (another storage type reads the stream alone).
+    CheckpointTrailer h;
+    bool exact = false;
+    if (bytes >= streamBytes + sizeof(h)) {
+        std::memcpy(&h, in + streamBytes, sizeof(h));
+        exact = std::memcmp(h.tag, kTrailerTag, sizeof(kTrailerTag)) == 0 && h.version == kTrailerVersion &&
+                h.storage == fluid->storage() && h.nx == lattice.nx && h.ny == lattice.ny && h.nz == lattice.nz &&
+                h.numParticles == numParticles &&
+                (h.rawPopulations == 0 || bytes >= streamBytes + sizeof(h) + fluid->stateBytes());
+    }
+    const char* populations = in + sizeof(head);
+    if (exact && h.rawPopulations)
+        fluid->copyStateIn(in + streamBytes + sizeof(h));
+    else
+        fluid->setStateByDirection([&](int q, double* values) {
+            const char* plane = populations + (size_t) q*n*e;
+            for (long long x = 0; x < n; x++)
+                values[x] = getValue(plane, e);
+        });
     stepForcesCurrent = false;
-    stepWallValid = h.stepWallValid != 0;
+    if (exact) {
+        fluid->restoreStats(h.stats);
+        stepWallValid = h.stepWallValid != 0;
+        stepIndex = h.stepIndex;
+        for (int a = 0; a < 3; a++)
+            hostWallMomentum[a] = h.hostWall[a];
+        return;
+    }
+    // A stream without the trailer: the wall momentum of the last step is the sum of the stored entries plus the
+    // static part (getWallForce, CommonLBMKernels.cpp:1918-1945), kept on the host until the next step.
+    double wall[3] = {0, 0, 0};
+    bool advanced = head[2] != 0;
+    if (advanced && !geometry.solidNodes.empty()) {
+        const char* p = populations + layout.populations*e;
+        std::vector<double> values;
+        if (numParticles > 0) {
+            p += 16*layout.particles;
+            for (size_t i = 0; i < 3*layout.particles; i++)
+                values.push_back(getValue(p, e));
+            for (int a = 0; a < 3; a++)
+                for (size_t i = 0; i < layout.particles; i++)
+                    wall[a] += values[a*layout.particles + i];
+        }
+        for (int a = 0; a < 3; a++)
+            for (size_t i = 0; i < layout.solidEntries; i++)
+                wall[a] += getValue(p, e);
+        for (int a = 0; a < 3; a++)
+            for (size_t i = 0; i < layout.boundaryNodes; i++)
+                wall[a] += getValue(p, e);
+        for (int a = 0; a < 3; a++)
+            wall[a] += staticWall[a];
+    }
+    stepWallValid = false;
     for (int a = 0; a < 3; a++)
-        hostWallMomentum[a] = h.hostWall[a];
+        hostWallMomentum[a] = wall[a]*wallMomentumScale();
 }
 
 } // namespace lbm

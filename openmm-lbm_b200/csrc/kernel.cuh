@@ -29,6 +29,8 @@ public:
     size_t checkpointSize();
     void createCheckpoint(void* buffer, size_t bytes);
     void loadCheckpoint(const void* buffer, size_t bytes);
+    void setCheckpointElementSize(int elementSize);
+    void checkpointLayout(size_t& streamBytes, size_t& trailerBytes);
     long long numNodes() const { return fluid->numNodes(); }
     int storage() const { return fluid->storage(); }
     cudaStream_t getStream() const { return stream; }
@@ -60,6 +62,12 @@ private:
     bool stepPending, stepForcesCurrent, stepWallValid;
     long long stepIndex;
     double hostWallMomentum[3];     // reflection at the walls and reactions on solid nodes, Da nm/ps
+    // The checkpoint stream of the reference's GPU platforms: its element size, and the static wall momentum (the part
+    // w_q of the populations, the same in every step) that its readers add to the stored momentum, lattice units.
+    int checkpointElementSize;
+    double staticWall[3];
+    bool rawPopulationsInTrailer() const;
+    double wallMomentumScale() const;
     // The OpenMM Context interface: couplingIndex[atom] (-1 for an atom that is not coupled) and the coupled atoms'
     // positions, velocities and other forces gathered into coupling order (device memory).
     int openmmAtoms = 0;

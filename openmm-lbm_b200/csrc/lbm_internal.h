@@ -50,5 +50,6 @@ struct Geometry {
 };
 
 void buildGeometry(const LbmLatticeParameters& lattice, int numSolid, const int* solid, Geometry& geometry);
+void staticWallMomentum(const LbmLatticeParameters& lattice, const Geometry& geometry, double momentum[3]);
 
 } // namespace lbm

@@ -10,6 +10,7 @@ import ctypes
 
 import numpy as np
 
+from . import checkpoint
 from .abi import LbmForceDescription, LbmLatticeParameters, check, dptr, load_library
 
 
@@ -33,6 +34,18 @@ class LBMForce:
         self.particles = []
         self.solid_nodes = []
         self.force_group = 0
+        self.name = 'LBMForce'
+        self.decomposition = (1, 1, 1)
+        self.particle_copies_check = True
+        self.density_halo_exchange = False
+        self.velocity_halo_exchange = False
+
+    # Name (OpenMM's Force::getName / setName: the class name by default)
+    def getName(self):
+        return self.name
+
+    def setName(self, name):
+        self.name = str(name)
 
     # Grid and fluid
     def getGridSize(self):
@@ -42,6 +55,38 @@ class LBMForce:
     def setGridSize(self, nx, ny, nz):
         d = self.description
         d.nx, d.ny, d.nz = nx, ny, nz
+
+    # Domain decomposition (LBMForce.h:180-263).  This library runs the whole lattice on one GPU: the settings are kept
+    # (and serialized), and a Context rejects more than one domain as the reference does without MPI.
+    def getDomainDecomposition(self):
+        return tuple(self.decomposition)
+
+    def setDomainDecomposition(self, px, py, pz):
+        if px < 0 or py < 0 or pz < 0:
+            raise ValueError('LBMForce: the domain decomposition (setDomainDecomposition()) cannot be negative')
+        self.decomposition = (int(px), int(py), int(pz))
+
+    @staticmethod
+    def isMPIAvailable():
+        return False
+
+    def getParticleCopiesCheck(self):
+        return self.particle_copies_check
+
+    def setParticleCopiesCheck(self, check):
+        self.particle_copies_check = bool(check)
+
+    def getDensityHaloExchange(self):
+        return self.density_halo_exchange
+
+    def setDensityHaloExchange(self, exchange):
+        self.density_halo_exchange = bool(exchange)
+
+    def getVelocityHaloExchange(self):
+        return self.velocity_halo_exchange
+
+    def setVelocityHaloExchange(self, exchange):
+        self.velocity_halo_exchange = bool(exchange)
 
     def getFluidDensity(self):
         return self.description.fluid_density
@@ -196,7 +241,13 @@ class LBMForce:
 
     # Lattice units
     def latticeParameters(self, box, step_size, system_masses):
-        """LBMForceImpl::computeLatticeParameters for a rectangular box (nm) and a step size (ps)."""
+        """LBMForceImpl::computeLatticeParameters for a rectangular box (nm) and a step size (ps).  More than one
+        domain is rejected as by the reference built without MPI (LBMDecomposition.cpp:113-124)."""
+        if any(p < 0 for p in self.decomposition):
+            raise ValueError('LBMForce: the domain decomposition (setDomainDecomposition()) cannot be negative')
+        if tuple(self.decomposition) != (1, 1, 1):
+            raise ValueError('LBMForce: setDomainDecomposition() asks for more than one domain, but this library runs '
+                             'the whole lattice on one GPU (no MPI decomposition)')
         lib = load_library()
         lattice = LbmLatticeParameters()
         masses = np.ascontiguousarray(system_masses, dtype=np.float64)
@@ -226,10 +277,14 @@ class LBMForce:
         return context.kernel.get_wall_force()
 
     def createCheckpoint(self, context):
-        return context.kernel.create_checkpoint()
+        """LBMForceImpl::createCheckpoint (LBMForceImpl.cpp:568-573): the header, then the kernel's stream."""
+        header = checkpoint.write_header(context.getPlatform().getName(), context.lattice, len(self.particles))
+        return header + context.kernel.create_checkpoint()
 
     def loadCheckpoint(self, context, data):
-        context.kernel.load_checkpoint(data)
+        """LBMForceImpl::loadCheckpoint (LBMForceImpl.cpp:575-580): the header is checked against the Context."""
+        start = checkpoint.read_header(data, context.getPlatform().getName(), context.lattice, len(self.particles))
+        context.kernel.load_checkpoint(bytes(data[start:]))
 
     def getLatticeParametersInContext(self, context):
         lattice = context.lattice

@@ -7,6 +7,8 @@ kernel's execute, since LBMForce must come last), then v(t + dt/2) = v(t - dt/2)
 x(t + dt) = x(t) + dt v(t + dt/2), then the step count is incremented.  A kernel factory selects the
 implementation (the B200 kernel by default); the parity tests pass the oracle's.
 """
+import struct
+
 import numpy as np
 
 from .force import LBMForce
@@ -92,6 +94,14 @@ class VerletIntegrator:
             self.context._step()
 
 
+class _Platform:
+    def __init__(self, name):
+        self.name = name
+
+    def getName(self):
+        return self.name
+
+
 class Context:
     """A System integrated with a VerletIntegrator, whose LBMForce runs on a kernel from kernel_factory
     (lattice, coupled masses, solid nodes) -> kernel; the default is the B200 kernel with
@@ -123,6 +133,26 @@ class Context:
             self.kernel = B200Kernel(self.lattice, coupled_masses, self.force.solid_nodes, precision)
         else:
             self.kernel = kernel_factory(self.lattice, coupled_masses, self.force.solid_nodes)
+
+    def getPlatform(self):
+        """The platform of the Context: the one whose CalcLBMForceKernel the kernel stands for (the B200 kernel replaces
+        the CUDA platform's), by name, as checkpoints record it."""
+        return _Platform(getattr(self.kernel, 'platform_name', self.kernel.name))
+
+    def createCheckpoint(self):
+        """The particle part of a checkpoint, in place of OpenMM's Context.createCheckpoint(): the step count, then the
+        positions and velocities (float64, little-endian)."""
+        return (struct.pack('<qq', self.step_count, len(self.positions)) +
+                np.concatenate([self.positions.ravel(), self.velocities.ravel()]).astype('<f8').tobytes())
+
+    def loadCheckpoint(self, data):
+        step, n = struct.unpack_from('<qq', data, 0)
+        if n != len(self.positions) or len(data) != 16 + 48*n:
+            raise ValueError('the checkpoint was written for another System')
+        values = np.frombuffer(data, dtype='<f8', count=6*n, offset=16).reshape(2, n, 3)
+        self.setPositions(values[0])
+        self.setVelocities(values[1])
+        self.step_count = step
 
     def setPositions(self, positions):
         self.positions = np.array(positions, dtype=np.float64).reshape(-1, 3)

@@ -43,6 +43,8 @@ class B200Kernel:
     """
 
     name = 'B200'
+    # The platform whose CalcLBMForceKernel this kernel replaces, as checkpoints record it.
+    platform_name = 'CUDA'
 
     def __init__(self, lattice, masses, solid_nodes, precision='single', device=0, stream=None):
         self.lib = load_library()
@@ -166,3 +168,14 @@ class B200Kernel:
     def load_checkpoint(self, data):
         buffer = ctypes.create_string_buffer(data, len(data))
         check(self.lib.lbm_load_checkpoint(self.handle, buffer, len(data)), self.lib)
+
+    def set_checkpoint_element_size(self, element_size):
+        """The element size of the checkpoint stream: 8 as the reference's GPU platforms write it in double and mixed
+        precision, 4 in single precision."""
+        check(self.lib.lbm_set_checkpoint_element_size(self.handle, int(element_size)), self.lib)
+
+    def checkpoint_layout(self):
+        """(bytes of the reference's kernel stream, bytes of this kernel's trailer) of a checkpoint."""
+        stream, trailer = ctypes.c_size_t(), ctypes.c_size_t()
+        check(self.lib.lbm_checkpoint_layout(self.handle, ctypes.byref(stream), ctypes.byref(trailer)), self.lib)
+        return stream.value, trailer.value

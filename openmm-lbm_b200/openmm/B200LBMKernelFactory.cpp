@@ -39,7 +39,9 @@ KernelImpl* B200LBMKernelFactory::createKernelImpl(std::string name, const Platf
             throw OpenMMException("LBMForce does not support running on multiple devices");
         CudaContext& cc = *data->contexts[0];
         std::string precision = cc.getUseDoublePrecision() ? "double" : cc.getUseMixedPrecision() ? "mixed" : "single";
-        return new B200CudaDataLBMKernel(name, platform, cc, storageFor(precision));
+        B200CalcLBMForceKernel* kernel = new B200CudaDataLBMKernel(name, platform, cc, storageFor(precision));
+        kernel->setCheckpointElementSize(precision == "single" ? 4 : 8);
+        return kernel;
     }
 #endif
     return new B200HostDataLBMKernel(name, platform, storageFor("double"), 0, NULL);

@@ -9,6 +9,7 @@
 #include "openmm/System.h"
 #include "openmm/reference/ReferencePlatform.h"
 #include <cmath>
+#include <cstring>
 #include <istream>
 #include <limits>
 #include <ostream>
@@ -50,7 +51,7 @@ LbmLatticeParameters toLbmLatticeParameters(const LBMLatticeParameters& l) {
 B200CalcLBMForceKernel::B200CalcLBMForceKernel(string name, const Platform& platform, int storage, int device,
                                                void* stream)
         : CalcLBMForceKernel(name, platform), kernel(NULL), numNodes(0), storage(storage), device(device),
-          stream(stream) {
+          stream(stream), checkpointElementSize(8) {
 }
 
 B200CalcLBMForceKernel::~B200CalcLBMForceKernel() {
@@ -79,6 +80,7 @@ void B200CalcLBMForceKernel::initialize(const System& system, const LBMForce& fo
     check(lbm_create(&p, &options, (int) masses.size(), masses.empty() ? NULL : masses.data(),
                      (int) l.solidNodes.size(), l.solidNodes.empty() ? NULL : l.solidNodes.data(), &kernel));
     numNodes = (long long) l.nx*l.ny*l.nz;
+    check(lbm_set_checkpoint_element_size(kernel, checkpointElementSize));
     initializeParticles(system, force);
 }
 
@@ -165,27 +167,36 @@ void B200CalcLBMForceKernel::setFluidState(ContextImpl& context, const vector<do
 }
 
 void B200CalcLBMForceKernel::createCheckpoint(ContextImpl& context, ostream& stream) {
-    // The kernel's byte image (populations in the storage type, step statistics, wall momentum, evaluation state),
-    // after LBMForceImpl's header (LBMForceImpl.cpp:514-528), with its length first.
+    // The kernel stream of the reference's GPU platforms (CommonLBMKernels.cpp:2019-2034), which LBMForceImpl writes
+    // after its header (LBMForceImpl.cpp:568-573), then this kernel's trailer, which the reference does not read.
     size_t bytes = 0;
     check(lbm_checkpoint_size(kernel, &bytes));
     vector<char> buffer(bytes);
     check(lbm_create_checkpoint(kernel, buffer.data(), bytes));
-    long long length = (long long) bytes;
-    stream.write((const char*) &length, sizeof(length));
     stream.write(buffer.data(), bytes);
 }
 
 void B200CalcLBMForceKernel::loadCheckpoint(ContextImpl& context, istream& stream) {
-    long long length = 0;
-    stream.read((char*) &length, sizeof(length));
-    if (!stream || length < 0 || length > ((long long) 1 << 40))
-        throw OpenMMException("LBMForce: the checkpoint is damaged");
-    vector<char> buffer((size_t) length);
-    stream.read(buffer.data(), length);
+    // The stream has no length: its size follows from the lattice and the precision (CommonLBMKernels.cpp:2036-2058).
+    // The trailer is read when it is there; a stream of the reference's CUDA kernel ends without it.
+    size_t streamBytes = 0, trailerBytes = 0;
+    check(lbm_checkpoint_layout(kernel, &streamBytes, &trailerBytes));
+    vector<char> buffer(streamBytes + trailerBytes);
+    stream.read(buffer.data(), sizeof(int));
     if (!stream)
         throw OpenMMException("LBMForce: the checkpoint is truncated");
-    check(lbm_load_checkpoint(kernel, buffer.data(), (size_t) length));
+    int elementSize;
+    memcpy(&elementSize, buffer.data(), sizeof(int));
+    if (elementSize != checkpointElementSize)
+        throw OpenMMException("LBMForce: the checkpoint was written with a different precision");
+    stream.read(buffer.data() + sizeof(int), streamBytes - sizeof(int));
+    if (!stream)
+        throw OpenMMException("LBMForce: the checkpoint is truncated");
+    stream.read(buffer.data() + streamBytes, trailerBytes);
+    size_t length = streamBytes + (size_t) stream.gcount();
+    if (!stream)
+        stream.clear();
+    check(lbm_load_checkpoint(kernel, buffer.data(), length));
 }
 
 void B200CalcLBMForceKernel::createRankCheckpoint(ContextImpl& context, ostream& stream) {

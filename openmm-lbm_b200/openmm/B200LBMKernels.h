@@ -49,6 +49,9 @@ public:
     void loadRankCheckpoint(OpenMM::ContextImpl& context, std::istream& stream);
     void resetRankState(OpenMM::ContextImpl& context);
     LbmKernel* handle() const { return kernel; }
+    /* The element size of the checkpoint stream, as the reference's GPU platforms write it: 8 in double and mixed
+       precision, 4 in single (CommonLBMKernels.cpp:243-244).  The kernel factory sets it from the Context. */
+    void setCheckpointElementSize(int size) { checkpointElementSize = size; }
 protected:
     /* Called by initialize() once the kernel exists: the platform's particle data set-up. */
     virtual void initializeParticles(const OpenMM::System& system, const LBMForce& force) = 0;
@@ -63,6 +66,7 @@ protected:
 private:
     int storage, device;
     void* stream;
+    int checkpointElementSize;
 };
 
 class B200HostDataLBMKernel : public B200CalcLBMForceKernel {

@@ -11,13 +11,11 @@ import struct
 
 import numpy as np
 
+from . import checkpoint
 from .force import LBMForce
 
 # Boltzmann's constant in kJ/mol/K (OpenMM's MOLAR_GAS_CONSTANT_R).
 KB = 6.02214076e23*1.380649e-23/1000.0
-
-_CHECKPOINT_TAG = b'OPENMMLBM-B200-CHECKPOINT-1\n'
-
 
 class State:
     """The State of a Context: step count, time (ps), positions (nm), velocities (nm/ps) and forces (kJ/mol/nm),
@@ -71,19 +69,15 @@ class Simulation:
 
 
 def saveCheckpoint(file, context, force):
-    """Save the state of a Context with an LBMForce (python/openmmlbm.i:513-550): the particles (positions,
-    velocities, step count) and the checkpoint of the force's kernel (the fluid, the step bookkeeping and the wall
-    momentum), written to file + '.tmp' and then renamed, so that an interrupted write never replaces a valid
-    checkpoint.  Like the reference's, the file is specific to the platform kernel, the precision and the System."""
-    kernelData = context.kernel.create_checkpoint()
-    particles = np.concatenate([context.positions.ravel(), context.velocities.ravel()]).astype('<f8').tobytes()
-    head = struct.pack('<qqq', context.getStepCount(), len(particles), len(kernelData))
+    """Save the state of a Context with an LBMForce in the reference's file format for one domain
+    (python/openmmlbm.i:513-550): the tag, the lengths, the Context's checkpoint (here the particles: step count,
+    positions, velocities) and LBMForce.createCheckpoint() (the header and the kernel's stream), written to file +
+    '.tmp' and then renamed, so that an interrupted write never replaces a valid checkpoint.  Like the reference's,
+    the file is specific to the platform, the precision and the System."""
+    data = checkpoint.pack_file(context.createCheckpoint(), force.createCheckpoint(context))
     temporary = file + '.tmp'
     with open(temporary, 'wb') as out:
-        out.write(_CHECKPOINT_TAG)
-        out.write(head)
-        out.write(particles)
-        out.write(kernelData)
+        out.write(data)
     os.replace(temporary, file)
 
 
@@ -92,18 +86,9 @@ def loadCheckpoint(file, context, force):
     the run continues exactly, bit for bit."""
     with open(file, 'rb') as stream:
         data = stream.read()
-    if not data.startswith(_CHECKPOINT_TAG):
-        raise ValueError('%s is not a checkpoint written by saveCheckpoint()' % file)
-    start = len(_CHECKPOINT_TAG)
-    step, particleBytes, kernelBytes = struct.unpack_from('<qqq', data, start)
-    start += 24
-    if len(data) != start + particleBytes + kernelBytes or particleBytes != 48*len(context.positions):
-        raise ValueError('%s is truncated, damaged or of another System' % file)
-    values = np.frombuffer(data, dtype='<f8', count=particleBytes//8, offset=start).reshape(2, -1, 3)
-    context.kernel.load_checkpoint(data[start + particleBytes:])
-    context.setPositions(values[0])
-    context.setVelocities(values[1])
-    context.setStepCount(step)
+    openmm_data, force_data = checkpoint.unpack_file(data, file)
+    context.loadCheckpoint(openmm_data)
+    force.loadCheckpoint(context, force_data)
 
 
 class LBMCheckpointReporter:

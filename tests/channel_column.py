@@ -17,8 +17,8 @@ import numpy as np
 
 # D3Q19 velocities in the kernel's order (openmm-lbm_b200/csrc/lbm_device.cuh cxOf/cyOf/czOf).
 CX = np.array([0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1])
-CY = np.array([0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 0, 0, 0, 0])
-CZ = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1])
+CY = np.array([0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 0, 0, 0, 0])
+CZ = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1])
 W = np.array([1/3] + [1/18]*6 + [1/36]*12)
 
 

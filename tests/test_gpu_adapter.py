@@ -121,3 +121,25 @@ def test_checkpoint_reporter_and_load_continue_bit_for_bit(tmp_path):
     context.close()
     for a, b in zip(expected, got):
         assert (a == b).all()
+
+
+def test_adapter_checkpoint_is_the_reference_stream():
+    """Through OpenMM's stream interface the platform kernel writes what the library writes (the kernel stream of
+    the reference's GPU platforms, CommonLBMKernels.cpp:2019-2034, then the B200 trailer), and it reads the stream
+    alone, as the reference's CUDA kernel writes it, from a stream that ends there."""
+    context, force = fluid_case('regularized', adapter)
+    context.integrator.step(5)
+    data = context.kernel.create_checkpoint()
+    state, wall = force.getFluidState(context), np.array(force.getWallForce(context))
+    context.close()
+    library, library_force = fluid_case('regularized', None, {'Precision': 'double'})
+    library.integrator.step(5)
+    stream_bytes, trailer_bytes = library.kernel.checkpoint_layout()
+    assert data == library.kernel.create_checkpoint()
+    assert len(data) == stream_bytes + trailer_bytes
+    library.close()
+    fresh, fresh_force = fluid_case('regularized', adapter)
+    fresh.kernel.load_checkpoint(data[:stream_bytes])
+    assert np.array_equal(fresh_force.getFluidState(fresh), state)
+    assert abs(np.array(fresh_force.getWallForce(fresh)) - wall).max() <= 1e-12*abs(wall).max()
+    fresh.close()

@@ -31,8 +31,8 @@ TOL_ANALYTIC_FP64 = 2.5e-4
 # D3Q19 velocities and weights in the kernel's order, and the 16-bit storage factors: the stored value of direction q
 # is (f_q - w_q) k_q (times 2^10 for FP16).
 CX = np.array([0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1])
-CY = np.array([0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 0, 0, 0, 0])
-CZ = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1])
+CY = np.array([0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 0, 0, 0, 0])
+CZ = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1])
 W = np.array([1/3] + [1/18]*6 + [1/36]*12)
 K = np.array([4.0] + [16.0]*6 + [32.0]*12)
 
