@@ -8,6 +8,8 @@
     batch    ReplicaBatch: many independent periodic replicas with their beads, advanced together
     reporters  saveCheckpoint / loadCheckpoint and the reference's reporters (checkpoints, temperature, VTK files),
              with a Simulation driver that calls them as OpenMM's does
+    checkpoint the reference's checkpoint header and checkpoint file around the kernel's stream
+    serialization  XmlSerializer: the reference's XML form of LBMForce (LBMForceProxy, version 9; reads 1 to 9)
 """
 from .batch import ReplicaBatch  # noqa: F401
 from .abi import LbmError, LbmLatticeParameters, load_library  # noqa: F401
@@ -17,3 +19,4 @@ from .kernel import B200Kernel  # noqa: F401
 from .md import BeadDynamics, random_walk_chains  # noqa: F401
 from .reporters import (LBMCheckpointReporter, LBMTemperatureReporter, LBMVTKReporter, Simulation,  # noqa: F401
                         loadCheckpoint, saveCheckpoint)
+from .serialization import XmlSerializer  # noqa: F401
