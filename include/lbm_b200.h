@@ -193,11 +193,12 @@ LbmStatus lbm_set_fluid_state(LbmKernel* kernel, const double* state);
      particles P > 0, P float4 of drawn numbers and 3*P values of E bytes of particle wall momentum (SoA); 3*max(1,
      solid nodes) values of E bytes of wall momentum (SoA); with boundary nodes B > 0 (regularized walls, open
      faces), 3*B values of E bytes (SoA);
-     the trailer: the tag "B200LBM1", the exact step statistics and evaluation state, and, when the populations of
-     FP64 storage were written with E = 4, their raw storage bytes.
+     the trailer: the tag "B200LBM1", the exact step statistics, the evaluation state and the random seed in use,
+     and, when the populations of FP64 storage were written with E = 4, their raw storage bytes.
    This kernel writes no drawn numbers (flags[0] = 0: its random numbers are a function of the seed, the step and
    the particle or node) and puts the wall momentum of the last step, less the static part that a reader adds, into
-   the first wall entry.  A checkpoint with its trailer restarts this kernel bit for bit; one without it (written
+   the first wall entry.  A checkpoint with its trailer restarts this kernel bit for bit (with the seed of the run
+   that wrote it, as the reference restores its generator state); one without it (written
    by the reference's CUDA kernel) restores the populations, the wall momentum and the flag "fluid advanced", and
    the next step draws new random numbers.  A checkpoint of another element size is rejected with "LBMForce: the
    checkpoint was written with a different precision". */

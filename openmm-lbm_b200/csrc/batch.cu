@@ -391,10 +391,13 @@ __device__ __forceinline__ void finishReplica(const PersistentArgs& a, int r, in
     __syncthreads();
 }
 
+constexpr int kPairTile = 256;     // beads per shared-memory tile of the pair forces
+
 template <typename T, typename R, bool FLUCT, int BT>
 __global__ void __launch_bounds__(BT, batchMinBlocks<R, BT>())
 batchPersistentKernel(PersistentArgs a) {
     typedef typename Vec4<R>::type V;
+    __shared__ double pairTile[3*kPairTile];
     const int lane = threadIdx.x%32, warp = threadIdx.x/32;
     const long long step0 = a.clock->step;
     const long long totalSlots = (long long) a.totalParticles*a.slots;
@@ -413,19 +416,34 @@ batchPersistentKernel(PersistentArgs a) {
             for (int r = blockIdx.x; r < a.numReplicas; r += gridDim.x)
                 finishReplica(a, r, BT/32);
         if (a.coupled) {
+            // Pair forces, all pairs of each replica in bead order (as batchPairKernel).  The positions were written in
+            // this launch by other blocks: they are read once through L2 into shared-memory tiles, which every bead of
+            // the block then reads.
             for (int r = blockIdx.x; r < a.numReplicas; r += gridDim.x) {
                 const ReplicaTable& rt = a.table[r];
                 const double* x = a.pos + 3*(size_t) rt.firstParticle;
                 double* out = a.fpair + 3*(size_t) rt.firstParticle;
-                for (int i = threadIdx.x; i < rt.numParticles; i += blockDim.x) {
-                    double f[3] = {0, 0, 0};
-                    if (a.pair.type != LBM_PAIR_NONE)
-                        for (int j = 0; j < rt.numParticles; j++) {
-                            if (j == i)
+                const int n = rt.numParticles;
+                for (int i0 = 0; i0 < n; i0 += blockDim.x) {
+                    const int i = i0 + threadIdx.x;
+                    double xi[3] = {0, 0, 0}, f[3] = {0, 0, 0};
+                    if (i < n)
+                        for (int k = 0; k < 3; k++)
+                            xi[k] = __ldcg(&x[3*i+k]);
+                    for (int j0 = 0; j0 < n && a.pair.type != LBM_PAIR_NONE; j0 += kPairTile) {
+                        const int count = min(kPairTile, n - j0);
+                        __syncthreads();
+                        for (int e = threadIdx.x; e < 3*count; e += blockDim.x)
+                            pairTile[e] = __ldcg(&x[3*j0 + e]);
+                        __syncthreads();
+                        if (i >= n)
+                            continue;
+                        for (int jj = 0; jj < count; jj++) {
+                            if (j0 + jj == i)
                                 continue;
                             double d[3];
                             for (int k = 0; k < 3; k++) {
-                                d[k] = __ldcg(&x[3*i+k]) - __ldcg(&x[3*j+k]);
+                                d[k] = xi[k] - pairTile[3*jj+k];
                                 d[k] -= rt.box[k]*rint(d[k]/rt.box[k]);
                             }
                             double r2 = d[0]*d[0] + d[1]*d[1] + d[2]*d[2];
@@ -436,8 +454,10 @@ batchPersistentKernel(PersistentArgs a) {
                             for (int k = 0; k < 3; k++)
                                 f[k] += scale*d[k];
                         }
-                    for (int k = 0; k < 3; k++)
-                        out[3*i+k] = f[k];
+                    }
+                    if (i < n)
+                        for (int k = 0; k < 3; k++)
+                            out[3*i+k] = f[k];
                 }
             }
             int* nodes = a.slotNode[buf];

@@ -25,6 +25,7 @@ struct CheckpointTrailer {
     int version, storage;
     int nx, ny, nz, numParticles;
     int stepWallValid, rawPopulations;    // rawPopulations: the raw storage bytes follow the trailer
+    int seed, pad;                        // the seed in use (a seed of 0 was replaced by a unique one at creation)
     long long stepIndex;
     double hostWall[3];
     StepStats stats;
@@ -482,6 +483,7 @@ void B200Kernel::createCheckpoint(void* buffer, size_t bytes) {
     h.numParticles = numParticles;
     h.stepWallValid = stepWallValid;
     h.rawPopulations = rawPopulationsInTrailer() ? 1 : 0;
+    h.seed = lattice.random_number_seed;
     h.stepIndex = stepIndex;
     for (int a = 0; a < 3; a++)
         h.hostWall[a] = hostWallMomentum[a];
@@ -528,6 +530,14 @@ void B200Kernel::loadCheckpoint(const void* buffer, size_t bytes) {
         });
     stepForcesCurrent = false;
     if (exact) {
+        // The random numbers are a function of (seed, step, index): the seed of the run continues it, as the
+        // reference's generator state does.
+        if (h.seed != 0 && h.seed != lattice.random_number_seed) {
+            lattice.random_number_seed = h.seed;
+            fluid->setParameters(lattice);
+            if (coupling)
+                coupling->setParameters(lattice);
+        }
         fluid->restoreStats(h.stats);
         stepWallValid = h.stepWallValid != 0;
         stepIndex = h.stepIndex;
