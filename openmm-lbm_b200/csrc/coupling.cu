@@ -451,9 +451,9 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
 // dozen entries per particle instead of a pass over the lattice nodes of all stencils.
 //   cgBinKernel     per particle: its cell (cells of kCgCellEdge nodes, on the first stencil index of the stencil
 //                   pass), inserted into a fixed-capacity cell list; per slot: w/rho
-//   cgRowsKernel    one warp per particle k: the particles of the neighbouring cells whose first stencil indices are
-//                   within a stencil width of k's on every axis, sorted by index (so that every row, and every sum
-//                   over it, has one order), and K_kl for each, a lane per entry
+//   cgRowsKernel    one thread per particle k: the particles of the neighbouring cells whose first stencil indices
+//                   are within a stencil width of k's on every axis, sorted by index (so that every row, and every sum
+//                   over it, has one order), and K_kl for each
 //   centeredSparseKernel  the conjugate gradients (same start, preconditioner, stopping rule and per-component
 //                   iteration as the kernel above) in one cooperative launch, two grid barriers per iteration
 // Rows are stored entry-major (entry e of row k at e np + k), so that the threads of consecutive rows read them
@@ -479,6 +479,15 @@ struct SparseCg {
     double* Ap;            // A p, 3 per particle
     int* overflow;         // nonzero: a cell or a row over its capacity
     int cells[3];          // cells per axis
+    // The connected components of the matrix (cgComponentKernel).
+    int* parent;           // union-find forest over the particles (a root is the smallest index of its component)
+    unsigned* rootKey;     // the root of each particle (sort keys), and
+    int* member;           // the particles (sort values): after the sort, the members of each component in a row
+    int* componentStart;   // per root: the first and one past the last sorted position of its component
+    int* componentEnd;
+    int* componentRoot;    // the roots, in no particular order
+    int* componentCount;   // number of components
+    int* componentOverflow;// nonzero: a component over the capacity (the cooperative solve takes the step)
 };
 
 template <typename R>
@@ -497,11 +506,43 @@ cgBinKernel(CouplingView c, const R* __restrict__ slotWeight, const typename Vec
                              min(first.z/kCgCellEdge, g.cells[2] - 1)};
         int key = cell[0] + g.cells[0]*(cell[1] + g.cells[1]*cell[2]);
         g.cellOf[i] = key;
+        g.parent[i] = i;
         unsigned slot = atomicAdd(&g.cellCount[key], 1u);
         if (slot < (unsigned) kCgCellCapacity)
             g.cellList[(long long) key*kCgCellCapacity + slot] = make_int4(i, first.x, first.y, first.z);
         else
             atomicExch(g.overflow, 1);
+    }
+}
+
+// Union-find over the particles, lock-free: a root is linked under a smaller root by atomicCAS, so every root is the
+// smallest index of its tree and no cycle forms; a find halves the paths it walks (a non-root only moves up).
+__device__ __forceinline__ int findRoot(int* parent, int x) {
+    volatile int* p = parent;
+    int up = p[x];
+    while (up != x) {
+        const int next = p[up];
+        if (next != up)
+            p[x] = next;
+        x = up;
+        up = next;
+    }
+    return x;
+}
+
+__device__ __forceinline__ void unite(int* parent, int a, int b) {
+    int ra = findRoot(parent, a), rb = findRoot(parent, b);
+    while (ra != rb) {
+        if (ra < rb) {
+            const int s = ra;
+            ra = rb;
+            rb = s;
+        }
+        const int old = atomicCAS(&parent[ra], ra, rb);
+        if (old == ra)
+            return;
+        ra = findRoot(parent, old);
+        rb = findRoot(parent, rb);
     }
 }
 
@@ -511,153 +552,128 @@ __device__ __forceinline__ int periodicDistance(int a, int b, int n) {
     return min(d, n - d);
 }
 
+// K_kl = sum over k's slots (ix, iy, iz) of (w/rho)_k times l's weight at the same node: the product of l's axis
+// weights at the entries with k's indices (on each axis the first such entry: later duplicates, at clamped open faces,
+// have weight zero).  In the precision of the fluid's arithmetic, in which the slots' w/rho are stored.
+template <typename R, int W>
+__device__ __forceinline__ R couplingEntry(const R* coefK, const int4 ik[3], const int4* __restrict__ axisIndex,
+                                           const double2* __restrict__ axisWeight, int l) {
+    R shifted[3][W];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const int4 il = axisIndex[3*l + a];
+        const double2 w01 = axisWeight[6*l + 2*a], w23 = axisWeight[6*l + 2*a + 1];
+        const int mine[4] = {ik[a].x, ik[a].y, ik[a].z, ik[a].w};
+#pragma unroll
+        for (int i = 0; i < W; i++) {
+            double v = 0.0;
+            if (mine[i] >= 0) {
+                if (il.w == mine[i]) v = w23.y;
+                if (il.z == mine[i]) v = w23.x;
+                if (il.y == mine[i]) v = w01.y;
+                if (il.x == mine[i]) v = w01.x;
+            }
+            shifted[a][i] = (R) v;
+        }
+    }
+    R K = 0;
+#pragma unroll
+    for (int iz = 0; iz < W; iz++) {
+        if (shifted[2][iz] == (R) 0)
+            continue;
+#pragma unroll
+        for (int iy = 0; iy < W; iy++) {
+            if (shifted[1][iy] == (R) 0)
+                continue;
+            const R wyz = shifted[1][iy]*shifted[2][iz];
+#pragma unroll
+            for (int ix = 0; ix < W; ix++)
+                K += coefK[ix + W*(iy + W*iz)]*(shifted[0][ix]*wyz);
+        }
+    }
+    return K;
+}
+
+// The entries of row k (sorted by particle index) and their values, and the union of k with the entries above it.
+template <typename R, int W>
+__device__ __forceinline__ void rowValues(const CouplingView& c, const R* __restrict__ coef, const SparseCg& g, int k,
+                                          const int* list, int found) {
+    R coefK[W*W*W];
+#pragma unroll
+    for (int s = 0; s < W*W*W; s++)
+        coefK[s] = coef[(long long) k*(W*W*W) + s];
+    const int4 ik[3] = {g.axisIndex[3*k], g.axisIndex[3*k + 1], g.axisIndex[3*k + 2]};
+    for (int j = 0; j < found; j++) {
+        const int l = list[j];
+        const R K = couplingEntry<R, W>(coefK, ik, g.axisIndex, g.axisWeight, l);
+        g.rowIndex[(long long) j*c.np + k] = l;
+        g.rowValue[(long long) j*c.np + k] = (double) K;
+        if (l > k)
+            unite(g.parent, k, l);
+    }
+}
+
+// One thread per particle k: the particles of the neighbouring cells whose first stencil indices are within a stencil
+// width of k's on every axis (k included), sorted by index so that every row, and every sum over it, has one order.
 template <typename R>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads)
 cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
-    __shared__ int candidates[kThreads/32][kCgRowCapacity];
-    __shared__ int sorted[kThreads/32][kCgRowCapacity];
-    __shared__ R rowCoef[kThreads/32][64];
-    __shared__ int cellEnd[kThreads/32][32], cellStart[kThreads/32][32], cellId[kThreads/32][32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int* list = candidates[warp];
-    const int firstWarp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
-    const int warps = (gridDim.x*blockDim.x) >> 5;
     const int size[3] = {c.nx, c.ny, c.nz};
-    const int w = c.width, S = c.slots;
-    for (int k = firstWarp; k < c.np; k += warps) {
-        for (int s = lane; s < S; s += 32)
-            rowCoef[warp][s] = coef[(long long) k*S + s];
+    for (int k = blockIdx.x*blockDim.x + threadIdx.x; k < c.np; k += gridDim.x*blockDim.x) {
         const int4 fk = g.firstIndex[k];
         const int key = g.cellOf[k];
         const int home[3] = {key%g.cells[0], (key/g.cells[0])%g.cells[1], key/(g.cells[0]*g.cells[1])};
-        // Lane j < 27 takes the neighbouring cell (j%3 - 1, j/3%3 - 1, j/9 - 1); a cell that an axis with fewer than
-        // 3 cells reaches twice is taken once (by its first offset).
-        int cell = -1, members = 0;
-        if (lane < 27) {
-            const int off[3] = {lane%3 - 1, (lane/3)%3 - 1, lane/9 - 1};
+        // The 27 neighbouring cells (j%3 - 1, j/3%3 - 1, j/9 - 1); a cell that an axis with fewer than 3 cells
+        // reaches twice is taken once (by its first offset).  Their counts are loaded together.
+        int cellId[27], count[27];
+#pragma unroll
+        for (int j = 0; j < 27; j++) {
+            const int off[3] = {j%3 - 1, (j/3)%3 - 1, j/9 - 1};
             bool first = true;
             int cc[3];
+#pragma unroll
             for (int a = 0; a < 3; a++) {
                 const int n = g.cells[a];
                 cc[a] = ((home[a] + off[a])%n + n)%n;
                 for (int d = -1; d < off[a]; d++)
                     first &= ((home[a] + d)%n + n)%n != cc[a];
             }
-            if (first) {
-                cell = cc[0] + g.cells[0]*(cc[1] + g.cells[1]*cc[2]);
-                members = min((int) g.cellCount[cell], kCgCellCapacity);
-            }
+            cellId[j] = first ? cc[0] + g.cells[0]*(cc[1] + g.cells[1]*cc[2]) : -1;
         }
-        // Exclusive scan of the member counts over the lanes.
-        int start = members;
-        for (int d = 1; d < 32; d *= 2) {
-            const int v = __shfl_up_sync(0xFFFFFFFFu, start, d);
-            if (lane >= d)
-                start += v;
-        }
-        const int total = __shfl_sync(0xFFFFFFFFu, start, 31);
-        cellEnd[warp][lane] = lane < 27 ? start : 0x7FFFFFFF;
-        cellStart[warp][lane] = start - members;
-        cellId[warp][lane] = cell;
-        __syncwarp();
-        int found = 0;     // the same in every lane
-        // Four rounds of 32 members at a time, their loads issued together.
-        for (int base = 0; base < total; base += 128) {
-            int lq[4];
-            bool nq[4];
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const int e = base + 32*r + lane;
-                lq[r] = -1;
-                nq[r] = false;
-                if (e < total) {
-                    // The cell holding member e: the first of the 27 whose running end exceeds e.
-                    int lo = 0, hi = 26;
-                    while (lo < hi) {
-                        const int mid = (lo + hi) >> 1;
-                        if (cellEnd[warp][mid] > e)
-                            hi = mid;
-                        else
-                            lo = mid + 1;
+        for (int j = 0; j < 27; j++)
+            count[j] = cellId[j] >= 0 ? min((int) g.cellCount[cellId[j]], kCgCellCapacity) : 0;
+        int list[kCgRowCapacity];
+        int found = 0;
+        for (int j = 0; j < 27; j++) {
+            const int cell = cellId[j], members = count[j];
+            for (int m = 0; m < members; m++) {
+                const int4 e = g.cellList[(long long) cell*kCgCellCapacity + m];
+                if (periodicDistance(e.y, fk.x, size[0]) < c.width && periodicDistance(e.z, fk.y, size[1]) < c.width &&
+                        periodicDistance(e.w, fk.z, size[2]) < c.width) {
+                    if (found < kCgRowCapacity) {
+                        // Insertion in index order.
+                        int at = found;
+                        while (at > 0 && list[at - 1] > e.x) {
+                            list[at] = list[at - 1];
+                            at--;
+                        }
+                        list[at] = e.x;
                     }
-                    const int4 m = g.cellList[(long long) cellId[warp][lo]*kCgCellCapacity + (e - cellStart[warp][lo])];
-                    lq[r] = m.x;
-                    nq[r] = periodicDistance(m.y, fk.x, size[0]) < c.width &&
-                            periodicDistance(m.z, fk.y, size[1]) < c.width &&
-                            periodicDistance(m.w, fk.z, size[2]) < c.width;
+                    found++;
                 }
             }
-#pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const unsigned ballot = __ballot_sync(0xFFFFFFFFu, nq[r]);
-                const int at = found + __popc(ballot & ((1u << lane) - 1u));
-                if (nq[r] && at < kCgRowCapacity)
-                    list[at] = lq[r];
-                found += __popc(ballot);
-            }
         }
-        __syncwarp();
         if (found > kCgRowCapacity) {
-            if (lane == 0)
-                atomicExch(g.overflow, 1);
+            atomicExch(g.overflow, 1);
             found = kCgRowCapacity;
         }
-        // Rank sort (particle indices are distinct).
-        for (int j = lane; j < found; j += 32) {
-            const int v = list[j];
-            int rank = 0;
-            for (int i = 0; i < found; i++)
-                rank += list[i] < v;
-            sorted[warp][rank] = v;
+        switch (c.width) {
+        case 2: rowValues<R, 2>(c, coef, g, k, list, found); break;
+        case 3: rowValues<R, 3>(c, coef, g, k, list, found); break;
+        default: rowValues<R, 4>(c, coef, g, k, list, found); break;
         }
-        __syncwarp();
-        // K_kl = sum over k's slots (ix, iy, iz) of (w/rho)_k times l's weight at the same node, the product of l's
-        // axis weights at the entries with k's indices (on each axis the first such entry: later duplicates, at
-        // clamped open faces, have weight zero).  Lanes over the row's entries.
-        const int4 ik[3] = {g.axisIndex[3*k], g.axisIndex[3*k + 1], g.axisIndex[3*k + 2]};
-        for (int j = lane; j < found; j += 32) {
-            const int l = sorted[warp][j];
-            // In the precision of the fluid's arithmetic (the slots' w/rho are stored in it).
-            R shifted[3][4];
-#pragma unroll
-            for (int a = 0; a < 3; a++) {
-                const int4 il = g.axisIndex[3*l + a];
-                const double2 w01 = g.axisWeight[6*l + 2*a], w23 = g.axisWeight[6*l + 2*a + 1];
-                const int mine[4] = {ik[a].x, ik[a].y, ik[a].z, ik[a].w};
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    double v = 0.0;
-                    if (mine[i] >= 0) {
-                        if (il.w == mine[i]) v = w23.y;
-                        if (il.z == mine[i]) v = w23.x;
-                        if (il.y == mine[i]) v = w01.y;
-                        if (il.x == mine[i]) v = w01.x;
-                    }
-                    shifted[a][i] = (R) v;
-                }
-            }
-            R K = 0;
-#pragma unroll
-            for (int iz = 0; iz < 4; iz++) {
-                if (iz >= w || shifted[2][iz] == (R) 0)
-                    continue;
-#pragma unroll
-                for (int iy = 0; iy < 4; iy++) {
-                    if (iy >= w || shifted[1][iy] == (R) 0)
-                        continue;
-                    const R wyz = shifted[1][iy]*shifted[2][iz];
-#pragma unroll
-                    for (int ix = 0; ix < 4; ix++)
-                        if (ix < w)
-                            K += rowCoef[warp][ix + w*(iy + w*iz)]*(shifted[0][ix]*wyz);
-                }
-            }
-            g.rowIndex[(long long) j*c.np + k] = l;
-            g.rowValue[(long long) j*c.np + k] = (double) K;
-        }
-        if (lane == 0)
-            g.rowCount[k] = found;
-        __syncwarp();
+        g.rowCount[k] = found;
     }
 }
 
@@ -681,31 +697,17 @@ __device__ __forceinline__ void rowProduct(const SparseCg& g, int np, int k, con
     out[2] = s2 + __shfl_xor_sync(0xFFFFFFFFu, s2, 1);
 }
 
+// The start of the centred drag's solve for every particle (ReferenceLBMKernels.cpp:758-782, 839-840): the right-hand
+// side b/m, the Jacobi diagonal and F = rhs/diag, 8 lanes per particle (4 particles per warp of the calling grid).
 template <typename R>
-__global__ void __launch_bounds__(kSolveThreads, 1)
-centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel, const double* __restrict__ fin,
-                     const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
-                     const typename Vec4<R>::type* __restrict__ slotU, long long step, int isStep, double tolerance,
-                     int maxIterations, CgBuffers b, SparseCg g, double* fout, R* reaction, uint32_t* mask,
-                     double* wall) {
+__device__ void startParticles(const CouplingView& c, const double* __restrict__ vel, const double* __restrict__ fin,
+                               const R* __restrict__ slotWeight, const typename Vec4<R>::type* __restrict__ slotU,
+                               long long step, const CgBuffers& b, int firstWarp, int warps) {
     typedef typename Vec4<R>::type V;
-    constexpr int G = 8;       // lanes per particle where a particle's slots are summed
+    constexpr int G = 8;
     const int lane = threadIdx.x & 31, sub = lane%G;
-    const int firstWarp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
-    const int warps = (gridDim.x*blockDim.x) >> 5;
-    const int firstThread = blockIdx.x*blockDim.x + threadIdx.x, threads = gridDim.x*blockDim.x;
-    // The rows of this block (a contiguous range, so that its threads read the entry-major rows coalesced).
-    const int rowBegin = (int) ((long long) c.np*blockIdx.x/gridDim.x);
-    const int rowEnd = (int) ((long long) c.np*(blockIdx.x + 1)/gridDim.x);
     const int S = c.slots;
     const double a = c.a;
-    // The cell list has been read (by the rows kernel): empty it for the next step.
-    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x)
-        g.cellCount[g.cellOf[i]] = 0u;
-    if (*((volatile int*) g.overflow) != 0)
-        return;
-    // Right-hand side, diagonal and the start F = rhs/diag (ReferenceLBMKernels.cpp:758-782, 839-840): 8 lanes per
-    // particle, 4 particles per warp.
     for (int base = firstWarp*(32/G); base < c.np; base += warps*(32/G)) {
         const int i = base + lane/G;
         const bool active = i < c.np;
@@ -745,6 +747,48 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
         }
         b.diag[i] = diag;
     }
+}
+
+// Forces and reactions of the solved drag (ReferenceLBMKernels.cpp:889-900): a thread per particle, then a thread per
+// slot.
+template <typename R>
+__device__ void finishParticles(const FluidView& f, const CouplingView& c, const int* __restrict__ slotNode,
+                                const R* __restrict__ slotWeight, int isStep, const CgBuffers& b, double* fout,
+                                R* reaction, uint32_t* mask, double* wall, int firstThread, int threads) {
+    const int S = c.slots;
+    for (int i = firstThread; i < c.np; i += threads)
+        for (int d = 0; d < 3; d++)
+            fout[3*i+d] = b.F[3*i+d]*c.forceScale;
+    if (isStep)
+        for (long long t = firstThread; t < (long long) c.np*S; t += threads) {
+            const int i = (int) (t/S);
+            const double w = (double) slotWeight[t];
+            if (w != 0.0)
+                addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*b.F[3*i], -w*b.F[3*i+1], -w*b.F[3*i+2]);
+        }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kSolveThreads, 1)
+centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel, const double* __restrict__ fin,
+                     const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
+                     const typename Vec4<R>::type* __restrict__ slotU, long long step, int isStep, double tolerance,
+                     int maxIterations, CgBuffers b, SparseCg g, double* fout, R* reaction, uint32_t* mask,
+                     double* wall) {
+    const int lane = threadIdx.x & 31;
+    const int firstWarp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
+    const int warps = (gridDim.x*blockDim.x) >> 5;
+    const int firstThread = blockIdx.x*blockDim.x + threadIdx.x, threads = gridDim.x*blockDim.x;
+    // The rows of this block (a contiguous range, so that its threads read the entry-major rows coalesced).
+    const int rowBegin = (int) ((long long) c.np*blockIdx.x/gridDim.x);
+    const int rowEnd = (int) ((long long) c.np*(blockIdx.x + 1)/gridDim.x);
+    const double a = c.a;
+    // The cell list has been read (by the rows kernel): empty it for the next step.
+    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x)
+        g.cellCount[g.cellOf[i]] = 0u;
+    if (*((volatile int*) g.overflow) != 0)
+        return;
+    startParticles<R>(c, vel, fin, slotWeight, slotU, step, b, firstWarp, warps);
     if (!gridSync(b.barrier, b.status, b.pollLimit))
         return;
     // r = rhs - A F, z = r/diag, p = z; r.z, the norm of the right-hand side and r.r per component.
@@ -847,17 +891,205 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
         *b.iterations = iteration;
     if (failed)
         return;
-    // Forces and reactions (ReferenceLBMKernels.cpp:889-900): a thread per particle, then a thread per slot.
-    for (int i = firstThread; i < c.np; i += threads)
-        for (int d = 0; d < 3; d++)
-            fout[3*i+d] = b.F[3*i+d]*c.forceScale;
-    if (isStep)
-        for (long long t = firstThread; t < (long long) c.np*S; t += threads) {
-            const int i = (int) (t/S);
-            const double w = (double) slotWeight[t];
-            if (w != 0.0)
-                addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*b.F[3*i], -w*b.F[3*i+1], -w*b.F[3*i+2]);
+    finishParticles<R>(f, c, slotNode, slotWeight, isStep, b, fout, reaction, mask, wall, firstThread, threads);
+}
+
+// ------------------------------------------------------------------------------------------------------
+// The conjugate gradients per connected component of the coupling matrix.
+//
+// Particles k and l are coupled when their stencils share a fluid node (an entry K_kl of the rows), so the matrix is
+// block diagonal over the connected components of that relation (a bead chain, a cluster of beads), and the
+// conjugate gradients of the whole system are those of its components taken together.  Each component is solved by one
+// block on its own, with block barriers where the whole system needs grid barriers.  Per component and axis the solve
+// stops when r.r <= tol^2 b.b (b the right-hand side), which implies the reference's rule over all particles (the sums
+// over the components of r.r and b.b, ReferenceLBMKernels.cpp:848-856).
+//   rows kernel       unites k with the entries l > k of its row (the union-find above)
+//   cgRootKernel      the root of each particle (the sort key), the start of the solve (startParticles), and the cell
+//                     list emptied for the next step
+//   radix sort        the particles by root, stably: the members of a component in a row, in ascending order
+//   cgSegmentKernel   the first and last sorted position of each component, and the list of roots
+//   cgComponentKernel one block per component: the Jacobi-preconditioned conjugate gradients
+//                     (ReferenceLBMKernels.cpp:834-888) over the component's rows, members in ascending order
+//   cgFinishKernel    forces and reactions (finishParticles), unless a solve failed or the cooperative solve is needed
+// A component of more than `capacity` particles is left to the cooperative solve over all particles.
+// ------------------------------------------------------------------------------------------------------
+
+constexpr int kComponentThreads = 256;
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads)
+cgRootKernel(CouplingView c, const double* __restrict__ vel, const double* __restrict__ fin,
+             const R* __restrict__ slotWeight, const typename Vec4<R>::type* __restrict__ slotU, long long step,
+             CgBuffers b, SparseCg g) {
+    const int firstThread = blockIdx.x*blockDim.x + threadIdx.x, threads = gridDim.x*blockDim.x;
+    for (int i = firstThread; i < c.np; i += threads) {
+        g.cellCount[g.cellOf[i]] = 0u;
+        g.rootKey[i] = (unsigned) findRoot(g.parent, i);
+        g.member[i] = i;
+    }
+    startParticles<R>(c, vel, fin, slotWeight, slotU, step, b, firstThread >> 5, threads >> 5);
+}
+
+__global__ void cgSegmentKernel(int np, const unsigned* __restrict__ key, SparseCg g) {
+    for (int p = blockIdx.x*blockDim.x + threadIdx.x; p < np; p += gridDim.x*blockDim.x) {
+        const int root = (int) key[p];
+        if (p == 0 || key[p-1] != key[p]) {
+            g.componentStart[root] = p;
+            g.componentRoot[atomicAdd(g.componentCount, 1)] = root;
         }
+        if (p == np - 1 || key[p+1] != key[p])
+            g.componentEnd[root] = p + 1;
+    }
+}
+
+// Sums of 6 values over the block, returned to every thread (two block barriers).
+__device__ __forceinline__ void componentSum(double v[6], double (*red)[6]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < 6; k++)
+        v[k] = warpSum(v[k]);
+    __syncthreads();
+    if (lane == 0)
+        for (int k = 0; k < 6; k++)
+            red[warp][k] = v[k];
+    __syncthreads();
+    for (int k = 0; k < 6; k++) {
+        double s = 0;
+        for (int w = 0; w < (int) (blockDim.x >> 5); w++)
+            s += red[w][k];
+        v[k] = s;
+    }
+}
+
+// (A v)_i = v_i (1 + a)/m_i + a sum_l K_il v_l over row i, for the three components.
+__device__ __forceinline__ void componentProduct(const SparseCg& g, const CouplingView& c, int i, const double* v,
+                                                 double out[3]) {
+    double s0 = 0, s1 = 0, s2 = 0;
+    const int n = g.rowCount[i];
+    for (int e = 0; e < n; e++) {
+        const int l = g.rowIndex[(long long) e*c.np + i];
+        const double K = g.rowValue[(long long) e*c.np + i];
+        s0 += K*v[3*l];
+        s1 += K*v[3*l+1];
+        s2 += K*v[3*l+2];
+    }
+    const double self = (1.0 + c.a)/c.mass[i];
+    out[0] = v[3*i]*self + s0*c.a;
+    out[1] = v[3*i+1]*self + s1*c.a;
+    out[2] = v[3*i+2]*self + s2*c.a;
+}
+
+__global__ void __launch_bounds__(kComponentThreads)
+cgComponentKernel(CouplingView c, double tolerance, int maxIterations, int capacity, CgBuffers b, SparseCg g) {
+    __shared__ double red[kComponentThreads/32][6];
+    if (*((volatile int*) g.overflow) != 0)
+        return;
+    const int components = *g.componentCount;
+    const double tol2 = tolerance*tolerance;
+    for (int ci = blockIdx.x; ci < components; ci += gridDim.x) {
+        const int root = g.componentRoot[ci];
+        const int start = g.componentStart[root], n = g.componentEnd[root] - start;
+        if (n > capacity) {
+            if (threadIdx.x == 0)
+                atomicExch(g.componentOverflow, 1);
+            continue;
+        }
+        const int* members = g.member + start;
+        // r = rhs - A F, z = r/diag, p = z (F = rhs/diag from the start); r.z, b.b and r.r per axis.
+        double acc[6] = {0, 0, 0, 0, 0, 0}, norm[3] = {0, 0, 0};
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const int i = members[j];
+            double AF[3];
+            componentProduct(g, c, i, b.F, AF);
+            const double diag = b.diag[i];
+            for (int d = 0; d < 3; d++) {
+                const double rhs = b.rhs[3*i+d];
+                const double r = rhs - AF[d], z = r*(1.0/diag);
+                b.r[3*i+d] = r;
+                b.z[3*i+d] = z;
+                b.p[3*i+d] = z;
+                acc[d] += r*z;
+                acc[3+d] += r*r;
+                norm[d] += rhs*rhs;
+            }
+        }
+        componentSum(acc, red);
+        double rz[3] = {acc[0], acc[1], acc[2]}, rr[3] = {acc[3], acc[4], acc[5]};
+        double nb[6] = {norm[0], norm[1], norm[2], 0, 0, 0};
+        componentSum(nb, red);
+        int iteration = 0;
+        bool failed = false;   // the same in every thread: every decision comes from the block sums
+        for (;; iteration++) {
+            bool converged = true;
+            for (int d = 0; d < 3; d++)
+                if (rr[d] > tol2*nb[d])
+                    converged = false;
+            if (converged)
+                break;
+            if (iteration == maxIterations) {
+                failed = true;
+                break;
+            }
+            // A p and p.Ap (p was written before the last block barrier).
+            double pAp[6] = {0, 0, 0, 0, 0, 0};
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                const int i = members[j];
+                double Ap[3];
+                componentProduct(g, c, i, b.p, Ap);
+                for (int d = 0; d < 3; d++) {
+                    g.Ap[3*i+d] = Ap[d];
+                    pAp[d] += b.p[3*i+d]*Ap[d];
+                }
+            }
+            componentSum(pAp, red);
+            double alpha[3];
+            for (int d = 0; d < 3; d++)
+                alpha[d] = pAp[d] > 0 ? rz[d]/pAp[d] : 0.0;
+            double next[6] = {0, 0, 0, 0, 0, 0};
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                const int i = members[j];
+                const double diag = b.diag[i];
+                for (int d = 0; d < 3; d++) {
+                    b.F[3*i+d] += alpha[d]*b.p[3*i+d];
+                    const double r = b.r[3*i+d] - alpha[d]*g.Ap[3*i+d];
+                    const double z = r*(1.0/diag);
+                    b.r[3*i+d] = r;
+                    b.z[3*i+d] = z;
+                    next[d] += r*z;
+                    next[3+d] += r*r;
+                }
+            }
+            componentSum(next, red);
+            double beta[3];
+            for (int d = 0; d < 3; d++) {
+                beta[d] = rz[d] > 0 ? next[d]/rz[d] : 0.0;
+                rz[d] = next[d];
+                rr[d] = next[3+d];
+            }
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                const int i = members[j];
+                for (int d = 0; d < 3; d++)
+                    b.p[3*i+d] = b.z[3*i+d] + beta[d]*b.p[3*i+d];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            atomicMax(b.iterations, iteration);
+            if (failed)
+                atomicExch(b.status, LBM_ERR_CG_NOT_CONVERGED);
+        }
+        __syncthreads();
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads)
+cgFinishKernel(FluidView f, CouplingView c, const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
+               int isStep, CgBuffers b, SparseCg g, double* fout, R* reaction, uint32_t* mask, double* wall) {
+    if (*((volatile int*) g.overflow) != 0 || *((volatile int*) g.componentOverflow) != 0 ||
+            *((volatile int*) b.status) != 0)
+        return;
+    finishParticles<R>(f, c, slotNode, slotWeight, isStep, b, fout, reaction, mask, wall,
+                       blockIdx.x*blockDim.x + threadIdx.x, gridDim.x*blockDim.x);
 }
 
 // Clear the reaction of the slots of the last step (and their mask words).
@@ -944,6 +1176,7 @@ struct CouplingEngine::Device {
     CgBuffers cg;
     SparseCg sparse;
     int sparseGrid = 0;
+    int componentGrid = 0;          // blocks of cgComponentKernel
     void* spread = nullptr;
     int4* axisIndex = nullptr;      // per particle: 3, the stencil's node indices on each axis
     double2* axisWeight = nullptr;  // per particle: 6, the stencil's weights on each axis
@@ -985,8 +1218,10 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
         CUDA_CHECK(cudaMalloc(&wallDev, sizeof(double)*8));
         CUDA_CHECK(cudaMemsetAsync(wallDev, 0, sizeof(double)*8, stream));
         dev->reflectWall = wallDev + 4;
-        CUDA_CHECK(cudaMalloc(&statusDev, sizeof(int)*4));
-        CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, stream));
+        // Status words: [0] solve status, [1] iterations, [2] overflow of the cell list or the rows, [3] arrivals at
+        // the grid barriers, [4] a component over kComponentCapacity, [5] number of components.
+        CUDA_CHECK(cudaMalloc(&statusDev, sizeof(int)*8));
+        CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*8, stream));
         size_t slots = (size_t) np*stencilSlots;
         CUDA_CHECK(cudaMalloc(&dev->slotNode, sizeof(int)*slots));
         CUDA_CHECK(cudaMalloc(&dev->slotWeight, r*slots));
@@ -999,7 +1234,8 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
         CUDA_CHECK(cudaMalloc(&dev->nodeStamp, sizeof(unsigned)*(size_t) f.numNodes()));
         CUDA_CHECK(cudaMemsetAsync(dev->nodeStamp, 0, sizeof(unsigned)*(size_t) f.numNodes(), stream));
         CUDA_CHECK(cudaMalloc(&dev->nodeU, 4*r*(size_t) f.numNodes()));
-        if (l.drag_scheme == LBM_DRAG_CENTERED && l.interpolation_stencil == LBM_STENCIL_NEAREST) {
+        if (l.drag_scheme == LBM_DRAG_CENTERED) {
+            // The sort of the particles by node (nearest node) or by component (stencils).
             int blocks = (np + kSortItems - 1)/kSortItems;
             dev->histCount = (size_t) 256*blocks;
             CUDA_CHECK(cudaMalloc(&dev->hist, sizeof(unsigned)*dev->histCount));
@@ -1056,10 +1292,19 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
             CUDA_CHECK(cudaMalloc(&g.rowValue, sizeof(double)*kCgRowCapacity*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.Ap, v3));
             g.overflow = statusDev + 2;
+            CUDA_CHECK(cudaMalloc(&g.parent, sizeof(int)*(size_t) np));
+            CUDA_CHECK(cudaMalloc(&g.componentStart, sizeof(int)*(size_t) np));
+            CUDA_CHECK(cudaMalloc(&g.componentEnd, sizeof(int)*(size_t) np));
+            CUDA_CHECK(cudaMalloc(&g.componentRoot, sizeof(int)*(size_t) np));
+            g.rootKey = dev->keys[0];
+            g.member = dev->values[0];
+            g.componentOverflow = statusDev + 4;
+            g.componentCount = statusDev + 5;
             if (f64)
                 CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, centeredSparseKernel<double>, kSolveThreads, 0));
             else
                 CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, centeredSparseKernel<float>, kSolveThreads, 0));
+            dev->componentGrid = std::max(1, std::min(np, 8*sms));
             long long wantedSolve = ((long long) np*32 + kSolveThreads - 1)/kSolveThreads;
             // No more blocks than the partial records hold (cgGrid of the 256-thread solve).
             dev->sparseGrid = (int) std::max(1LL, std::min(std::min(wantedSolve, (long long) std::max(1, perSM)*sms),
@@ -1099,6 +1344,7 @@ void CouplingEngine::release() {
         SparseCg& g = dev->sparse;
         cudaFree(g.cellOf); cudaFree(g.cellCount); cudaFree(g.cellList);
         cudaFree(g.rowCount); cudaFree(g.rowIndex); cudaFree(g.rowValue); cudaFree(g.Ap);
+        cudaFree(g.parent); cudaFree(g.componentStart); cudaFree(g.componentEnd); cudaFree(g.componentRoot);
         delete dev;
         dev = nullptr;
     }
@@ -1206,7 +1452,7 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     int* sn = dev->slotNode;
     FluidView fv = f;
     CouplingView cc = c;
-    int status[3] = {0, 0, 0};
+    int status[6] = {0, 0, 0, 0, 0, 0};
     static const bool spreadOnly = [] {
         const char* e = std::getenv("LBM_B200_SPREAD_CG");
         return e != nullptr && e[0] == '1';
@@ -1214,17 +1460,44 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     if (!spreadOnly) {
         long long total = (long long) np*c.slots;
         int gridSlots = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
+        int gridLanes = (int) std::max(1LL, std::min(4736LL, ((long long) np*8 + kThreads - 1)/kThreads));
+        CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*8, stream));
         cgBinKernel<R><<<gridSlots, kThreads, 0, stream>>>(c, sw, su, coef, g);
         CUDA_CHECK(cudaGetLastError());
-        cgRowsKernel<R><<<warpGrid(np), kThreads, 0, stream>>>(c, coef, g);
+        cgRowsKernel<R><<<gridP, kThreads, 0, stream>>>(c, coef, g);
         CUDA_CHECK(cudaGetLastError());
-        void* sparseArgs[] = {&fv, &cc, &vel, &fin, &sn, &sw, &su, &stepArg, &isStepArg, &tolerance, &maxIterations, &b,
-                              &g, &fout, &reaction, &mask, &wall};
-        CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredSparseKernel<R>, dev->sparseGrid, kSolveThreads,
-                                               sparseArgs, 0, stream));
-        fluid.launches += 3;
-        CUDA_CHECK(cudaMemcpyAsync(status, statusDev, sizeof(int)*3, cudaMemcpyDeviceToHost, stream));
+        // The components: roots, the particles sorted by root, the segments; then a block per component.
+        cgRootKernel<R><<<gridLanes, kThreads, 0, stream>>>(c, vel, fin, sw, su, stepArg, b, g);
+        CUDA_CHECK(cudaGetLastError());
+        int bits = 1;
+        while (bits < 31 && (1LL << bits) < np)
+            bits++;
+        int cur = radixSortByKey(dev->keys, dev->values, dev->hist, np, bits, stream);
+        cgSegmentKernel<<<gridP, kThreads, 0, stream>>>(np, dev->keys[cur], g);
+        CUDA_CHECK(cudaGetLastError());
+        SparseCg sorted = g;
+        sorted.member = dev->values[cur];
+        cgComponentKernel<<<dev->componentGrid, kComponentThreads, 0, stream>>>(c, tolerance, maxIterations,
+                                                                                 componentCapacity, b, sorted);
+        CUDA_CHECK(cudaGetLastError());
+        cgFinishKernel<R><<<gridSlots, kThreads, 0, stream>>>(f, c, dev->slotNode, sw, isStepArg, b, g, fout, reaction,
+                                                              mask, wall);
+        CUDA_CHECK(cudaGetLastError());
+        fluid.launches += 7 + 3*((bits + 7)/8);
+        CUDA_CHECK(cudaMemcpyAsync(status, statusDev, sizeof(int)*6, cudaMemcpyDeviceToHost, stream));
         CUDA_CHECK(cudaStreamSynchronize(stream));
+        if (status[2] == 0 && status[4] != 0) {
+            // A component too large for one block: the cooperative solve over all particles (its own start; the
+            // rows stay).
+            CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, stream));
+            void* sparseArgs[] = {&fv, &cc, &vel, &fin, &sn, &sw, &su, &stepArg, &isStepArg, &tolerance, &maxIterations,
+                                  &b, &g, &fout, &reaction, &mask, &wall};
+            CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredSparseKernel<R>, dev->sparseGrid, kSolveThreads,
+                                                   sparseArgs, 0, stream));
+            fluid.launches++;
+            CUDA_CHECK(cudaMemcpyAsync(status, statusDev, sizeof(int)*3, cudaMemcpyDeviceToHost, stream));
+            CUDA_CHECK(cudaStreamSynchronize(stream));
+        }
     }
     if (spreadOnly || status[2] != 0) {
         CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, stream));
@@ -1244,6 +1517,10 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
         // The blocks left the solve at different barriers; the arrival counter holds a partial count, which the
         // memset before the next cooperative launch clears.
         throw Error(LBM_ERR_DEVICE_TIMEOUT, "LBMForce: a grid barrier of the conjugate gradients timed out");
+}
+
+void CouplingEngine::setComponentCapacity(int particles) {
+    componentCapacity = particles > 0 ? particles : particles == 0 ? kDefaultComponentCapacity : 0;
 }
 
 void CouplingEngine::setSolverLimits(int maxIterations, long long barrierPolls) {
