@@ -451,8 +451,8 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
 // dozen entries per particle instead of a pass over the lattice nodes of all stencils.
 //   cgBinKernel     per particle: its cell (cells of kCgCellEdge nodes, on the first stencil index of the stencil
 //                   pass), inserted into a fixed-capacity cell list; per slot: w/rho
-//   cgRowsKernel    one thread per particle k: the particles of the neighbouring cells whose first stencil indices
-//                   are within a stencil width of k's on every axis, sorted by index (so that every row, and every sum
+//   cgRowsKernel    8 lanes per particle k: the particles of the neighbouring cells whose first stencil indices are
+//                   within a stencil width of k's on every axis, sorted by index (so that every row, and every sum
 //                   over it, has one order), and K_kl for each
 //   centeredSparseKernel  the conjugate gradients (same start, preconditioner, stopping rule and per-component
 //                   iteration as the kernel above) in one cooperative launch, two grid barriers per iteration
@@ -465,6 +465,8 @@ constexpr int kCgCellEdge = 4;      // nodes per cell edge (no less than the wid
 constexpr int kCgCellCapacity = 64; // particles per cell
 constexpr int kCgRowCapacity = 128; // entries per row of K
 constexpr int kSolveThreads = 1024; // threads per block of the solve (one block per SM: few barrier arrivals)
+constexpr int kRowLanes = 8;        // lanes of a warp per row of the rows kernel (4 rows per warp)
+constexpr int kRowsThreads = 128;   // threads per block of the rows kernel (16 rows, 26-30 KB of shared memory)
 
 struct SparseCg {
     int4* axisIndex;       // 3 per particle: the stencil's node indices on each axis (-1 past the width)
@@ -594,17 +596,14 @@ __device__ __forceinline__ R couplingEntry(const R* coefK, const int4 ik[3], con
     return K;
 }
 
-// The entries of row k (sorted by particle index) and their values, and the union of k with the entries above it.
+// The values of row k, entries j = sub, sub + kRowLanes, ... of the sorted list, and the union of k with the entries
+// above it.
 template <typename R, int W>
-__device__ __forceinline__ void rowValues(const CouplingView& c, const R* __restrict__ coef, const SparseCg& g, int k,
-                                          const int* list, int found) {
-    R coefK[W*W*W];
-#pragma unroll
-    for (int s = 0; s < W*W*W; s++)
-        coefK[s] = coef[(long long) k*(W*W*W) + s];
+__device__ __forceinline__ void rowValues(const CouplingView& c, const SparseCg& g, int k, const R* coefK,
+                                          const int* sorted, int found, int sub) {
     const int4 ik[3] = {g.axisIndex[3*k], g.axisIndex[3*k + 1], g.axisIndex[3*k + 2]};
-    for (int j = 0; j < found; j++) {
-        const int l = list[j];
+    for (int j = sub; j < found; j += kRowLanes) {
+        const int l = sorted[j];
         const R K = couplingEntry<R, W>(coefK, ik, g.axisIndex, g.axisWeight, l);
         g.rowIndex[(long long) j*c.np + k] = l;
         g.rowValue[(long long) j*c.np + k] = (double) K;
@@ -613,67 +612,116 @@ __device__ __forceinline__ void rowValues(const CouplingView& c, const R* __rest
     }
 }
 
-// One thread per particle k: the particles of the neighbouring cells whose first stencil indices are within a stencil
-// width of k's on every axis (k included), sorted by index so that every row, and every sum over it, has one order.
+// kRowLanes lanes per particle k (32/kRowLanes particles per warp): the particles of the neighbouring cells whose first
+// stencil indices are within a stencil width of k's on every axis (k included), sorted by index (so that every row,
+// and every sum over it, has one order), and K_kl for each.  Lane groups that run out of work still take part in the
+// warp's ballots.
 template <typename R>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kRowsThreads)
 cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
+    constexpr int P = 32/kRowLanes, GW = kRowsThreads/kRowLanes;     // particles per warp, per block
+    __shared__ int candidates[GW][kCgRowCapacity];
+    __shared__ int sorted[GW][kCgRowCapacity];
+    __shared__ R rowCoef[GW][64];
+    __shared__ int cellEnd[GW][28], cellStart[GW][28], cellId[GW][28];
+    const int lane = threadIdx.x & 31, sub = lane%kRowLanes, group = lane/kRowLanes;
+    const int slot = threadIdx.x/kRowLanes;                       // this lane group's arrays
+    const unsigned groupMask = ((1u << kRowLanes) - 1u) << (group*kRowLanes);
     const int size[3] = {c.nx, c.ny, c.nz};
-    for (int k = blockIdx.x*blockDim.x + threadIdx.x; k < c.np; k += gridDim.x*blockDim.x) {
-        const int4 fk = g.firstIndex[k];
-        const int key = g.cellOf[k];
-        const int home[3] = {key%g.cells[0], (key/g.cells[0])%g.cells[1], key/(g.cells[0]*g.cells[1])};
-        // The 27 neighbouring cells (j%3 - 1, j/3%3 - 1, j/9 - 1); a cell that an axis with fewer than 3 cells
-        // reaches twice is taken once (by its first offset).  Their counts are loaded together.
-        int cellId[27], count[27];
-#pragma unroll
-        for (int j = 0; j < 27; j++) {
-            const int off[3] = {j%3 - 1, (j/3)%3 - 1, j/9 - 1};
-            bool first = true;
-            int cc[3];
-#pragma unroll
-            for (int a = 0; a < 3; a++) {
-                const int n = g.cells[a];
-                cc[a] = ((home[a] + off[a])%n + n)%n;
-                for (int d = -1; d < off[a]; d++)
-                    first &= ((home[a] + d)%n + n)%n != cc[a];
-            }
-            cellId[j] = first ? cc[0] + g.cells[0]*(cc[1] + g.cells[1]*cc[2]) : -1;
-        }
-#pragma unroll
-        for (int j = 0; j < 27; j++)
-            count[j] = cellId[j] >= 0 ? min((int) g.cellCount[cellId[j]], kCgCellCapacity) : 0;
-        int list[kCgRowCapacity];
-        int found = 0;
-        for (int j = 0; j < 27; j++) {
-            const int cell = cellId[j], members = count[j];
-            for (int m = 0; m < members; m++) {
-                const int4 e = g.cellList[(long long) cell*kCgCellCapacity + m];
-                if (periodicDistance(e.y, fk.x, size[0]) < c.width && periodicDistance(e.z, fk.y, size[1]) < c.width &&
-                        periodicDistance(e.w, fk.z, size[2]) < c.width) {
-                    if (found < kCgRowCapacity) {
-                        // Insertion in index order.
-                        int at = found;
-                        while (at > 0 && list[at - 1] > e.x) {
-                            list[at] = list[at - 1];
-                            at--;
-                        }
-                        list[at] = e.x;
-                    }
-                    found++;
+    const int S = c.slots;
+    const int firstWarp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
+    const int warps = (gridDim.x*blockDim.x) >> 5;
+    for (int base = firstWarp*P; base < c.np; base += warps*P) {
+        const int k = base + group;
+        const bool active = k < c.np;
+        int4 fk = make_int4(0, 0, 0, 0);
+        if (active) {
+            for (int s = sub; s < S; s += kRowLanes)
+                rowCoef[slot][s] = coef[(long long) k*S + s];
+            fk = g.firstIndex[k];
+            const int key = g.cellOf[k];
+            const int home[3] = {key%g.cells[0], (key/g.cells[0])%g.cells[1], key/(g.cells[0]*g.cells[1])};
+            // The 27 neighbouring cells (j%3 - 1, j/3%3 - 1, j/9 - 1), lane sub taking j = sub, sub + kRowLanes, ...;
+            // a cell that an axis with fewer than 3 cells reaches twice is taken once (by its first offset).
+            for (int j = sub; j < 27; j += kRowLanes) {
+                const int off[3] = {j%3 - 1, (j/3)%3 - 1, j/9 - 1};
+                bool first = true;
+                int cc[3];
+                for (int a = 0; a < 3; a++) {
+                    const int n = g.cells[a];
+                    cc[a] = ((home[a] + off[a])%n + n)%n;
+                    for (int d = -1; d < off[a]; d++)
+                        first &= ((home[a] + d)%n + n)%n != cc[a];
                 }
+                const int cell = first ? cc[0] + g.cells[0]*(cc[1] + g.cells[1]*cc[2]) : -1;
+                cellId[slot][j] = cell;
+                cellEnd[slot][j] = cell >= 0 ? min((int) g.cellCount[cell], kCgCellCapacity) : 0;
             }
         }
+        __syncwarp();
+        // Running ends of the member counts (lane 0 of the group; 27 adds).
+        int total = 0;
+        if (active && sub == 0) {
+            for (int j = 0; j < 27; j++) {
+                cellStart[slot][j] = total;
+                total += cellEnd[slot][j];
+                cellEnd[slot][j] = total;
+            }
+        }
+        total = __shfl_sync(0xFFFFFFFFu, total, group*kRowLanes);
+        __syncwarp();
+        int found = 0;     // the same in every lane of the group
+        for (int e0 = 0; __any_sync(0xFFFFFFFFu, e0 < total); e0 += kRowLanes) {
+            const int e = e0 + sub;
+            bool near = false;
+            int l = -1;
+            if (e < total) {
+                // The cell holding member e: the first of the 27 whose running end exceeds e.
+                int lo = 0, hi = 26;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (cellEnd[slot][mid] > e)
+                        hi = mid;
+                    else
+                        lo = mid + 1;
+                }
+                const int4 m = g.cellList[(long long) cellId[slot][lo]*kCgCellCapacity + (e - cellStart[slot][lo])];
+                l = m.x;
+                near = periodicDistance(m.y, fk.x, size[0]) < c.width && periodicDistance(m.z, fk.y, size[1]) < c.width &&
+                       periodicDistance(m.w, fk.z, size[2]) < c.width;
+            }
+            const unsigned ballot = __ballot_sync(0xFFFFFFFFu, near) & groupMask;
+            const int at = found + __popc(ballot & ((1u << lane) - 1u));
+            if (near && at < kCgRowCapacity)
+                candidates[slot][at] = l;
+            found += __popc(ballot);
+        }
+        __syncwarp();
         if (found > kCgRowCapacity) {
-            atomicExch(g.overflow, 1);
+            if (active && sub == 0)
+                atomicExch(g.overflow, 1);
             found = kCgRowCapacity;
         }
-        switch (c.width) {
-        case 2: rowValues<R, 2>(c, coef, g, k, list, found); break;
-        case 3: rowValues<R, 3>(c, coef, g, k, list, found); break;
-        default: rowValues<R, 4>(c, coef, g, k, list, found); break;
+        // Rank sort (particle indices are distinct).
+        if (active)
+            for (int j = sub; j < found; j += kRowLanes) {
+                const int v = candidates[slot][j];
+                int rank = 0;
+                for (int i = 0; i < found; i++)
+                    rank += candidates[slot][i] < v;
+                sorted[slot][rank] = v;
+            }
+        __syncwarp();
+        if (active) {
+            switch (c.width) {
+            case 2: rowValues<R, 2>(c, g, k, rowCoef[slot], sorted[slot], found, sub); break;
+            case 3: rowValues<R, 3>(c, g, k, rowCoef[slot], sorted[slot], found, sub); break;
+            default: rowValues<R, 4>(c, g, k, rowCoef[slot], sorted[slot], found, sub); break;
+            }
+            if (sub == 0)
+                g.rowCount[k] = found;
         }
-        g.rowCount[k] = found;
+        __syncwarp();
     }
 }
 
@@ -1159,6 +1207,11 @@ int warpGrid(long long particles) {
     return (int) std::max(1LL, std::min(4736LL, (particles*32 + kThreads - 1)/kThreads));
 }
 
+// Blocks of the rows kernel: kRowLanes lanes per particle.
+int rowsGrid(long long particles) {
+    return (int) std::max(1LL, std::min(8*1184LL, (particles*kRowLanes + kRowsThreads - 1)/kRowsThreads));
+}
+
 } // namespace
 
 // ------------------------------------------------------------------------------------------------------
@@ -1464,7 +1517,7 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
         CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*8, stream));
         cgBinKernel<R><<<gridSlots, kThreads, 0, stream>>>(c, sw, su, coef, g);
         CUDA_CHECK(cudaGetLastError());
-        cgRowsKernel<R><<<gridP, kThreads, 0, stream>>>(c, coef, g);
+        cgRowsKernel<R><<<rowsGrid(np), kRowsThreads, 0, stream>>>(c, coef, g);
         CUDA_CHECK(cudaGetLastError());
         // The components: roots, the particles sorted by root, the segments; then a block per component.
         cgRootKernel<R><<<gridLanes, kThreads, 0, stream>>>(c, vel, fin, sw, su, stepArg, b, g);

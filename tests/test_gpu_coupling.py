@@ -77,6 +77,7 @@ def chain_case(stencil, factory, props, capacity=0):
     force.setDragScheme(LBMForce.Centered)
     force.setInterpolationStencil(getattr(LBMForce, stencil))
     force.setFriction(10.0)
+    force.setTemperature(0.0)
     force.setFluidMomentumRemovalFrequency(0)
     context = lbm_b200.Context(system, lbm_b200.VerletIntegrator(0.01), factory, props)
     context.setPositions(np.mod(np.array(positions), 6.0))
