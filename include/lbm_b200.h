@@ -279,7 +279,7 @@ LbmStatus lbm_set_solver_limits(LbmKernel* kernel, int max_iterations, long long
 
 /* The centred stencil drag solves each connected component of its coupling matrix (particles whose stencils share
    nodes: a bead chain, a cluster) by the conjugate gradients in one thread block, and a component of more than
-   `particles` particles (default 4096; 0 restores it, a negative value sends every component there) by the
+   `particles` particles (default and maximum 1024; 0 restores it, a negative value sends every component there) by the
    cooperative solve over all particles, whose grid barriers the poll limit above bounds.  Both give the reference's
    solution within its tolerance. */
 LbmStatus lbm_set_component_capacity(LbmKernel* kernel, int particles);

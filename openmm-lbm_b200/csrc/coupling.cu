@@ -477,6 +477,7 @@ struct SparseCg {
     int4* cellList;        // kCgCellCapacity per cell: the particle and its first stencil index on each axis
     int* rowCount;         // entries per row
     int* rowIndex;         // entry e of row k at e np + k: the column particle
+    int* rowLocal;         // same layout: the column's position among the members of its component
     double* rowValue;      // K_kl, same layout
     double* Ap;            // A p, 3 per particle
     int* overflow;         // nonzero: a cell or a row over its capacity
@@ -963,6 +964,8 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
 // ------------------------------------------------------------------------------------------------------
 
 constexpr int kComponentThreads = 256;
+static_assert(kDefaultComponentCapacity <= 1024, "the component kernel holds at most 1024 members");
+constexpr int kComponentMembers = 1024;    // members of a component held in shared memory
 
 template <typename R>
 __global__ void __launch_bounds__(kThreads)
@@ -1008,31 +1011,32 @@ __device__ __forceinline__ void componentSum(double v[6], double (*red)[6]) {
     }
 }
 
-// (A v)_i = v_i (1 + a)/m_i + a sum_l K_il v_l over row i, for the three components.
-__device__ __forceinline__ void componentProduct(const SparseCg& g, const CouplingView& c, int i, const double* v,
-                                                 double out[3]) {
-    double s0 = 0, s1 = 0, s2 = 0;
-    const int n = g.rowCount[i];
-    for (int e = 0; e < n; e++) {
-        const int l = g.rowIndex[(long long) e*c.np + i];
-        const double K = g.rowValue[(long long) e*c.np + i];
-        s0 += K*v[3*l];
-        s1 += K*v[3*l+1];
-        s2 += K*v[3*l+2];
+// Position of particle l among the n sorted members of a component (l is one of them).
+__device__ __forceinline__ int memberPosition(const int* members, int n, int l) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (members[mid] < l)
+            lo = mid + 1;
+        else
+            hi = mid;
     }
-    const double self = (1.0 + c.a)/c.mass[i];
-    out[0] = v[3*i]*self + s0*c.a;
-    out[1] = v[3*i+1]*self + s1*c.a;
-    out[2] = v[3*i+2]*self + s2*c.a;
+    return lo;
 }
 
+// One block per component of at most kComponentMembers particles: the members and the search direction p in shared
+// memory, the rows of the members (their entries replaced by member positions in the first product, rowLocal) and the
+// other vectors in global memory, each thread owning the rows j = threadIdx.x, + blockDim.x, ...
 __global__ void __launch_bounds__(kComponentThreads)
 cgComponentKernel(CouplingView c, double tolerance, int maxIterations, int capacity, CgBuffers b, SparseCg g) {
     __shared__ double red[kComponentThreads/32][6];
+    __shared__ int memberS[kComponentMembers];
+    __shared__ double pS[3*kComponentMembers];
     if (*((volatile int*) g.overflow) != 0)
         return;
     const int components = *g.componentCount;
-    const double tol2 = tolerance*tolerance;
+    const double tol2 = tolerance*tolerance, a = c.a;
+    const long long np = c.np;
     for (int ci = blockIdx.x; ci < components; ci += gridDim.x) {
         const int root = g.componentRoot[ci];
         const int start = g.componentStart[root], n = g.componentEnd[root] - start;
@@ -1041,35 +1045,45 @@ cgComponentKernel(CouplingView c, double tolerance, int maxIterations, int capac
                 atomicExch(g.componentOverflow, 1);
             continue;
         }
-        const int* members = g.member + start;
-        // r = rhs - A F, z = r/diag, p = z (F = rhs/diag from the start); r.z, b.b and r.r per axis.
-        double acc[6] = {0, 0, 0, 0, 0, 0}, norm[3] = {0, 0, 0};
+        for (int j = threadIdx.x; j < n; j += blockDim.x)
+            memberS[j] = g.member[start + j];
+        __syncthreads();
+        // r = rhs - A F, z = r/diag, p = z (F = rhs/diag from the start); r.z, r.r and b.b per axis.  The product
+        // reads F of the other members from global memory and records each entry's member position.
+        double acc[6] = {0, 0, 0, 0, 0, 0}, norm[6] = {0, 0, 0, 0, 0, 0};
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
-            const int i = members[j];
-            double AF[3];
-            componentProduct(g, c, i, b.F, AF);
-            const double diag = b.diag[i];
+            const int i = memberS[j];
+            const int entries = g.rowCount[i];
+            double s0 = 0, s1 = 0, s2 = 0;
+            for (int e = 0; e < entries; e++) {
+                const int l = g.rowIndex[e*np + i];
+                const double K = g.rowValue[e*np + i];
+                g.rowLocal[e*np + i] = memberPosition(memberS, n, l);
+                s0 += K*b.F[3*l];
+                s1 += K*b.F[3*l+1];
+                s2 += K*b.F[3*l+2];
+            }
+            const double self = (1.0 + a)/c.mass[i], diag = b.diag[i], s[3] = {s0, s1, s2};
             for (int d = 0; d < 3; d++) {
                 const double rhs = b.rhs[3*i+d];
-                const double r = rhs - AF[d], z = r*(1.0/diag);
+                const double r = rhs - (b.F[3*i+d]*self + s[d]*a), z = r*(1.0/diag);
                 b.r[3*i+d] = r;
                 b.z[3*i+d] = z;
-                b.p[3*i+d] = z;
+                pS[3*j+d] = z;
                 acc[d] += r*z;
                 acc[3+d] += r*r;
                 norm[d] += rhs*rhs;
             }
         }
         componentSum(acc, red);
+        componentSum(norm, red);
         double rz[3] = {acc[0], acc[1], acc[2]}, rr[3] = {acc[3], acc[4], acc[5]};
-        double nb[6] = {norm[0], norm[1], norm[2], 0, 0, 0};
-        componentSum(nb, red);
         int iteration = 0;
         bool failed = false;   // the same in every thread: every decision comes from the block sums
         for (;; iteration++) {
             bool converged = true;
             for (int d = 0; d < 3; d++)
-                if (rr[d] > tol2*nb[d])
+                if (rr[d] > tol2*norm[d])
                     converged = false;
             if (converged)
                 break;
@@ -1080,12 +1094,22 @@ cgComponentKernel(CouplingView c, double tolerance, int maxIterations, int capac
             // A p and p.Ap (p was written before the last block barrier).
             double pAp[6] = {0, 0, 0, 0, 0, 0};
             for (int j = threadIdx.x; j < n; j += blockDim.x) {
-                const int i = members[j];
-                double Ap[3];
-                componentProduct(g, c, i, b.p, Ap);
+                const int i = memberS[j];
+                const int entries = g.rowCount[i];
+                double s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll 4
+                for (int e = 0; e < entries; e++) {
+                    const int lj = g.rowLocal[e*np + i];
+                    const double K = g.rowValue[e*np + i];
+                    s0 += K*pS[3*lj];
+                    s1 += K*pS[3*lj+1];
+                    s2 += K*pS[3*lj+2];
+                }
+                const double self = (1.0 + a)/c.mass[i], s[3] = {s0, s1, s2};
                 for (int d = 0; d < 3; d++) {
-                    g.Ap[3*i+d] = Ap[d];
-                    pAp[d] += b.p[3*i+d]*Ap[d];
+                    const double Ap = pS[3*j+d]*self + s[d]*a;
+                    g.Ap[3*i+d] = Ap;
+                    pAp[d] += pS[3*j+d]*Ap;
                 }
             }
             componentSum(pAp, red);
@@ -1094,10 +1118,10 @@ cgComponentKernel(CouplingView c, double tolerance, int maxIterations, int capac
                 alpha[d] = pAp[d] > 0 ? rz[d]/pAp[d] : 0.0;
             double next[6] = {0, 0, 0, 0, 0, 0};
             for (int j = threadIdx.x; j < n; j += blockDim.x) {
-                const int i = members[j];
+                const int i = memberS[j];
                 const double diag = b.diag[i];
                 for (int d = 0; d < 3; d++) {
-                    b.F[3*i+d] += alpha[d]*b.p[3*i+d];
+                    b.F[3*i+d] += alpha[d]*pS[3*j+d];
                     const double r = b.r[3*i+d] - alpha[d]*g.Ap[3*i+d];
                     const double z = r*(1.0/diag);
                     b.r[3*i+d] = r;
@@ -1114,9 +1138,9 @@ cgComponentKernel(CouplingView c, double tolerance, int maxIterations, int capac
                 rr[d] = next[3+d];
             }
             for (int j = threadIdx.x; j < n; j += blockDim.x) {
-                const int i = members[j];
+                const int i = memberS[j];
                 for (int d = 0; d < 3; d++)
-                    b.p[3*i+d] = b.z[3*i+d] + beta[d]*b.p[3*i+d];
+                    pS[3*j+d] = b.z[3*i+d] + beta[d]*pS[3*j+d];
             }
             __syncthreads();
         }
@@ -1343,6 +1367,7 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
             CUDA_CHECK(cudaMalloc(&g.rowCount, sizeof(int)*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.rowIndex, sizeof(int)*kCgRowCapacity*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.rowValue, sizeof(double)*kCgRowCapacity*(size_t) np));
+            CUDA_CHECK(cudaMalloc(&g.rowLocal, sizeof(int)*kCgRowCapacity*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.Ap, v3));
             g.overflow = statusDev + 2;
             CUDA_CHECK(cudaMalloc(&g.parent, sizeof(int)*(size_t) np));
@@ -1397,7 +1422,7 @@ void CouplingEngine::release() {
         SparseCg& g = dev->sparse;
         cudaFree(g.cellOf); cudaFree(g.cellCount); cudaFree(g.cellList);
         cudaFree(g.rowCount); cudaFree(g.rowIndex); cudaFree(g.rowValue); cudaFree(g.Ap);
-        cudaFree(g.parent); cudaFree(g.componentStart); cudaFree(g.componentEnd); cudaFree(g.componentRoot);
+        cudaFree(g.rowLocal); cudaFree(g.parent); cudaFree(g.componentStart); cudaFree(g.componentEnd); cudaFree(g.componentRoot);
         delete dev;
         dev = nullptr;
     }
@@ -1573,7 +1598,8 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
 }
 
 void CouplingEngine::setComponentCapacity(int particles) {
-    componentCapacity = particles > 0 ? particles : particles == 0 ? kDefaultComponentCapacity : 0;
+    componentCapacity = particles > 0 ? std::min(particles, kComponentMembers) :
+                        particles == 0 ? kDefaultComponentCapacity : 0;
 }
 
 void CouplingEngine::setSolverLimits(int maxIterations, long long barrierPolls) {

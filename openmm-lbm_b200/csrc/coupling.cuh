@@ -13,7 +13,7 @@ struct CouplingView;
 // (ReferenceLBMKernels.cpp:864-866) and the polls after which a block waiting at a grid barrier gives up.
 constexpr int kDefaultCgIterations = 1000;
 constexpr long long kDefaultBarrierPolls = 1LL << 26;
-constexpr int kDefaultComponentCapacity = 4096;   // particles of a component solved by one thread block
+constexpr int kDefaultComponentCapacity = 1024;   // particles of a component solved by one thread block (at most)
 
 class CouplingEngine {
 public:
