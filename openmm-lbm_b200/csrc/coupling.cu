@@ -451,9 +451,10 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
 // dozen entries per particle instead of a pass over the lattice nodes of all stencils.
 //   cgBinKernel     per particle: its cell (cells of kCgCellEdge nodes, on the first stencil index of the stencil
 //                   pass), inserted into a fixed-capacity cell list; per slot: w/rho
-//   cgRowsKernel    8 lanes per particle k: the particles of the neighbouring cells whose first stencil indices are
+//   cgRowsKernel    one warp per particle k: the particles of the neighbouring cells whose first stencil indices are
 //                   within a stencil width of k's on every axis, sorted by index (so that every row, and every sum
-//                   over it, has one order), and K_kl for each
+//                   over it, has one order), and K_kl for each, a lane per entry; and the union of k with the
+//                   entries above it
 //   centeredSparseKernel  the conjugate gradients (same start, preconditioner, stopping rule and per-component
 //                   iteration as the kernel above) in one cooperative launch, two grid barriers per iteration
 // Rows are stored entry-major (entry e of row k at e np + k), so that the threads of consecutive rows read them
@@ -465,8 +466,6 @@ constexpr int kCgCellEdge = 4;      // nodes per cell edge (no less than the wid
 constexpr int kCgCellCapacity = 64; // particles per cell
 constexpr int kCgRowCapacity = 128; // entries per row of K
 constexpr int kSolveThreads = 1024; // threads per block of the solve (one block per SM: few barrier arrivals)
-constexpr int kRowLanes = 8;        // lanes of a warp per row of the rows kernel (4 rows per warp)
-constexpr int kRowsThreads = 128;   // threads per block of the rows kernel (16 rows, 26-30 KB of shared memory)
 
 struct SparseCg {
     int4* axisIndex;       // 3 per particle: the stencil's node indices on each axis (-1 past the width)
@@ -555,173 +554,154 @@ __device__ __forceinline__ int periodicDistance(int a, int b, int n) {
     return min(d, n - d);
 }
 
-// K_kl = sum over k's slots (ix, iy, iz) of (w/rho)_k times l's weight at the same node: the product of l's axis
-// weights at the entries with k's indices (on each axis the first such entry: later duplicates, at clamped open faces,
-// have weight zero).  In the precision of the fluid's arithmetic, in which the slots' w/rho are stored.
-template <typename R, int W>
-__device__ __forceinline__ R couplingEntry(const R* coefK, const int4 ik[3], const int4* __restrict__ axisIndex,
-                                           const double2* __restrict__ axisWeight, int l) {
-    R shifted[3][W];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        const int4 il = axisIndex[3*l + a];
-        const double2 w01 = axisWeight[6*l + 2*a], w23 = axisWeight[6*l + 2*a + 1];
-        const int mine[4] = {ik[a].x, ik[a].y, ik[a].z, ik[a].w};
-#pragma unroll
-        for (int i = 0; i < W; i++) {
-            double v = 0.0;
-            if (mine[i] >= 0) {
-                if (il.w == mine[i]) v = w23.y;
-                if (il.z == mine[i]) v = w23.x;
-                if (il.y == mine[i]) v = w01.y;
-                if (il.x == mine[i]) v = w01.x;
-            }
-            shifted[a][i] = (R) v;
-        }
-    }
-    R K = 0;
-#pragma unroll
-    for (int iz = 0; iz < W; iz++) {
-        if (shifted[2][iz] == (R) 0)
-            continue;
-#pragma unroll
-        for (int iy = 0; iy < W; iy++) {
-            if (shifted[1][iy] == (R) 0)
-                continue;
-            const R wyz = shifted[1][iy]*shifted[2][iz];
-#pragma unroll
-            for (int ix = 0; ix < W; ix++)
-                K += coefK[ix + W*(iy + W*iz)]*(shifted[0][ix]*wyz);
-        }
-    }
-    return K;
-}
-
-// The values of row k, entries j = sub, sub + kRowLanes, ... of the sorted list, and the union of k with the entries
-// above it.
-template <typename R, int W>
-__device__ __forceinline__ void rowValues(const CouplingView& c, const SparseCg& g, int k, const R* coefK,
-                                          const int* sorted, int found, int sub) {
-    const int4 ik[3] = {g.axisIndex[3*k], g.axisIndex[3*k + 1], g.axisIndex[3*k + 2]};
-    for (int j = sub; j < found; j += kRowLanes) {
-        const int l = sorted[j];
-        const R K = couplingEntry<R, W>(coefK, ik, g.axisIndex, g.axisWeight, l);
-        g.rowIndex[(long long) j*c.np + k] = l;
-        g.rowValue[(long long) j*c.np + k] = (double) K;
-        if (l > k)
-            unite(g.parent, k, l);
-    }
-}
-
-// kRowLanes lanes per particle k (32/kRowLanes particles per warp): the particles of the neighbouring cells whose first
-// stencil indices are within a stencil width of k's on every axis (k included), sorted by index (so that every row,
-// and every sum over it, has one order), and K_kl for each.  Lane groups that run out of work still take part in the
-// warp's ballots.
 template <typename R>
-__global__ void __launch_bounds__(kRowsThreads)
+__global__ void __launch_bounds__(kThreads, 4)
 cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
-    constexpr int P = 32/kRowLanes, GW = kRowsThreads/kRowLanes;     // particles per warp, per block
-    __shared__ int candidates[GW][kCgRowCapacity];
-    __shared__ int sorted[GW][kCgRowCapacity];
-    __shared__ R rowCoef[GW][64];
-    __shared__ int cellEnd[GW][28], cellStart[GW][28], cellId[GW][28];
-    const int lane = threadIdx.x & 31, sub = lane%kRowLanes, group = lane/kRowLanes;
-    const int slot = threadIdx.x/kRowLanes;                       // this lane group's arrays
-    const unsigned groupMask = ((1u << kRowLanes) - 1u) << (group*kRowLanes);
-    const int size[3] = {c.nx, c.ny, c.nz};
-    const int S = c.slots;
+    __shared__ int candidates[kThreads/32][kCgRowCapacity];
+    __shared__ int sorted[kThreads/32][kCgRowCapacity];
+    __shared__ R rowCoef[kThreads/32][64];
+    __shared__ int cellEnd[kThreads/32][32], cellStart[kThreads/32][32], cellId[kThreads/32][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int* list = candidates[warp];
     const int firstWarp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
     const int warps = (gridDim.x*blockDim.x) >> 5;
-    for (int base = firstWarp*P; base < c.np; base += warps*P) {
-        const int k = base + group;
-        const bool active = k < c.np;
-        int4 fk = make_int4(0, 0, 0, 0);
-        if (active) {
-            for (int s = sub; s < S; s += kRowLanes)
-                rowCoef[slot][s] = coef[(long long) k*S + s];
-            fk = g.firstIndex[k];
-            const int key = g.cellOf[k];
-            const int home[3] = {key%g.cells[0], (key/g.cells[0])%g.cells[1], key/(g.cells[0]*g.cells[1])};
-            // The 27 neighbouring cells (j%3 - 1, j/3%3 - 1, j/9 - 1), lane sub taking j = sub, sub + kRowLanes, ...;
-            // a cell that an axis with fewer than 3 cells reaches twice is taken once (by its first offset).
-            for (int j = sub; j < 27; j += kRowLanes) {
-                const int off[3] = {j%3 - 1, (j/3)%3 - 1, j/9 - 1};
-                bool first = true;
-                int cc[3];
-                for (int a = 0; a < 3; a++) {
-                    const int n = g.cells[a];
-                    cc[a] = ((home[a] + off[a])%n + n)%n;
-                    for (int d = -1; d < off[a]; d++)
-                        first &= ((home[a] + d)%n + n)%n != cc[a];
-                }
-                const int cell = first ? cc[0] + g.cells[0]*(cc[1] + g.cells[1]*cc[2]) : -1;
-                cellId[slot][j] = cell;
-                cellEnd[slot][j] = cell >= 0 ? min((int) g.cellCount[cell], kCgCellCapacity) : 0;
+    const int size[3] = {c.nx, c.ny, c.nz};
+    const int w = c.width, S = c.slots;
+    for (int k = firstWarp; k < c.np; k += warps) {
+        for (int s = lane; s < S; s += 32)
+            rowCoef[warp][s] = coef[(long long) k*S + s];
+        const int4 fk = g.firstIndex[k];
+        const int key = g.cellOf[k];
+        const int home[3] = {key%g.cells[0], (key/g.cells[0])%g.cells[1], key/(g.cells[0]*g.cells[1])};
+        // Lane j < 27 takes the neighbouring cell (j%3 - 1, j/3%3 - 1, j/9 - 1); a cell that an axis with fewer than
+        // 3 cells reaches twice is taken once (by its first offset).
+        int cell = -1, members = 0;
+        if (lane < 27) {
+            const int off[3] = {lane%3 - 1, (lane/3)%3 - 1, lane/9 - 1};
+            bool first = true;
+            int cc[3];
+            for (int a = 0; a < 3; a++) {
+                const int n = g.cells[a];
+                cc[a] = ((home[a] + off[a])%n + n)%n;
+                for (int d = -1; d < off[a]; d++)
+                    first &= ((home[a] + d)%n + n)%n != cc[a];
+            }
+            if (first) {
+                cell = cc[0] + g.cells[0]*(cc[1] + g.cells[1]*cc[2]);
+                members = min((int) g.cellCount[cell], kCgCellCapacity);
             }
         }
-        __syncwarp();
-        // Running ends of the member counts (lane 0 of the group; 27 adds).
-        int total = 0;
-        if (active && sub == 0) {
-            for (int j = 0; j < 27; j++) {
-                cellStart[slot][j] = total;
-                total += cellEnd[slot][j];
-                cellEnd[slot][j] = total;
-            }
+        // Exclusive scan of the member counts over the lanes.
+        int start = members;
+        for (int d = 1; d < 32; d *= 2) {
+            const int v = __shfl_up_sync(0xFFFFFFFFu, start, d);
+            if (lane >= d)
+                start += v;
         }
-        total = __shfl_sync(0xFFFFFFFFu, total, group*kRowLanes);
+        const int total = __shfl_sync(0xFFFFFFFFu, start, 31);
+        cellEnd[warp][lane] = lane < 27 ? start : 0x7FFFFFFF;
+        cellStart[warp][lane] = start - members;
+        cellId[warp][lane] = cell;
         __syncwarp();
-        int found = 0;     // the same in every lane of the group
-        for (int e0 = 0; __any_sync(0xFFFFFFFFu, e0 < total); e0 += kRowLanes) {
-            const int e = e0 + sub;
-            bool near = false;
-            int l = -1;
-            if (e < total) {
-                // The cell holding member e: the first of the 27 whose running end exceeds e.
-                int lo = 0, hi = 26;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (cellEnd[slot][mid] > e)
-                        hi = mid;
-                    else
-                        lo = mid + 1;
+        int found = 0;     // the same in every lane
+        // Four rounds of 32 members at a time, their loads issued together.
+        for (int base = 0; base < total; base += 128) {
+            int lq[4];
+            bool nq[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int e = base + 32*r + lane;
+                lq[r] = -1;
+                nq[r] = false;
+                if (e < total) {
+                    // The cell holding member e: the first of the 27 whose running end exceeds e.
+                    int lo = 0, hi = 26;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (cellEnd[warp][mid] > e)
+                            hi = mid;
+                        else
+                            lo = mid + 1;
+                    }
+                    const int4 m = g.cellList[(long long) cellId[warp][lo]*kCgCellCapacity + (e - cellStart[warp][lo])];
+                    lq[r] = m.x;
+                    nq[r] = periodicDistance(m.y, fk.x, size[0]) < c.width &&
+                            periodicDistance(m.z, fk.y, size[1]) < c.width &&
+                            periodicDistance(m.w, fk.z, size[2]) < c.width;
                 }
-                const int4 m = g.cellList[(long long) cellId[slot][lo]*kCgCellCapacity + (e - cellStart[slot][lo])];
-                l = m.x;
-                near = periodicDistance(m.y, fk.x, size[0]) < c.width && periodicDistance(m.z, fk.y, size[1]) < c.width &&
-                       periodicDistance(m.w, fk.z, size[2]) < c.width;
             }
-            const unsigned ballot = __ballot_sync(0xFFFFFFFFu, near) & groupMask;
-            const int at = found + __popc(ballot & ((1u << lane) - 1u));
-            if (near && at < kCgRowCapacity)
-                candidates[slot][at] = l;
-            found += __popc(ballot);
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const unsigned ballot = __ballot_sync(0xFFFFFFFFu, nq[r]);
+                const int at = found + __popc(ballot & ((1u << lane) - 1u));
+                if (nq[r] && at < kCgRowCapacity)
+                    list[at] = lq[r];
+                found += __popc(ballot);
+            }
         }
         __syncwarp();
         if (found > kCgRowCapacity) {
-            if (active && sub == 0)
+            if (lane == 0)
                 atomicExch(g.overflow, 1);
             found = kCgRowCapacity;
         }
         // Rank sort (particle indices are distinct).
-        if (active)
-            for (int j = sub; j < found; j += kRowLanes) {
-                const int v = candidates[slot][j];
-                int rank = 0;
-                for (int i = 0; i < found; i++)
-                    rank += candidates[slot][i] < v;
-                sorted[slot][rank] = v;
-            }
-        __syncwarp();
-        if (active) {
-            switch (c.width) {
-            case 2: rowValues<R, 2>(c, g, k, rowCoef[slot], sorted[slot], found, sub); break;
-            case 3: rowValues<R, 3>(c, g, k, rowCoef[slot], sorted[slot], found, sub); break;
-            default: rowValues<R, 4>(c, g, k, rowCoef[slot], sorted[slot], found, sub); break;
-            }
-            if (sub == 0)
-                g.rowCount[k] = found;
+        for (int j = lane; j < found; j += 32) {
+            const int v = list[j];
+            int rank = 0;
+            for (int i = 0; i < found; i++)
+                rank += list[i] < v;
+            sorted[warp][rank] = v;
         }
+        __syncwarp();
+        // K_kl = sum over k's slots (ix, iy, iz) of (w/rho)_k times l's weight at the same node, the product of l's
+        // axis weights at the entries with k's indices (on each axis the first such entry: later duplicates, at
+        // clamped open faces, have weight zero).  Lanes over the row's entries.
+        const int4 ik[3] = {g.axisIndex[3*k], g.axisIndex[3*k + 1], g.axisIndex[3*k + 2]};
+        for (int j = lane; j < found; j += 32) {
+            const int l = sorted[warp][j];
+            // In the precision of the fluid's arithmetic (the slots' w/rho are stored in it).
+            R shifted[3][4];
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const int4 il = g.axisIndex[3*l + a];
+                const double2 w01 = g.axisWeight[6*l + 2*a], w23 = g.axisWeight[6*l + 2*a + 1];
+                const int mine[4] = {ik[a].x, ik[a].y, ik[a].z, ik[a].w};
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    double v = 0.0;
+                    if (mine[i] >= 0) {
+                        if (il.w == mine[i]) v = w23.y;
+                        if (il.z == mine[i]) v = w23.x;
+                        if (il.y == mine[i]) v = w01.y;
+                        if (il.x == mine[i]) v = w01.x;
+                    }
+                    shifted[a][i] = (R) v;
+                }
+            }
+            R K = 0;
+#pragma unroll
+            for (int iz = 0; iz < 4; iz++) {
+                if (iz >= w || shifted[2][iz] == (R) 0)
+                    continue;
+#pragma unroll
+                for (int iy = 0; iy < 4; iy++) {
+                    if (iy >= w || shifted[1][iy] == (R) 0)
+                        continue;
+                    const R wyz = shifted[1][iy]*shifted[2][iz];
+#pragma unroll
+                    for (int ix = 0; ix < 4; ix++)
+                        if (ix < w)
+                            K += rowCoef[warp][ix + w*(iy + w*iz)]*(shifted[0][ix]*wyz);
+                }
+            }
+            g.rowIndex[(long long) j*c.np + k] = l;
+            g.rowValue[(long long) j*c.np + k] = (double) K;
+            if (l > k)
+                unite(g.parent, k, l);
+        }
+        if (lane == 0)
+            g.rowCount[k] = found;
         __syncwarp();
     }
 }
@@ -966,6 +946,7 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
 constexpr int kComponentThreads = 256;
 static_assert(kDefaultComponentCapacity <= 1024, "the component kernel holds at most 1024 members");
 constexpr int kComponentMembers = 1024;    // members of a component held in shared memory
+static_assert(kComponentMembers <= 4*kComponentThreads, "a thread of the component kernel owns at most 4 rows");
 
 template <typename R>
 __global__ void __launch_bounds__(kThreads)
@@ -1045,36 +1026,46 @@ cgComponentKernel(CouplingView c, double tolerance, int maxIterations, int capac
                 atomicExch(g.componentOverflow, 1);
             continue;
         }
-        for (int j = threadIdx.x; j < n; j += blockDim.x)
-            memberS[j] = g.member[start + j];
-        __syncthreads();
-        // r = rhs - A F, z = r/diag, p = z (F = rhs/diag from the start); r.z, r.r and b.b per axis.  The product
-        // reads F of the other members from global memory and records each entry's member position.
-        double acc[6] = {0, 0, 0, 0, 0, 0}, norm[6] = {0, 0, 0, 0, 0, 0};
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const int i = g.member[start + j];
+            memberS[j] = i;
+            for (int d = 0; d < 3; d++)
+                pS[3*j+d] = b.F[3*i+d];
+        }
+        __syncthreads();
+        // r = rhs - A F, z = r/diag, p = z (F = rhs/diag from the start, in pS for this product); r.z, r.r and b.b per
+        // axis.  The product records each entry's member position.
+        double acc[6] = {0, 0, 0, 0, 0, 0}, norm[6] = {0, 0, 0, 0, 0, 0};
+        double zOwn[4][3];     // z of the rows of this thread (at most 1024/256), written to pS after the barrier
+        for (int j = threadIdx.x, o = 0; j < n; j += blockDim.x, o++) {
             const int i = memberS[j];
             const int entries = g.rowCount[i];
             double s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll 4
             for (int e = 0; e < entries; e++) {
-                const int l = g.rowIndex[e*np + i];
+                const int lj = memberPosition(memberS, n, g.rowIndex[e*np + i]);
                 const double K = g.rowValue[e*np + i];
-                g.rowLocal[e*np + i] = memberPosition(memberS, n, l);
-                s0 += K*b.F[3*l];
-                s1 += K*b.F[3*l+1];
-                s2 += K*b.F[3*l+2];
+                g.rowLocal[e*np + i] = lj;
+                s0 += K*pS[3*lj];
+                s1 += K*pS[3*lj+1];
+                s2 += K*pS[3*lj+2];
             }
             const double self = (1.0 + a)/c.mass[i], diag = b.diag[i], s[3] = {s0, s1, s2};
             for (int d = 0; d < 3; d++) {
                 const double rhs = b.rhs[3*i+d];
-                const double r = rhs - (b.F[3*i+d]*self + s[d]*a), z = r*(1.0/diag);
+                const double r = rhs - (pS[3*j+d]*self + s[d]*a), z = r*(1.0/diag);
                 b.r[3*i+d] = r;
                 b.z[3*i+d] = z;
-                pS[3*j+d] = z;
+                zOwn[o][d] = z;
                 acc[d] += r*z;
                 acc[3+d] += r*r;
                 norm[d] += rhs*rhs;
             }
         }
+        __syncthreads();
+        for (int j = threadIdx.x, o = 0; j < n; j += blockDim.x, o++)
+            for (int d = 0; d < 3; d++)
+                pS[3*j+d] = zOwn[o][d];
         componentSum(acc, red);
         componentSum(norm, red);
         double rz[3] = {acc[0], acc[1], acc[2]}, rr[3] = {acc[3], acc[4], acc[5]};
@@ -1229,11 +1220,6 @@ int widthOf(int stencil) {
 // Blocks for one warp per particle.
 int warpGrid(long long particles) {
     return (int) std::max(1LL, std::min(4736LL, (particles*32 + kThreads - 1)/kThreads));
-}
-
-// Blocks of the rows kernel: kRowLanes lanes per particle.
-int rowsGrid(long long particles) {
-    return (int) std::max(1LL, std::min(8*1184LL, (particles*kRowLanes + kRowsThreads - 1)/kRowsThreads));
 }
 
 } // namespace
@@ -1542,7 +1528,7 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
         CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*8, stream));
         cgBinKernel<R><<<gridSlots, kThreads, 0, stream>>>(c, sw, su, coef, g);
         CUDA_CHECK(cudaGetLastError());
-        cgRowsKernel<R><<<rowsGrid(np), kRowsThreads, 0, stream>>>(c, coef, g);
+        cgRowsKernel<R><<<warpGrid(np), kThreads, 0, stream>>>(c, coef, g);
         CUDA_CHECK(cudaGetLastError());
         // The components: roots, the particles sorted by root, the segments; then a block per component.
         cgRootKernel<R><<<gridLanes, kThreads, 0, stream>>>(c, vel, fin, sw, su, stepArg, b, g);

@@ -5,14 +5,12 @@
 //  convWeightGradKernel dW[cout][k] = sum_voxels dy[voxel][cout] A[voxel][k]; CTAs over (cout tile, k tile, voxel
 //                       split), the K dimension of the GEMM being the voxels; results added with FP32 atomics
 //
-// The GEMM core: 128 x N tiles, K in stages of 64 BF16 (one 128-byte row), two shared-memory buffers used in turn.
-// All 128 threads gather a stage into its buffer in the canonical K-major layout with the 128-byte swizzle (8-row
-// atoms of 128-byte rows, the 16-byte chunk index XOR the row within the atom), make it visible to the tensor core's
-// proxy, and one thread issues four tcgen05.mma (K = 16 each, BF16 x BF16 -> FP32 in tensor memory) and commits them
-// to the buffer's mbarrier; the threads go on to gather the next stage into the other buffer while the tensor cores
-// work, and wait on a buffer's mbarrier only before they write it again (bounded: a wait that gives up sets the
-// status flag and the CTA leaves after the MMAs in flight are done and its tensor memory is freed).  The epilogue
-// reads the accumulators with tcgen05.ld (warp w owns lanes 32w..32w+31 = rows of the tile).
+// The GEMM core: 128 x N tiles, K in stages of 64 BF16 (one 128-byte row).  All 128 threads gather a stage into
+// shared memory in the canonical K-major layout with the 128-byte swizzle (8-row atoms of 128-byte rows, the 16-byte
+// chunk index XOR the row within the atom), make it visible to the tensor core's proxy, and one thread issues four
+// tcgen05.mma (K = 16 each, BF16 x BF16 -> FP32 in tensor memory) and commits them to an mbarrier that every
+// thread waits on (bounded: a wait that gives up sets the status flag and the CTA leaves after freeing its tensor
+// memory).  The epilogue reads the accumulators with tcgen05.ld (warp w owns lanes 32w..32w+31 = rows of the tile).
 // Descriptor layouts: the shared-memory matrix descriptor (start >> 4, leading offset, stride offset 1024 B >> 4,
 // version 1, swizzle mode 2 = 128 B) and the instruction descriptor (F32 accumulator, BF16 A and B, both K-major,
 // N >> 3, M >> 4) of the PTX ISA's tcgen05 matrix and instruction descriptor formats.
@@ -101,40 +99,29 @@ __device__ __forceinline__ uint32_t tmemColumns(int n) {
     return n <= 32 ? 32u : (n <= 64 ? 64u : (n <= 128 ? 128u : 256u));
 }
 
-// Setup common to both kernels: two 1024-byte aligned pairs of tiles (stages), tensor memory of `ncols` columns
-// (warp 0), an mbarrier per stage.  Stage c of the K loop uses buffer c & 1; its MMAs are committed to that buffer's
-// mbarrier, whose (c >> 1)-th phase completes when they (and every earlier MMA) are done.  The gather of stage c + 1
-// runs while the tensor cores work on stage c; a buffer is written again only after the MMAs of two stages before
-// have completed.
-constexpr int kStages = 2;
-
-struct Stages {
-    uint8_t* tileA[kStages];
-    uint8_t* tileB[kStages];
-    uint32_t mbar[kStages];
+// Setup common to both kernels: 1024-byte aligned tiles, tensor memory of `ncols` columns (warp 0), the mbarrier.
+struct Stage {
+    uint8_t* tileA;
+    uint8_t* tileB;
+    uint32_t mbar;
     uint32_t tmem;
 };
 
-__device__ __forceinline__ Stages setupStages(uint8_t* raw, int rowsB, uint32_t ncols) {
+__device__ __forceinline__ Stage setupStage(uint8_t* raw, int rowsB, uint32_t ncols) {
     uint32_t s = smemAddr(raw);
     uint8_t* base = raw + ((1024 - (s & 1023)) & 1023);
-    const size_t tileBytes = (size_t) kTileM*128 + (size_t) ((rowsB*128 + 1023)/1024)*1024;
-    Stages st;
-    for (int k = 0; k < kStages; k++) {
-        st.tileA[k] = base + k*tileBytes;
-        st.tileB[k] = st.tileA[k] + kTileM*128;
-    }
-    uint64_t* bar = reinterpret_cast<uint64_t*>(base + kStages*tileBytes);
-    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + kStages);
-    for (int k = 0; k < kStages; k++)
-        st.mbar[k] = smemAddr(bar + k);
+    Stage st;
+    st.tileA = base;
+    st.tileB = base + kTileM*128;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(st.tileB + rowsB*128);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 1);
+    st.mbar = smemAddr(bar);
     if (threadIdx.x/32 == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(smemAddr(slot)), "r"(ncols) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (threadIdx.x == 0) {
-        for (int k = 0; k < kStages; k++)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(st.mbar[k]), "r"(1) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(st.mbar), "r"(1) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     fenceBeforeSync();
@@ -144,38 +131,34 @@ __device__ __forceinline__ Stages setupStages(uint8_t* raw, int rowsB, uint32_t 
     return st;
 }
 
-__device__ __forceinline__ void releaseStages(const Stages& st, uint32_t ncols) {
+__device__ __forceinline__ void releaseStage(const Stage& st, uint32_t ncols) {
     fenceBeforeSync();
     __syncthreads();
     if (threadIdx.x/32 == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(st.tmem), "r"(ncols) : "memory");
 }
 
-// Wait (every thread, bounded) until the MMAs of stage c are done; false, for every thread, if a wait gave up.
-__device__ __forceinline__ bool waitStage(const Stages& st, int c, long long limit) {
-    bool ok = waitParity(st.mbar[c & 1], (uint32_t) ((c >> 1) & 1), limit);
-    return __syncthreads_and(ok) != 0;
-}
-
-// Issue stage c: the tiles of buffer c & 1 are in shared memory; thread 0 issues the four K = 16 MMAs and commits them.
-__device__ __forceinline__ void issueStage(const Stages& st, uint32_t idesc, int c) {
+// One stage: the tiles are in shared memory; thread 0 issues the four K = 16 MMAs and commits; all threads wait.
+// Returns false (for every thread) if the wait gave up; the caller then drains the stage (drainStage) before it
+// frees the tensor memory that the MMAs may still be writing.
+__device__ __forceinline__ bool runStage(const Stage& st, uint32_t idesc, int stage, long long limit) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (threadIdx.x == 0) {
         fenceAfterSync();
-        const int b = c & 1;
-        uint32_t a = smemAddr(st.tileA[b]), bb = smemAddr(st.tileB[b]);
+        uint32_t a = smemAddr(st.tileA), b = smemAddr(st.tileB);
         for (int j = 0; j < 4; j++)
-            mmaBf16(st.tmem, smemDescriptor(a + 32*j), smemDescriptor(bb + 32*j), idesc, (c > 0 || j > 0) ? 1u : 0u);
-        commitTo(st.mbar[b]);
+            mmaBf16(st.tmem, smemDescriptor(a + 32*j), smemDescriptor(b + 32*j), idesc, (stage > 0 || j > 0) ? 1u : 0u);
+        commitTo(st.mbar);
     }
+    bool ok = waitParity(st.mbar, (uint32_t) (stage & 1), limit);
+    return __syncthreads_and(ok) != 0;
 }
 
-// After a wait that gave up: wait once more, with the full limit, for the last issued stage (its commit tracks every
-// earlier MMA), so that the tensor memory and the tiles are released only when the tensor cores are done with them.
-__device__ __forceinline__ void drainStages(const Stages& st, int lastIssued) {
-    if (lastIssued >= 0)
-        waitParity(st.mbar[lastIssued & 1], (uint32_t) ((lastIssued >> 1) & 1), kSpinLimit);
+// After a wait that gave up: wait once more, with the full limit, for the MMAs of that stage (the only ones in flight),
+// so that the tensor memory and the shared-memory tiles are released only when the tensor cores are done with them.
+__device__ __forceinline__ void drainStage(const Stage& st, int stage) {
+    waitParity(st.mbar, (uint32_t) (stage & 1), kSpinLimit);
     __syncthreads();
 }
 
@@ -184,7 +167,7 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
                   __nv_bfloat16* __restrict__ y, int batch, int D, int H, int W, int cin, int cout, int relu) {
     extern __shared__ uint8_t smemRaw[];
     const uint32_t ncols = tmemColumns(cout);
-    Stages st = setupStages(smemRaw, cout, ncols);
+    Stage st = setupStage(smemRaw, cout, ncols);
     const int tid = threadIdx.x, warp = tid/32, lane = tid%32;
     const long long M = (long long) batch*D*H*W;
     const int K = 27*cin, stages = (K + kChunk - 1)/kChunk;
@@ -201,42 +184,32 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
     }
     const long long limit = convWaitPolls;
     bool ok = true;
-    int lastIssued = -1;
-    for (int c = 0; c < stages; c++) {
-        // Buffer c & 1 is free once the MMAs of stage c - 2 are done.
-        if (c >= kStages && !(ok = waitStage(st, c - kStages, limit)))
-            break;
-        uint8_t* tileA = st.tileA[c & 1];
-        uint8_t* tileB = st.tileB[c & 1];
-        uint4 val[8];
-#pragma unroll
+    int failedStage = -1;
+    for (int c = 0; c < stages && ok; c++) {
         for (int kv = 0; kv < 8; kv++) {
             int k = c*kChunk + kv*8;
-            val[kv] = make_uint4(0, 0, 0, 0);
+            uint4 val = make_uint4(0, 0, 0, 0);
             if (valid && k < K) {
                 int tap = k/cin, ci = k - tap*cin;
                 int zz = vz + tap/9 - 1, yy = vy + (tap/3)%3 - 1, xx = vx + tap%3 - 1;
                 if (zz >= 0 && zz < D && yy >= 0 && yy < H && xx >= 0 && xx < W)
-                    val[kv] = __ldg(reinterpret_cast<const uint4*>(x + ((((long long) vn*D + zz)*H + yy)*W + xx)*cin + ci));
+                    val = __ldg(reinterpret_cast<const uint4*>(x + ((((long long) vn*D + zz)*H + yy)*W + xx)*cin + ci));
             }
+            *reinterpret_cast<uint4*>(st.tileA + swizzled(tid, kv)) = val;
         }
-#pragma unroll
-        for (int kv = 0; kv < 8; kv++)
-            *reinterpret_cast<uint4*>(tileA + swizzled(tid, kv)) = val[kv];
         for (int i = tid; i < cout*8; i += kThreads) {
             int row = i >> 3, kv = i & 7, k = c*kChunk + kv*8;
-            uint4 v = make_uint4(0, 0, 0, 0);
+            uint4 val = make_uint4(0, 0, 0, 0);
             if (k < K)
-                v = __ldg(reinterpret_cast<const uint4*>(w + (long long) row*K + k));
-            *reinterpret_cast<uint4*>(tileB + swizzled(row, kv)) = v;
+                val = __ldg(reinterpret_cast<const uint4*>(w + (long long) row*K + k));
+            *reinterpret_cast<uint4*>(st.tileB + swizzled(row, kv)) = val;
         }
-        issueStage(st, idesc, c);
-        lastIssued = c;
+        ok = runStage(st, idesc, c, limit);
+        if (!ok)
+            failedStage = c;
     }
-    if (ok)
-        ok = waitStage(st, stages - 1, limit);
     if (!ok)
-        drainStages(st, lastIssued);
+        drainStage(st, failedStage);
     fenceAfterSync();
     if (ok) {
         const int row = warp*32 + lane;
@@ -256,7 +229,7 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
     }
     else if (tid == 0)
         atomicExch(&convStatus, (int) LBM_ERR_DEVICE_TIMEOUT);
-    releaseStages(st, ncols);
+    releaseStage(st, ncols);
 }
 
 // dW[cout][k] += sum_m dy[m][cout] A[m][k]: A tile rows = cout (tile of 128), B tile rows = k (tile of nt), the GEMM's
@@ -266,7 +239,7 @@ convWeightGradKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* _
                      int batch, int D, int H, int W, int cin, int cout, int nt) {
     extern __shared__ uint8_t smemRaw[];
     const uint32_t ncols = tmemColumns(nt);
-    Stages st = setupStages(smemRaw, nt, ncols);
+    Stage st = setupStage(smemRaw, nt, ncols);
     const int tid = threadIdx.x, warp = tid/32, lane = tid%32;
     const long long M = (long long) batch*D*H*W;
     const int K = 27*cin;
@@ -276,12 +249,8 @@ convWeightGradKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* _
     const int col = tid%kChunk, half = tid/kChunk;       // this thread's voxel column and row-group parity
     const long long limit = convWaitPolls;
     bool ok = true;
-    int stage = 0, lastIssued = -1;
-    for (long long c = blockIdx.z; c < stagesTotal; c += gridDim.z, stage++) {
-        if (stage >= kStages && !(ok = waitStage(st, stage - kStages, limit)))
-            break;
-        uint8_t* tileA = st.tileA[stage & 1];
-        uint8_t* tileB = st.tileB[stage & 1];
+    int stage = 0;
+    for (long long c = blockIdx.z; c < stagesTotal && ok; c += gridDim.z, stage++) {
         const long long m = c*kChunk + col;
         const bool valid = m < M;
         int vx = 0, vy = 0, vz = 0, vn = 0;
@@ -300,7 +269,7 @@ convWeightGradKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* _
                 val = __ldg(reinterpret_cast<const uint4*>(dy + m*cout + co));
             const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(&val);
             for (int i = 0; i < 8; i++)
-                *reinterpret_cast<__nv_bfloat16*>(tileA + swizzled(8*g + i, col >> 3) + colOffset) = e[i];
+                *reinterpret_cast<__nv_bfloat16*>(st.tileA + swizzled(8*g + i, col >> 3) + colOffset) = e[i];
         }
         // B: rows k = k0 + 8 g + i (one tap and 8 channels per group), column = this voxel.
         for (int g = half; g < nt/8; g += 2) {
@@ -314,15 +283,12 @@ convWeightGradKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* _
             }
             const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(&val);
             for (int i = 0; i < 8; i++)
-                *reinterpret_cast<__nv_bfloat16*>(tileB + swizzled(8*g + i, col >> 3) + colOffset) = e[i];
+                *reinterpret_cast<__nv_bfloat16*>(st.tileB + swizzled(8*g + i, col >> 3) + colOffset) = e[i];
         }
-        issueStage(st, idesc, stage);
-        lastIssued = stage;
+        ok = runStage(st, idesc, stage, limit);
+        if (!ok)
+            drainStage(st, stage);
     }
-    if (ok && stage > 0)
-        ok = waitStage(st, stage - 1, limit);
-    if (!ok)
-        drainStages(st, lastIssued);
     fenceAfterSync();
     if (ok && stage > 0) {
         const int row = warp*32 + lane, co = co0 + row;
@@ -339,11 +305,11 @@ convWeightGradKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* _
     }
     else if (!ok && tid == 0)
         atomicExch(&convStatus, (int) LBM_ERR_DEVICE_TIMEOUT);
-    releaseStages(st, ncols);
+    releaseStage(st, ncols);
 }
 
 size_t stageBytes(int rowsB) {
-    return 1024 + kStages*((size_t) kTileM*128 + (size_t) ((rowsB*128 + 1023)/1024)*1024) + 64;
+    return 1024 + (size_t) kTileM*128 + (size_t) rowsB*128 + 64;
 }
 
 LbmStatus launchError(cudaError_t e) {
