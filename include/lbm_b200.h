@@ -277,13 +277,6 @@ LbmStatus lbm_execute_openmm(LbmKernel* kernel, long long step_count, const LbmO
    No counterpart in the reference, whose cap is fixed and whose solve has no device-side wait. */
 LbmStatus lbm_set_solver_limits(LbmKernel* kernel, int max_iterations, long long barrier_polls);
 
-/* The centred stencil drag solves each connected component of its coupling matrix (particles whose stencils share
-   nodes: a bead chain, a cluster) by the conjugate gradients in one thread block, and a component of more than
-   `particles` particles (default and maximum 1024; 0 restores it, a negative value sends every component there) by the
-   cooperative solve over all particles, whose grid barriers the poll limit above bounds.  Both give the reference's
-   solution within its tolerance. */
-LbmStatus lbm_set_component_capacity(LbmKernel* kernel, int particles);
-
 /* The steady-state residual r = max_nodes |u - u_prev| / (interval max_nodes |u|) over the fluid nodes, in FP64 on the
    device, with u = j/rho of the current (post-stream) state and u_prev the velocities recorded by the previous call,
    which this call replaces; the first call records them and returns infinity.  Called every `interval` steps it is the

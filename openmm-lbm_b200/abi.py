@@ -115,7 +115,6 @@ SIGNATURES = {
     'lbm_dense_kernel_time': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong), _D]),
     'lbm_kernel_launches': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     'lbm_solver_iterations': (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
-    'lbm_set_component_capacity': (ctypes.c_int, [_P, ctypes.c_int]),
     'lbm_set_coupled_atoms': (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     'lbm_begin_step_openmm': (ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(LbmOpenMMBuffers)]),
     'lbm_execute_openmm': (ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(LbmOpenMMBuffers), ctypes.c_int,

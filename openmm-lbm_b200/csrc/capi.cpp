@@ -256,11 +256,6 @@ LbmStatus lbm_set_solver_limits(LbmKernel* kernel, int max_iterations, long long
     return guard([&] { kernel->impl->setSolverLimits(max_iterations, barrier_polls); });
 }
 
-LbmStatus lbm_set_component_capacity(LbmKernel* kernel, int particles) {
-    CHECK_HANDLE(kernel);
-    return guard([&] { kernel->impl->setComponentCapacity(particles); });
-}
-
 LbmStatus lbm_solver_fallback_steps(LbmKernel* kernel, long long* steps) {
     CHECK_HANDLE(kernel);
     if (!steps)

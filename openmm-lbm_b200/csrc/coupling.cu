@@ -453,12 +453,11 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
 //                   pass), inserted into a fixed-capacity cell list; per slot: w/rho
 //   cgRowsKernel    one warp per particle k: the particles of the neighbouring cells whose first stencil indices are
 //                   within a stencil width of k's on every axis, sorted by index (so that every row, and every sum
-//                   over it, has one order), and K_kl for each, a lane per entry; and the union of k with the
-//                   entries above it
+//                   over it, has one order), and K_kl for each, a lane per entry
 //   centeredSparseKernel  the conjugate gradients (same start, preconditioner, stopping rule and per-component
 //                   iteration as the kernel above) in one cooperative launch, two grid barriers per iteration
-// Rows are stored entry-major (entry e of row k at e np + k), so that the threads of consecutive rows read them
-// coalesced; two threads share a row in the products.  A cell or a row over its capacity sets a flag; the host then
+// Rows are stored row-major (entry e of row k at k kCgRowCapacity + e), so that the kProductLanes threads that share a
+// row in the products read its entries coalesced.  A cell or a row over its capacity sets a flag; the host then
 // runs the spread-and-gather kernel for that step.
 // ------------------------------------------------------------------------------------------------------
 
@@ -475,21 +474,11 @@ struct SparseCg {
     unsigned* cellCount;   // particles per cell (cleared by the solve kernel)
     int4* cellList;        // kCgCellCapacity per cell: the particle and its first stencil index on each axis
     int* rowCount;         // entries per row
-    int* rowIndex;         // entry e of row k at e np + k: the column particle
-    int* rowLocal;         // same layout: the column's position among the members of its component
+    int* rowIndex;         // entry e of row k at k kCgRowCapacity + e: the column particle
     double* rowValue;      // K_kl, same layout
     double* Ap;            // A p, 3 per particle
     int* overflow;         // nonzero: a cell or a row over its capacity
     int cells[3];          // cells per axis
-    // The connected components of the matrix (cgComponentKernel).
-    int* parent;           // union-find forest over the particles (a root is the smallest index of its component)
-    unsigned* rootKey;     // the root of each particle (sort keys), and
-    int* member;           // the particles (sort values): after the sort, the members of each component in a row
-    int* componentStart;   // per root: the first and one past the last sorted position of its component
-    int* componentEnd;
-    int* componentRoot;    // the roots, in no particular order
-    int* componentCount;   // number of components
-    int* componentOverflow;// nonzero: a component over the capacity (the cooperative solve takes the step)
 };
 
 template <typename R>
@@ -508,43 +497,11 @@ cgBinKernel(CouplingView c, const R* __restrict__ slotWeight, const typename Vec
                              min(first.z/kCgCellEdge, g.cells[2] - 1)};
         int key = cell[0] + g.cells[0]*(cell[1] + g.cells[1]*cell[2]);
         g.cellOf[i] = key;
-        g.parent[i] = i;
         unsigned slot = atomicAdd(&g.cellCount[key], 1u);
         if (slot < (unsigned) kCgCellCapacity)
             g.cellList[(long long) key*kCgCellCapacity + slot] = make_int4(i, first.x, first.y, first.z);
         else
             atomicExch(g.overflow, 1);
-    }
-}
-
-// Union-find over the particles, lock-free: a root is linked under a smaller root by atomicCAS, so every root is the
-// smallest index of its tree and no cycle forms; a find halves the paths it walks (a non-root only moves up).
-__device__ __forceinline__ int findRoot(int* parent, int x) {
-    volatile int* p = parent;
-    int up = p[x];
-    while (up != x) {
-        const int next = p[up];
-        if (next != up)
-            p[x] = next;
-        x = up;
-        up = next;
-    }
-    return x;
-}
-
-__device__ __forceinline__ void unite(int* parent, int a, int b) {
-    int ra = findRoot(parent, a), rb = findRoot(parent, b);
-    while (ra != rb) {
-        if (ra < rb) {
-            const int s = ra;
-            ra = rb;
-            rb = s;
-        }
-        const int old = atomicCAS(&parent[ra], ra, rb);
-        if (old == ra)
-            return;
-        ra = findRoot(parent, old);
-        rb = findRoot(parent, rb);
     }
 }
 
@@ -695,10 +652,8 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
                             K += rowCoef[warp][ix + w*(iy + w*iz)]*(shifted[0][ix]*wyz);
                 }
             }
-            g.rowIndex[(long long) j*c.np + k] = l;
-            g.rowValue[(long long) j*c.np + k] = (double) K;
-            if (l > k)
-                unite(g.parent, k, l);
+            g.rowIndex[(long long) k*kCgRowCapacity + j] = l;
+            g.rowValue[(long long) k*kCgRowCapacity + j] = (double) K;
         }
         if (lane == 0)
             g.rowCount[k] = found;
@@ -706,37 +661,62 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
     }
 }
 
-// (K v)_k for the three components of v, by the two threads 2j, 2j + 1 of a row (the even and the odd entries, then
-// their sum), in both; k < 0: no row (the threads still take part in the exchange).  Called by every thread of the warp.
-__device__ __forceinline__ void rowProduct(const SparseCg& g, int np, int k, const double* v, double out[3]) {
+// (K v)_k for the three components of v, by the kProductLanes threads of a row (entries sub, sub + kProductLanes, ...,
+// then the sum over the lanes), in all of them; k < 0: no row (the threads still take part in the exchange).  Called
+// by every thread of the warp.
+constexpr int kProductLanes = 8;
+
+__device__ __forceinline__ void rowProduct(const SparseCg& g, int k, const double* v, double out[3]) {
     double s0 = 0, s1 = 0, s2 = 0;
     if (k >= 0) {
         const int n = g.rowCount[k];
-#pragma unroll 4
-        for (int e = threadIdx.x & 1; e < n; e += 2) {
-            const int l = g.rowIndex[(long long) e*np + k];
-            const double K = g.rowValue[(long long) e*np + k];
+        const int* index = g.rowIndex + (long long) k*kCgRowCapacity;
+        const double* value = g.rowValue + (long long) k*kCgRowCapacity;
+#pragma unroll 2
+        for (int e = threadIdx.x%kProductLanes; e < n; e += kProductLanes) {
+            const int l = index[e];
+            const double K = value[e];
             s0 += K*v[3*l];
             s1 += K*v[3*l+1];
             s2 += K*v[3*l+2];
         }
     }
-    out[0] = s0 + __shfl_xor_sync(0xFFFFFFFFu, s0, 1);
-    out[1] = s1 + __shfl_xor_sync(0xFFFFFFFFu, s1, 1);
-    out[2] = s2 + __shfl_xor_sync(0xFFFFFFFFu, s2, 1);
+#pragma unroll
+    for (int o = 1; o < kProductLanes; o <<= 1) {
+        s0 += __shfl_xor_sync(0xFFFFFFFFu, s0, o);
+        s1 += __shfl_xor_sync(0xFFFFFFFFu, s1, o);
+        s2 += __shfl_xor_sync(0xFFFFFFFFu, s2, o);
+    }
+    out[0] = s0;
+    out[1] = s1;
+    out[2] = s2;
 }
 
-// The start of the centred drag's solve for every particle (ReferenceLBMKernels.cpp:758-782, 839-840): the right-hand
-// side b/m, the Jacobi diagonal and F = rhs/diag, 8 lanes per particle (4 particles per warp of the calling grid).
 template <typename R>
-__device__ void startParticles(const CouplingView& c, const double* __restrict__ vel, const double* __restrict__ fin,
-                               const R* __restrict__ slotWeight, const typename Vec4<R>::type* __restrict__ slotU,
-                               long long step, const CgBuffers& b, int firstWarp, int warps) {
+__global__ void __launch_bounds__(kSolveThreads, 1)
+centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel, const double* __restrict__ fin,
+                     const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
+                     const typename Vec4<R>::type* __restrict__ slotU, long long step, int isStep, double tolerance,
+                     int maxIterations, CgBuffers b, SparseCg g, double* fout, R* reaction, uint32_t* mask,
+                     double* wall) {
     typedef typename Vec4<R>::type V;
-    constexpr int G = 8;
+    constexpr int G = 8;       // lanes per particle where a particle's slots are summed
     const int lane = threadIdx.x & 31, sub = lane%G;
+    const int firstWarp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
+    const int warps = (gridDim.x*blockDim.x) >> 5;
+    const int firstThread = blockIdx.x*blockDim.x + threadIdx.x, threads = gridDim.x*blockDim.x;
+    // The rows of this block (a contiguous range).
+    const int rowBegin = (int) ((long long) c.np*blockIdx.x/gridDim.x);
+    const int rowEnd = (int) ((long long) c.np*(blockIdx.x + 1)/gridDim.x);
     const int S = c.slots;
     const double a = c.a;
+    // The cell list has been read (by the rows kernel): empty it for the next step.
+    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x)
+        g.cellCount[g.cellOf[i]] = 0u;
+    if (*((volatile int*) g.overflow) != 0)
+        return;
+    // Right-hand side, diagonal and the start F = rhs/diag (ReferenceLBMKernels.cpp:758-782, 839-840): 8 lanes per
+    // particle, 4 particles per warp.
     for (int base = firstWarp*(32/G); base < c.np; base += warps*(32/G)) {
         const int i = base + lane/G;
         const bool active = i < c.np;
@@ -776,57 +756,15 @@ __device__ void startParticles(const CouplingView& c, const double* __restrict__
         }
         b.diag[i] = diag;
     }
-}
-
-// Forces and reactions of the solved drag (ReferenceLBMKernels.cpp:889-900): a thread per particle, then a thread per
-// slot.
-template <typename R>
-__device__ void finishParticles(const FluidView& f, const CouplingView& c, const int* __restrict__ slotNode,
-                                const R* __restrict__ slotWeight, int isStep, const CgBuffers& b, double* fout,
-                                R* reaction, uint32_t* mask, double* wall, int firstThread, int threads) {
-    const int S = c.slots;
-    for (int i = firstThread; i < c.np; i += threads)
-        for (int d = 0; d < 3; d++)
-            fout[3*i+d] = b.F[3*i+d]*c.forceScale;
-    if (isStep)
-        for (long long t = firstThread; t < (long long) c.np*S; t += threads) {
-            const int i = (int) (t/S);
-            const double w = (double) slotWeight[t];
-            if (w != 0.0)
-                addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*b.F[3*i], -w*b.F[3*i+1], -w*b.F[3*i+2]);
-        }
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kSolveThreads, 1)
-centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel, const double* __restrict__ fin,
-                     const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
-                     const typename Vec4<R>::type* __restrict__ slotU, long long step, int isStep, double tolerance,
-                     int maxIterations, CgBuffers b, SparseCg g, double* fout, R* reaction, uint32_t* mask,
-                     double* wall) {
-    const int lane = threadIdx.x & 31;
-    const int firstWarp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
-    const int warps = (gridDim.x*blockDim.x) >> 5;
-    const int firstThread = blockIdx.x*blockDim.x + threadIdx.x, threads = gridDim.x*blockDim.x;
-    // The rows of this block (a contiguous range, so that its threads read the entry-major rows coalesced).
-    const int rowBegin = (int) ((long long) c.np*blockIdx.x/gridDim.x);
-    const int rowEnd = (int) ((long long) c.np*(blockIdx.x + 1)/gridDim.x);
-    const double a = c.a;
-    // The cell list has been read (by the rows kernel): empty it for the next step.
-    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x)
-        g.cellCount[g.cellOf[i]] = 0u;
-    if (*((volatile int*) g.overflow) != 0)
-        return;
-    startParticles<R>(c, vel, fin, slotWeight, slotU, step, b, firstWarp, warps);
     if (!gridSync(b.barrier, b.status, b.pollLimit))
         return;
     // r = rhs - A F, z = r/diag, p = z; r.z, the norm of the right-hand side and r.r per component.
     double acc[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int base = rowBegin; base < rowEnd; base += blockDim.x/2) {
-        const int i = base + threadIdx.x/2;
+    for (int base = rowBegin; base < rowEnd; base += blockDim.x/kProductLanes) {
+        const int i = base + threadIdx.x/kProductLanes;
         double g3[3];
-        rowProduct(g, c.np, i < rowEnd ? i : -1, b.F, g3);
-        if (i >= rowEnd || (threadIdx.x & 1))
+        rowProduct(g, i < rowEnd ? i : -1, b.F, g3);
+        if (i >= rowEnd || threadIdx.x%kProductLanes != 0)
             continue;
         double m = c.mass[i], diag = b.diag[i];
         for (int d = 0; d < 3; d++) {
@@ -866,11 +804,11 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
         }
         // p = z + beta p and A p = A z + beta A p (p = z at the first iteration), with p.Ap.
         double acc3[kPartial] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-        for (int base = rowBegin; base < rowEnd; base += blockDim.x/2) {
-            const int i = base + threadIdx.x/2;
+        for (int base = rowBegin; base < rowEnd; base += blockDim.x/kProductLanes) {
+            const int i = base + threadIdx.x/kProductLanes;
             double g3[3];
-            rowProduct(g, c.np, i < rowEnd ? i : -1, b.z, g3);
-            if (i >= rowEnd || (threadIdx.x & 1))
+            rowProduct(g, i < rowEnd ? i : -1, b.z, g3);
+            if (i >= rowEnd || threadIdx.x%kProductLanes != 0)
                 continue;
             double m = c.mass[i];
             for (int d = 0; d < 3; d++) {
@@ -920,239 +858,17 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
         *b.iterations = iteration;
     if (failed)
         return;
-    finishParticles<R>(f, c, slotNode, slotWeight, isStep, b, fout, reaction, mask, wall, firstThread, threads);
-}
-
-// ------------------------------------------------------------------------------------------------------
-// The conjugate gradients per connected component of the coupling matrix.
-//
-// Particles k and l are coupled when their stencils share a fluid node (an entry K_kl of the rows), so the matrix is
-// block diagonal over the connected components of that relation (a bead chain, a cluster of beads), and the
-// conjugate gradients of the whole system are those of its components taken together.  Each component is solved by one
-// block on its own, with block barriers where the whole system needs grid barriers.  Per component and axis the solve
-// stops when r.r <= tol^2 b.b (b the right-hand side), which implies the reference's rule over all particles (the sums
-// over the components of r.r and b.b, ReferenceLBMKernels.cpp:848-856).
-//   rows kernel       unites k with the entries l > k of its row (the union-find above)
-//   cgRootKernel      the root of each particle (the sort key), the start of the solve (startParticles), and the cell
-//                     list emptied for the next step
-//   radix sort        the particles by root, stably: the members of a component in a row, in ascending order
-//   cgSegmentKernel   the first and last sorted position of each component, and the list of roots
-//   cgComponentKernel one block per component: the Jacobi-preconditioned conjugate gradients
-//                     (ReferenceLBMKernels.cpp:834-888) over the component's rows, members in ascending order
-//   cgFinishKernel    forces and reactions (finishParticles), unless a solve failed or the cooperative solve is needed
-// A component of more than `capacity` particles is left to the cooperative solve over all particles.
-// ------------------------------------------------------------------------------------------------------
-
-constexpr int kComponentThreads = 256;
-static_assert(kDefaultComponentCapacity <= 1024, "the component kernel holds at most 1024 members");
-constexpr int kComponentMembers = 1024;    // members of a component held in shared memory
-static_assert(kComponentMembers <= 4*kComponentThreads, "a thread of the component kernel owns at most 4 rows");
-
-template <typename R>
-__global__ void __launch_bounds__(kThreads)
-cgRootKernel(CouplingView c, const double* __restrict__ vel, const double* __restrict__ fin,
-             const R* __restrict__ slotWeight, const typename Vec4<R>::type* __restrict__ slotU, long long step,
-             CgBuffers b, SparseCg g) {
-    const int firstThread = blockIdx.x*blockDim.x + threadIdx.x, threads = gridDim.x*blockDim.x;
-    for (int i = firstThread; i < c.np; i += threads) {
-        g.cellCount[g.cellOf[i]] = 0u;
-        g.rootKey[i] = (unsigned) findRoot(g.parent, i);
-        g.member[i] = i;
-    }
-    startParticles<R>(c, vel, fin, slotWeight, slotU, step, b, firstThread >> 5, threads >> 5);
-}
-
-__global__ void cgSegmentKernel(int np, const unsigned* __restrict__ key, SparseCg g) {
-    for (int p = blockIdx.x*blockDim.x + threadIdx.x; p < np; p += gridDim.x*blockDim.x) {
-        const int root = (int) key[p];
-        if (p == 0 || key[p-1] != key[p]) {
-            g.componentStart[root] = p;
-            g.componentRoot[atomicAdd(g.componentCount, 1)] = root;
+    // Forces and reactions (ReferenceLBMKernels.cpp:889-900): a thread per particle, then a thread per slot.
+    for (int i = firstThread; i < c.np; i += threads)
+        for (int d = 0; d < 3; d++)
+            fout[3*i+d] = b.F[3*i+d]*c.forceScale;
+    if (isStep)
+        for (long long t = firstThread; t < (long long) c.np*S; t += threads) {
+            const int i = (int) (t/S);
+            const double w = (double) slotWeight[t];
+            if (w != 0.0)
+                addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*b.F[3*i], -w*b.F[3*i+1], -w*b.F[3*i+2]);
         }
-        if (p == np - 1 || key[p+1] != key[p])
-            g.componentEnd[root] = p + 1;
-    }
-}
-
-// Sums of 6 values over the block, returned to every thread (two block barriers).
-__device__ __forceinline__ void componentSum(double v[6], double (*red)[6]) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = 0; k < 6; k++)
-        v[k] = warpSum(v[k]);
-    __syncthreads();
-    if (lane == 0)
-        for (int k = 0; k < 6; k++)
-            red[warp][k] = v[k];
-    __syncthreads();
-    for (int k = 0; k < 6; k++) {
-        double s = 0;
-        for (int w = 0; w < (int) (blockDim.x >> 5); w++)
-            s += red[w][k];
-        v[k] = s;
-    }
-}
-
-// Position of particle l among the n sorted members of a component (l is one of them).
-__device__ __forceinline__ int memberPosition(const int* members, int n, int l) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (members[mid] < l)
-            lo = mid + 1;
-        else
-            hi = mid;
-    }
-    return lo;
-}
-
-// One block per component of at most kComponentMembers particles: the members and the search direction p in shared
-// memory, the rows of the members (their entries replaced by member positions in the first product, rowLocal) and the
-// other vectors in global memory, each thread owning the rows j = threadIdx.x, + blockDim.x, ...
-__global__ void __launch_bounds__(kComponentThreads)
-cgComponentKernel(CouplingView c, double tolerance, int maxIterations, int capacity, CgBuffers b, SparseCg g) {
-    __shared__ double red[kComponentThreads/32][6];
-    __shared__ int memberS[kComponentMembers];
-    __shared__ double pS[3*kComponentMembers];
-    if (*((volatile int*) g.overflow) != 0)
-        return;
-    const int components = *g.componentCount;
-    const double tol2 = tolerance*tolerance, a = c.a;
-    const long long np = c.np;
-    for (int ci = blockIdx.x; ci < components; ci += gridDim.x) {
-        const int root = g.componentRoot[ci];
-        const int start = g.componentStart[root], n = g.componentEnd[root] - start;
-        if (n > capacity) {
-            if (threadIdx.x == 0)
-                atomicExch(g.componentOverflow, 1);
-            continue;
-        }
-        for (int j = threadIdx.x; j < n; j += blockDim.x) {
-            const int i = g.member[start + j];
-            memberS[j] = i;
-            for (int d = 0; d < 3; d++)
-                pS[3*j+d] = b.F[3*i+d];
-        }
-        __syncthreads();
-        // r = rhs - A F, z = r/diag, p = z (F = rhs/diag from the start, in pS for this product); r.z, r.r and b.b per
-        // axis.  The product records each entry's member position.
-        double acc[6] = {0, 0, 0, 0, 0, 0}, norm[6] = {0, 0, 0, 0, 0, 0};
-        double zOwn[4][3];     // z of the rows of this thread (at most 1024/256), written to pS after the barrier
-        for (int j = threadIdx.x, o = 0; j < n; j += blockDim.x, o++) {
-            const int i = memberS[j];
-            const int entries = g.rowCount[i];
-            double s0 = 0, s1 = 0, s2 = 0;
-#pragma unroll 4
-            for (int e = 0; e < entries; e++) {
-                const int lj = memberPosition(memberS, n, g.rowIndex[e*np + i]);
-                const double K = g.rowValue[e*np + i];
-                g.rowLocal[e*np + i] = lj;
-                s0 += K*pS[3*lj];
-                s1 += K*pS[3*lj+1];
-                s2 += K*pS[3*lj+2];
-            }
-            const double self = (1.0 + a)/c.mass[i], diag = b.diag[i], s[3] = {s0, s1, s2};
-            for (int d = 0; d < 3; d++) {
-                const double rhs = b.rhs[3*i+d];
-                const double r = rhs - (pS[3*j+d]*self + s[d]*a), z = r*(1.0/diag);
-                b.r[3*i+d] = r;
-                b.z[3*i+d] = z;
-                zOwn[o][d] = z;
-                acc[d] += r*z;
-                acc[3+d] += r*r;
-                norm[d] += rhs*rhs;
-            }
-        }
-        __syncthreads();
-        for (int j = threadIdx.x, o = 0; j < n; j += blockDim.x, o++)
-            for (int d = 0; d < 3; d++)
-                pS[3*j+d] = zOwn[o][d];
-        componentSum(acc, red);
-        componentSum(norm, red);
-        double rz[3] = {acc[0], acc[1], acc[2]}, rr[3] = {acc[3], acc[4], acc[5]};
-        int iteration = 0;
-        bool failed = false;   // the same in every thread: every decision comes from the block sums
-        for (;; iteration++) {
-            bool converged = true;
-            for (int d = 0; d < 3; d++)
-                if (rr[d] > tol2*norm[d])
-                    converged = false;
-            if (converged)
-                break;
-            if (iteration == maxIterations) {
-                failed = true;
-                break;
-            }
-            // A p and p.Ap (p was written before the last block barrier).
-            double pAp[6] = {0, 0, 0, 0, 0, 0};
-            for (int j = threadIdx.x; j < n; j += blockDim.x) {
-                const int i = memberS[j];
-                const int entries = g.rowCount[i];
-                double s0 = 0, s1 = 0, s2 = 0;
-#pragma unroll 4
-                for (int e = 0; e < entries; e++) {
-                    const int lj = g.rowLocal[e*np + i];
-                    const double K = g.rowValue[e*np + i];
-                    s0 += K*pS[3*lj];
-                    s1 += K*pS[3*lj+1];
-                    s2 += K*pS[3*lj+2];
-                }
-                const double self = (1.0 + a)/c.mass[i], s[3] = {s0, s1, s2};
-                for (int d = 0; d < 3; d++) {
-                    const double Ap = pS[3*j+d]*self + s[d]*a;
-                    g.Ap[3*i+d] = Ap;
-                    pAp[d] += pS[3*j+d]*Ap;
-                }
-            }
-            componentSum(pAp, red);
-            double alpha[3];
-            for (int d = 0; d < 3; d++)
-                alpha[d] = pAp[d] > 0 ? rz[d]/pAp[d] : 0.0;
-            double next[6] = {0, 0, 0, 0, 0, 0};
-            for (int j = threadIdx.x; j < n; j += blockDim.x) {
-                const int i = memberS[j];
-                const double diag = b.diag[i];
-                for (int d = 0; d < 3; d++) {
-                    b.F[3*i+d] += alpha[d]*pS[3*j+d];
-                    const double r = b.r[3*i+d] - alpha[d]*g.Ap[3*i+d];
-                    const double z = r*(1.0/diag);
-                    b.r[3*i+d] = r;
-                    b.z[3*i+d] = z;
-                    next[d] += r*z;
-                    next[3+d] += r*r;
-                }
-            }
-            componentSum(next, red);
-            double beta[3];
-            for (int d = 0; d < 3; d++) {
-                beta[d] = rz[d] > 0 ? next[d]/rz[d] : 0.0;
-                rz[d] = next[d];
-                rr[d] = next[3+d];
-            }
-            for (int j = threadIdx.x; j < n; j += blockDim.x) {
-                const int i = memberS[j];
-                for (int d = 0; d < 3; d++)
-                    pS[3*j+d] = b.z[3*i+d] + beta[d]*pS[3*j+d];
-            }
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) {
-            atomicMax(b.iterations, iteration);
-            if (failed)
-                atomicExch(b.status, LBM_ERR_CG_NOT_CONVERGED);
-        }
-        __syncthreads();
-    }
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kThreads)
-cgFinishKernel(FluidView f, CouplingView c, const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
-               int isStep, CgBuffers b, SparseCg g, double* fout, R* reaction, uint32_t* mask, double* wall) {
-    if (*((volatile int*) g.overflow) != 0 || *((volatile int*) g.componentOverflow) != 0 ||
-            *((volatile int*) b.status) != 0)
-        return;
-    finishParticles<R>(f, c, slotNode, slotWeight, isStep, b, fout, reaction, mask, wall,
-                       blockIdx.x*blockDim.x + threadIdx.x, gridDim.x*blockDim.x);
 }
 
 // Clear the reaction of the slots of the last step (and their mask words).
@@ -1239,7 +955,6 @@ struct CouplingEngine::Device {
     CgBuffers cg;
     SparseCg sparse;
     int sparseGrid = 0;
-    int componentGrid = 0;          // blocks of cgComponentKernel
     void* spread = nullptr;
     int4* axisIndex = nullptr;      // per particle: 3, the stencil's node indices on each axis
     double2* axisWeight = nullptr;  // per particle: 6, the stencil's weights on each axis
@@ -1281,10 +996,8 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
         CUDA_CHECK(cudaMalloc(&wallDev, sizeof(double)*8));
         CUDA_CHECK(cudaMemsetAsync(wallDev, 0, sizeof(double)*8, stream));
         dev->reflectWall = wallDev + 4;
-        // Status words: [0] solve status, [1] iterations, [2] overflow of the cell list or the rows, [3] arrivals at
-        // the grid barriers, [4] a component over kComponentCapacity, [5] number of components.
-        CUDA_CHECK(cudaMalloc(&statusDev, sizeof(int)*8));
-        CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*8, stream));
+        CUDA_CHECK(cudaMalloc(&statusDev, sizeof(int)*4));
+        CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, stream));
         size_t slots = (size_t) np*stencilSlots;
         CUDA_CHECK(cudaMalloc(&dev->slotNode, sizeof(int)*slots));
         CUDA_CHECK(cudaMalloc(&dev->slotWeight, r*slots));
@@ -1297,8 +1010,7 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
         CUDA_CHECK(cudaMalloc(&dev->nodeStamp, sizeof(unsigned)*(size_t) f.numNodes()));
         CUDA_CHECK(cudaMemsetAsync(dev->nodeStamp, 0, sizeof(unsigned)*(size_t) f.numNodes(), stream));
         CUDA_CHECK(cudaMalloc(&dev->nodeU, 4*r*(size_t) f.numNodes()));
-        if (l.drag_scheme == LBM_DRAG_CENTERED) {
-            // The sort of the particles by node (nearest node) or by component (stencils).
+        if (l.drag_scheme == LBM_DRAG_CENTERED && l.interpolation_stencil == LBM_STENCIL_NEAREST) {
             int blocks = (np + kSortItems - 1)/kSortItems;
             dev->histCount = (size_t) 256*blocks;
             CUDA_CHECK(cudaMalloc(&dev->hist, sizeof(unsigned)*dev->histCount));
@@ -1353,22 +1065,12 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
             CUDA_CHECK(cudaMalloc(&g.rowCount, sizeof(int)*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.rowIndex, sizeof(int)*kCgRowCapacity*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.rowValue, sizeof(double)*kCgRowCapacity*(size_t) np));
-            CUDA_CHECK(cudaMalloc(&g.rowLocal, sizeof(int)*kCgRowCapacity*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.Ap, v3));
             g.overflow = statusDev + 2;
-            CUDA_CHECK(cudaMalloc(&g.parent, sizeof(int)*(size_t) np));
-            CUDA_CHECK(cudaMalloc(&g.componentStart, sizeof(int)*(size_t) np));
-            CUDA_CHECK(cudaMalloc(&g.componentEnd, sizeof(int)*(size_t) np));
-            CUDA_CHECK(cudaMalloc(&g.componentRoot, sizeof(int)*(size_t) np));
-            g.rootKey = dev->keys[0];
-            g.member = dev->values[0];
-            g.componentOverflow = statusDev + 4;
-            g.componentCount = statusDev + 5;
             if (f64)
                 CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, centeredSparseKernel<double>, kSolveThreads, 0));
             else
                 CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, centeredSparseKernel<float>, kSolveThreads, 0));
-            dev->componentGrid = std::max(1, std::min(np, 8*sms));
             long long wantedSolve = ((long long) np*32 + kSolveThreads - 1)/kSolveThreads;
             // No more blocks than the partial records hold (cgGrid of the 256-thread solve).
             dev->sparseGrid = (int) std::max(1LL, std::min(std::min(wantedSolve, (long long) std::max(1, perSM)*sms),
@@ -1408,7 +1110,6 @@ void CouplingEngine::release() {
         SparseCg& g = dev->sparse;
         cudaFree(g.cellOf); cudaFree(g.cellCount); cudaFree(g.cellList);
         cudaFree(g.rowCount); cudaFree(g.rowIndex); cudaFree(g.rowValue); cudaFree(g.Ap);
-        cudaFree(g.rowLocal); cudaFree(g.parent); cudaFree(g.componentStart); cudaFree(g.componentEnd); cudaFree(g.componentRoot);
         delete dev;
         dev = nullptr;
     }
@@ -1516,7 +1217,7 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     int* sn = dev->slotNode;
     FluidView fv = f;
     CouplingView cc = c;
-    int status[6] = {0, 0, 0, 0, 0, 0};
+    int status[3] = {0, 0, 0};
     static const bool spreadOnly = [] {
         const char* e = std::getenv("LBM_B200_SPREAD_CG");
         return e != nullptr && e[0] == '1';
@@ -1524,44 +1225,17 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     if (!spreadOnly) {
         long long total = (long long) np*c.slots;
         int gridSlots = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
-        int gridLanes = (int) std::max(1LL, std::min(4736LL, ((long long) np*8 + kThreads - 1)/kThreads));
-        CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*8, stream));
         cgBinKernel<R><<<gridSlots, kThreads, 0, stream>>>(c, sw, su, coef, g);
         CUDA_CHECK(cudaGetLastError());
         cgRowsKernel<R><<<warpGrid(np), kThreads, 0, stream>>>(c, coef, g);
         CUDA_CHECK(cudaGetLastError());
-        // The components: roots, the particles sorted by root, the segments; then a block per component.
-        cgRootKernel<R><<<gridLanes, kThreads, 0, stream>>>(c, vel, fin, sw, su, stepArg, b, g);
-        CUDA_CHECK(cudaGetLastError());
-        int bits = 1;
-        while (bits < 31 && (1LL << bits) < np)
-            bits++;
-        int cur = radixSortByKey(dev->keys, dev->values, dev->hist, np, bits, stream);
-        cgSegmentKernel<<<gridP, kThreads, 0, stream>>>(np, dev->keys[cur], g);
-        CUDA_CHECK(cudaGetLastError());
-        SparseCg sorted = g;
-        sorted.member = dev->values[cur];
-        cgComponentKernel<<<dev->componentGrid, kComponentThreads, 0, stream>>>(c, tolerance, maxIterations,
-                                                                                 componentCapacity, b, sorted);
-        CUDA_CHECK(cudaGetLastError());
-        cgFinishKernel<R><<<gridSlots, kThreads, 0, stream>>>(f, c, dev->slotNode, sw, isStepArg, b, g, fout, reaction,
-                                                              mask, wall);
-        CUDA_CHECK(cudaGetLastError());
-        fluid.launches += 7 + 3*((bits + 7)/8);
-        CUDA_CHECK(cudaMemcpyAsync(status, statusDev, sizeof(int)*6, cudaMemcpyDeviceToHost, stream));
+        void* sparseArgs[] = {&fv, &cc, &vel, &fin, &sn, &sw, &su, &stepArg, &isStepArg, &tolerance, &maxIterations, &b,
+                              &g, &fout, &reaction, &mask, &wall};
+        CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredSparseKernel<R>, dev->sparseGrid, kSolveThreads,
+                                               sparseArgs, 0, stream));
+        fluid.launches += 3;
+        CUDA_CHECK(cudaMemcpyAsync(status, statusDev, sizeof(int)*3, cudaMemcpyDeviceToHost, stream));
         CUDA_CHECK(cudaStreamSynchronize(stream));
-        if (status[2] == 0 && status[4] != 0) {
-            // A component too large for one block: the cooperative solve over all particles (its own start; the
-            // rows stay).
-            CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, stream));
-            void* sparseArgs[] = {&fv, &cc, &vel, &fin, &sn, &sw, &su, &stepArg, &isStepArg, &tolerance, &maxIterations,
-                                  &b, &g, &fout, &reaction, &mask, &wall};
-            CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredSparseKernel<R>, dev->sparseGrid, kSolveThreads,
-                                                   sparseArgs, 0, stream));
-            fluid.launches++;
-            CUDA_CHECK(cudaMemcpyAsync(status, statusDev, sizeof(int)*3, cudaMemcpyDeviceToHost, stream));
-            CUDA_CHECK(cudaStreamSynchronize(stream));
-        }
     }
     if (spreadOnly || status[2] != 0) {
         CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, stream));
@@ -1581,11 +1255,6 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
         // The blocks left the solve at different barriers; the arrival counter holds a partial count, which the
         // memset before the next cooperative launch clears.
         throw Error(LBM_ERR_DEVICE_TIMEOUT, "LBMForce: a grid barrier of the conjugate gradients timed out");
-}
-
-void CouplingEngine::setComponentCapacity(int particles) {
-    componentCapacity = particles > 0 ? std::min(particles, kComponentMembers) :
-                        particles == 0 ? kDefaultComponentCapacity : 0;
 }
 
 void CouplingEngine::setSolverLimits(int maxIterations, long long barrierPolls) {

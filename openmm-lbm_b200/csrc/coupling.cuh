@@ -13,7 +13,6 @@ struct CouplingView;
 // (ReferenceLBMKernels.cpp:864-866) and the polls after which a block waiting at a grid barrier gives up.
 constexpr int kDefaultCgIterations = 1000;
 constexpr long long kDefaultBarrierPolls = 1LL << 26;
-constexpr int kDefaultComponentCapacity = 1024;   // particles of a component solved by one thread block (at most)
 
 class CouplingEngine {
 public:
@@ -43,7 +42,6 @@ public:
     const double* couplingForces() const { return forceOutDev; }
     // Lower limits make the failure paths reachable in tests; 0 restores a default.
     void setSolverLimits(int maxIterations, long long barrierPolls);
-    void setComponentCapacity(int particles);
 private:
     struct Device;
     void release();
@@ -63,7 +61,6 @@ private:
     int stencilSlots;
     int cgMaxIterations = kDefaultCgIterations;
     long long barrierPollLimit = kDefaultBarrierPolls;
-    int componentCapacity = kDefaultComponentCapacity;
 };
 
 } // namespace lbm

@@ -379,11 +379,6 @@ long long B200Kernel::solverFallbackSteps() const {
     return coupling ? coupling->spreadSteps : 0;
 }
 
-void B200Kernel::setComponentCapacity(int particles) {
-    if (coupling)
-        coupling->setComponentCapacity(particles);
-}
-
 void B200Kernel::setSolverLimits(int maxIterations, long long barrierPolls) {
     if (maxIterations < 0 || barrierPolls < 0)
         throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_set_solver_limits: the limits must not be negative");

@@ -38,7 +38,6 @@ public:
     int solverIterations() const;
     long long solverFallbackSteps() const;
     void setSolverLimits(int maxIterations, long long barrierPolls);
-    void setComponentCapacity(int particles);
     // The OpenMM Context interface: coupled atoms as System indices, then beginStep/execute on its buffers.
     void setCoupledAtoms(int numAtoms, int numCoupled, const int* particles);
     void beginStepOpenMM(long long stepCount, const LbmOpenMMBuffers* buffers);

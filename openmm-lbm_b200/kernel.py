@@ -131,11 +131,6 @@ class B200Kernel:
         """Iteration cap and barrier poll limit of the centred stencil drag's solve (0 restores the default)."""
         check(self.lib.lbm_set_solver_limits(self.handle, int(max_iterations), int(barrier_polls)), self.lib)
 
-    def set_component_capacity(self, particles=0):
-        """Largest connected component of the centred stencil drag solved by one thread block (0: the default,
-        negative: none, every solve cooperative over all particles)."""
-        check(self.lib.lbm_set_component_capacity(self.handle, int(particles)), self.lib)
-
     def solver_fallback_steps(self):
         """Steps whose centred stencil drag was solved by spread and gather on the nodes (capacity overflow)."""
         n = ctypes.c_longlong()

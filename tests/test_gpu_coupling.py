@@ -50,11 +50,10 @@ def cluster_case(count, spread, stencil, factory, props, seed=3):
     return context, force
 
 
-def chain_case(stencil, factory, props, capacity=0):
+def chain_case(stencil, factory, props):
     """Five random-walk chains of 12 beads (bond 0.5 nm, one lattice spacing) and 8 free beads in a 12^3 lattice,
-    centred drag with friction 10/ps and a field: the coupling matrix has a component per chain (chains that come
-    within a stencil width merge) and singletons, as the beads of the scale configuration.  capacity: the largest
-    component solved by one thread block (negative: the cooperative solve over all particles)."""
+    centred drag with friction 10/ps and a field: rows of the coupling matrix along the chains and between chains
+    that come within a stencil width, as for the beads of the scale configuration."""
     import lbm_b200
     system = lbm_b200.System()
     system.setDefaultPeriodicBoxVectors((6, 0, 0), (0, 6, 0), (0, 0, 6))
@@ -82,29 +81,24 @@ def chain_case(stencil, factory, props, capacity=0):
     context = lbm_b200.Context(system, lbm_b200.VerletIntegrator(0.01), factory, props)
     context.setPositions(np.mod(np.array(positions), 6.0))
     context.setVelocities(rng.normal(0.0, 0.5, (len(positions), 3)))
-    if capacity:
-        context.kernel.set_component_capacity(capacity)
     return context, force
 
 
 @pytest.mark.parametrize('stencil', ['Trilinear', 'ThreePoint', 'Keys'])
-def test_component_solves_agree_with_cooperative_solve_and_oracle(stencil):
-    """The centred stencil drag solved per connected component of the coupling matrix (one thread block each) gives
-    the trajectory of the cooperative solve over all particles (1e-12) and of the oracle's spread-and-gather solve
-    (FP64, 1e-10)."""
+def test_centred_drag_of_bead_chains_agrees_with_oracle(stencil):
+    """The centred stencil drag of bead chains through the explicit coupling matrix gives the trajectory of the
+    oracle's spread-and-gather solve (FP64, 1e-10)."""
     results = []
-    for factory, props, capacity in ((OracleKernel, None, 0), (None, {'Precision': 'double'}, 0),
-                                     (None, {'Precision': 'double'}, -1)):
-        context, force = chain_case(stencil, factory, props, capacity)
+    for factory, props in ((OracleKernel, None), (None, {'Precision': 'double'})):
+        context, force = chain_case(stencil, factory, props)
         context.integrator.step(10)
         results.append((context.positions.copy(), context.velocities.copy(), force.getFluidState(context)))
         if factory is None:
             assert context.kernel.solver_fallback_steps() == 0
             assert context.kernel.solver_iterations() > 0
         context.close()
-    for a, b, c, name in zip(results[0], results[1], results[2], ('positions', 'velocities', 'state')):
+    for a, b, name in zip(results[0], results[1], ('positions', 'velocities', 'state')):
         assert abs(b - a).max() <= 1e-10*max(1.0, abs(a).max()), name
-        assert abs(b - c).max() <= 1e-12*max(1.0, abs(c).max()), name
 
 
 @pytest.mark.parametrize('count,spread,stencil', [(80, 1.9, 'Keys'), (200, 3.4, 'Keys'), (160, 2.4, 'ThreePoint')])

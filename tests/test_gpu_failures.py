@@ -1,7 +1,7 @@
 """GPU tests of the failure paths, made to fire without any fault: the iteration cap of the centred stencil drag's
-conjugate gradients (LBM_ERR_CG_NOT_CONVERGED with the reference's message, ReferenceLBMKernels.cpp:864-866), in the
-per-component solve and in the cooperative one, the bounded grid barrier of the cooperative solve
-(LBM_ERR_DEVICE_TIMEOUT), and the bounded wait for the tensor cores of the warm start's convolutions.  The limits are lowered through the ABI; every wait still ends, and the tests check
+conjugate gradients (LBM_ERR_CG_NOT_CONVERGED with the reference's message, ReferenceLBMKernels.cpp:864-866), the
+bounded grid barrier of its cooperative solve (LBM_ERR_DEVICE_TIMEOUT), and the bounded wait for the tensor cores of
+the warm start's convolutions.  The limits are lowered through the ABI; every wait still ends, and the tests check
 that a failed call leaves nothing behind: the next call gives what a run without the failure gives."""
 import numpy as np
 import pytest
@@ -13,25 +13,21 @@ from lbm_b200.abi import LBM_ERR_CG_NOT_CONVERGED, LBM_ERR_DEVICE_TIMEOUT, LbmEr
 pytestmark = pytest.mark.gpu
 
 
-def centred_case(cooperative=False):
-    context, force = coupling_case(False, 'Centered', 'Keys', None, {'Precision': 'double'}, seed=3)
-    if cooperative:
-        context.kernel.set_component_capacity(-1)
-    return context, force
+def centred_case():
+    return coupling_case(False, 'Centered', 'Keys', None, {'Precision': 'double'}, seed=3)
 
 
-def uninterrupted(steps, cooperative):
-    context, force = centred_case(cooperative)
+def uninterrupted(steps):
+    context, force = centred_case()
     context.integrator.step(steps)
     out = (context.positions.copy(), context.velocities.copy(), force.getFluidState(context))
     context.close()
     return out
 
 
-@pytest.mark.parametrize('cooperative', [False, True])
-def test_cg_iteration_cap_reports_non_convergence_and_leaves_no_reaction(cooperative):
-    expected = uninterrupted(5, cooperative)
-    context, force = centred_case(cooperative)
+def test_cg_iteration_cap_reports_non_convergence_and_leaves_no_reaction():
+    expected = uninterrupted(5)
+    context, force = centred_case()
     context.integrator.step(2)
     context.kernel.set_solver_limits(max_iterations=1)
     with pytest.raises(LbmError) as failure:
@@ -50,7 +46,7 @@ def test_cg_iteration_cap_reports_non_convergence_and_leaves_no_reaction(coopera
 
 def crowded_case(count=600):
     """`count` particles of mass 100 spread over a 16^3 lattice, Keys stencil, centred drag with friction 10/ps and a
-    field, solved by the cooperative solve over all particles (count/32 blocks of 1024 threads)."""
+    field: the cooperative solve runs on count/32 blocks of 1024 threads (one warp per particle)."""
     import lbm_b200
     from lbm_b200 import LBMForce
     system = lbm_b200.System()
@@ -71,7 +67,6 @@ def crowded_case(count=600):
     rng = np.random.default_rng(21)
     context.setPositions(rng.uniform(0.0, 8.0, (count, 3)))
     context.setVelocities(rng.normal(0.0, 0.5, (count, 3)))
-    context.kernel.set_component_capacity(-1)
     return context, force
 
 
