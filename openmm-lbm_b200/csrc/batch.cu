@@ -17,6 +17,7 @@
 #include "lbm_b200_batch.h"
 #include "lbm_b200_md.h"
 #include "collide.cuh"
+#include "collide_pair.cuh"
 #include "coupling_device.cuh"
 #include "grid_barrier.cuh"
 #include "lbm_internal.h"
@@ -26,6 +27,7 @@
 #include <new>
 #include <random>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace lbm {
@@ -42,9 +44,10 @@ struct BatchClock {
 
 // Per replica, on the device.
 struct ReplicaTable {
-    unsigned nodeOffset;     // first node of the replica in the concatenated populations (19 arrays of N_r each)
+    unsigned nodeOffset;     // first node of the replica in the concatenated populations (19 arrays of N_r each; even)
     unsigned numNodes;
     int firstItem, numItems; // work items of the dense kernel
+    int paired;              // FP32 storage and an even nx: two x-adjacent nodes per thread (2 BT nodes per item)
     int firstParticle, numParticles;
     int removeFrequency;
     double dt;               // ps
@@ -68,6 +71,54 @@ __device__ __forceinline__ double warpReduceSum(double v) {
     return v;
 }
 
+// Pair `pair` of a replica with an even nx and FP32 storage: nodes 2 pair and 2 pair + 1 of one row, by the paired body
+// of the single-lattice kernel (collide_pair.cuh) with the replica's view; the pulls are aligned float2 words (the
+// replica's arrays start at an even node, and its planes hold an even number of nodes).  COHERENT: the inputs were
+// written by other blocks of the same launch, so they are read through L2.
+template <bool REACT, bool FLUCT, bool COHERENT>
+__device__ __forceinline__ void pairedItem(const float* __restrict__ A, float* __restrict__ B, const FluidView& v,
+                                           unsigned N, unsigned pair, int remove, const double ucm[3], long long step,
+                                           float (&sums)[4]) {
+    const unsigned node = 2*pair;
+    if (node >= N)
+        return;
+    const int nx = v.nx, ny = v.ny, nz = v.nz;
+    const unsigned row = node/(unsigned) nx;
+    const int x0 = (int) (node - row*(unsigned) nx), y = (int) (row%(unsigned) ny), z = (int) (row/(unsigned) ny);
+    const float2* aw = reinterpret_cast<const float2*>(A);
+    float2* bw = reinterpret_cast<float2*>(B);
+    const unsigned halfN = N/2;
+    const int ys[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};
+    const int zs[3] = {z == 0 ? nz - 1 : z - 1, z, z == nz - 1 ? 0 : z + 1};
+    const int xl = x0 == 0 ? nx - 2 : x0 - 2, xr = x0 + 2 == nx ? 0 : x0 + 2;
+    auto load = [&](const float2* p) { return COHERENT ? __ldcg(p) : __ldg(p); };
+    F2 r[19];
+    staticFor<19>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+        const unsigned base = ((unsigned) zs[1-cz]*ny + ys[1-cy])*nx;
+        const float2* plane = aw + (size_t) q*halfN;
+        float2 w;
+        if (cx == 0)
+            w = load(plane + (base + x0)/2);
+        else if (cx == 1)
+            w = PairIO<float>::left(load(plane + (base + xl)/2), load(plane + (base + x0)/2));
+        else
+            w = PairIO<float>::right(load(plane + (base + x0)/2), load(plane + (base + xr)/2));
+        r[q] = PairIO<float>::decode(w);
+    });
+    bool reactA = false, reactB = false;
+    if (REACT) {
+        const uint32_t* mp = &v.reactMask[(size_t) row*v.wordsPerRow + (x0 >> 5)];
+        const uint32_t word = COHERENT ? __ldcg(mp) : __ldg(mp);
+        reactA = (word >> (x0 & 31)) & 1u;
+        reactB = (word >> ((x0 + 1) & 31)) & 1u;
+    }
+    const PairConstants c = pairConstants(v, remove, step, ucm);
+    collidePair<float, false, REACT, FLUCT, COHERENT>(r, v, c, remove, step, node, false, false, reactA, reactB,
+                                                      bw + node/2, halfN, sums);
+}
+
 template <typename T, typename R, bool REACT, bool FLUCT, int BT>
 __global__ void __launch_bounds__(BT, batchMinBlocks<R, BT>())
 batchStreamCollideKernel(const T* __restrict__ A, T* __restrict__ B, const FluidView* __restrict__ views,
@@ -80,8 +131,23 @@ batchStreamCollideKernel(const T* __restrict__ A, T* __restrict__ B, const Fluid
         const FluidView& v = views[r];
         const ReplicaTable& rt = table[r];
         const int remove = rt.removeFrequency > 0 && step%rt.removeFrequency == 0;
-        const CollideConstants<R> k = collideConstants<R>(v.omega, v.g, v.stats->ucm, remove, v.mu, v.seed);
         const unsigned N = rt.numNodes;
+        const size_t base = (size_t) 19*rt.nodeOffset;
+        if constexpr (std::is_same<T, float>::value) {
+            if (rt.paired) {
+                float sums[4] = {0, 0, 0, 0};
+                pairedItem<REACT, FLUCT, false>(A + base, B + base, v, N, (unsigned) (w - rt.firstItem)*BT + threadIdx.x,
+                                                remove, v.stats->ucm, step, sums);
+                double s0 = warpReduceSum((double) sums[0]), s1 = warpReduceSum((double) sums[1]);
+                double s2 = warpReduceSum((double) sums[2]), s3 = warpReduceSum((double) sums[3]);
+                if (lane == 0) {
+                    double* out = partials + 4*((size_t) w*(BT/32) + warp);
+                    out[0] = s0; out[1] = s1; out[2] = s2; out[3] = s3;
+                }
+                continue;
+            }
+        }
+        const CollideConstants<R> k = collideConstants<R>(v.omega, v.g, v.stats->ucm, remove, v.mu, v.seed);
         const unsigned local = (unsigned) (w - rt.firstItem)*BT + threadIdx.x;
         R sm = 0, sx = 0, sy = 0, sz = 0;
         if (local < N) {
@@ -99,7 +165,6 @@ batchStreamCollideKernel(const T* __restrict__ A, T* __restrict__ B, const Fluid
                     ez = rp[2];
                 }
             }
-            const size_t base = (size_t) 19*rt.nodeOffset;
             collideNode<T, R, FLUCT>(A + base, B + base, N, local, x, y, z, nx, ny, nz, k, ex, ey, ez, step, sm, sx, sy, sz);
         }
         double s0 = warpReduceSum((double) sm), s1 = warpReduceSum((double) sx);
@@ -518,8 +583,26 @@ batchPersistentKernel(PersistentArgs a) {
             const int remove = rt.removeFrequency > 0 && step%rt.removeFrequency == 0;
             // The removal velocity of this step, written by phase 1 of this launch: read through L2.
             const double ucm[3] = {__ldcg(&v.stats->ucm[0]), __ldcg(&v.stats->ucm[1]), __ldcg(&v.stats->ucm[2])};
-            const CollideConstants<R> k = collideConstants<R>(v.omega, v.g, ucm, remove, v.mu, v.seed);
             const unsigned N = rt.numNodes;
+            if constexpr (std::is_same<T, float>::value) {
+                if (rt.paired) {
+                    float sums[4] = {0, 0, 0, 0};
+                    const size_t base = (size_t) 19*rt.nodeOffset;
+                    const unsigned pair = (unsigned) (w - rt.firstItem)*BT + threadIdx.x;
+                    if (a.coupled)
+                        pairedItem<true, FLUCT, true>(A + base, B + base, v, N, pair, remove, ucm, step, sums);
+                    else
+                        pairedItem<false, FLUCT, true>(A + base, B + base, v, N, pair, remove, ucm, step, sums);
+                    double s0 = warpReduceSum((double) sums[0]), s1 = warpReduceSum((double) sums[1]);
+                    double s2 = warpReduceSum((double) sums[2]), s3 = warpReduceSum((double) sums[3]);
+                    if (lane == 0) {
+                        double* out = a.partials + 4*((size_t) w*(BT/32) + warp);
+                        out[0] = s0; out[1] = s1; out[2] = s2; out[3] = s3;
+                    }
+                    continue;
+                }
+            }
+            const CollideConstants<R> k = collideConstants<R>(v.omega, v.g, ucm, remove, v.mu, v.seed);
             const unsigned local = (unsigned) (w - rt.firstItem)*BT + threadIdx.x;
             R sm = 0, sx = 0, sy = 0, sz = 0;
             if (local < N) {
@@ -672,13 +755,14 @@ BatchEngine::BatchEngine(int nr, const LbmLatticeParameters* ls, const int* np, 
         long long n = (long long) l.nx*l.ny*l.nz;
         t.nodeOffset = (unsigned) totalNodes;
         t.numNodes = (unsigned) n;
+        t.paired = storage == LBM_STORAGE_F32 && l.nx%2 == 0;
         t.firstParticle = totalParticles;
         t.numParticles = np[r];
         t.removeFrequency = l.momentum_removal_frequency;
         t.dt = l.dt;
         t.box[0] = l.nx*l.dx; t.box[1] = l.ny*l.dx; t.box[2] = l.nz*l.dx;
         tableHost.push_back(t);
-        totalNodes += n;
+        totalNodes += n + (n & 1);       // every replica starts at an even node (aligned float2 words)
         totalParticles += np[r];
         maskWords += (unsigned) (((l.nx + 31)/32)*l.ny*l.nz);
         if (totalNodes >= (1LL << 32) - 1024)
@@ -850,13 +934,15 @@ void BatchEngine::release() {
     stream = nullptr;
 }
 
-// Work items of `bt` consecutive nodes of one replica, and the per-warp partial sums they write.
+// Work items of `bt` consecutive nodes of one replica (2 bt for a paired replica), and the per-warp partial sums they
+// write.
 void BatchEngine::buildItems(int bt) {
     std::vector<int> itemReplica;
     for (int r = 0; r < numReplicas; r++) {
         ReplicaTable& t = tableHost[r];
         t.firstItem = (int) itemReplica.size();
-        t.numItems = (int) ((t.numNodes + bt - 1)/bt);
+        const unsigned span = t.paired ? 2*bt : bt;
+        t.numItems = (int) ((t.numNodes + span - 1)/span);
         itemReplica.insert(itemReplica.end(), t.numItems, r);
     }
     numItems = (int) itemReplica.size();
