@@ -1087,6 +1087,13 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
 }
 
 void CouplingEngine::release() {
+    if (side != nullptr) {
+        cudaStreamSynchronize(side);
+        cudaEventDestroy(begun);
+        cudaEventDestroy(ready);
+        cudaStreamDestroy(side);
+        side = nullptr;
+    }
     cudaFree(posDev); cudaFree(velDev); cudaFree(forceInDev); cudaFree(forceOutDev); cudaFree(massDev);
     cudaFree(wallDev); cudaFree(statusDev);
     posDev = velDev = forceInDev = forceOutDev = massDev = wallDev = nullptr;
@@ -1163,8 +1170,23 @@ static void launchStencil(const void* A, const FluidView& f, const CouplingView&
                                                      (const V*) nodeU, (V*) slotU);
 }
 
+// The cell list and the rows of the coupling matrix, after the status words are cleared (their overflow flag).
 template <typename R>
-void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView* cv) {
+void CouplingEngine::launchMatrix(const CouplingView* cv, cudaStream_t s) {
+    const CouplingView& c = *cv;
+    CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, s));
+    long long total = (long long) np*c.slots;
+    int gridSlots = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
+    cgBinKernel<R><<<gridSlots, kThreads, 0, s>>>(c, (const R*) dev->slotWeight,
+                                                 (const typename Vec4<R>::type*) dev->slotU, (R*) dev->coef, dev->sparse);
+    CUDA_CHECK(cudaGetLastError());
+    cgRowsKernel<R><<<warpGrid(np), kThreads, 0, s>>>(c, (const R*) dev->coef, dev->sparse);
+    CUDA_CHECK(cudaGetLastError());
+    fluid.launches += 2;
+}
+
+template <typename R>
+void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView* cv, bool matrixReady) {
     const CouplingView& c = *cv;
     const FluidView& f = fluid.deviceView();
     bool centred = lattice.drag_scheme == LBM_DRAG_CENTERED;
@@ -1200,9 +1222,9 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     // 1e-13 in double; 1e-5 with single-precision arithmetic, as the reference's GPU platforms in single precision),
     // through the explicit coupling matrix; the spread-and-gather kernel serves a step whose cell list or matrix rows
     // overflow their capacity (and every step with LBM_B200_SPREAD_CG=1 in the environment, for comparisons).
+    // The status words are cleared with the matrix (launchMatrix), or before the spread-and-gather solve below.
     CgBuffers b = dev->cg;
     SparseCg g = dev->sparse;
-    CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, stream));
     double tolerance = std::is_same<R, double>::value ? 1e-13 : 1e-5;
     int maxIterations = cgMaxIterations;
     b.pollLimit = barrierPollLimit;
@@ -1218,22 +1240,15 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     FluidView fv = f;
     CouplingView cc = c;
     int status[3] = {0, 0, 0};
-    static const bool spreadOnly = [] {
-        const char* e = std::getenv("LBM_B200_SPREAD_CG");
-        return e != nullptr && e[0] == '1';
-    }();
+    const bool spreadOnly = !matrixSolve();
     if (!spreadOnly) {
-        long long total = (long long) np*c.slots;
-        int gridSlots = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
-        cgBinKernel<R><<<gridSlots, kThreads, 0, stream>>>(c, sw, su, coef, g);
-        CUDA_CHECK(cudaGetLastError());
-        cgRowsKernel<R><<<warpGrid(np), kThreads, 0, stream>>>(c, coef, g);
-        CUDA_CHECK(cudaGetLastError());
+        if (!matrixReady)
+            launchMatrix<R>(&c, stream);
         void* sparseArgs[] = {&fv, &cc, &vel, &fin, &sn, &sw, &su, &stepArg, &isStepArg, &tolerance, &maxIterations, &b,
                               &g, &fout, &reaction, &mask, &wall};
         CUDA_CHECK(cudaLaunchCooperativeKernel((const void*) centeredSparseKernel<R>, dev->sparseGrid, kSolveThreads,
                                                sparseArgs, 0, stream));
-        fluid.launches += 3;
+        fluid.launches++;
         CUDA_CHECK(cudaMemcpyAsync(status, statusDev, sizeof(int)*3, cudaMemcpyDeviceToHost, stream));
         CUDA_CHECK(cudaStreamSynchronize(stream));
     }
@@ -1264,32 +1279,87 @@ void CouplingEngine::setSolverLimits(int maxIterations, long long barrierPolls) 
     barrierPollLimit = barrierPolls > 0 ? barrierPolls : kDefaultBarrierPolls;
 }
 
-void CouplingEngine::couple(long long step, bool isStep, bool remove) {
+void CouplingEngine::launchStencilPass(const CouplingView& c, bool remove, cudaStream_t s) {
     const FluidView& f = fluid.deviceView();
-    CouplingView c = makeCouplingView(lattice, f, np, widthOf(lattice.interpolation_stencil), massDev);
     bool centred = lattice.drag_scheme == LBM_DRAG_CENTERED;
     const void* A = fluid.inputArray();
     if (++dev->stamp == 0u) {     // the stamps wrapped around: no node may carry a stale stamp
-        CUDA_CHECK(cudaMemsetAsync(dev->nodeStamp, 0, sizeof(unsigned)*(size_t) f.n, stream));
+        CUDA_CHECK(cudaMemsetAsync(dev->nodeStamp, 0, sizeof(unsigned)*(size_t) f.n, s));
         dev->stamp = 1u;
     }
     unsigned* ns = dev->nodeStamp;
     void* nu = dev->nodeU;
     unsigned st = dev->stamp;
     switch (storageType) {
-    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, stream); break;
-    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, stream); break;
-    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, stream); break;
-    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, stream); break;
+    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, s); break;
+    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, s); break;
+    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, s); break;
+    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, s); break;
     }
     CUDA_CHECK(cudaGetLastError());
     fluid.launches += 3;
+}
+
+// The centred stencil drag through the explicit coupling matrix (not the spread-and-gather solve of every step).
+bool CouplingEngine::matrixSolve() const {
+    static const bool spreadOnly = [] {
+        const char* e = std::getenv("LBM_B200_SPREAD_CG");
+        return e != nullptr && e[0] == '1';
+    }();
+    return lattice.drag_scheme == LBM_DRAG_CENTERED && lattice.interpolation_stencil != LBM_STENCIL_NEAREST &&
+           !spreadOnly;
+}
+
+void CouplingEngine::prepare(const LbmParticleArrays* p, long long step, bool remove) {
+    discardPrepared();
+    size_t v3 = sizeof(double)*3*(size_t) np;
+    cudaMemcpyKind kind = p->memory == LBM_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CUDA_CHECK(cudaMemcpyAsync(posDev, p->positions, v3, kind, stream));
+    if (side == nullptr) {
+        CUDA_CHECK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        CUDA_CHECK(cudaEventCreateWithFlags(&begun, cudaEventDisableTiming));
+        CUDA_CHECK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    }
+    CUDA_CHECK(cudaEventRecord(begun, stream));
+    CUDA_CHECK(cudaStreamWaitEvent(side, begun, 0));
+    const FluidView& f = fluid.deviceView();
+    CouplingView c = makeCouplingView(lattice, f, np, widthOf(lattice.interpolation_stencil), massDev);
+    launchStencilPass(c, remove, side);
+    if (matrixSolve()) {
+        if (storageType == LBM_STORAGE_F64)
+            launchMatrix<double>(&c, side);
+        else
+            launchMatrix<float>(&c, side);
+    }
+    CUDA_CHECK(cudaEventRecord(ready, side));
+    prepared = true;
+    preparedStep = step;
+    preparedRemove = remove;
+}
+
+void CouplingEngine::joinPrepared() {
+    if (prepared)
+        CUDA_CHECK(cudaStreamWaitEvent(stream, ready, 0));
+}
+
+void CouplingEngine::discardPrepared() {
+    joinPrepared();
+    prepared = false;
+}
+
+void CouplingEngine::couple(long long step, bool isStep, bool remove) {
+    const FluidView& f = fluid.deviceView();
+    CouplingView c = makeCouplingView(lattice, f, np, widthOf(lattice.interpolation_stencil), massDev);
+    const bool usePrepared = prepared && isStep && step == preparedStep && remove == preparedRemove;
+    discardPrepared();
+    if (!usePrepared)
+        launchStencilPass(c, remove, stream);
     if (isStep)
         CUDA_CHECK(cudaMemsetAsync(wallDev, 0, sizeof(double)*3, stream));
     if (storageType == LBM_STORAGE_F64)
-        coupleWith<double>(step, isStep, &c);
+        coupleWith<double>(step, isStep, &c, usePrepared);
     else
-        coupleWith<float>(step, isStep, &c);
+        coupleWith<float>(step, isStep, &c, usePrepared);
 }
 
 void CouplingEngine::addForces(const LbmParticleArrays* p) {

@@ -28,6 +28,14 @@ public:
     // Coupling forces of step `step` on the current fluid (isStep: also the reaction on the fluid, with the
     // momentum removal `remove`).  Returns the momentum of the reactions on solid nodes, Da nm/ps (isStep only).
     void couple(long long step, bool isStep, bool remove);
+    // The part of step `step`'s coupling that needs only the positions and the fluid (the stencil pass and, for the
+    // centred stencil drag, the cell list and the rows of the coupling matrix), launched at beginStep on a second
+    // stream, so that it runs while the caller computes its other forces; couple() of that step continues from it.
+    void prepare(const LbmParticleArrays* particles, long long step, bool remove);
+    // The kernel's stream waits for prepared work (before anything that changes its inputs); discardPrepared() also
+    // forgets it (the fluid or the parameters changed, or another evaluation comes first).
+    void joinPrepared();
+    void discardPrepared();
     // Add the coupling forces to the force array of the call.
     void addForces(const LbmParticleArrays* particles);
     // Clear the reaction of the last step from the fluid's reaction buffers.
@@ -46,7 +54,15 @@ private:
     struct Device;
     void release();
     template <typename R>
-    void coupleWith(long long step, bool isStep, const CouplingView* view);
+    void coupleWith(long long step, bool isStep, const CouplingView* view, bool matrixReady);
+    template <typename R>
+    void launchMatrix(const CouplingView* view, cudaStream_t s);
+    void launchStencilPass(const CouplingView& view, bool remove, cudaStream_t s);
+    bool matrixSolve() const;
+    cudaStream_t side = nullptr;          // stream of the prepared work
+    cudaEvent_t begun = nullptr, ready = nullptr;
+    bool prepared = false, preparedRemove = false;
+    long long preparedStep = -1;
     LbmLatticeParameters lattice;
     FluidEngine& fluid;
     cudaStream_t stream;

@@ -143,6 +143,12 @@ void B200Kernel::beginStep(long long stepCount, const LbmParticleArrays* particl
             throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_begin_step: the particle arrays are missing");
         coupling->reflect(particles, hostWallMomentum);
     }
+    // The positions are those of the step's evaluation: the stencil pass (and the coupling matrix) of the step starts
+    // now, beside the caller's other forces.
+    if (numParticles > 0 && particles != nullptr) {
+        bool remove = lattice.momentum_removal_frequency > 0 && stepCount%lattice.momentum_removal_frequency == 0;
+        coupling->prepare(particles, stepCount, remove);
+    }
 }
 
 // execute (ReferenceLBMKernels.cpp:341-365).
@@ -209,8 +215,8 @@ void B200Kernel::beginStepOpenMM(long long stepCount, const LbmOpenMMBuffers* bu
     validateOpenMMBuffers(buffers, openmmAtoms);
     LbmParticleArrays a = stagingArrays();
     bool reflects = !geometry.solidNodes.empty();
-    if (reflects)
-        gatherOpenMM(*buffers, couplingIndexDev, a.positions, a.velocities, nullptr, false, stream);
+    // The positions also start the step's coupling (beginStep prepares it).
+    gatherOpenMM(*buffers, couplingIndexDev, a.positions, a.velocities, nullptr, false, stream);
     beginStep(stepCount, &a);
     if (reflects)
         scatterVelocitiesOpenMM(*buffers, couplingIndexDev, a.velocities, stream);
@@ -238,6 +244,7 @@ void B200Kernel::advanceFluid(const LbmParticleArrays* particles) {
     bool remove = lattice.momentum_removal_frequency > 0 && stepIndex%lattice.momentum_removal_frequency == 0;
     bool react = false;
     if (numParticles > 0) {
+        coupling->joinPrepared();
         coupling->load(particles, lattice.drag_scheme == LBM_DRAG_CENTERED);
         try {
             coupling->couple(stepIndex, true, remove);
@@ -264,6 +271,7 @@ void B200Kernel::advanceFluid(const LbmParticleArrays* particles) {
 void B200Kernel::computeNextStepForces(long long stepCount, const LbmParticleArrays* particles) {
     stepForcesCurrent = false;
     bool remove = lattice.momentum_removal_frequency > 0 && stepCount%lattice.momentum_removal_frequency == 0;
+    coupling->discardPrepared();
     coupling->load(particles, lattice.drag_scheme == LBM_DRAG_CENTERED);
     coupling->couple(stepCount, false, remove);
 }
@@ -282,6 +290,9 @@ void B200Kernel::checkMachNumber() {
 
 void B200Kernel::copyParameters(const LbmLatticeParameters& l) {
     CUDA_CHECK(cudaSetDevice(device));
+    // The fluid or the parameters change: prepared coupling work is waited for and dropped.
+    if (coupling)
+        coupling->discardPrepared();
     if (l.nx != lattice.nx || l.ny != lattice.ny || l.nz != lattice.nz)
         throw Error(LBM_ERR_INVALID_ARGUMENT, "updateParametersInContext: the grid size cannot be changed");
     if (l.density != lattice.density || l.tau != lattice.tau)
@@ -314,6 +325,9 @@ void B200Kernel::getFluidFields(double* density, double* velocity) {
 
 void B200Kernel::setFluidEquilibrium(const double* density, const double* velocity, bool onDevice, bool strain) {
     CUDA_CHECK(cudaSetDevice(device));
+    // The fluid or the parameters change: prepared coupling work is waited for and dropped.
+    if (coupling)
+        coupling->discardPrepared();
     fluid->setEquilibrium(density, velocity, onDevice, lattice.density, lattice.dx/lattice.dt, strain);
 }
 
@@ -322,6 +336,9 @@ void B200Kernel::setFluidEquilibrium(const double* density, const double* veloci
 long long B200Kernel::steadySolve(long long firstStep, int interval, double tolerance, long long maxSteps,
                                   double* residual) {
     CUDA_CHECK(cudaSetDevice(device));
+    // The fluid or the parameters change: prepared coupling work is waited for and dropped.
+    if (coupling)
+        coupling->discardPrepared();
     if (numParticles > 0)
         throw Error(LBM_ERR_NOT_SUPPORTED, "lbm_steady_solve: the steady solve advances a fluid without coupled particles");
     if (interval <= 0 || maxSteps < 0)
@@ -394,6 +411,9 @@ void B200Kernel::getFluidState(double* state) {
 // setFluidState (ReferenceLBMKernels.cpp:1488-1505).
 void B200Kernel::setFluidState(const double* state) {
     CUDA_CHECK(cudaSetDevice(device));
+    // The fluid or the parameters change: prepared coupling work is waited for and dropped.
+    if (coupling)
+        coupling->discardPrepared();
     fluid->setState(state);
     stepForcesCurrent = false;
 }
@@ -496,6 +516,9 @@ void B200Kernel::createCheckpoint(void* buffer, size_t bytes) {
 
 void B200Kernel::loadCheckpoint(const void* buffer, size_t bytes) {
     CUDA_CHECK(cudaSetDevice(device));
+    // The fluid or the parameters change: prepared coupling work is waited for and dropped.
+    if (coupling)
+        coupling->discardPrepared();
     const char* in = (const char*) buffer;
     int head[3];
     if (bytes < sizeof(head))
