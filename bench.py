@@ -251,9 +251,7 @@ def run_batch(args, w, rank, world, device):
     ms = start.elapsed_time(stop)
     launches = batch.info()['launches'] - launches0
     if world > 1:
-        t = torch.tensor([ms], device='cuda')
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms)
     # End to end through the C ABI: every run of graph_steps steps takes the beads' velocities from host memory and
     # returns their positions and velocities to host memory.
     pos_h, vel_h = batch.particles_state()
@@ -335,6 +333,22 @@ def separate_launch_mlups(lbm, w, lattices, positions, precision, steps):
         kernel.close()
         md.close()
     return w.fluid_nodes()*steps/(ms*1e-3)/1e6
+
+
+def max_over_ranks(value):
+    """The largest of a value over the ranks of the job (a time: the slowest rank sets the job's time).  Every rank
+    takes this collective at the same point; with the NCCL backend the value goes through the rank's GPU."""
+    import torch
+    device = 'cuda' if torch.distributed.get_backend() == 'nccl' else 'cpu'
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mlups(world, nodes, steps, ms):
+    """Node updates per second of the whole job: every rank advances its own replica of `nodes` nodes (replicas only,
+    no exchange), so the job updates world x nodes x steps nodes in the slowest rank's time."""
+    return world*nodes*steps/(ms*1e-3)/1e6
 
 
 def peaks():
@@ -449,9 +463,7 @@ def run_b200(args, w, rank, world, device):
     lib.lbm_kernel_launches(kernel.handle, ctypes.byref(launches1))
     gpu_launches = int(launches1.value - launches0.value) + ((md.launches() - md0) if md else 0)
     if dist:
-        t = torch.tensor([ms], device='cuda')
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms)
 
     # End to end through the C ABI with the particles in pinned host memory: every step copies the beads'
     # positions and velocities to the device, runs the step, and reads them back.
@@ -478,9 +490,7 @@ def run_b200(args, w, rank, world, device):
         s += 1
     e2e_s = time.perf_counter() - t0
     if dist:
-        t = torch.tensor([e2e_s], device='cuda')
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s = max_over_ranks(e2e_s)
 
     observables = {}
     if rank == 0 and args.observables:
@@ -496,8 +506,8 @@ def run_b200(args, w, rank, world, device):
             observables['cg_iterations_last_step'] = iterations.value
     kernel.close()
 
-    value = world*nodes*args.steps/(ms*1e-3)/1e6
-    e2e_value = world*nodes*e2e_steps/e2e_s/1e6
+    value = job_mlups(world, nodes, args.steps, ms)
+    e2e_value = job_mlups(world, nodes, e2e_steps, e2e_s*1e3)
     bytes_per_node = 2*19*STORAGE_BYTES[args.precision]
     avg_dense_s = dense_ms.value*1e-3/max(1, dense_launches.value)
     achieved = bytes_per_node*nodes/avg_dense_s/1e9
