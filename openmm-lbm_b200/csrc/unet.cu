@@ -163,6 +163,82 @@ __device__ __forceinline__ void drainStage(const Stage& st, int stage) {
     __syncthreads();
 }
 
+// Two pairs of tiles used in turn (the forward kernel): stage c of the K loop uses buffer c & 1, and its MMAs are
+// committed to that buffer's mbarrier, whose (c >> 1)-th phase completes when they (and every earlier MMA) are done;
+// the threads assemble stage c + 1 while the tensor cores run stage c.
+constexpr int kStages = 2;
+
+struct Stages {
+    uint8_t* tileA[kStages];
+    uint8_t* tileB[kStages];
+    uint32_t mbar[kStages];
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ Stages setupStages(uint8_t* raw, int rowsB, uint32_t ncols) {
+    uint32_t s = smemAddr(raw);
+    uint8_t* base = raw + ((1024 - (s & 1023)) & 1023);
+    const size_t tileBytes = (size_t) kTileM*128 + (size_t) ((rowsB*128 + 1023)/1024)*1024;
+    Stages st;
+    for (int k = 0; k < kStages; k++) {
+        st.tileA[k] = base + k*tileBytes;
+        st.tileB[k] = st.tileA[k] + kTileM*128;
+    }
+    uint64_t* bar = reinterpret_cast<uint64_t*>(base + kStages*tileBytes);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + kStages);
+    for (int k = 0; k < kStages; k++)
+        st.mbar[k] = smemAddr(bar + k);
+    if (threadIdx.x/32 == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(smemAddr(slot)), "r"(ncols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kStages; k++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(st.mbar[k]), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    fenceBeforeSync();
+    __syncthreads();
+    fenceAfterSync();
+    st.tmem = *slot;
+    return st;
+}
+
+__device__ __forceinline__ void releaseStages(const Stages& st, uint32_t ncols) {
+    fenceBeforeSync();
+    __syncthreads();
+    if (threadIdx.x/32 == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(st.tmem), "r"(ncols) : "memory");
+}
+
+// Wait (every thread, bounded) until the MMAs of stage c are done; false, for every thread, if a wait gave up.
+__device__ __forceinline__ bool waitStage(const Stages& st, int c, long long limit) {
+    bool ok = waitParity(st.mbar[c & 1], (uint32_t) ((c >> 1) & 1), limit);
+    return __syncthreads_and(ok) != 0;
+}
+
+// Issue stage c: the tiles of buffer c & 1 are in shared memory; thread 0 issues the four K = 16 MMAs and commits them.
+__device__ __forceinline__ void issueStage(const Stages& st, uint32_t idesc, int c) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        fenceAfterSync();
+        const int b = c & 1;
+        uint32_t a = smemAddr(st.tileA[b]), bb = smemAddr(st.tileB[b]);
+        for (int j = 0; j < 4; j++)
+            mmaBf16(st.tmem, smemDescriptor(a + 32*j), smemDescriptor(bb + 32*j), idesc, (c > 0 || j > 0) ? 1u : 0u);
+        commitTo(st.mbar[b]);
+    }
+}
+
+// After a wait that gave up: wait once more, with the full limit, for the last issued stage (its commit tracks every
+// earlier MMA), so that the tensor memory and the tiles are released only when the tensor cores are done with them.
+__device__ __forceinline__ void drainStages(const Stages& st, int lastIssued) {
+    if (lastIssued >= 0)
+        waitParity(st.mbar[lastIssued & 1], (uint32_t) ((lastIssued >> 1) & 1), kSpinLimit);
+    __syncthreads();
+}
+
 // The forward convolution over tiles of 128 output voxels, tx x ty voxels of one z-plane of one batch item (tx ty = 128),
 // in the GEMM's K order of channel chunks: for each chunk of at most 64 input channels the block loads the halo brick of
 // its tile, (tx + 2) x (ty + 2) x 3 voxels of the chunk's channels, once from global memory into shared memory, and
@@ -174,10 +250,10 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
                   __nv_bfloat16* __restrict__ y, int batch, int D, int H, int W, int cin, int cout, int relu, int tx) {
     extern __shared__ uint8_t smemRaw[];
     const uint32_t ncols = tmemColumns(cout);
-    Stage st = setupStage(smemRaw, cout, ncols);
+    Stages st = setupStages(smemRaw, cout, ncols);
     const int ty = kTileM/tx, bx = tx + 2, by = ty + 2;
-    // The brick after the B tile and the mbarrier and tensor-memory slot that follow it (16 bytes at tileB + cout 128).
-    uint8_t* brick = st.tileB + (size_t) cout*128 + 1024;
+    // The brick after the second pair of tiles and the mbarriers and tensor-memory slot that follow it (24 bytes).
+    uint8_t* brick = st.tileA[1] + (size_t) kTileM*128 + (size_t) ((cout*128 + 1023)/1024)*1024 + 1024;
     const int tid = threadIdx.x, warp = tid/32, lane = tid%32;
     const int K = 27*cin;
     const uint32_t idesc = instrDescriptor(cout);
@@ -192,12 +268,12 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
     const int mx = tid%tx, my = tid/tx;
     const long long limit = convWaitPolls;
     bool ok = true;
-    int failedStage = -1, stage = 0;
+    int stage = 0, lastIssued = -1;
     for (int c0 = 0; c0 < cin && ok; c0 += 64) {
         const int cc = min(64, cin - c0);        // channels of this chunk (a multiple of 8)
         const int groups = cc/8;
-        // The halo brick of the chunk: [z 3][y by][x bx][cc] BF16, zeros outside the volume.  The barrier before the
-        // first write: the previous chunk's last stage has been assembled by every thread (runStage ends with one).
+        // The halo brick of the chunk: [z 3][y by][x bx][cc] BF16, zeros outside the volume.  Every thread has
+        // assembled the previous chunk's stages (each issue begins with a block barrier); the MMAs read only the tiles.
         const int bricks = 3*by*bx*groups;
         for (int i = tid; i < bricks; i += kThreads) {
             const int g = i%groups;
@@ -213,7 +289,12 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
         }
         __syncthreads();
         const int Kc = 27*cc, stages = (Kc + kChunk - 1)/kChunk;
-        for (int s = 0; s < stages && ok; s++, stage++) {
+        for (int s = 0; s < stages; s++, stage++) {
+            // Buffer stage & 1 is free once the MMAs of stage - 2 are done.
+            if (stage >= kStages && !(ok = waitStage(st, stage - kStages, limit)))
+                break;
+            uint8_t* tileA = st.tileA[stage & 1];
+            uint8_t* tileB = st.tileB[stage & 1];
             // A: row tid, 8 chunks of 8 channels: k' = s*64 + 8 kv within the chunk's [tap][channel] range.
             for (int kv = 0; kv < 8; kv++) {
                 const int kk = s*kChunk + kv*8;
@@ -223,7 +304,7 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
                     const int bzi = tap/9, byi = my + (tap/3)%3, bxi = mx + tap%3;
                     val = *reinterpret_cast<const uint4*>(brick + (size_t) 2*(((bzi*by + byi)*bx + bxi)*cc + ci));
                 }
-                *reinterpret_cast<uint4*>(st.tileA + swizzled(tid, kv)) = val;
+                *reinterpret_cast<uint4*>(tileA + swizzled(tid, kv)) = val;
             }
             // B: the weights of the same K slice, W[n][tap cin + c0 + ci].
             for (int i = tid; i < cout*8; i += kThreads) {
@@ -233,15 +314,16 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
                     const int tap = kk/cc, ci = kk - tap*cc;
                     val = __ldg(reinterpret_cast<const uint4*>(w + (long long) row*K + tap*cin + c0 + ci));
                 }
-                *reinterpret_cast<uint4*>(st.tileB + swizzled(row, kv)) = val;
+                *reinterpret_cast<uint4*>(tileB + swizzled(row, kv)) = val;
             }
-            ok = runStage(st, idesc, stage, limit);
-            if (!ok)
-                failedStage = stage;
+            issueStage(st, idesc, stage);
+            lastIssued = stage;
         }
     }
+    if (ok && lastIssued >= 0)
+        ok = waitStage(st, lastIssued, limit);
     if (!ok)
-        drainStage(st, failedStage);
+        drainStages(st, lastIssued);
     fenceAfterSync();
     if (ok) {
         const int row = warp*32 + lane;
@@ -263,7 +345,7 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
     }
     else if (tid == 0)
         atomicExch(&convStatus, (int) LBM_ERR_DEVICE_TIMEOUT);
-    releaseStage(st, ncols);
+    releaseStages(st, ncols);
 }
 
 // dW[cout][k] += sum_m dy[m][cout] A[m][k]: A tile rows = cout (tile of 128), B tile rows = k (tile of nt), the GEMM's
@@ -372,9 +454,10 @@ LbmStatus lbm_conv3d_forward(const void* x, const void* w, const float* bias, vo
         ty *= 2;
     const int tx = kTileM/ty;
     const int cc = std::min(64, cin);
-    // stageBytes: 1024 of alignment slack, the A and B tiles, 64 for the mbarrier and the slot; then 1024 more, which
-    // the brick starts after (tileB + cout 128 + 1024), and the brick.
-    size_t smem = stageBytes(cout) + 1024 + (size_t) 3*(tx + 2)*(ty + 2)*cc*2;
+    // 1024 of alignment slack, two pairs of tiles (the B tile rounded to 1024), 1024 for the mbarriers and the slot,
+    // then the brick.
+    size_t smem = 1024 + 2*((size_t) kTileM*128 + (size_t) ((cout*128 + 1023)/1024)*1024) + 1024 +
+                  (size_t) 3*(tx + 2)*(ty + 2)*cc*2;
     cudaError_t e = cudaFuncSetAttribute(convForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess)
         return launchError(e);
