@@ -1,8 +1,7 @@
 // Tensor-core 3x3x3 convolutions of the learned warm start (include/lbm_b200_warmstart.h), written for sm_100a:
 //
 //  convForwardKernel    y[voxel][cout] = sum_k A[voxel][k] W[cout][k], k = tap*cin + ci, A the implicit im2col of x
-//                       (zero padding); one CTA per tile of 128 voxels, all cout in one N tile (<= 256), the A tiles
-//                       assembled from a halo brick of the input held in shared memory
+//                       (zero padding); one CTA per 128 voxels, all cout in one N tile (<= 256)
 //  convWeightGradKernel dW[cout][k] = sum_voxels dy[voxel][cout] A[voxel][k]; CTAs over (cout tile, k tile, voxel
 //                       split), the K dimension of the GEMM being the voxels; results added with FP32 atomics
 //
@@ -163,181 +162,66 @@ __device__ __forceinline__ void drainStage(const Stage& st, int stage) {
     __syncthreads();
 }
 
-// Two pairs of tiles used in turn (the forward kernel): stage c of the K loop uses buffer c & 1, and its MMAs are
-// committed to that buffer's mbarrier, whose (c >> 1)-th phase completes when they (and every earlier MMA) are done;
-// the threads assemble stage c + 1 while the tensor cores run stage c.
-constexpr int kStages = 2;
-
-struct Stages {
-    uint8_t* tileA[kStages];
-    uint8_t* tileB[kStages];
-    uint32_t mbar[kStages];
-    uint32_t tmem;
-};
-
-__device__ __forceinline__ Stages setupStages(uint8_t* raw, int rowsB, uint32_t ncols) {
-    uint32_t s = smemAddr(raw);
-    uint8_t* base = raw + ((1024 - (s & 1023)) & 1023);
-    const size_t tileBytes = (size_t) kTileM*128 + (size_t) ((rowsB*128 + 1023)/1024)*1024;
-    Stages st;
-    for (int k = 0; k < kStages; k++) {
-        st.tileA[k] = base + k*tileBytes;
-        st.tileB[k] = st.tileA[k] + kTileM*128;
-    }
-    uint64_t* bar = reinterpret_cast<uint64_t*>(base + kStages*tileBytes);
-    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + kStages);
-    for (int k = 0; k < kStages; k++)
-        st.mbar[k] = smemAddr(bar + k);
-    if (threadIdx.x/32 == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(smemAddr(slot)), "r"(ncols) : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < kStages; k++)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(st.mbar[k]), "r"(1) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    fenceBeforeSync();
-    __syncthreads();
-    fenceAfterSync();
-    st.tmem = *slot;
-    return st;
-}
-
-__device__ __forceinline__ void releaseStages(const Stages& st, uint32_t ncols) {
-    fenceBeforeSync();
-    __syncthreads();
-    if (threadIdx.x/32 == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(st.tmem), "r"(ncols) : "memory");
-}
-
-// Wait (every thread, bounded) until the MMAs of stage c are done; false, for every thread, if a wait gave up.
-__device__ __forceinline__ bool waitStage(const Stages& st, int c, long long limit) {
-    bool ok = waitParity(st.mbar[c & 1], (uint32_t) ((c >> 1) & 1), limit);
-    return __syncthreads_and(ok) != 0;
-}
-
-// Issue stage c: the tiles of buffer c & 1 are in shared memory; thread 0 issues the four K = 16 MMAs and commits them.
-__device__ __forceinline__ void issueStage(const Stages& st, uint32_t idesc, int c) {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        fenceAfterSync();
-        const int b = c & 1;
-        uint32_t a = smemAddr(st.tileA[b]), bb = smemAddr(st.tileB[b]);
-        for (int j = 0; j < 4; j++)
-            mmaBf16(st.tmem, smemDescriptor(a + 32*j), smemDescriptor(bb + 32*j), idesc, (c > 0 || j > 0) ? 1u : 0u);
-        commitTo(st.mbar[b]);
-    }
-}
-
-// After a wait that gave up: wait once more, with the full limit, for the last issued stage (its commit tracks every
-// earlier MMA), so that the tensor memory and the tiles are released only when the tensor cores are done with them.
-__device__ __forceinline__ void drainStages(const Stages& st, int lastIssued) {
-    if (lastIssued >= 0)
-        waitParity(st.mbar[lastIssued & 1], (uint32_t) ((lastIssued >> 1) & 1), kSpinLimit);
-    __syncthreads();
-}
-
-// The forward convolution over tiles of 128 output voxels, tx x ty voxels of one z-plane of one batch item (tx ty = 128),
-// in the GEMM's K order of channel chunks: for each chunk of at most 64 input channels the block loads the halo brick of
-// its tile, (tx + 2) x (ty + 2) x 3 voxels of the chunk's channels, once from global memory into shared memory, and
-// assembles the A tile of every K stage of the chunk (27 taps x the chunk's channels, 64 at a time) from the brick; the
-// B tile is the matching slice of the weights.  Each input voxel is read from global memory once per tile instead of
-// once per tap.
 __global__ void __launch_bounds__(kThreads)
 convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ w, const float* __restrict__ bias,
-                  __nv_bfloat16* __restrict__ y, int batch, int D, int H, int W, int cin, int cout, int relu, int tx) {
+                  __nv_bfloat16* __restrict__ y, int batch, int D, int H, int W, int cin, int cout, int relu) {
     extern __shared__ uint8_t smemRaw[];
     const uint32_t ncols = tmemColumns(cout);
-    Stages st = setupStages(smemRaw, cout, ncols);
-    const int ty = kTileM/tx, bx = tx + 2, by = ty + 2;
-    // The brick after the second pair of tiles and the mbarriers and tensor-memory slot that follow it (24 bytes).
-    uint8_t* brick = st.tileA[1] + (size_t) kTileM*128 + (size_t) ((cout*128 + 1023)/1024)*1024 + 1024;
+    Stage st = setupStage(smemRaw, cout, ncols);
     const int tid = threadIdx.x, warp = tid/32, lane = tid%32;
-    const int K = 27*cin;
+    const long long M = (long long) batch*D*H*W;
+    const int K = 27*cin, stages = (K + kChunk - 1)/kChunk;
     const uint32_t idesc = instrDescriptor(cout);
-    // The tile: blockIdx.x over (x tiles, y tiles, z, batch).
-    const int tilesX = (W + tx - 1)/tx, tilesY = (H + ty - 1)/ty;
-    long long t = blockIdx.x;
-    const int x0 = (int) (t%tilesX)*tx; t /= tilesX;
-    const int y0 = (int) (t%tilesY)*ty; t /= tilesY;
-    const int z0 = (int) (t%D);
-    const int vn = (int) (t/D);
-    // This thread's row of A: voxel (x0 + mx, y0 + my, z0).
-    const int mx = tid%tx, my = tid/tx;
+    // The voxel of this thread's row of A.
+    const long long m = (long long) blockIdx.x*kTileM + tid;
+    const bool valid = m < M;
+    int vx = 0, vy = 0, vz = 0, vn = 0;
+    if (valid) {
+        long long r = m;
+        vx = (int) (r%W); r /= W;
+        vy = (int) (r%H); r /= H;
+        vz = (int) (r%D); vn = (int) (r/D);
+    }
     const long long limit = convWaitPolls;
     bool ok = true;
-    int stage = 0, lastIssued = -1;
-    for (int c0 = 0; c0 < cin && ok; c0 += 64) {
-        const int cc = min(64, cin - c0);        // channels of this chunk (a multiple of 8)
-        const int groups = cc/8;
-        // The halo brick of the chunk: [z 3][y by][x bx][cc] BF16, zeros outside the volume.  Every thread has
-        // assembled the previous chunk's stages (each issue begins with a block barrier); the MMAs read only the tiles.
-        const int bricks = 3*by*bx*groups;
-        for (int i = tid; i < bricks; i += kThreads) {
-            const int g = i%groups;
-            int v = i/groups;
-            const int bxi = v%bx; v /= bx;
-            const int byi = v%by;
-            const int bzi = v/by;
-            const int xx = x0 + bxi - 1, yy = y0 + byi - 1, zz = z0 + bzi - 1;
+    int failedStage = -1;
+    for (int c = 0; c < stages && ok; c++) {
+        for (int kv = 0; kv < 8; kv++) {
+            int k = c*kChunk + kv*8;
             uint4 val = make_uint4(0, 0, 0, 0);
-            if (xx >= 0 && xx < W && yy >= 0 && yy < H && zz >= 0 && zz < D)
-                val = __ldg(reinterpret_cast<const uint4*>(x + ((((long long) vn*D + zz)*H + yy)*W + xx)*cin + c0 + 8*g));
-            *reinterpret_cast<uint4*>(brick + (size_t) 16*i) = val;
-        }
-        __syncthreads();
-        const int Kc = 27*cc, stages = (Kc + kChunk - 1)/kChunk;
-        for (int s = 0; s < stages; s++, stage++) {
-            // Buffer stage & 1 is free once the MMAs of stage - 2 are done.
-            if (stage >= kStages && !(ok = waitStage(st, stage - kStages, limit)))
-                break;
-            uint8_t* tileA = st.tileA[stage & 1];
-            uint8_t* tileB = st.tileB[stage & 1];
-            // A: row tid, 8 chunks of 8 channels: k' = s*64 + 8 kv within the chunk's [tap][channel] range.
-            for (int kv = 0; kv < 8; kv++) {
-                const int kk = s*kChunk + kv*8;
-                uint4 val = make_uint4(0, 0, 0, 0);
-                if (kk < Kc) {
-                    const int tap = kk/cc, ci = kk - tap*cc;
-                    const int bzi = tap/9, byi = my + (tap/3)%3, bxi = mx + tap%3;
-                    val = *reinterpret_cast<const uint4*>(brick + (size_t) 2*(((bzi*by + byi)*bx + bxi)*cc + ci));
-                }
-                *reinterpret_cast<uint4*>(tileA + swizzled(tid, kv)) = val;
+            if (valid && k < K) {
+                int tap = k/cin, ci = k - tap*cin;
+                int zz = vz + tap/9 - 1, yy = vy + (tap/3)%3 - 1, xx = vx + tap%3 - 1;
+                if (zz >= 0 && zz < D && yy >= 0 && yy < H && xx >= 0 && xx < W)
+                    val = __ldg(reinterpret_cast<const uint4*>(x + ((((long long) vn*D + zz)*H + yy)*W + xx)*cin + ci));
             }
-            // B: the weights of the same K slice, W[n][tap cin + c0 + ci].
-            for (int i = tid; i < cout*8; i += kThreads) {
-                const int row = i >> 3, kv = i & 7, kk = s*kChunk + kv*8;
-                uint4 val = make_uint4(0, 0, 0, 0);
-                if (kk < Kc) {
-                    const int tap = kk/cc, ci = kk - tap*cc;
-                    val = __ldg(reinterpret_cast<const uint4*>(w + (long long) row*K + tap*cin + c0 + ci));
-                }
-                *reinterpret_cast<uint4*>(tileB + swizzled(row, kv)) = val;
-            }
-            issueStage(st, idesc, stage);
-            lastIssued = stage;
+            *reinterpret_cast<uint4*>(st.tileA + swizzled(tid, kv)) = val;
         }
+        for (int i = tid; i < cout*8; i += kThreads) {
+            int row = i >> 3, kv = i & 7, k = c*kChunk + kv*8;
+            uint4 val = make_uint4(0, 0, 0, 0);
+            if (k < K)
+                val = __ldg(reinterpret_cast<const uint4*>(w + (long long) row*K + k));
+            *reinterpret_cast<uint4*>(st.tileB + swizzled(row, kv)) = val;
+        }
+        ok = runStage(st, idesc, c, limit);
+        if (!ok)
+            failedStage = c;
     }
-    if (ok && lastIssued >= 0)
-        ok = waitStage(st, lastIssued, limit);
     if (!ok)
-        drainStages(st, lastIssued);
+        drainStage(st, failedStage);
     fenceAfterSync();
     if (ok) {
         const int row = warp*32 + lane;
-        const int ox = x0 + row%tx, oy = y0 + row/tx;
-        const bool inside = ox < W && oy < H;
-        const long long mo = (((long long) vn*D + z0)*H + oy)*W + ox;
+        const long long mo = (long long) blockIdx.x*kTileM + row;
         for (int col = 0; col < cout; col += 8) {
             float v[8];
             tmemLoad8(st.tmem + ((uint32_t) (warp*32) << 16) + (uint32_t) col, v);
-            if (inside) {
+            if (mo < M) {
                 __align__(16) __nv_bfloat16 out[8];
                 for (int i = 0; i < 8; i++) {
-                    float tv = v[i] + (bias ? bias[col + i] : 0.0f);
-                    out[i] = __float2bfloat16_rn(relu ? fmaxf(tv, 0.0f) : tv);
+                    float t = v[i] + (bias ? bias[col + i] : 0.0f);
+                    out[i] = __float2bfloat16_rn(relu ? fmaxf(t, 0.0f) : t);
                 }
                 *reinterpret_cast<uint4*>(y + mo*cout + col) = *reinterpret_cast<const uint4*>(out);
             }
@@ -345,7 +229,7 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
     }
     else if (tid == 0)
         atomicExch(&convStatus, (int) LBM_ERR_DEVICE_TIMEOUT);
-    releaseStages(st, ncols);
+    releaseStage(st, ncols);
 }
 
 // dW[cout][k] += sum_m dy[m][cout] A[m][k]: A tile rows = cout (tile of 128), B tile rows = k (tile of nt), the GEMM's
@@ -448,25 +332,15 @@ LbmStatus lbm_conv3d_forward(const void* x, const void* w, const float* bias, vo
         return invalid("lbm_conv3d_forward: null pointer or empty volume");
     if (cin <= 0 || cin%8 != 0 || cout < 16 || cout > 256 || cout%16 != 0)
         return invalid("lbm_conv3d_forward: cin must be a multiple of 8 and cout a multiple of 16 up to 256");
-    // Tiles of tx x ty = 128 voxels: ty the smallest power of two >= the height, between 4 and 16.
-    int ty = 4;
-    while (ty < 16 && ty < height)
-        ty *= 2;
-    const int tx = kTileM/ty;
-    const int cc = std::min(64, cin);
-    // 1024 of alignment slack, two pairs of tiles (the B tile rounded to 1024), 1024 for the mbarriers and the slot,
-    // then the brick.
-    size_t smem = 1024 + 2*((size_t) kTileM*128 + (size_t) ((cout*128 + 1023)/1024)*1024) + 1024 +
-                  (size_t) 3*(tx + 2)*(ty + 2)*cc*2;
+    long long voxels = (long long) batch*depth*height*width;
+    size_t smem = stageBytes(cout);
     cudaError_t e = cudaFuncSetAttribute(convForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess)
         return launchError(e);
-    long long tiles = (long long) ((width + tx - 1)/tx)*((height + ty - 1)/ty)*depth*batch;
-    if (tiles > 0x7FFFFFFFLL)
-        return invalid("lbm_conv3d_forward: the volume is too large");
-    convForwardKernel<<<(unsigned) tiles, kThreads, smem, (cudaStream_t) stream>>>(
+    unsigned grid = (unsigned) ((voxels + kTileM - 1)/kTileM);
+    convForwardKernel<<<grid, kThreads, smem, (cudaStream_t) stream>>>(
         (const __nv_bfloat16*) x, (const __nv_bfloat16*) w, bias, (__nv_bfloat16*) y, batch, depth, height, width, cin,
-        cout, relu, tx);
+        cout, relu);
     e = cudaGetLastError();
     return e == cudaSuccess ? LBM_OK : launchError(e);
 }
