@@ -2,8 +2,6 @@
 //
 //  convForwardKernel    y[voxel][cout] = sum_k A[voxel][k] W[cout][k], k = tap*cin + ci, A the implicit im2col of x
 //                       (zero padding); one CTA per 128 voxels, all cout in one N tile (<= 256)
-//  convForwardDirectKernel  the same for 16 <= cin <= 64 with the weights in shared memory: A read straight from a
-//                       halo brick of the input (see there)
 //  convWeightGradKernel dW[cout][k] = sum_voxels dy[voxel][cout] A[voxel][k]; CTAs over (cout tile, k tile, voxel
 //                       split), the K dimension of the GEMM being the voxels; results added with FP32 atomics
 //
@@ -97,7 +95,7 @@ __device__ __forceinline__ void tmemLoad8(uint32_t addr, float v[8]) {
         v[i] = __uint_as_float(r[i]);
 }
 
-__host__ __device__ __forceinline__ uint32_t tmemColumns(int n) {
+__device__ __forceinline__ uint32_t tmemColumns(int n) {
     return n <= 32 ? 32u : (n <= 64 ? 64u : (n <= 128 ? 128u : 256u));
 }
 
@@ -234,150 +232,6 @@ convForwardKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __re
     releaseStage(st, ncols);
 }
 
-// The forward convolution of a layer with 16 <= cin <= 64 (a multiple of 16) whose weights fit in shared memory: tiles of
-// 8 x 16 output voxels of one z-plane, the A operand read straight from a halo brick of the input.  The brick holds
-// the tile's 10 x 18 x 3 input voxels as [z][y][channel group of 8][x][8 channels], so 8 x-adjacent voxels of one
-// channel group form a contiguous core matrix (8 rows of 16 bytes) of the canonical K-major layout without swizzle:
-// the MMA of tap (dz, dy, dx) and channel groups g, g + 1 starts at the brick's (dz, dy, g, dx), with its 16 rows of
-// core matrices (the tile's y) a y-stride apart (stride byte offset) and its two K core matrices a group apart (leading
-// byte offset).  The weights are held whole, K-major with the 128-byte swizzle (atoms of 64 K values, as the gather
-// kernel's B tiles).  All 27 cin/16 MMAs of a tile are issued back to back and committed once; the CTAs loop over the
-// tiles, loading the weights once.
-constexpr int kDirectTX = 8, kDirectTY = 16, kDirectBX = kDirectTX + 2, kDirectBY = kDirectTY + 2;
-
-// Shared-memory matrix descriptor of a K-major operand without swizzle: core matrices of 8 rows x 16 bytes, `lbo` bytes
-// apart along K and `sbo` bytes apart along M (N).
-__device__ __forceinline__ uint64_t smemDescriptorInterleaved(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t) ((addr >> 4) & 0x3FFFu)
-         | ((uint64_t) ((lbo >> 4) & 0x3FFFu) << 16)
-         | ((uint64_t) ((sbo >> 4) & 0x3FFFu) << 32)
-         | ((uint64_t) 1 << 46);                   // descriptor version of sm_100; swizzle mode 0 (none)
-}
-
-size_t directWeightBytes(int cin, int cout) {
-    const int atoms = (27*cin + kChunk - 1)/kChunk;
-    return (size_t) atoms*cout*128;
-}
-
-size_t directBrickBytes(int cin) {
-    return (size_t) 3*kDirectBY*kDirectBX*cin*2;
-}
-
-__global__ void __launch_bounds__(kThreads)
-convForwardDirectKernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ w,
-                        const float* __restrict__ bias, __nv_bfloat16* __restrict__ y, int batch, int D, int H, int W,
-                        int cin, int cout, int relu) {
-    extern __shared__ uint8_t smemRaw[];
-    const uint32_t ncols = tmemColumns(cout);
-    // Layout: [weights: atoms x cout x 128 B][mbarrier, slot: 1024 B][brick], from a 1024-aligned base.
-    const uint32_t s0 = smemAddr(smemRaw);
-    uint8_t* base = smemRaw + ((1024 - (s0 & 1023)) & 1023);
-    const int K = 27*cin, atoms = (K + kChunk - 1)/kChunk, groups = cin/8;
-    uint8_t* weights = base;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(base + (size_t) atoms*cout*128);
-    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 1);
-    uint8_t* brick = base + (size_t) atoms*cout*128 + 1024;
-    const uint32_t mbar = smemAddr(bar);
-    const int tid = threadIdx.x, warp = tid/32, lane = tid%32;
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(smemAddr(slot)), "r"(ncols) : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(mbar), "r"(1) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    // The weights, W[n][k], into 128-byte-swizzled K-major atoms of 64 K values (zeros past K).
-    for (int i = tid; i < atoms*cout*8; i += kThreads) {
-        const int kv = i & 7, row = (i >> 3)%cout, atom = (i >> 3)/cout;
-        const int k = atom*kChunk + kv*8;
-        uint4 val = make_uint4(0, 0, 0, 0);
-        if (k < K)
-            val = __ldg(reinterpret_cast<const uint4*>(w + (long long) row*K + k));
-        *reinterpret_cast<uint4*>(weights + (size_t) atom*cout*128 + swizzled(row, kv)) = val;
-    }
-    fenceBeforeSync();
-    __syncthreads();
-    fenceAfterSync();
-    const uint32_t tmem = *slot;
-    const uint32_t idesc = instrDescriptor(cout);
-    const uint32_t lbo = kDirectBX*16, sbo = groups*kDirectBX*16;
-    const int tilesX = (W + kDirectTX - 1)/kDirectTX, tilesY = (H + kDirectTY - 1)/kDirectTY;
-    const long long tiles = (long long) tilesX*tilesY*D*batch;
-    const long long limit = convWaitPolls;
-    bool ok = true;
-    int phase = 0;
-    for (long long tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, phase ^= 1) {
-        long long t = tile;
-        const int x0 = (int) (t%tilesX)*kDirectTX; t /= tilesX;
-        const int y0 = (int) (t%tilesY)*kDirectTY; t /= tilesY;
-        const int z0 = (int) (t%D);
-        const int vn = (int) (t/D);
-        // The brick [z][y][g][x][8], zeros outside the volume.  The previous tile's MMAs are done (its wait) and its
-        // accumulators read (the barrier after the epilogue).
-        for (int i = tid; i < 3*kDirectBY*groups*kDirectBX; i += kThreads) {
-            const int bxi = i%kDirectBX;
-            int v = i/kDirectBX;
-            const int g = v%groups; v /= groups;
-            const int byi = v%kDirectBY;
-            const int bzi = v/kDirectBY;
-            const int xx = x0 + bxi - 1, yy = y0 + byi - 1, zz = z0 + bzi - 1;
-            uint4 val = make_uint4(0, 0, 0, 0);
-            if (xx >= 0 && xx < W && yy >= 0 && yy < H && zz >= 0 && zz < D)
-                val = __ldg(reinterpret_cast<const uint4*>(x + ((((long long) vn*D + zz)*H + yy)*W + xx)*cin + 8*g));
-            *reinterpret_cast<uint4*>(brick + (size_t) 16*i) = val;
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
-            fenceAfterSync();
-            const uint32_t b0 = smemAddr(brick), w0 = smemAddr(weights);
-            for (int tap = 0; tap < 27; tap++) {
-                const int dz = tap/9, dy = (tap/3)%3, dx = tap%3;
-                for (int g = 0; g < groups; g += 2) {
-                    const uint32_t a = b0 + (uint32_t) ((((dz*kDirectBY + dy)*groups + g)*kDirectBX + dx)*16);
-                    const int k = tap*cin + 8*g;
-                    const uint32_t bb = w0 + (uint32_t) ((k/kChunk)*cout*128 + (k%kChunk)*2);
-                    mmaBf16(tmem, smemDescriptorInterleaved(a, lbo, sbo), smemDescriptor(bb), idesc,
-                            (tap > 0 || g > 0) ? 1u : 0u);
-                }
-            }
-            commitTo(mbar);
-        }
-        ok = __syncthreads_and(waitParity(mbar, (uint32_t) phase, limit)) != 0;
-        if (!ok) {
-            // Wait once more, with the full limit, before the tensor memory is freed.
-            waitParity(mbar, (uint32_t) phase, kSpinLimit);
-            break;
-        }
-        fenceAfterSync();
-        const int row = warp*32 + lane;
-        const int ox = x0 + row%kDirectTX, oy = y0 + row/kDirectTX;
-        const bool inside = ox < W && oy < H;
-        const long long mo = (((long long) vn*D + z0)*H + oy)*W + ox;
-        for (int col = 0; col < cout; col += 8) {
-            float v[8];
-            tmemLoad8(tmem + ((uint32_t) (warp*32) << 16) + (uint32_t) col, v);
-            if (inside) {
-                __align__(16) __nv_bfloat16 out[8];
-                for (int i = 0; i < 8; i++) {
-                    float tv = v[i] + (bias ? bias[col + i] : 0.0f);
-                    out[i] = __float2bfloat16_rn(relu ? fmaxf(tv, 0.0f) : tv);
-                }
-                *reinterpret_cast<uint4*>(y + mo*cout + col) = *reinterpret_cast<const uint4*>(out);
-            }
-        }
-        fenceBeforeSync();
-        __syncthreads();
-    }
-    if (!ok && tid == 0)
-        atomicExch(&convStatus, (int) LBM_ERR_DEVICE_TIMEOUT);
-    fenceBeforeSync();
-    __syncthreads();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(ncols) : "memory");
-}
-
 // dW[cout][k] += sum_m dy[m][cout] A[m][k]: A tile rows = cout (tile of 128), B tile rows = k (tile of nt), the GEMM's
 // K = voxels in stages of 64.  Both tiles are gathered transposed (voxel along the 128-byte rows).
 __global__ void __launch_bounds__(kThreads)
@@ -478,32 +332,9 @@ LbmStatus lbm_conv3d_forward(const void* x, const void* w, const float* bias, vo
         return invalid("lbm_conv3d_forward: null pointer or empty volume");
     if (cin <= 0 || cin%8 != 0 || cout < 16 || cout > 256 || cout%16 != 0)
         return invalid("lbm_conv3d_forward: cin must be a multiple of 8 and cout a multiple of 16 up to 256");
-    cudaError_t e;
-    const size_t direct = 1024 + directWeightBytes(cin, cout) + 1024 + directBrickBytes(cin);
-    if (cin%16 == 0 && cin <= 64 && direct <= 112*1024) {
-        // 1024 of alignment slack, the weights, 1024 for the mbarrier and the slot, the brick.
-        e = cudaFuncSetAttribute(convForwardDirectKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) direct);
-        if (e != cudaSuccess)
-            return launchError(e);
-        int device = 0, sms = 148, perSM = 0;
-        cudaGetDevice(&device);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, convForwardDirectKernel, kThreads, direct);
-        if (e != cudaSuccess)
-            return launchError(e);
-        long long tiles = (long long) ((width + kDirectTX - 1)/kDirectTX)*((height + kDirectTY - 1)/kDirectTY)*depth*batch;
-        // Resident CTAs, limited as well by the tensor memory (512 columns per SM).
-        int tmemPerSM = (int) (512/tmemColumns(cout));
-        long long grid = std::min(tiles, (long long) sms*std::max(1, std::min(perSM, tmemPerSM)));
-        convForwardDirectKernel<<<(unsigned) grid, kThreads, direct, (cudaStream_t) stream>>>(
-            (const __nv_bfloat16*) x, (const __nv_bfloat16*) w, bias, (__nv_bfloat16*) y, batch, depth, height, width,
-            cin, cout, relu);
-        e = cudaGetLastError();
-        return e == cudaSuccess ? LBM_OK : launchError(e);
-    }
     long long voxels = (long long) batch*depth*height*width;
     size_t smem = stageBytes(cout);
-    e = cudaFuncSetAttribute(convForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    cudaError_t e = cudaFuncSetAttribute(convForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess)
         return launchError(e);
     unsigned grid = (unsigned) ((voxels + kTileM - 1)/kTileM);
