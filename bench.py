@@ -522,7 +522,7 @@ def run_b200(args, w, rank, world, device):
         'ms_per_step': ms/args.steps, 'coupled_steps_per_s': 1e3*args.steps/ms, 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None, 'dtype': DTYPE[args.precision],
         'data': data_name(w), 'config': config,
-        'roofline': {'bound': 'hbm', 'kernel': 'streamCollideKernel', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+        'roofline': {'bound': 'hbm', 'kernel': dense_kernel_name(args, w), 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                      'frac': achieved/peak, 'peak_kind': peak_kind, 'algorithmic_bytes_per_launch': bytes_per_node*nodes,
                      'algorithmic_bytes_per_node': bytes_per_node, 'avg_launch_ms': avg_dense_s*1e3,
                      'launches': dense_launches.value, 'traffic': traffic_per_launch(args, w)},
@@ -595,6 +595,18 @@ def data_name(w):
     if w.kT > 0:
         return 'synthetic: a fluid at rest, thermal noise from Philox'
     return 'synthetic: a fluid started from rest'
+
+
+def dense_kernel_name(args, w):
+    """The dense kernel that the library launches for this workload: four nodes per thread for 16-bit storage without
+    fluctuations (nx a multiple of 4), two for FP32 and 16-bit storage (nx even), else one."""
+    nx = w.shape[0]
+    fluct = getattr(w, 'kT', 0) > 0
+    if args.precision in ('half', 'bfloat16') and not fluct and nx % 4 == 0 and os.environ.get('LBM_B200_QUAD16') != '0':
+        return 'streamCollideQuadKernel'
+    if args.precision != 'double' and nx % 2 == 0:
+        return 'streamCollidePairKernel'
+    return 'streamCollideKernel'
 
 
 def traffic_per_launch(args, w):

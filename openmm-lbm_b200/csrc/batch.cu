@@ -115,8 +115,9 @@ __device__ __forceinline__ void pairedItem(const float* __restrict__ A, float* _
         reactB = (word >> ((x0 + 1) & 31)) & 1u;
     }
     const PairConstants c = pairConstants(v, remove, step, ucm);
-    collidePair<float, false, REACT, FLUCT, COHERENT>(r, v, c, remove, step, node, false, false, reactA, reactB,
-                                                      bw + node/2, halfN, sums);
+    PairStore<float, false> out{bw + node/2, halfN, false, false};
+    collidePair<float, false, REACT, FLUCT, COHERENT>(r, v, c, remove, step, node, false, false, reactA, reactB, out,
+                                                      sums);
 }
 
 template <typename T, typename R, bool REACT, bool FLUCT, int BT>

@@ -87,21 +87,25 @@ constexpr int PAIR_TX = 64;         // nodes per tile row: 2 per lane
 // Stores the pair `value` (stored units) of one direction; the half of a solid node stays untouched (as in the
 // one-node kernel).  16-bit storage rounds stochastically with the dither bits of the two nodes, node A's in the low
 // half of `dither` and node B's in the high half.
+// The packed 16-bit word w of two nodes; the half of a solid node stays untouched.
+template <bool SOLID>
+__device__ __forceinline__ void storeWord16(uint32_t* p, uint32_t w, bool solidA, bool solidB) {
+    if (SOLID && (solidA || solidB)) {
+        unsigned short* h = reinterpret_cast<unsigned short*>(p);
+        if (!solidA)
+            h[0] = (unsigned short) (w & 0xFFFFu);
+        if (!solidB)
+            h[1] = (unsigned short) (w >> 16);
+        return;
+    }
+    *p = w;
+}
+
 template <typename T, bool SOLID>
 __device__ __forceinline__ void storePair(typename PairIO<T>::Word* p, F2 value, uint32_t dither, bool solidA,
                                           bool solidB) {
-    if constexpr (sizeof(T) == 2) {
-        uint32_t w = PairIO<T>::pack(value.v.x, value.v.y, dither);
-        if (SOLID && (solidA || solidB)) {
-            unsigned short* h = reinterpret_cast<unsigned short*>(p);
-            if (!solidA)
-                h[0] = (unsigned short) (w & 0xFFFFu);
-            if (!solidB)
-                h[1] = (unsigned short) (w >> 16);
-            return;
-        }
-        *p = w;
-    }
+    if constexpr (sizeof(T) == 2)
+        storeWord16<SOLID>(p, PairIO<T>::pack(value.v.x, value.v.y, dither), solidA, solidB);
     else {
         if (SOLID && (solidA || solidB)) {
             float* h = reinterpret_cast<float*>(p);
@@ -114,6 +118,18 @@ __device__ __forceinline__ void storePair(typename PairIO<T>::Word* p, F2 value,
         *p = value.v;
     }
 }
+
+// Where collidePair puts the post-collision values of direction q (stored units, with their dither bits): the pair's
+// word in each direction plane (`out` is its word in plane 0, planes `halfN` words apart).
+template <typename T, bool SOLID>
+struct PairStore {
+    typename PairIO<T>::Word* out;
+    unsigned halfN;
+    bool solidA, solidB;
+    template <int q> __device__ __forceinline__ void put(F2 value, uint32_t dither) {
+        storePair<T, SOLID>(out + (size_t) q*halfN, value, dither, solidA, solidB);
+    }
+};
 
 // Ghost-mode parts of direction q for a pair of nodes, without the weight: sums over the odd and the even modes
 // k = 10..18 of e_k(c_q) a_k.
@@ -175,8 +191,8 @@ __device__ __forceinline__ PairConstants pairConstants(const FluidView& v, int r
     return c;
 }
 
-// The collision of the x-adjacent nodes `node` and `node + 1` from their pulled words r (stored units): stores the
-// 19 post-collision words at outPlane + q halfN (word index node/2) and adds the pair's mass and momentum to sums.
+// The collision of the x-adjacent nodes `node` and `node + 1` from their pulled words r (stored units): hands the 19
+// post-collision pairs to out.put<q>() and adds the pair's mass and momentum to sums.
 // reactA, reactB flag nodes whose reaction force the coupling left in v.reaction.
 // hi + t as the rounded sum hi and its exact rounding error, added to lo (Knuth's TwoSum: six rounded operations, valid
 // whatever the magnitudes; the packed intrinsics are never re-associated by the compiler).
@@ -202,24 +218,40 @@ template <typename T, bool FLUCT> LBM_HD constexpr int compensationLevel() {
     return FLUCT ? 0 : (sizeof(T) == 4 ? 2 : LBM_COMPENSATED_16BIT);
 }
 
-template <typename T, bool SOLID, bool REACT, bool FLUCT, bool COHERENT = false>
+// The pulled values of a pair as collidePair reads them (stored units): from decoded pairs, or from packed 16-bit words
+// decoded where the moment sums use them (so that the 19 decoded pairs need not be live at once).
+struct PulledPairs {
+    const F2 (&r)[19];
+    template <int q> __device__ __forceinline__ F2 get() const { return r[q]; }
+};
+template <typename T>
+struct PulledWords {
+    const uint32_t (&w)[19];
+    template <int q> __device__ __forceinline__ F2 get() const { return PairIO<T>::decode(w[q]); }
+};
+
+template <typename T, bool SOLID, bool REACT, bool FLUCT, bool COHERENT = false, typename Out>
 __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& v, const PairConstants& c, int remove,
                                             long long step, unsigned node, bool solidA, bool solidB, bool reactA,
-                                            bool reactB, typename PairIO<T>::Word* outPlane, unsigned halfN,
-                                            float (&sums)[4]) {
+                                            bool reactB, Out& out, float (&sums)[4]);
+template <typename T, bool SOLID, bool REACT, bool FLUCT, bool COHERENT = false, typename In, typename Out>
+__device__ __forceinline__ void collidePulled(const In& in, const FluidView& v, const PairConstants& c, int remove,
+                                            long long step, unsigned node, bool solidA, bool solidB, bool reactA,
+                                            bool reactB, Out& out, float (&sums)[4]) {
     constexpr bool dithered = sizeof(T) == 2;
     constexpr int level = compensationLevel<T, FLUCT>();
     constexpr bool comp = level >= 1, compSums = level >= 2;
     // Moments (deviations), the storage factors folded into the FMAs.  With comp the momentum is summed with its
     // rounding errors in jxl, jyl, jzl (the terms cx s D are exact: s is a power of two).
-    F2 dr = f2(Storage<T>::template scale<0>())*r[0];
+    F2 dr = f2(Storage<T>::template scale<0>())*in.template get<0>();
     F2 jx = f2(0), jy = f2(0), jz = f2(0), sxx = f2(0), syy = f2(0), szz = f2(0), sxy = f2(0), sxz = f2(0), syz = f2(0);
     F2 jxl = f2(0), jyl = f2(0), jzl = f2(0);
     staticFor<9>([&](auto pc) {
         constexpr int q = 2*decltype(pc)::value + 1;
         constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
         constexpr float s = Storage<T>::template scale<q>();
-        const F2 S = r[q] + r[q+1], D = r[q] - r[q+1];
+        const F2 rq = in.template get<q>(), rq1 = in.template get<q + 1>();
+        const F2 S = rq + rq1, D = rq - rq1;
         dr = fma2(f2(s), S, dr);
         if constexpr (compSums) {
             // The first term of each component (q = 1, 3, 5) starts the sum exactly.
@@ -327,8 +359,7 @@ __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& 
             ghostSums2<0>(a, e, o);
             value = fma2(e, f2(wOf<float>(0)), value);
         }
-        storePair<T, SOLID>(outPlane, value*f2(storeScale<T, 0>()),
-                            __byte_perm(hashA*0x9E3779B1u, hashB*0x9E3779B1u, 0x5410), solidA, solidB);
+        out.template put<0>(value*f2(storeScale<T, 0>()), __byte_perm(hashA*0x9E3779B1u, hashB*0x9E3779B1u, 0x5410));
     }
     staticFor<9>([&](auto pc) {
         constexpr int p = decltype(pc)::value;
@@ -386,8 +417,8 @@ __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& 
             wb = hashB*(0x9E3779B1u + 0x3C6EF372u*(uint32_t) (p + 1));
         }
         // Direction q takes the low halves of the nodes' words, q + 1 the high halves.
-        storePair<T, SOLID>(outPlane + (size_t) q*halfN, even + odd, __byte_perm(wa, wb, 0x5410), solidA, solidB);
-        storePair<T, SOLID>(outPlane + (size_t) (q + 1)*halfN, even - odd, __byte_perm(wa, wb, 0x7632), solidA, solidB);
+        out.template put<q>(even + odd, __byte_perm(wa, wb, 0x5410));
+        out.template put<q + 1>(even - odd, __byte_perm(wa, wb, 0x7632));
     });
     if (!solidA) {
         sums[0] += dr.v.x; sums[1] += px.v.x; sums[2] += py.v.x; sums[3] += pz.v.x;
@@ -395,6 +426,14 @@ __device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& 
     if (!solidB) {
         sums[0] += dr.v.y; sums[1] += px.v.y; sums[2] += py.v.y; sums[3] += pz.v.y;
     }
+}
+
+template <typename T, bool SOLID, bool REACT, bool FLUCT, bool COHERENT, typename Out>
+__device__ __forceinline__ void collidePair(const F2 (&r)[19], const FluidView& v, const PairConstants& c, int remove,
+                                            long long step, unsigned node, bool solidA, bool solidB, bool reactA,
+                                            bool reactB, Out& out, float (&sums)[4]) {
+    collidePulled<T, SOLID, REACT, FLUCT, COHERENT>(PulledPairs{r}, v, c, remove, step, node, solidA, solidB, reactA,
+                                                    reactB, out, sums);
 }
 
 } // namespace

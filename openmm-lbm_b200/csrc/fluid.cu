@@ -227,8 +227,122 @@ streamCollidePairKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v,
             reactA = (word >> (x0 & 31)) & 1u;
             reactB = (word >> ((x0 + 1) & 31)) & 1u;
         }
-        collidePair<T, SOLID, REACT, FLUCT>(r, v, c, remove, step, node, solidA, solidB, reactA, reactB, bw + node/2,
-                                            halfN, sums);
+        PairStore<T, SOLID> out{bw + node/2, halfN, solidA, solidB};
+        collidePair<T, SOLID, REACT, FLUCT>(r, v, c, remove, step, node, solidA, solidB, reactA, reactB, out, sums);
+    }
+    double acc[NPART] = {(double) sums[0], (double) sums[1], (double) sums[2], (double) sums[3], 0, 0, 0, 0};
+    blockReduceStore(acc, v.partials + NPART*(long long) blockIdx.x);
+}
+
+// The dense step for 16-bit storage without fluctuations, four x-adjacent nodes per thread (nx a multiple of 4):
+// each direction's four sources are one aligned 64-bit word of the source row, with c_x = +1 the high half of the
+// 32-bit word to the left in front of its first three, with c_x = -1 the low half of the word to the right after its
+// last three; the four post-collision values of a direction go out as one 64-bit word.  The nodes are collided as two
+// pairs (collidePulled, the same arithmetic and dither bits as the paired kernel, so the results are the paired
+// kernel's bit for bit); the first pair's packed words wait in registers for the second's.  A warp takes a row tile
+// of QUAD_TX nodes.  Against the paired kernel this halves the loads, stores and address arithmetic per node (29 loads
+// and 19 stores per 4 nodes) and doubles the bytes in flight per warp: FP16 channel step 0.578 -> 0.511 ms, BF16
+// 0.571 -> 0.503 ms.  Measured slower: 4 or 6 blocks per SM (0.527 / 0.548 ms FP16), the first pair's words held in
+// shared memory (0.592 ms at 6 blocks), and each pair storing its own 32-bit words (0.599 ms).
+constexpr int QUAD_TX = 128;        // nodes per warp row tile: 4 per lane
+#ifndef LBM_QUAD_THREADS
+#define LBM_QUAD_THREADS 128
+#endif
+#ifndef LBM_QUAD_MIN_BLOCKS
+#define LBM_QUAD_MIN_BLOCKS 5
+#endif
+
+// The first pair of a quad: its packed words, held until the second pair's are ready.
+template <typename T>
+struct QuadHold {
+    uint32_t word[19];
+    template <int q> __device__ __forceinline__ void put(F2 value, uint32_t dither) {
+        word[q] = PairIO<T>::pack(value.v.x, value.v.y, dither);
+    }
+};
+
+// The second pair: stores both pairs' words of direction q as one 64-bit word (word halves per node when a node of
+// the quad is solid).
+template <typename T, bool SOLID>
+struct QuadStore {
+    uint2* out;                   // the quad's word in plane 0
+    unsigned quarterN;            // 64-bit words per plane
+    const QuadHold<T>& first;
+    uint32_t solidBits;           // bit i: node x0 + i is solid
+    template <int q> __device__ __forceinline__ void put(F2 value, uint32_t dither) {
+        const uint32_t second = PairIO<T>::pack(value.v.x, value.v.y, dither);
+        uint2* p = out + (size_t) q*quarterN;
+        if (SOLID && solidBits != 0) {
+            uint32_t* w = reinterpret_cast<uint32_t*>(p);
+            storeWord16<SOLID>(w, first.word[q], solidBits & 1u, solidBits & 2u);
+            storeWord16<SOLID>(w + 1, second, solidBits & 4u, solidBits & 8u);
+            return;
+        }
+        *p = make_uint2(first.word[q], second);
+    }
+};
+
+template <typename T, bool SOLID, bool REACT>
+__global__ void __launch_bounds__(LBM_QUAD_THREADS, LBM_QUAD_MIN_BLOCKS)
+streamCollideQuadKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v, int remove, long long step) {
+    static_assert(sizeof(T) == 2, "the quad kernel is for 16-bit storage");
+    const int lane = threadIdx.x%32;
+    const unsigned N = (unsigned) v.n;
+    const int nx = v.nx, ny = v.ny, nz = v.nz;
+    const uint32_t* __restrict__ a32 = reinterpret_cast<const uint32_t*>(A);
+    const uint2* __restrict__ a64 = reinterpret_cast<const uint2*>(A);
+    uint2* __restrict__ b64 = reinterpret_cast<uint2*>(B);
+    const unsigned halfN = N/2, quarterN = N/4;     // 32-bit and 64-bit words per direction plane (N % 4 == 0)
+    const PairConstants c = pairConstants(v, remove, step);
+    float sums[4] = {0, 0, 0, 0};
+    const int tilesX = (nx + QUAD_TX - 1)/QUAD_TX;
+    const unsigned numTiles = (unsigned) tilesX*ny*nz, warps = blockDim.x/32;
+    for (unsigned t = blockIdx.x*warps + threadIdx.x/32; t < numTiles; t += gridDim.x*warps) {
+        const int tx = (int) (t%tilesX);
+        const unsigned row = t/tilesX;
+        const int y = (int) (row%(unsigned) ny), z = (int) (row/(unsigned) ny);
+        const int x0 = tx*QUAD_TX + 4*lane;
+        if (x0 >= nx)
+            continue;
+        uint32_t solidBits = 0;
+        if (SOLID) {
+            // x0 % 4 == 0: the quad's four bits sit in one mask word.
+            solidBits = (__ldg(&v.solidMask[(size_t) row*v.wordsPerRow + (x0 >> 5)]) >> (x0 & 31)) & 0xFu;
+            if (solidBits == 0xFu)
+                continue;
+        }
+        const unsigned node = row*nx + x0;
+        const int ys[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};
+        const int zs[3] = {z == 0 ? nz - 1 : z - 1, z, z == nz - 1 ? 0 : z + 1};
+        const int xl = x0 == 0 ? nx - 2 : x0 - 2, xr = x0 + 4 == nx ? 0 : x0 + 4;
+        uint32_t wa[19], wb[19];
+        staticFor<19>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+            const unsigned base = ((unsigned) zs[1-cz]*ny + ys[1-cy])*nx;
+            const uint2 w = __ldg(a64 + (size_t) q*quarterN + (base + x0)/4);
+            if (cx == 0) {
+                wa[q] = w.x;
+                wb[q] = w.y;
+            }
+            else if (cx == 1) {
+                wa[q] = __byte_perm(__ldg(a32 + (size_t) q*halfN + (base + xl)/2), w.x, 0x5432);
+                wb[q] = __byte_perm(w.x, w.y, 0x5432);
+            }
+            else {
+                wa[q] = __byte_perm(w.x, w.y, 0x5432);
+                wb[q] = __byte_perm(w.y, __ldg(a32 + (size_t) q*halfN + (base + xr)/2), 0x5432);
+            }
+        });
+        uint32_t reactBits = 0;
+        if (REACT)
+            reactBits = (__ldg(&v.reactMask[(size_t) row*v.wordsPerRow + (x0 >> 5)]) >> (x0 & 31)) & 0xFu;
+        QuadHold<T> first;
+        collidePulled<T, SOLID, REACT, false>(PulledWords<T>{wa}, v, c, remove, step, node, solidBits & 1u,
+                                              solidBits & 2u, reactBits & 1u, reactBits & 2u, first, sums);
+        QuadStore<T, SOLID> out{b64 + node/4, quarterN, first, solidBits};
+        collidePulled<T, SOLID, REACT, false>(PulledWords<T>{wb}, v, c, remove, step, node + 2, solidBits & 4u,
+                                              solidBits & 8u, reactBits & 4u, reactBits & 8u, out, sums);
     }
     double acc[NPART] = {(double) sums[0], (double) sums[1], (double) sums[2], (double) sums[3], 0, 0, 0, 0};
     blockReduceStore(acc, v.partials + NPART*(long long) blockIdx.x);
@@ -238,34 +352,44 @@ streamCollidePairKernel(const T* __restrict__ A, T* __restrict__ B, FluidView v,
 // Bounce-back over the wall links (after the dense step, on the output array).
 // ---------------------------------------------------------------------------------------------------
 
+// One wall node per thread (a grid of up to kGridWall blocks covers the channel's wall planes in one pass): the
+// node's wall links are known at compile time per direction, so the loads of all its links are issued before any of
+// the stores (a store may alias a later load as far as the compiler knows) and do not wait on one another.
 template <typename T, typename R>
 __global__ void __launch_bounds__(THREADS)
 bounceBackKernel(T* __restrict__ B, const int* __restrict__ wall, int numWall, FluidView v, double* partials) {
     double acc[NPART] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int b = blockIdx.x*blockDim.x + threadIdx.x; b < numWall; b += gridDim.x*blockDim.x) {
-        long long node = wall[2*b];
-        int links = wall[2*b+1];
-        Coords c = nodeCoords(node, v.nx, v.ny);
-        for (int q = 1; q < 19; q++) {
-            if (!(links & (1<<q)))
-                continue;
-            // The population x built for q streamed into the solid node s = x + c_q; x takes it back along
-            // -c_q, so it goes into the slot of s that x pulls for opp(q).  Opposite directions have the same
-            // weight, so the stored element is copied as it is.
-            long long s = shifted(v, c.x, c.y, c.z, cxr(q), cyr(q), czr(q));
-            T raw = B[(long long) q*v.n + node];
-            B[(long long) oppOf(q)*v.n + s] = raw;
-            double value = (double) loadq<T, R>(&raw, q);
-            double w = weightOf<double>(q);
-            // The fluid momentum of the population is reversed; the wall receives 2 c_q (f + w)
-            // (ReferenceLBMKernels.cpp:1176-1205, momentum exchange of Ladd 1994).
-            acc[1] -= 2.0*cxr(q)*value;
-            acc[2] -= 2.0*cyr(q)*value;
-            acc[3] -= 2.0*czr(q)*value;
-            acc[4] += 2.0*cxr(q)*(value + w);
-            acc[5] += 2.0*cyr(q)*(value + w);
-            acc[6] += 2.0*czr(q)*(value + w);
-        }
+        const int2 entry = __ldg(reinterpret_cast<const int2*>(wall) + b);
+        const long long node = (unsigned) entry.x;
+        const int links = entry.y;
+        const Coords c = nodeCoords(node, v.nx, v.ny);
+        T raw[19];
+        staticFor<18>([&](auto qc) {
+            constexpr int q = decltype(qc)::value + 1;
+            if (links & (1 << q))
+                raw[q] = B[(long long) q*v.n + node];
+        });
+        staticFor<18>([&](auto qc) {
+            constexpr int q = decltype(qc)::value + 1;
+            if (links & (1 << q)) {
+                // The population x built for q streamed into the solid node s = x + c_q; x takes it back along
+                // -c_q, so it goes into the slot of s that x pulls for opp(q).  Opposite directions have the same
+                // weight, so the stored element is copied as it is.
+                const long long s = shifted(v, c.x, c.y, c.z, cxOf(q), cyOf(q), czOf(q));
+                B[(long long) oppOf(q)*v.n + s] = raw[q];
+                const double value = (double) loadq<T, R>(&raw[q], q);
+                const double w = weightOf<double>(q);
+                // The fluid momentum of the population is reversed; the wall receives 2 c_q (f + w)
+                // (ReferenceLBMKernels.cpp:1176-1205, momentum exchange of Ladd 1994).
+                acc[1] -= 2.0*cxOf(q)*value;
+                acc[2] -= 2.0*cyOf(q)*value;
+                acc[3] -= 2.0*czOf(q)*value;
+                acc[4] += 2.0*cxOf(q)*(value + w);
+                acc[5] += 2.0*cyOf(q)*(value + w);
+                acc[6] += 2.0*czOf(q)*(value + w);
+            }
+        });
     }
     blockReduceStore(acc, partials + NPART*(long long) blockIdx.x);
 }
@@ -462,7 +586,10 @@ __global__ void __launch_bounds__(THREADS) finishKernel(const double* partials, 
     // mode 0: the sums of a step (mass, momentum, ucm, wall); 1: a moments pass that sets the sums and the largest
     // speed; 2: a moments pass for the largest speed only (the sums of the step are kept).
     double acc[NPART] = {0, 0, 0, 0, 0, 0, 0, 0};
+    // Several records in flight per thread (the loads do not wait on the sums).
+#pragma unroll 4
     for (int i = threadIdx.x; i < count; i += blockDim.x)
+#pragma unroll
         for (int k = 0; k < NPART; k++)
             acc[k] = (k == NPART-1 ? fmax(acc[k], partials[NPART*(long long) i + k]) : acc[k] + partials[NPART*(long long) i + k]);
     __shared__ double total[NPART];
@@ -775,6 +902,15 @@ struct Launcher {
         return enabled == 1;
     }
 
+    // The quad kernel for 16-bit storage without fluctuations (nx % 4 == 0); LBM_B200_QUAD16 = 0 in the environment
+    // selects the paired kernel instead (for comparisons).
+    static bool quadKernels() {
+        static int enabled = -2;
+        if (enabled == -2)
+            enabled = pairChoice("LBM_B200_QUAD16") == 0 ? 0 : 1;
+        return enabled == 1;
+    }
+
     // The persistent grid of a kernel variant: one wave of resident blocks (blocks per SM of this variant times
     // the SMs), so that every block processes the same number of tiles in one wave.
     template <bool S, bool RE, bool FL>
@@ -802,8 +938,29 @@ struct Launcher {
         long long tiles = (long long) ((v.nx + PAIR_TX - 1)/PAIR_TX)*v.tilesY*v.nz;
         return (int) std::max(1LL, std::min((long long) blocks, tiles));
     }
+    template <bool S, bool RE>
+    static int quadGrid(const FluidView& v) {
+        static int blocks = 0;
+        if (blocks == 0) {
+            int perSM = 0, device = 0, sms = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, streamCollideQuadKernel<T, S, RE>, LBM_QUAD_THREADS, 0);
+            cudaGetDevice(&device);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+            blocks = std::max(1, perSM)*std::max(1, sms);
+        }
+        const long long warps = LBM_QUAD_THREADS/32;
+        long long tiles = (long long) ((v.nx + QUAD_TX - 1)/QUAD_TX)*v.ny*v.nz;
+        return (int) std::max(1LL, std::min((long long) blocks, (tiles + warps - 1)/warps));
+    }
     template <bool S, bool RE, bool FL>
     static int dense(const void* A, void* B, const FluidView& v, int remove, long long step, int maxGrid, cudaStream_t s) {
+        if constexpr (sizeof(T) == 2 && !FL) {
+            if (v.nx%4 == 0 && pairedKernels<FL>() && quadKernels()) {
+                int grid = std::min(maxGrid, quadGrid<S, RE>(v));
+                streamCollideQuadKernel<T, S, RE><<<grid, LBM_QUAD_THREADS, 0, s>>>((const T*) A, (T*) B, v, remove, step);
+                return grid;
+            }
+        }
         if constexpr (sizeof(T) <= 4) {
             if (v.nx%2 == 0 && pairedKernels<FL>()) {
                 int grid = std::min(maxGrid, pairGrid<S, RE, FL>(v));
@@ -844,6 +1001,15 @@ struct Launcher {
             probe(streamCollidePairKernel<T, false, false, false>);
             probe(streamCollidePairKernel<T, false, true, true>);
             probe(streamCollidePairKernel<T, true, true, true>);
+        }
+        if constexpr (sizeof(T) == 2) {
+            auto probeQuad = [&](auto kernel) {
+                int blocks = 0;
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, LBM_QUAD_THREADS, 0);
+                best = std::max(best, blocks);
+            };
+            probeQuad(streamCollideQuadKernel<T, false, false>);
+            probeQuad(streamCollideQuadKernel<T, true, true>);
         }
         return best;
     }
@@ -901,6 +1067,7 @@ size_t elementSizeOf(int storage) {
 }
 
 const int kGridSparse = 148;      // blocks of the sparse passes (one wave)
+const int kGridWall = 4*148;      // blocks of the bounce-back pass (a wall node per thread on the largest lattices)
 
 } // namespace
 
@@ -939,7 +1106,7 @@ FluidEngine::FluidEngine(const LbmLatticeParameters& l, int storage, const Geome
         dispatchStorage(storage, [&](auto L) { occupancy = decltype(L)::occupancy(); });
         long long wanted = (long long) sms*occupancy;
         gridBlocks = (int) std::max(1LL, std::min(wanted, view.numTiles));
-        extraBlocks = 2*kGridSparse;
+        extraBlocks = kGridWall + kGridSparse;
         CUDA_CHECK(cudaMalloc(&partialsDev, sizeof(double)*NPART*(size_t) (gridBlocks + extraBlocks + 1)));
         CUDA_CHECK(cudaMalloc(&statsDev, sizeof(StepStats)));
         CUDA_CHECK(cudaMemsetAsync(statsDev, 0, sizeof(StepStats), stream));
@@ -1093,7 +1260,7 @@ void FluidEngine::step(long long stepIndex, bool remove, bool react) {
     }
     int count = denseGrid;
     if (numWall > 0) {
-        int grid = std::min(kGridSparse, (numWall + THREADS - 1)/THREADS);
+        int grid = std::min(kGridWall, (numWall + THREADS - 1)/THREADS);
         double* part = partialsDev + NPART*(size_t) count;
         dispatchStorage(storageType, [&](auto L) { decltype(L)::bounceBack(B, wallDev, numWall, view, part, grid, stream); });
         CUDA_CHECK(cudaGetLastError());

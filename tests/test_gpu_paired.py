@@ -2,7 +2,16 @@
 than one tile: FP32 storage follows the oracle (1e-5 of the largest population of the fluid nodes, as the other FP32
 parity tests) with ragged tiles (ny not a multiple of the 8 rows of a tile), several tiles along x (the pulls across
 the tile edges and the periodic wrap at both ends), solid nodes (pairs with one or both nodes solid) under bounce-back
-or regularized walls, open faces, fluctuations and coupled particles."""
+or regularized walls, open faces, fluctuations and coupled particles.
+
+The quad kernel of 16-bit storage (four x-adjacent nodes per thread, nx a multiple of 4, no fluctuations) collides
+its nodes as two pairs with the paired kernel's arithmetic and dither bits, so without the momentum removal (whose
+sums the two kernels add in different orders) its runs are bitwise those of the paired kernel, which a subprocess
+selects with LBM_B200_QUAD16=0."""
+import os
+import subprocess
+import sys
+
 import numpy as np
 import pytest
 
@@ -24,7 +33,7 @@ def solid_nodes(shape, walls):
             [i + nx*(j + ny*k) for k in (1, 2) for j in (2, 3) for i in (2, 3, nx - 1)])
 
 
-def wide_case(shape, walls, fluct, particles, kernel_factory=None, properties=None):
+def wide_case(shape, walls, fluct, particles, kernel_factory=None, properties=None, removal=None):
     """A perturbed fluid of `shape` nodes (tau 0.8, body force, momentum removal every third step unless faces are
     open), with the wall plane j = 0 and a block of solid nodes, bounce-back ('walls') or regularized
     ('regularized', 'dvfaces'), open x faces ('dvfaces'), fluctuations and particle noise at 300 K (else 0 K), and
@@ -37,7 +46,7 @@ def wide_case(shape, walls, fluct, particles, kernel_factory=None, properties=No
     force.setKinematicViscosity((0.8 - 0.5)/3*DX*DX/DT)
     force.setBodyAcceleration((0.5, -0.2, 0.1))
     force.setInitialFluidVelocity((0.5, 0.2, -0.3))
-    force.setFluidMomentumRemovalFrequency(0 if walls == 'dvfaces' else 3)
+    force.setFluidMomentumRemovalFrequency(removal if removal is not None else (0 if walls == 'dvfaces' else 3))
     if walls != 'periodic':
         force.setSolidNodes(solid_nodes(shape, walls))
     if walls in ('regularized', 'dvfaces'):
@@ -91,3 +100,32 @@ def test_paired_fp32_agrees_with_oracle(shape, walls, fluct, particles):
     assert abs(got - ref).max() <= 1e-5*abs(ref).max()
     assert abs(pos - ref_pos).max() <= 1e-6*abs(ref_pos).max()
     assert abs(wall - ref_wall).max() <= 1e-5*max(1.0, abs(ref_wall).max())
+
+
+QUAD_CASES = [((64, 13, 5), 'walls', 3), ((128, 9, 4), 'regularized', 0), ((128, 9, 4), 'dvfaces', 2),
+              ((256, 6, 3), 'periodic', 0)]
+
+
+def run_wide_16bit(shape, walls, particles, precision, steps=30):
+    context, force = wide_case(shape, walls, False, particles, None, {'Precision': precision}, removal=0)
+    context.integrator.step(steps)
+    result = (force.getFluidState(context), context.positions.copy())
+    context.close()
+    return result
+
+
+@pytest.mark.parametrize('precision', ['half', 'bfloat16'])
+@pytest.mark.parametrize('shape,walls,particles', QUAD_CASES)
+def test_quad_kernel_is_bitwise_the_paired_kernel(shape, walls, particles, precision, tmp_path):
+    """Quads with one to three solid nodes (the block at x = 2, 3 and nx - 1), pulls across the 128-node row tiles and
+    the periodic wrap, open faces and coupled particles (the reaction forces of the quad's nodes)."""
+    out = str(tmp_path/'paired.npz')
+    code = ('import sys; sys.path.insert(0, %r); import conftest, numpy; from test_gpu_paired import run_wide_16bit; '
+            'state, positions = run_wide_16bit(%r, %r, %d, %r); numpy.savez(%r, state=state, positions=positions)'
+            % (os.path.dirname(os.path.abspath(__file__)), shape, walls, particles, precision, out))
+    env = dict(os.environ, LBM_B200_QUAD16='0')
+    subprocess.run([sys.executable, '-c', code], env=env, check=True, timeout=300)
+    paired = np.load(out)
+    state, positions = run_wide_16bit(shape, walls, particles, precision)
+    assert np.array_equal(state, paired['state'])
+    assert np.array_equal(positions, paired['positions'])
