@@ -47,7 +47,9 @@ struct ReplicaTable {
     unsigned nodeOffset;     // first node of the replica in the concatenated populations (19 arrays of N_r each; even)
     unsigned numNodes;
     int firstItem, numItems; // work items of the dense kernel
-    int paired;              // FP32 storage and an even nx: two x-adjacent nodes per thread (2 BT nodes per item)
+    int paired;              // FP32 storage, two x-adjacent nodes per thread: 1 for an even nx (aligned pairs of the
+                             // replica's node order), 2 for an odd nx (pairs within each row); 0: one node per thread
+    unsigned units;          // threads of the dense step: nodes, pairs, or pairs and row ends
     int firstParticle, numParticles;
     int removeFrequency;
     double dt;               // ps
@@ -71,52 +73,102 @@ __device__ __forceinline__ double warpReduceSum(double v) {
     return v;
 }
 
-// Pair `pair` of a replica with an even nx and FP32 storage: nodes 2 pair and 2 pair + 1 of one row, by the paired body
-// of the single-lattice kernel (collide_pair.cuh) with the replica's view; the pulls are aligned float2 words (the
-// replica's arrays start at an even node, and its planes hold an even number of nodes).  COHERENT: the inputs were
-// written by other blocks of the same launch, so they are read through L2.
+// Where the paired body puts a pair's values: as one aligned float2 per direction (an even nx: the replica's arrays
+// start at an even node and its planes hold an even number of nodes), or as single floats (an odd nx, whose rows
+// start at nodes of either parity), the copy of a row's last node (`single`) discarded.  Planes are N floats apart.
+struct UnitStore {
+    float* out;         // the pair's first node in plane 0
+    unsigned N;
+    bool aligned, single;
+    template <int q> __device__ __forceinline__ void put(F2 value, uint32_t) {
+        float* p = out + (size_t) q*N;
+        if (aligned) {
+            *reinterpret_cast<float2*>(p) = value.v;
+            return;
+        }
+        p[0] = value.v.x;
+        if (!single)
+            p[1] = value.v.y;
+    }
+};
+
+// Unit `unit` of a replica with FP32 storage, by the paired body of the single-lattice kernel (collide_pair.cuh) with
+// the replica's view.  paired == 1 (an even nx): nodes 2 unit and 2 unit + 1, pulled as aligned float2 words.
+// paired == 2 (an odd nx): a row holds (nx + 1)/2 units, unit u the nodes 2u and 2u + 1 of its row, the last one
+// (2u = nx - 1) its row's last node alone, collided as a pair with itself and the copy discarded (its sums left out);
+// the pulls are single floats.  The random numbers of a node are those of the one-node body.  COHERENT: the inputs
+// were written by other blocks of the same launch, so they are read through L2.  One instantiation of the collision
+// serves both forms.
 template <bool REACT, bool FLUCT, bool COHERENT>
-__device__ __forceinline__ void pairedItem(const float* __restrict__ A, float* __restrict__ B, const FluidView& v,
-                                           unsigned N, unsigned pair, int remove, const double ucm[3], long long step,
-                                           float (&sums)[4]) {
-    const unsigned node = 2*pair;
-    if (node >= N)
-        return;
+__device__ __forceinline__ void pairedUnit(const float* __restrict__ A, float* __restrict__ B, const FluidView& v,
+                                           unsigned N, unsigned unit, int paired, int remove, const double ucm[3],
+                                           long long step, float (&sums)[4]) {
     const int nx = v.nx, ny = v.ny, nz = v.nz;
-    const unsigned row = node/(unsigned) nx;
-    const int x0 = (int) (node - row*(unsigned) nx), y = (int) (row%(unsigned) ny), z = (int) (row/(unsigned) ny);
-    const float2* aw = reinterpret_cast<const float2*>(A);
-    float2* bw = reinterpret_cast<float2*>(B);
-    const unsigned halfN = N/2;
+    unsigned row, node;
+    int x0;
+    bool single = false;
+    if (paired == 1) {
+        node = 2*unit;
+        if (node >= N)
+            return;
+        row = node/(unsigned) nx;
+        x0 = (int) (node - row*(unsigned) nx);
+    }
+    else {
+        const unsigned perRow = (unsigned) (nx + 1)/2;
+        row = unit/perRow;
+        if (row >= (unsigned) ny*(unsigned) nz)
+            return;
+        x0 = 2*(int) (unit - row*perRow);
+        single = x0 + 1 == nx;
+        node = row*(unsigned) nx + (unsigned) x0;
+    }
+    const int x1 = single ? x0 : x0 + 1;
+    const int y = (int) (row%(unsigned) ny), z = (int) (row/(unsigned) ny);
     const int ys[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};
     const int zs[3] = {z == 0 ? nz - 1 : z - 1, z, z == nz - 1 ? 0 : z + 1};
-    const int xl = x0 == 0 ? nx - 2 : x0 - 2, xr = x0 + 2 == nx ? 0 : x0 + 2;
-    auto load = [&](const float2* p) { return COHERENT ? __ldcg(p) : __ldg(p); };
     F2 r[19];
-    staticFor<19>([&](auto qc) {
-        constexpr int q = decltype(qc)::value;
-        constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
-        const unsigned base = ((unsigned) zs[1-cz]*ny + ys[1-cy])*nx;
-        const float2* plane = aw + (size_t) q*halfN;
-        float2 w;
-        if (cx == 0)
-            w = load(plane + (base + x0)/2);
-        else if (cx == 1)
-            w = PairIO<float>::left(load(plane + (base + xl)/2), load(plane + (base + x0)/2));
-        else
-            w = PairIO<float>::right(load(plane + (base + x0)/2), load(plane + (base + xr)/2));
-        r[q] = PairIO<float>::decode(w);
-    });
+    if (paired == 1) {
+        const float2* aw = reinterpret_cast<const float2*>(A);
+        const unsigned halfN = N/2;
+        const int xl = x0 == 0 ? nx - 2 : x0 - 2, xr = x0 + 2 == nx ? 0 : x0 + 2;
+        auto load = [&](const float2* p) { return COHERENT ? __ldcg(p) : __ldg(p); };
+        staticFor<19>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+            const unsigned base = ((unsigned) zs[1-cz]*ny + ys[1-cy])*nx;
+            const float2* plane = aw + (size_t) q*halfN;
+            float2 w;
+            if (cx == 0)
+                w = load(plane + (base + x0)/2);
+            else if (cx == 1)
+                w = PairIO<float>::left(load(plane + (base + xl)/2), load(plane + (base + x0)/2));
+            else
+                w = PairIO<float>::right(load(plane + (base + x0)/2), load(plane + (base + xr)/2));
+            r[q] = PairIO<float>::decode(w);
+        });
+    }
+    else {
+        auto load = [&](const float* p) { return COHERENT ? __ldcg(p) : __ldg(p); };
+        auto wrapX = [&](int x) { return x < 0 ? x + nx : (x >= nx ? x - nx : x); };
+        staticFor<19>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            constexpr int cx = cxOf(q), cy = cyOf(q), cz = czOf(q);
+            const float* plane = A + (size_t) q*N + ((unsigned) zs[1-cz]*ny + ys[1-cy])*nx;
+            r[q] = F2{make_float2(load(plane + wrapX(x0 - cx)), load(plane + wrapX(x1 - cx)))};
+        });
+    }
     bool reactA = false, reactB = false;
     if (REACT) {
-        const uint32_t* mp = &v.reactMask[(size_t) row*v.wordsPerRow + (x0 >> 5)];
-        const uint32_t word = COHERENT ? __ldcg(mp) : __ldg(mp);
-        reactA = (word >> (x0 & 31)) & 1u;
-        reactB = (word >> ((x0 + 1) & 31)) & 1u;
+        const uint32_t* mp = &v.reactMask[(size_t) row*v.wordsPerRow];
+        const uint32_t wordA = COHERENT ? __ldcg(mp + (x0 >> 5)) : __ldg(mp + (x0 >> 5));
+        const uint32_t wordB = COHERENT ? __ldcg(mp + (x1 >> 5)) : __ldg(mp + (x1 >> 5));
+        reactA = (wordA >> (x0 & 31)) & 1u;
+        reactB = !single && ((wordB >> (x1 & 31)) & 1u);
     }
     const PairConstants c = pairConstants(v, remove, step, ucm);
-    PairStore<float, false> out{bw + node/2, halfN, false, false};
-    collidePair<float, false, REACT, FLUCT, COHERENT>(r, v, c, remove, step, node, false, false, reactA, reactB, out,
+    UnitStore out{B + node, N, paired == 1, single};
+    collidePair<float, false, REACT, FLUCT, COHERENT>(r, v, c, remove, step, node, false, single, reactA, reactB, out,
                                                       sums);
 }
 
@@ -137,8 +189,9 @@ batchStreamCollideKernel(const T* __restrict__ A, T* __restrict__ B, const Fluid
         if constexpr (std::is_same<T, float>::value) {
             if (rt.paired) {
                 float sums[4] = {0, 0, 0, 0};
-                pairedItem<REACT, FLUCT, false>(A + base, B + base, v, N, (unsigned) (w - rt.firstItem)*BT + threadIdx.x,
-                                                remove, v.stats->ucm, step, sums);
+                const unsigned unit = (unsigned) (w - rt.firstItem)*BT + threadIdx.x;
+                pairedUnit<REACT, FLUCT, false>(A + base, B + base, v, N, unit, rt.paired, remove, v.stats->ucm, step,
+                                                sums);
                 double s0 = warpReduceSum((double) sums[0]), s1 = warpReduceSum((double) sums[1]);
                 double s2 = warpReduceSum((double) sums[2]), s3 = warpReduceSum((double) sums[3]);
                 if (lane == 0) {
@@ -589,11 +642,11 @@ batchPersistentKernel(PersistentArgs a) {
                 if (rt.paired) {
                     float sums[4] = {0, 0, 0, 0};
                     const size_t base = (size_t) 19*rt.nodeOffset;
-                    const unsigned pair = (unsigned) (w - rt.firstItem)*BT + threadIdx.x;
+                    const unsigned unit = (unsigned) (w - rt.firstItem)*BT + threadIdx.x;
                     if (a.coupled)
-                        pairedItem<true, FLUCT, true>(A + base, B + base, v, N, pair, remove, ucm, step, sums);
+                        pairedUnit<true, FLUCT, true>(A + base, B + base, v, N, unit, rt.paired, remove, ucm, step, sums);
                     else
-                        pairedItem<false, FLUCT, true>(A + base, B + base, v, N, pair, remove, ucm, step, sums);
+                        pairedUnit<false, FLUCT, true>(A + base, B + base, v, N, unit, rt.paired, remove, ucm, step, sums);
                     double s0 = warpReduceSum((double) sums[0]), s1 = warpReduceSum((double) sums[1]);
                     double s2 = warpReduceSum((double) sums[2]), s3 = warpReduceSum((double) sums[3]);
                     if (lane == 0) {
@@ -756,7 +809,9 @@ BatchEngine::BatchEngine(int nr, const LbmLatticeParameters* ls, const int* np, 
         long long n = (long long) l.nx*l.ny*l.nz;
         t.nodeOffset = (unsigned) totalNodes;
         t.numNodes = (unsigned) n;
-        t.paired = storage == LBM_STORAGE_F32 && l.nx%2 == 0;
+        t.paired = storage != LBM_STORAGE_F32 ? 0 : (l.nx%2 == 0 ? 1 : 2);
+        t.units = t.paired == 0 ? (unsigned) n : t.paired == 1 ? (unsigned) (n/2)
+                                                               : (unsigned) (((l.nx + 1)/2)*(long long) l.ny*l.nz);
         t.firstParticle = totalParticles;
         t.numParticles = np[r];
         t.removeFrequency = l.momentum_removal_frequency;
@@ -935,15 +990,14 @@ void BatchEngine::release() {
     stream = nullptr;
 }
 
-// Work items of `bt` consecutive nodes of one replica (2 bt for a paired replica), and the per-warp partial sums they
-// write.
+// Work items of `bt` consecutive units of one replica (nodes, or pairs of a paired replica), and the per-warp partial
+// sums they write.
 void BatchEngine::buildItems(int bt) {
     std::vector<int> itemReplica;
     for (int r = 0; r < numReplicas; r++) {
         ReplicaTable& t = tableHost[r];
         t.firstItem = (int) itemReplica.size();
-        const unsigned span = t.paired ? 2*bt : bt;
-        t.numItems = (int) ((t.numNodes + span - 1)/span);
+        t.numItems = (int) ((t.units + bt - 1)/bt);
         itemReplica.insert(itemReplica.end(), t.numItems, r);
     }
     numItems = (int) itemReplica.size();

@@ -100,12 +100,15 @@ def run_oracle(lattice, positions, steps):
     return out
 
 
-@pytest.mark.parametrize('precision,steps,tolerance', [('double', 30, 1e-9), ('single', 10, 1e-5)])
-def test_batch_follows_oracle(precision, steps, tolerance):
+@pytest.mark.parametrize('precision,steps,tolerance,sizes', [('double', 30, 1e-9, (12, 16, 10, 14)),
+                                                               ('single', 10, 1e-5, (12, 16, 10, 14)),
+                                                               ('single', 10, 1e-5, (13, 16, 9, 15))])
+def test_batch_follows_oracle(precision, steps, tolerance, sizes):
     """Each replica of a batch of the batching configuration (fluctuating fluid, three-point stencil, explicit drag,
     Lennard-Jones beads) follows the CPU oracle path by path: FP64 within 1e-9 over 30 steps (the bead pair forces
-    are summed in another order and the bead dynamics amplify the last bits), FP32 storage within 1e-5 over 10."""
-    sizes, beads = [12, 16, 10, 14], [20, 35, 8, 26]
+    are summed in another order and the bead dynamics amplify the last bits), FP32 storage within 1e-5 over 10.  FP32
+    replicas of an odd edge pair the nodes within each row, the row's last node alone."""
+    beads = [20, 35, 8, 26]
     lattices, positions = make_replicas(sizes, beads, seed=99)
     batch = ReplicaBatch(lattices, beads, np.ones(sum(beads)), np.concatenate(positions), pair=('lj', SIGMA, KT, CUTOFF),
                          precision=precision)
