@@ -60,11 +60,12 @@ __global__ void stencilAxesKernel(CouplingView c, const double* __restrict__ pos
 template <typename T, typename R>
 __global__ void stencilClaimKernel(const T* __restrict__ A, FluidView f, CouplingView c, const int4* __restrict__ axisIndex,
                                    const double2* __restrict__ axisWeight, int remove, int centred, int* slotNode,
-                                   R* slotWeight, unsigned* nodeStamp, unsigned stamp, typename Vec4<R>::type* nodeU) {
+                                   R* slotWeight, unsigned* nodeStamp, unsigned stamp, typename Vec4<R>::type* nodeU,
+                                   uint32_t* mark) {
     long long total = (long long) c.np*c.slots;
     for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x)
         stencilClaimSlot<T, R>(A, f, c, axisIndex, axisWeight, t, remove, centred, slotNode, slotWeight, nodeStamp,
-                               stamp, nodeU);
+                               stamp, nodeU, mark);
 }
 
 template <typename R>
@@ -1158,14 +1159,15 @@ void CouplingEngine::reflect(const LbmParticleArrays* p, double wallMomentum[3])
 template <typename T, typename R>
 static void launchStencil(const void* A, const FluidView& f, const CouplingView& c, const double* pos, int remove, int centred,
                           int* slotNode, void* slotWeight, void* slotU, unsigned* nodeStamp, unsigned stamp,
-                          void* nodeU, int4* axisIndex, double2* axisWeight, int4* firstIndex, cudaStream_t s) {
+                          void* nodeU, int4* axisIndex, double2* axisWeight, int4* firstIndex, uint32_t* mark,
+                          cudaStream_t s) {
     typedef typename Vec4<R>::type V;
     long long total = (long long) c.np*c.slots;
     int grid = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
     stencilAxesKernel<<<std::max(1, (c.np + kThreads - 1)/kThreads), kThreads, 0, s>>>(c, pos, axisIndex, axisWeight,
                                                                                       firstIndex);
     stencilClaimKernel<T, R><<<grid, kThreads, 0, s>>>((const T*) A, f, c, axisIndex, axisWeight, remove, centred,
-                                                        slotNode, (R*) slotWeight, nodeStamp, stamp, (V*) nodeU);
+                                                        slotNode, (R*) slotWeight, nodeStamp, stamp, (V*) nodeU, mark);
     stencilGatherKernel<R><<<grid, kThreads, 0, s>>>(c, slotNode, (const R*) slotWeight, nodeStamp, stamp,
                                                      (const V*) nodeU, (V*) slotU);
 }
@@ -1191,7 +1193,7 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
     const FluidView& f = fluid.deviceView();
     bool centred = lattice.drag_scheme == LBM_DRAG_CENTERED;
     R* reaction = (R*) fluid.reactionBuffer();
-    uint32_t* mask = fluid.reactMask();
+    uint32_t* mask = nullptr;        // the stencil pass of the step flagged the nodes of its reactions
     const R* sw = (const R*) dev->slotWeight;
     const typename Vec4<R>::type* su = (const typename Vec4<R>::type*) dev->slotU;
     if (!centred) {
@@ -1279,8 +1281,9 @@ void CouplingEngine::setSolverLimits(int maxIterations, long long barrierPolls) 
     barrierPollLimit = barrierPolls > 0 ? barrierPolls : kDefaultBarrierPolls;
 }
 
-void CouplingEngine::launchStencilPass(const CouplingView& c, bool remove, cudaStream_t s) {
+void CouplingEngine::launchStencilPass(const CouplingView& c, bool remove, bool mark, cudaStream_t s) {
     const FluidView& f = fluid.deviceView();
+    uint32_t* m = mark ? fluid.reactMask() : nullptr;
     bool centred = lattice.drag_scheme == LBM_DRAG_CENTERED;
     const void* A = fluid.inputArray();
     if (++dev->stamp == 0u) {     // the stamps wrapped around: no node may carry a stale stamp
@@ -1291,10 +1294,10 @@ void CouplingEngine::launchStencilPass(const CouplingView& c, bool remove, cudaS
     void* nu = dev->nodeU;
     unsigned st = dev->stamp;
     switch (storageType) {
-    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, s); break;
-    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, s); break;
-    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, s); break;
-    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, s); break;
+    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, s); break;
+    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, s); break;
+    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, s); break;
+    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, s); break;
     }
     CUDA_CHECK(cudaGetLastError());
     fluid.launches += 3;
@@ -1324,7 +1327,7 @@ void CouplingEngine::prepare(const LbmParticleArrays* p, long long step, bool re
     CUDA_CHECK(cudaStreamWaitEvent(side, begun, 0));
     const FluidView& f = fluid.deviceView();
     CouplingView c = makeCouplingView(lattice, f, np, widthOf(lattice.interpolation_stencil), massDev);
-    launchStencilPass(c, remove, side);
+    launchStencilPass(c, remove, true, side);
     if (matrixSolve()) {
         if (storageType == LBM_STORAGE_F64)
             launchMatrix<double>(&c, side);
@@ -1353,7 +1356,7 @@ void CouplingEngine::couple(long long step, bool isStep, bool remove) {
     const bool usePrepared = prepared && isStep && step == preparedStep && remove == preparedRemove;
     discardPrepared();
     if (!usePrepared)
-        launchStencilPass(c, remove, stream);
+        launchStencilPass(c, remove, isStep, stream);
     if (isStep)
         CUDA_CHECK(cudaMemsetAsync(wallDev, 0, sizeof(double)*3, stream));
     if (storageType == LBM_STORAGE_F64)

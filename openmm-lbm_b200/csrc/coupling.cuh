@@ -57,7 +57,7 @@ private:
     void coupleWith(long long step, bool isStep, const CouplingView* view, bool matrixReady);
     template <typename R>
     void launchMatrix(const CouplingView* view, cudaStream_t s);
-    void launchStencilPass(const CouplingView& view, bool remove, cudaStream_t s);
+    void launchStencilPass(const CouplingView& view, bool remove, bool mark, cudaStream_t s);
     bool matrixSolve() const;
     cudaStream_t side = nullptr;          // stream of the prepared work
     cudaEvent_t begun = nullptr, ready = nullptr;

@@ -268,13 +268,15 @@ __device__ __forceinline__ void stencilSlot(const T* __restrict__ A, const Fluid
 // per particle by stencilAxes), with the moments computed once per node: the first slot of a fluid node to claim it in
 // this pass (nodeStamp[node] set to `stamp`) pulls the node's moments into nodeU[node]; stencilGatherSlot then copies
 // them to every slot of the node.  The moments of a node are the same for all its slots, and overlapping stencils
-// share most of their nodes.
+// share most of their nodes.  With `mark` (the fluid's reaction mask, for the pass of a step) the claiming slot also
+// flags the node, once per node: every fluid node of a slot with a nonzero weight receives a reaction in this step, so
+// the reactions are then added without touching the mask.
 template <typename T, typename R>
 __device__ __forceinline__ void stencilClaimSlot(const T* __restrict__ A, const FluidView& f, const CouplingView& c,
                                                  const int4* __restrict__ axisIndex,
                                                  const double2* __restrict__ axisWeight, long long t, int remove,
                                                  int centred, int* slotNode, R* slotWeight, unsigned* nodeStamp,
-                                                 unsigned stamp, typename Vec4<R>::type* nodeU) {
+                                                 unsigned stamp, typename Vec4<R>::type* nodeU, uint32_t* mark) {
     const int i = (int) (t/c.slots), s = (int) (t - (long long) i*c.slots);
     const int sub[3] = {s%c.width, (s/c.width)%c.width, s/(c.width*c.width)};
     int idx[3];
@@ -310,6 +312,10 @@ __device__ __forceinline__ void stencilClaimSlot(const T* __restrict__ A, const 
             jz += c.h*rho*c.g[2];
         }
         nodeU[node] = Vec4<R>::make((R) (jx*(1.0/rho)), (R) (jy*(1.0/rho)), (R) (jz*(1.0/rho)), (R) rho);
+        if (mark != nullptr) {
+            const size_t row = (size_t) idx[1] + (size_t) c.ny*idx[2];
+            atomicOr(&mark[row*f.wordsPerRow + idx[0]/32], 1u << (idx[0]%32));
+        }
     }
 }
 
@@ -325,8 +331,9 @@ __device__ __forceinline__ void stencilGatherSlot(long long t, const int* __rest
     slotU[t] = u;
 }
 
-// Reaction (fx, fy, fz) on a node: added into the fluid's reaction buffer and the node flagged, or for a solid node
-// counted as momentum given to the wall (applyReaction, ReferenceLBMKernels.cpp:959-971).
+// Reaction (fx, fy, fz) on a node: added into the fluid's reaction buffer and the node flagged in `mask` (nullptr: the
+// stencil pass flagged it), or for a solid node counted as momentum given to the wall (applyReaction,
+// ReferenceLBMKernels.cpp:959-971).
 template <typename R>
 __device__ void addReaction(const FluidView& f, const CouplingView& c, R* reaction, uint32_t* mask, double* wall,
                             long long node, double fx, double fy, double fz) {
@@ -337,6 +344,8 @@ __device__ void addReaction(const FluidView& f, const CouplingView& c, R* reacti
         return;
     }
     atomicAdd3(reaction + 4*node, fx, fy, fz);
+    if (mask == nullptr)
+        return;
     const unsigned row = (unsigned) node/(unsigned) f.nx;
     const int x = (int) ((unsigned) node - row*(unsigned) f.nx);
     uint32_t bit = 1u << (x%32);
