@@ -863,13 +863,16 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
     for (int i = firstThread; i < c.np; i += threads)
         for (int d = 0; d < 3; d++)
             fout[3*i+d] = b.F[3*i+d]*c.forceScale;
-    if (isStep)
-        for (long long t = firstThread; t < (long long) c.np*S; t += threads) {
-            const int i = (int) (t/S);
+    // (np S < 2^31, which the constructor checks: the slots are indexed by int.)
+    if (isStep) {
+        const int total = c.np*S;
+        for (int t = firstThread; t < total; t += threads) {
+            const int i = t/S;
             const double w = (double) slotWeight[t];
             if (w != 0.0)
                 addReaction<R>(f, c, reaction, mask, wall, slotNode[t], -w*b.F[3*i], -w*b.F[3*i+1], -w*b.F[3*i+2]);
         }
+    }
 }
 
 // Clear the reaction of the slots of the last step (and their mask words).
@@ -981,6 +984,10 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
     bool f64 = storageType == LBM_STORAGE_F64;
     size_t r = f64 ? 8 : 4;
     try {
+        // The stencil slots of all particles are indexed by int in the solves.
+        if ((long long) np*stencilSlots >= (1LL << 31))
+            throw Error(LBM_ERR_INVALID_ARGUMENT, "LBMForce: too many coupled particles for the interpolation stencil "
+                        "(particles x stencil nodes must stay below 2^31)");
         size_t v3 = sizeof(double)*3*(size_t) np;
         CUDA_CHECK(cudaMalloc(&posDev, v3));
         CUDA_CHECK(cudaMalloc(&velDev, v3));
