@@ -530,9 +530,12 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
             rowCoef[warp][s] = coef[(long long) k*S + s];
         const int4 fk = g.firstIndex[k];
         const int key = g.cellOf[k];
-        const int home[3] = {key%g.cells[0], (key/g.cells[0])%g.cells[1], key/(g.cells[0]*g.cells[1])};
+        const int keyYZ = key/g.cells[0];
+        const int home[3] = {key - keyYZ*g.cells[0], keyYZ%g.cells[1], keyYZ/g.cells[1]};
         // Lane j < 27 takes the neighbouring cell (j%3 - 1, j/3%3 - 1, j/9 - 1); a cell that an axis with fewer than
-        // 3 cells reaches twice is taken once (by its first offset).
+        // 3 cells reaches twice is taken once (by its first offset).  The offsets are -1, 0 or 1, so one conditional
+        // wrap replaces the modulo (whose integer divisions by the runtime cell counts were a quarter of the kernel's
+        // instructions).
         int cell = -1, members = 0;
         if (lane < 27) {
             const int off[3] = {lane%3 - 1, (lane/3)%3 - 1, lane/9 - 1};
@@ -540,9 +543,13 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
             int cc[3];
             for (int a = 0; a < 3; a++) {
                 const int n = g.cells[a];
-                cc[a] = ((home[a] + off[a])%n + n)%n;
-                for (int d = -1; d < off[a]; d++)
-                    first &= ((home[a] + d)%n + n)%n != cc[a];
+                const int v = home[a] + off[a];
+                cc[a] = v < 0 ? v + n : (v >= n ? v - n : v);
+                if (n < 3)
+                    for (int d = -1; d < off[a]; d++) {
+                        const int u = home[a] + d;
+                        first &= (u < 0 ? u + n : (u >= n ? u - n : u)) != cc[a];
+                    }
             }
             if (first) {
                 cell = cc[0] + g.cells[0]*(cc[1] + g.cells[1]*cc[2]);
