@@ -57,15 +57,15 @@ __global__ void stencilAxesKernel(CouplingView c, const double* __restrict__ pos
     }
 }
 
-template <typename T, typename R>
+template <typename T, typename R, int W>
 __global__ void stencilClaimKernel(const T* __restrict__ A, FluidView f, CouplingView c, const int4* __restrict__ axisIndex,
                                    const double2* __restrict__ axisWeight, int remove, int centred, int* slotNode,
                                    R* slotWeight, unsigned* nodeStamp, unsigned stamp, typename Vec4<R>::type* nodeU,
                                    uint32_t* mark) {
-    long long total = (long long) c.np*c.slots;
-    for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x)
-        stencilClaimSlot<T, R>(A, f, c, axisIndex, axisWeight, t, remove, centred, slotNode, slotWeight, nodeStamp,
-                               stamp, nodeU, mark);
+    const int total = c.np*c.slots;     // below 2^31 (the coupling's constructor checks it)
+    for (int t = blockIdx.x*blockDim.x + threadIdx.x; t < total; t += gridDim.x*blockDim.x)
+        stencilClaimSlot<T, R, W>(A, f, c, axisIndex, axisWeight, t, remove, centred, slotNode, slotWeight, nodeStamp,
+                                  stamp, nodeU, mark);
 }
 
 template <typename R>
@@ -1180,8 +1180,19 @@ static void launchStencil(const void* A, const FluidView& f, const CouplingView&
     int grid = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
     stencilAxesKernel<<<std::max(1, (c.np + kThreads - 1)/kThreads), kThreads, 0, s>>>(c, pos, axisIndex, axisWeight,
                                                                                       firstIndex);
-    stencilClaimKernel<T, R><<<grid, kThreads, 0, s>>>((const T*) A, f, c, axisIndex, axisWeight, remove, centred,
-                                                        slotNode, (R*) slotWeight, nodeStamp, stamp, (V*) nodeU, mark);
+    // The stencil widths: 1 (nearest node), 2 (trilinear), 3 (three-point), 4 (Keys).
+    auto claim = [&](auto w) {
+        stencilClaimKernel<T, R, decltype(w)::value><<<grid, kThreads, 0, s>>>(
+            (const T*) A, f, c, axisIndex, axisWeight, remove, centred, slotNode, (R*) slotWeight, nodeStamp, stamp,
+            (V*) nodeU, mark);
+    };
+    switch (c.width) {
+    case 1: claim(std::integral_constant<int, 1>()); break;
+    case 2: claim(std::integral_constant<int, 2>()); break;
+    case 3: claim(std::integral_constant<int, 3>()); break;
+    case 4: claim(std::integral_constant<int, 4>()); break;
+    default: claim(std::integral_constant<int, 0>()); break;
+    }
     stencilGatherKernel<R><<<grid, kThreads, 0, s>>>(c, slotNode, (const R*) slotWeight, nodeStamp, stamp,
                                                      (const V*) nodeU, (V*) slotU);
 }

@@ -271,14 +271,17 @@ __device__ __forceinline__ void stencilSlot(const T* __restrict__ A, const Fluid
 // share most of their nodes.  With `mark` (the fluid's reaction mask, for the pass of a step) the claiming slot also
 // flags the node, once per node: every fluid node of a slot with a nonzero weight receives a reaction in this step, so
 // the reactions are then added without touching the mask.
-template <typename T, typename R>
+// W: the stencil width when it is known at compile time (the slot's particle and axis entries then come from
+// divisions by constants), 0 for c.width.  The slots of all particles are fewer than 2^31.
+template <typename T, typename R, int W = 0>
 __device__ __forceinline__ void stencilClaimSlot(const T* __restrict__ A, const FluidView& f, const CouplingView& c,
                                                  const int4* __restrict__ axisIndex,
                                                  const double2* __restrict__ axisWeight, long long t, int remove,
                                                  int centred, int* slotNode, R* slotWeight, unsigned* nodeStamp,
                                                  unsigned stamp, typename Vec4<R>::type* nodeU, uint32_t* mark) {
-    const int i = (int) (t/c.slots), s = (int) (t - (long long) i*c.slots);
-    const int sub[3] = {s%c.width, (s/c.width)%c.width, s/(c.width*c.width)};
+    const int width = W > 0 ? W : c.width, slots = W > 0 ? W*W*W : c.slots;
+    const int i = (int) t/slots, s = (int) t - i*slots;
+    const int sub[3] = {s%width, (s/width)%width, s/(width*width)};
     int idx[3];
     double w = 1.0;
     for (int a = 0; a < 3; a++) {
