@@ -71,10 +71,11 @@ __global__ void stencilClaimKernel(const T* __restrict__ A, FluidView f, Couplin
 template <typename R>
 __global__ void stencilGatherKernel(CouplingView c, const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
                                     const unsigned* __restrict__ nodeStamp, unsigned stamp,
-                                    const typename Vec4<R>::type* __restrict__ nodeU, typename Vec4<R>::type* slotU) {
+                                    const typename Vec4<R>::type* __restrict__ nodeU, typename Vec4<R>::type* slotU,
+                                    R* coef) {
     long long total = (long long) c.np*c.slots;
     for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x)
-        stencilGatherSlot<R>(t, slotNode, slotWeight, nodeStamp, stamp, nodeU, slotU);
+        stencilGatherSlot<R>(t, slotNode, slotWeight, nodeStamp, stamp, nodeU, slotU, coef);
 }
 
 // One warp per particle.
@@ -451,7 +452,8 @@ centeredStencilKernel(FluidView f, CouplingView c, const double* __restrict__ ve
 // particles within one stencil width), so it is built once per step and every iteration is a sparse product over a few
 // dozen entries per particle instead of a pass over the lattice nodes of all stencils.
 //   cgBinKernel     per particle: its cell (cells of kCgCellEdge nodes, on the first stencil index of the stencil
-//                   pass), inserted into a fixed-capacity cell list; per slot: w/rho
+//                   pass), inserted into a fixed-capacity cell list (w/rho of every slot comes from the stencil
+//                   pass's slot copy)
 //   cgRowsKernel    one warp per particle k: the particles of the neighbouring cells whose first stencil indices are
 //                   within a stencil width of k's on every axis, sorted by index (so that every row, and every sum
 //                   over it, has one order), and K_kl for each, a lane per entry
@@ -482,16 +484,8 @@ struct SparseCg {
     int cells[3];          // cells per axis
 };
 
-template <typename R>
 __global__ void __launch_bounds__(kThreads)
-cgBinKernel(CouplingView c, const R* __restrict__ slotWeight, const typename Vec4<R>::type* __restrict__ slotU, R* coef,
-            SparseCg g) {
-    const long long total = (long long) c.np*c.slots;
-    for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x; t < total; t += (long long) gridDim.x*blockDim.x) {
-        double w = (double) slotWeight[t];
-        double rho = (double) slotU[t].w;
-        coef[t] = (R) (rho > 0 ? w/rho : 0.0);
-    }
+cgBinKernel(CouplingView c, SparseCg g) {
     for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < c.np; i += gridDim.x*blockDim.x) {
         const int4 first = g.firstIndex[i];
         const int cell[3] = {min(first.x/kCgCellEdge, g.cells[0] - 1), min(first.y/kCgCellEdge, g.cells[1] - 1),
@@ -1174,7 +1168,7 @@ template <typename T, typename R>
 static void launchStencil(const void* A, const FluidView& f, const CouplingView& c, const double* pos, int remove, int centred,
                           int* slotNode, void* slotWeight, void* slotU, unsigned* nodeStamp, unsigned stamp,
                           void* nodeU, int4* axisIndex, double2* axisWeight, int4* firstIndex, uint32_t* mark,
-                          cudaStream_t s) {
+                          void* coef, cudaStream_t s) {
     typedef typename Vec4<R>::type V;
     long long total = (long long) c.np*c.slots;
     int grid = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
@@ -1194,7 +1188,7 @@ static void launchStencil(const void* A, const FluidView& f, const CouplingView&
     default: claim(std::integral_constant<int, 0>()); break;
     }
     stencilGatherKernel<R><<<grid, kThreads, 0, s>>>(c, slotNode, (const R*) slotWeight, nodeStamp, stamp,
-                                                     (const V*) nodeU, (V*) slotU);
+                                                     (const V*) nodeU, (V*) slotU, (R*) coef);
 }
 
 // The cell list and the rows of the coupling matrix, after the status words are cleared (their overflow flag).
@@ -1202,10 +1196,7 @@ template <typename R>
 void CouplingEngine::launchMatrix(const CouplingView* cv, cudaStream_t s) {
     const CouplingView& c = *cv;
     CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, s));
-    long long total = (long long) np*c.slots;
-    int gridSlots = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
-    cgBinKernel<R><<<gridSlots, kThreads, 0, s>>>(c, (const R*) dev->slotWeight,
-                                                 (const typename Vec4<R>::type*) dev->slotU, (R*) dev->coef, dev->sparse);
+    cgBinKernel<<<std::max(1, std::min(1184, (np + kThreads - 1)/kThreads)), kThreads, 0, s>>>(c, dev->sparse);
     CUDA_CHECK(cudaGetLastError());
     cgRowsKernel<R><<<warpGrid(np), kThreads, 0, s>>>(c, (const R*) dev->coef, dev->sparse);
     CUDA_CHECK(cudaGetLastError());
@@ -1309,6 +1300,7 @@ void CouplingEngine::setSolverLimits(int maxIterations, long long barrierPolls) 
 void CouplingEngine::launchStencilPass(const CouplingView& c, bool remove, bool mark, cudaStream_t s) {
     const FluidView& f = fluid.deviceView();
     uint32_t* m = mark ? fluid.reactMask() : nullptr;
+    void* cf = matrixSolve() ? dev->coef : nullptr;     // w/rho of the slots for the coupling matrix
     bool centred = lattice.drag_scheme == LBM_DRAG_CENTERED;
     const void* A = fluid.inputArray();
     if (++dev->stamp == 0u) {     // the stamps wrapped around: no node may carry a stale stamp
@@ -1319,10 +1311,10 @@ void CouplingEngine::launchStencilPass(const CouplingView& c, bool remove, bool 
     void* nu = dev->nodeU;
     unsigned st = dev->stamp;
     switch (storageType) {
-    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, s); break;
-    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, s); break;
-    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, s); break;
-    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, s); break;
+    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, cf, s); break;
+    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, cf, s); break;
+    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, cf, s); break;
+    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, cf, s); break;
     }
     CUDA_CHECK(cudaGetLastError());
     fluid.launches += 3;

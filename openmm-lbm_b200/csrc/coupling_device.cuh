@@ -323,15 +323,21 @@ __device__ __forceinline__ void stencilClaimSlot(const T* __restrict__ A, const 
 }
 
 template <typename R>
+// With `coef` (the coupling matrix's solve) it also stores w/rho of the slot (0 where rho is 0).
 __device__ __forceinline__ void stencilGatherSlot(long long t, const int* __restrict__ slotNode,
                                                   const R* __restrict__ slotWeight, const unsigned* __restrict__ nodeStamp,
                                                   unsigned stamp, const typename Vec4<R>::type* __restrict__ nodeU,
-                                                  typename Vec4<R>::type* slotU) {
+                                                  typename Vec4<R>::type* slotU, R* coef) {
     const long long node = slotNode[t];
+    const R weight = slotWeight[t];
     typename Vec4<R>::type u = Vec4<R>::make(0, 0, 0, 0);
-    if (slotWeight[t] != (R) 0 && nodeStamp[node] == stamp)
+    if (weight != (R) 0 && nodeStamp[node] == stamp)
         u = nodeU[node];
     slotU[t] = u;
+    if (coef != nullptr) {
+        const double w = (double) weight, rho = (double) u.w;
+        coef[t] = (R) (rho > 0 ? w/rho : 0.0);
+    }
 }
 
 // Reaction (fx, fy, fz) on a node: added into the fluid's reaction buffer and the node flagged in `mask` (nullptr: the
