@@ -480,6 +480,7 @@ struct SparseCg {
     int* rowIndex;         // entry e of row k at k kCgRowCapacity + e: the column particle
     double* rowValue;      // K_kl, same layout
     double* Ap;            // A p, 3 per particle
+    double* slotSums;      // per particle: sum w u over its fluid slots (3) and sum w^2/rho (written by the rows)
     int* overflow;         // nonzero: a cell or a row over its capacity
     int cells[3];          // cells per axis
 };
@@ -508,7 +509,8 @@ __device__ __forceinline__ int periodicDistance(int a, int b, int n) {
 
 template <typename R>
 __global__ void __launch_bounds__(kThreads, 4)
-cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
+cgRowsKernel(CouplingView c, const R* __restrict__ coef, const R* __restrict__ slotWeight,
+             const typename Vec4<R>::type* __restrict__ slotU, SparseCg g) {
     __shared__ int candidates[kThreads/32][kCgRowCapacity];
     __shared__ int sorted[kThreads/32][kCgRowCapacity];
     __shared__ R rowCoef[kThreads/32][64];
@@ -520,8 +522,25 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, SparseCg g) {
     const int size[3] = {c.nx, c.ny, c.nz};
     const int w = c.width, S = c.slots;
     for (int k = firstWarp; k < c.np; k += warps) {
-        for (int s = lane; s < S; s += 32)
-            rowCoef[warp][s] = coef[(long long) k*S + s];
+        // The particle's sums over its slots for the solve's right-hand side and diagonal (ReferenceLBMKernels.cpp:
+        // 758-782): u = sum w u_node over the fluid slots and sum w^2/rho; they need no velocities or forces.
+        double su[4] = {0, 0, 0, 0};
+        for (int s = lane; s < S; s += 32) {
+            const long long t = (long long) k*S + s;
+            rowCoef[warp][s] = coef[t];
+            const typename Vec4<R>::type u = slotU[t];
+            const double wt = (double) slotWeight[t];
+            if (u.w > 0) {
+                su[0] += (double) u.x*wt;
+                su[1] += (double) u.y*wt;
+                su[2] += (double) u.z*wt;
+                su[3] += wt*wt/(double) u.w;
+            }
+        }
+        for (int d = 0; d < 4; d++)
+            su[d] = warpSum(su[d]);
+        if (lane == 0)
+            reinterpret_cast<double4*>(g.slotSums)[k] = make_double4(su[0], su[1], su[2], su[3]);
         const int4 fk = g.firstIndex[k];
         const int key = g.cellOf[k];
         const int keyYZ = key/g.cells[0];
@@ -701,11 +720,8 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
                      const typename Vec4<R>::type* __restrict__ slotU, long long step, int isStep, double tolerance,
                      int maxIterations, CgBuffers b, SparseCg g, double* fout, R* reaction, uint32_t* mask,
                      double* wall) {
-    typedef typename Vec4<R>::type V;
-    constexpr int G = 8;       // lanes per particle where a particle's slots are summed
-    const int lane = threadIdx.x & 31, sub = lane%G;
+    const int lane = threadIdx.x & 31;
     const int firstWarp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
-    const int warps = (gridDim.x*blockDim.x) >> 5;
     const int firstThread = blockIdx.x*blockDim.x + threadIdx.x, threads = gridDim.x*blockDim.x;
     // The rows of this block (a contiguous range).
     const int rowBegin = (int) ((long long) c.np*blockIdx.x/gridDim.x);
@@ -717,31 +733,11 @@ centeredSparseKernel(FluidView f, CouplingView c, const double* __restrict__ vel
         g.cellCount[g.cellOf[i]] = 0u;
     if (*((volatile int*) g.overflow) != 0)
         return;
-    // Right-hand side, diagonal and the start F = rhs/diag (ReferenceLBMKernels.cpp:758-782, 839-840): 8 lanes per
-    // particle, 4 particles per warp.
-    for (int base = firstWarp*(32/G); base < c.np; base += warps*(32/G)) {
-        const int i = base + lane/G;
-        const bool active = i < c.np;
-        double u[3] = {0, 0, 0}, self = 0;
-        if (active)
-            for (int s = sub; s < S; s += G) {
-                long long t = (long long) i*S + s;
-                V su = slotU[t];
-                double w = (double) slotWeight[t];
-                if (su.w > 0) {
-                    u[0] += (double) su.x*w;
-                    u[1] += (double) su.y*w;
-                    u[2] += (double) su.z*w;
-                    self += w*w/(double) su.w;
-                }
-            }
-        for (int o = G/2; o > 0; o /= 2) {
-            for (int d = 0; d < 3; d++)
-                u[d] += __shfl_xor_sync(0xFFFFFFFFu, u[d], o);
-            self += __shfl_xor_sync(0xFFFFFFFFu, self, o);
-        }
-        if (!active || sub != 0)
-            continue;
+    // Right-hand side, diagonal and the start F = rhs/diag (ReferenceLBMKernels.cpp:758-782, 839-840), a thread per
+    // particle, from the sums over its slots that the rows kernel formed.
+    for (int i = firstThread; i < c.np; i += threads) {
+        const double4 su = reinterpret_cast<const double4*>(g.slotSums)[i];
+        const double u[3] = {su.x, su.y, su.z}, self = su.w;
         double m = c.mass[i];
         double xi[3] = {0, 0, 0};
         if (c.randomForce)
@@ -1075,6 +1071,7 @@ CouplingEngine::CouplingEngine(const LbmLatticeParameters& l, FluidEngine& f, co
             CUDA_CHECK(cudaMalloc(&g.rowIndex, sizeof(int)*kCgRowCapacity*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.rowValue, sizeof(double)*kCgRowCapacity*(size_t) np));
             CUDA_CHECK(cudaMalloc(&g.Ap, v3));
+            CUDA_CHECK(cudaMalloc(&g.slotSums, sizeof(double)*4*(size_t) np));
             g.overflow = statusDev + 2;
             if (f64)
                 CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, centeredSparseKernel<double>, kSolveThreads, 0));
@@ -1125,7 +1122,7 @@ void CouplingEngine::release() {
         cudaFree(dev->spread);
         SparseCg& g = dev->sparse;
         cudaFree(g.cellOf); cudaFree(g.cellCount); cudaFree(g.cellList);
-        cudaFree(g.rowCount); cudaFree(g.rowIndex); cudaFree(g.rowValue); cudaFree(g.Ap);
+        cudaFree(g.rowCount); cudaFree(g.rowIndex); cudaFree(g.rowValue); cudaFree(g.Ap); cudaFree(g.slotSums);
         delete dev;
         dev = nullptr;
     }
@@ -1198,7 +1195,8 @@ void CouplingEngine::launchMatrix(const CouplingView* cv, cudaStream_t s) {
     CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, s));
     cgBinKernel<<<std::max(1, std::min(1184, (np + kThreads - 1)/kThreads)), kThreads, 0, s>>>(c, dev->sparse);
     CUDA_CHECK(cudaGetLastError());
-    cgRowsKernel<R><<<warpGrid(np), kThreads, 0, s>>>(c, (const R*) dev->coef, dev->sparse);
+    cgRowsKernel<R><<<warpGrid(np), kThreads, 0, s>>>(c, (const R*) dev->coef, (const R*) dev->slotWeight,
+                                                     (const typename Vec4<R>::type*) dev->slotU, dev->sparse);
     CUDA_CHECK(cudaGetLastError());
     fluid.launches += 2;
 }
