@@ -61,11 +61,11 @@ template <typename T, typename R, int W>
 __global__ void stencilClaimKernel(const T* __restrict__ A, FluidView f, CouplingView c, const int4* __restrict__ axisIndex,
                                    const double2* __restrict__ axisWeight, int remove, int centred, int* slotNode,
                                    R* slotWeight, unsigned* nodeStamp, unsigned stamp, typename Vec4<R>::type* nodeU,
-                                   uint32_t* mark) {
+                                   uint32_t* mark, R* reaction) {
     const int total = c.np*c.slots;     // below 2^31 (the coupling's constructor checks it)
     for (int t = blockIdx.x*blockDim.x + threadIdx.x; t < total; t += gridDim.x*blockDim.x)
         stencilClaimSlot<T, R, W>(A, f, c, axisIndex, axisWeight, t, remove, centred, slotNode, slotWeight, nodeStamp,
-                                  stamp, nodeU, mark);
+                                  stamp, nodeU, mark, reaction);
 }
 
 template <typename R>
@@ -1165,7 +1165,7 @@ template <typename T, typename R>
 static void launchStencil(const void* A, const FluidView& f, const CouplingView& c, const double* pos, int remove, int centred,
                           int* slotNode, void* slotWeight, void* slotU, unsigned* nodeStamp, unsigned stamp,
                           void* nodeU, int4* axisIndex, double2* axisWeight, int4* firstIndex, uint32_t* mark,
-                          void* coef, cudaStream_t s) {
+                          void* reaction, void* coef, cudaStream_t s) {
     typedef typename Vec4<R>::type V;
     long long total = (long long) c.np*c.slots;
     int grid = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
@@ -1175,7 +1175,7 @@ static void launchStencil(const void* A, const FluidView& f, const CouplingView&
     auto claim = [&](auto w) {
         stencilClaimKernel<T, R, decltype(w)::value><<<grid, kThreads, 0, s>>>(
             (const T*) A, f, c, axisIndex, axisWeight, remove, centred, slotNode, (R*) slotWeight, nodeStamp, stamp,
-            (V*) nodeU, mark);
+            (V*) nodeU, mark, (R*) reaction);
     };
     switch (c.width) {
     case 1: claim(std::integral_constant<int, 1>()); break;
@@ -1309,10 +1309,10 @@ void CouplingEngine::launchStencilPass(const CouplingView& c, bool remove, bool 
     void* nu = dev->nodeU;
     unsigned st = dev->stamp;
     switch (storageType) {
-    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, cf, s); break;
-    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, cf, s); break;
-    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, cf, s); break;
-    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, cf, s); break;
+    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, m != nullptr ? fluid.reactionBuffer() : nullptr, cf, s); break;
+    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, m != nullptr ? fluid.reactionBuffer() : nullptr, cf, s); break;
+    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, m != nullptr ? fluid.reactionBuffer() : nullptr, cf, s); break;
+    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, m != nullptr ? fluid.reactionBuffer() : nullptr, cf, s); break;
     }
     CUDA_CHECK(cudaGetLastError());
     fluid.launches += 3;
@@ -1393,6 +1393,10 @@ void CouplingEngine::addForces(const LbmParticleArrays* p) {
     CUDA_CHECK(cudaStreamSynchronize(stream));
     for (size_t i = 0; i < count; i++)
         p->forces[i] += pinned[i];
+}
+
+void CouplingEngine::clearReactionFlags() {
+    fluid.clearReactMask(stream);
 }
 
 void CouplingEngine::clearReaction() {

@@ -40,6 +40,8 @@ public:
     void addForces(const LbmParticleArrays* particles);
     // Clear the reaction of the last step from the fluid's reaction buffers.
     void clearReaction();
+    // Clear the flags of the last step's reactions (the next step's stencil pass zeroes the reactions it flags).
+    void clearReactionFlags();
     // Momentum given to solid nodes by the reactions of the last coupling step (lattice units), read on demand.
     void reactionWallMomentum(double out[3]);
     int numParticles() const { return np; }

@@ -269,8 +269,9 @@ __device__ __forceinline__ void stencilSlot(const T* __restrict__ A, const Fluid
 // this pass (nodeStamp[node] set to `stamp`) pulls the node's moments into nodeU[node]; stencilGatherSlot then copies
 // them to every slot of the node.  The moments of a node are the same for all its slots, and overlapping stencils
 // share most of their nodes.  With `mark` (the fluid's reaction mask, for the pass of a step) the claiming slot also
-// flags the node, once per node: every fluid node of a slot with a nonzero weight receives a reaction in this step, so
-// the reactions are then added without touching the mask.
+// flags the node and zeroes its reaction, once per node: every fluid node of a slot with a nonzero weight receives a
+// reaction in this step, so the reactions are then added without touching the mask, and the end of a step clears the
+// mask alone.
 // W: the stencil width when it is known at compile time (the slot's particle and axis entries then come from
 // divisions by constants), 0 for c.width.  The slots of all particles are fewer than 2^31.
 template <typename T, typename R, int W = 0>
@@ -278,7 +279,8 @@ __device__ __forceinline__ void stencilClaimSlot(const T* __restrict__ A, const 
                                                  const int4* __restrict__ axisIndex,
                                                  const double2* __restrict__ axisWeight, long long t, int remove,
                                                  int centred, int* slotNode, R* slotWeight, unsigned* nodeStamp,
-                                                 unsigned stamp, typename Vec4<R>::type* nodeU, uint32_t* mark) {
+                                                 unsigned stamp, typename Vec4<R>::type* nodeU, uint32_t* mark,
+                                                 R* reaction) {
     const int width = W > 0 ? W : c.width, slots = W > 0 ? W*W*W : c.slots;
     const int i = (int) t/slots, s = (int) t - i*slots;
     const int sub[3] = {s%width, (s/width)%width, s/(width*width)};
@@ -318,6 +320,8 @@ __device__ __forceinline__ void stencilClaimSlot(const T* __restrict__ A, const 
         if (mark != nullptr) {
             const size_t row = (size_t) idx[1] + (size_t) c.ny*idx[2];
             atomicOr(&mark[row*f.wordsPerRow + idx[0]/32], 1u << (idx[0]%32));
+            // The node's reaction starts from zero (the last step's were left in place; only their flags were cleared).
+            *reinterpret_cast<typename Vec4<R>::type*>(reaction + 4*node) = Vec4<R>::make(0, 0, 0, 0);
         }
     }
 }

@@ -1233,6 +1233,11 @@ void FluidEngine::enableReaction() {
     view.reaction = reactionDev;
 }
 
+void FluidEngine::clearReactMask(cudaStream_t s) {
+    if (reactMaskDev != nullptr)
+        CUDA_CHECK(cudaMemsetAsync(reactMaskDev, 0, sizeof(uint32_t)*(size_t) view.wordsPerRow*lattice.ny*lattice.nz, s));
+}
+
 void FluidEngine::step(long long stepIndex, bool remove, bool react) {
     const void* A = pop[cur];
     void* B = pop[1-cur];

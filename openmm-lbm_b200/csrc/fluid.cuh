@@ -84,6 +84,7 @@ public:
     // Reaction buffers, owned here so that the dense kernel reads them directly.
     void enableReaction();
     uint32_t* reactMask() { return reactMaskDev; }
+    void clearReactMask(cudaStream_t s);
     void* reactionBuffer() { return reactionDev; }
     const FluidView& deviceView() const { return view; }
     const void* inputArray() const { return pop[cur]; }

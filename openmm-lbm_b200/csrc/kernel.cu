@@ -259,7 +259,7 @@ void B200Kernel::advanceFluid(const LbmParticleArrays* particles) {
     }
     fluid->step(stepIndex, remove, react);
     if (react)
-        coupling->clearReaction();
+        coupling->clearReactionFlags();
     stepWallValid = true;
     stepForcesCurrent = true;
     stepIndex++;
