@@ -509,8 +509,9 @@ __device__ __forceinline__ int periodicDistance(int a, int b, int n) {
 
 template <typename R>
 __global__ void __launch_bounds__(kThreads, 4)
-cgRowsKernel(CouplingView c, const R* __restrict__ coef, const R* __restrict__ slotWeight,
-             const typename Vec4<R>::type* __restrict__ slotU, SparseCg g) {
+cgRowsKernel(CouplingView c, const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
+             const unsigned* __restrict__ nodeStamp, unsigned stamp, const typename Vec4<R>::type* __restrict__ nodeU,
+             SparseCg g) {
     __shared__ int candidates[kThreads/32][kCgRowCapacity];
     __shared__ int sorted[kThreads/32][kCgRowCapacity];
     __shared__ R rowCoef[kThreads/32][64];
@@ -524,12 +525,18 @@ cgRowsKernel(CouplingView c, const R* __restrict__ coef, const R* __restrict__ s
     for (int k = firstWarp; k < c.np; k += warps) {
         // The particle's sums over its slots for the solve's right-hand side and diagonal (ReferenceLBMKernels.cpp:
         // 758-782): u = sum w u_node over the fluid slots and sum w^2/rho; they need no velocities or forces.
+        // The slot's moments are its node's from the stencil pass (a node that no slot claimed in the pass, a solid
+        // one, has none: rho = 0), and (w/rho)_k, the row's factor for K, goes to shared memory.
         double su[4] = {0, 0, 0, 0};
         for (int s = lane; s < S; s += 32) {
             const long long t = (long long) k*S + s;
-            rowCoef[warp][s] = coef[t];
-            const typename Vec4<R>::type u = slotU[t];
-            const double wt = (double) slotWeight[t];
+            const R weight = slotWeight[t];
+            const long long node = slotNode[t];
+            typename Vec4<R>::type u = Vec4<R>::make(0, 0, 0, 0);
+            if (weight != (R) 0 && nodeStamp[node] == stamp)
+                u = nodeU[node];
+            const double wt = (double) weight, rho = (double) u.w;
+            rowCoef[warp][s] = (R) (rho > 0 ? wt/rho : 0.0);
             if (u.w > 0) {
                 su[0] += (double) u.x*wt;
                 su[1] += (double) u.y*wt;
@@ -1184,8 +1191,20 @@ static void launchStencil(const void* A, const FluidView& f, const CouplingView&
     case 4: claim(std::integral_constant<int, 4>()); break;
     default: claim(std::integral_constant<int, 0>()); break;
     }
+    if (slotU != nullptr)
+        stencilGatherKernel<R><<<grid, kThreads, 0, s>>>(c, slotNode, (const R*) slotWeight, nodeStamp, stamp,
+                                                         (const V*) nodeU, (V*) slotU, (R*) coef);
+}
+
+// The moments of every slot from its node (the slot copy of the stencil pass), for the kernels that read them per slot.
+template <typename R>
+static void launchSlotMoments(const CouplingView& c, const int* slotNode, const void* slotWeight,
+                              const unsigned* nodeStamp, unsigned stamp, const void* nodeU, void* slotU, cudaStream_t s) {
+    typedef typename Vec4<R>::type V;
+    long long total = (long long) c.np*c.slots;
+    int grid = (int) std::max(1LL, std::min(4736LL, (total + kThreads - 1)/kThreads));
     stencilGatherKernel<R><<<grid, kThreads, 0, s>>>(c, slotNode, (const R*) slotWeight, nodeStamp, stamp,
-                                                     (const V*) nodeU, (V*) slotU, (R*) coef);
+                                                     (const V*) nodeU, (V*) slotU, (R*) nullptr);
 }
 
 // The cell list and the rows of the coupling matrix, after the status words are cleared (their overflow flag).
@@ -1195,8 +1214,9 @@ void CouplingEngine::launchMatrix(const CouplingView* cv, cudaStream_t s) {
     CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, s));
     cgBinKernel<<<std::max(1, std::min(1184, (np + kThreads - 1)/kThreads)), kThreads, 0, s>>>(c, dev->sparse);
     CUDA_CHECK(cudaGetLastError());
-    cgRowsKernel<R><<<warpGrid(np), kThreads, 0, s>>>(c, (const R*) dev->coef, (const R*) dev->slotWeight,
-                                                     (const typename Vec4<R>::type*) dev->slotU, dev->sparse);
+    cgRowsKernel<R><<<warpGrid(np), kThreads, 0, s>>>(c, dev->slotNode, (const R*) dev->slotWeight, dev->nodeStamp,
+                                                     dev->stamp, (const typename Vec4<R>::type*) dev->nodeU,
+                                                     dev->sparse);
     CUDA_CHECK(cudaGetLastError());
     fluid.launches += 2;
 }
@@ -1269,6 +1289,7 @@ void CouplingEngine::coupleWith(long long step, bool isStep, const CouplingView*
         CUDA_CHECK(cudaStreamSynchronize(stream));
     }
     if (spreadOnly || status[2] != 0) {
+        launchSlotMomentsNow();
         CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, stream));
         void* args[] = {&fv, &cc, &vel, &fin, &sn, &sw, &su, &coef, &stepArg, &isStepArg, &tolerance, &maxIterations, &b,
                         &spread, &fout, &reaction, &mask, &wall};
@@ -1298,7 +1319,11 @@ void CouplingEngine::setSolverLimits(int maxIterations, long long barrierPolls) 
 void CouplingEngine::launchStencilPass(const CouplingView& c, bool remove, bool mark, cudaStream_t s) {
     const FluidView& f = fluid.deviceView();
     uint32_t* m = mark ? fluid.reactMask() : nullptr;
-    void* cf = matrixSolve() ? dev->coef : nullptr;     // w/rho of the slots for the coupling matrix
+    // The coupling matrix's rows read the node moments of their slots themselves; the per-slot copy then waits for
+    // a step that falls back to the spread-and-gather solve (launchSlotMomentsNow).
+    void* su = matrixSolve() ? nullptr : dev->slotU;
+    slotMomentsPending = su == nullptr;
+    void* cf = nullptr;
     bool centred = lattice.drag_scheme == LBM_DRAG_CENTERED;
     const void* A = fluid.inputArray();
     if (++dev->stamp == 0u) {     // the stamps wrapped around: no node may carry a stale stamp
@@ -1309,13 +1334,27 @@ void CouplingEngine::launchStencilPass(const CouplingView& c, bool remove, bool 
     void* nu = dev->nodeU;
     unsigned st = dev->stamp;
     switch (storageType) {
-    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, m != nullptr ? fluid.reactionBuffer() : nullptr, cf, s); break;
-    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, m != nullptr ? fluid.reactionBuffer() : nullptr, cf, s); break;
-    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, m != nullptr ? fluid.reactionBuffer() : nullptr, cf, s); break;
-    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, dev->slotU, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, m != nullptr ? fluid.reactionBuffer() : nullptr, cf, s); break;
+    case LBM_STORAGE_F64: launchStencil<double, double>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, su, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, m != nullptr ? fluid.reactionBuffer() : nullptr, cf, s); break;
+    case LBM_STORAGE_F32: launchStencil<float, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, su, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, m != nullptr ? fluid.reactionBuffer() : nullptr, cf, s); break;
+    case LBM_STORAGE_F16: launchStencil<__half, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, su, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, m != nullptr ? fluid.reactionBuffer() : nullptr, cf, s); break;
+    default: launchStencil<__nv_bfloat16, float>(A, f, c, posDev, remove, centred, dev->slotNode, dev->slotWeight, su, ns, st, nu, dev->axisIndex, dev->axisWeight, dev->firstIndex, m, m != nullptr ? fluid.reactionBuffer() : nullptr, cf, s); break;
     }
     CUDA_CHECK(cudaGetLastError());
-    fluid.launches += 3;
+    fluid.launches += su != nullptr ? 3 : 2;
+}
+
+// The per-slot moments of the last stencil pass, if it left them out.
+void CouplingEngine::launchSlotMomentsNow() {
+    if (!slotMomentsPending)
+        return;
+    const CouplingView c = makeCouplingView(lattice, fluid.deviceView(), np, widthOf(lattice.interpolation_stencil), massDev);
+    if (storageType == LBM_STORAGE_F64)
+        launchSlotMoments<double>(c, dev->slotNode, dev->slotWeight, dev->nodeStamp, dev->stamp, dev->nodeU, dev->slotU, stream);
+    else
+        launchSlotMoments<float>(c, dev->slotNode, dev->slotWeight, dev->nodeStamp, dev->stamp, dev->nodeU, dev->slotU, stream);
+    CUDA_CHECK(cudaGetLastError());
+    fluid.launches++;
+    slotMomentsPending = false;
 }
 
 // The centred stencil drag through the explicit coupling matrix (not the spread-and-gather solve of every step).

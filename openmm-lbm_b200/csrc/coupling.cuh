@@ -61,6 +61,8 @@ private:
     void launchMatrix(const CouplingView* view, cudaStream_t s);
     void launchStencilPass(const CouplingView& view, bool remove, bool mark, cudaStream_t s);
     bool matrixSolve() const;
+    void launchSlotMomentsNow();
+    bool slotMomentsPending = false;      // the last stencil pass left the per-slot moments out (the matrix reads nodes)
     cudaStream_t side = nullptr;          // stream of the prepared work
     cudaEvent_t begun = nullptr, ready = nullptr;
     bool prepared = false, preparedRemove = false;
