@@ -507,21 +507,23 @@ __device__ __forceinline__ int periodicDistance(int a, int b, int n) {
     return min(d, n - d);
 }
 
-template <typename R>
+// W: the stencil width when known at compile time (0: c.width).  With W = 4 in single precision a row of k's w/rho
+// (4 x-adjacent slots) is one 16-byte shared-memory load in the values' loop.
+template <typename R, int W>
 __global__ void __launch_bounds__(kThreads, 4)
 cgRowsKernel(CouplingView c, const int* __restrict__ slotNode, const R* __restrict__ slotWeight,
              const unsigned* __restrict__ nodeStamp, unsigned stamp, const typename Vec4<R>::type* __restrict__ nodeU,
              SparseCg g) {
     __shared__ int candidates[kThreads/32][kCgRowCapacity];
     __shared__ int sorted[kThreads/32][kCgRowCapacity];
-    __shared__ R rowCoef[kThreads/32][64];
+    __shared__ __align__(16) R rowCoef[kThreads/32][64];
     __shared__ int cellEnd[kThreads/32][32], cellStart[kThreads/32][32], cellId[kThreads/32][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int* list = candidates[warp];
     const int firstWarp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
     const int warps = (gridDim.x*blockDim.x) >> 5;
     const int size[3] = {c.nx, c.ny, c.nz};
-    const int w = c.width, S = c.slots;
+    const int w = W > 0 ? W : c.width, S = W > 0 ? W*W*W : c.slots;
     for (int k = firstWarp; k < c.np; k += warps) {
         // The particle's sums over its slots for the solve's right-hand side and diagonal (ReferenceLBMKernels.cpp:
         // 758-782): u = sum w u_node over the fluid slots and sum w^2/rho; they need no velocities or forces.
@@ -674,10 +676,19 @@ cgRowsKernel(CouplingView c, const int* __restrict__ slotNode, const R* __restri
                     if (iy >= w || shifted[1][iy] == (R) 0)
                         continue;
                     const R wyz = shifted[1][iy]*shifted[2][iz];
+                    if constexpr (W == 4 && std::is_same<R, float>::value) {
+                        const float4 cf = *reinterpret_cast<const float4*>(&rowCoef[warp][4*(iy + 4*iz)]);
+                        K += cf.x*(shifted[0][0]*wyz);
+                        K += cf.y*(shifted[0][1]*wyz);
+                        K += cf.z*(shifted[0][2]*wyz);
+                        K += cf.w*(shifted[0][3]*wyz);
+                    }
+                    else {
 #pragma unroll
-                    for (int ix = 0; ix < 4; ix++)
-                        if (ix < w)
-                            K += rowCoef[warp][ix + w*(iy + w*iz)]*(shifted[0][ix]*wyz);
+                        for (int ix = 0; ix < 4; ix++)
+                            if (ix < w)
+                                K += rowCoef[warp][ix + w*(iy + w*iz)]*(shifted[0][ix]*wyz);
+                    }
                 }
             }
             g.rowIndex[(long long) k*kCgRowCapacity + j] = l;
@@ -1214,9 +1225,17 @@ void CouplingEngine::launchMatrix(const CouplingView* cv, cudaStream_t s) {
     CUDA_CHECK(cudaMemsetAsync(statusDev, 0, sizeof(int)*4, s));
     cgBinKernel<<<std::max(1, std::min(1184, (np + kThreads - 1)/kThreads)), kThreads, 0, s>>>(c, dev->sparse);
     CUDA_CHECK(cudaGetLastError());
-    cgRowsKernel<R><<<warpGrid(np), kThreads, 0, s>>>(c, dev->slotNode, (const R*) dev->slotWeight, dev->nodeStamp,
-                                                     dev->stamp, (const typename Vec4<R>::type*) dev->nodeU,
-                                                     dev->sparse);
+    auto rows = [&](auto w) {
+        cgRowsKernel<R, decltype(w)::value><<<warpGrid(np), kThreads, 0, s>>>(
+            c, dev->slotNode, (const R*) dev->slotWeight, dev->nodeStamp, dev->stamp,
+            (const typename Vec4<R>::type*) dev->nodeU, dev->sparse);
+    };
+    switch (c.width) {
+    case 2: rows(std::integral_constant<int, 2>()); break;
+    case 3: rows(std::integral_constant<int, 3>()); break;
+    case 4: rows(std::integral_constant<int, 4>()); break;
+    default: rows(std::integral_constant<int, 0>()); break;
+    }
     CUDA_CHECK(cudaGetLastError());
     fluid.launches += 2;
 }
