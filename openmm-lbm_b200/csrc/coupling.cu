@@ -703,7 +703,7 @@ cgRowsKernel(CouplingView c, const int* __restrict__ slotNode, const R* __restri
 // (K v)_k for the three components of v, by the kProductLanes threads of a row (entries sub, sub + kProductLanes, ...,
 // then the sum over the lanes), in all of them; k < 0: no row (the threads still take part in the exchange).  Called
 // by every thread of the warp.
-constexpr int kProductLanes = 8;
+constexpr int kProductLanes = 4;
 
 __device__ __forceinline__ void rowProduct(const SparseCg& g, int k, const double* v, double out[3]) {
     double s0 = 0, s1 = 0, s2 = 0;
@@ -711,7 +711,7 @@ __device__ __forceinline__ void rowProduct(const SparseCg& g, int k, const doubl
         const int n = g.rowCount[k];
         const int* index = g.rowIndex + (long long) k*kCgRowCapacity;
         const double* value = g.rowValue + (long long) k*kCgRowCapacity;
-#pragma unroll 2
+#pragma unroll 4
         for (int e = threadIdx.x%kProductLanes; e < n; e += kProductLanes) {
             const int l = index[e];
             const double K = value[e];
