@@ -829,6 +829,9 @@ BatchEngine::BatchEngine(int nr, const LbmLatticeParameters* ls, const int* np, 
     coupled = totalParticles > 0;
     slots = stencilWidth(stencil);
     slots = slots*slots*slots;
+    if ((long long) totalParticles*slots >= (1LL << 31))
+        throw Error(LBM_ERR_INVALID_ARGUMENT, "lbm_batch_create: too many particles for the interpolation stencil "
+                    "(particles x stencil nodes must stay below 2^31)");
     if (pair != nullptr) {
         pairParams.type = pair->pair_type;
         pairParams.sigma2 = pair->sigma*pair->sigma;

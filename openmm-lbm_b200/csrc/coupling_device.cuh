@@ -213,8 +213,9 @@ template <typename T, typename R, bool COHERENT = false>
 __device__ __forceinline__ void stencilSlot(const T* __restrict__ A, const FluidView& f, const CouplingView& c,
                                             const double* __restrict__ posIn, long long t, int remove, int centred,
                                             int* slotNode, R* slotWeight, typename Vec4<R>::type* slotU) {
-    // COHERENT: the positions were written by the same launch (a persistent kernel): read them through L2.
-    int i = (int) (t/c.slots), s = (int) (t%c.slots);
+    // COHERENT: the positions were written by the same launch (a persistent kernel): read them through L2.  The slots
+    // of all particles are fewer than 2^31: 32-bit division.
+    const int i = (int) t/c.slots, s = (int) t - i*c.slots;
     double pos[3];
     for (int a = 0; a < 3; a++)
         pos[a] = COHERENT ? __ldcg(&posIn[3*i+a]) : posIn[3*i+a];
