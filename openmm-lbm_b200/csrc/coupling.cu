@@ -1392,7 +1392,10 @@ void CouplingEngine::prepare(const LbmParticleArrays* p, long long step, bool re
     cudaMemcpyKind kind = p->memory == LBM_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     CUDA_CHECK(cudaMemcpyAsync(posDev, p->positions, v3, kind, stream));
     if (side == nullptr) {
-        CUDA_CHECK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        // The prepared work is the step's critical path (the caller's forces run beside it): its blocks go first.
+        int least = 0, greatest = 0;
+        CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CUDA_CHECK(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, greatest));
         CUDA_CHECK(cudaEventCreateWithFlags(&begun, cudaEventDisableTiming));
         CUDA_CHECK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
     }
